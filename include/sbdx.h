@@ -1,0 +1,146 @@
+/*
+ * sbdx.h: C-ABI of the B200 (sm_100a) implementation of the sbd
+ * tensor-product-basis selected-CI hot path (walkup/sbd-ykt, namespace
+ * sbd::tpb). Plain pointers and sizes only; every call returns an int status
+ * (SBDX_OK = 0) and sbdx_last_error() describes the last failure. No C++
+ * exception crosses this boundary. A context is affine to one host thread and
+ * one CUDA device; it owns every device buffer it allocates, the caller owns
+ * every host buffer it passes.
+ *
+ * Layout conventions (shared by all entry points):
+ *   - a spin string is one uint64, bit p = spatial orbital p, L <= 64. The
+ *     reference packs bit_length bits per size_t word
+ *     (framework/bit_manipulation.h:158-172); numeric uint64 order equals the
+ *     reference's word-reversed lexicographic order (bit_manipulation.h:26-43);
+ *   - determinant (ia, ib) has vector index ia*nb + ib (alpha-major), as the
+ *     reference's braIdx (chemistry/tpb/mult.h:487-488);
+ *   - h is the L*L one-electron matrix (row-major, symmetric); eri is the
+ *     8-fold packed two-electron array of twoInt::store
+ *     (chemistry/basic/integrals.h:51-59): index canon(pq, rs) with
+ *     pq = max(p,q)*(max(p,q)+1)/2 + min(p,q) and
+ *     canon(x, y) = max(x,y)*(max(x,y)+1)/2 + min(x,y);
+ *   - 1-RDM: 2 blocks of L*L, element [s][p + L*q]; 2-RDM: 4 blocks of L^4,
+ *     element [s + 2t][i + L*j + L^2*k + L^3*l], the reference's
+ *     one_p_rdm / two_p_rdm (chemistry/tpb/correlation.h:211-218).
+ */
+#ifndef SBDX_H
+#define SBDX_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SBDX_OK 0
+#define SBDX_ERR_ARG 1      /* invalid argument (size, pointer, range)         */
+#define SBDX_ERR_CUDA 2     /* CUDA runtime error                               */
+#define SBDX_ERR_STATE 3    /* call out of order (e.g. sigma before strings)    */
+#define SBDX_ERR_NOMEM 4    /* device allocation failed                         */
+#define SBDX_ERR_NUMERIC 5  /* non-finite input or breakdown                    */
+
+#define SBDX_FP64 0
+#define SBDX_FP32 1
+
+typedef struct sbdx_ctx sbdx_ctx;
+
+/* Context lifetime. Replaces the MPI communicator set-up of tpb::diag at
+ * world size 1 (chemistry/tpb/helper.h:199-233, TaskCommunicator). */
+int sbdx_ctx_create(sbdx_ctx** ctx, int device);
+int sbdx_ctx_destroy(sbdx_ctx* ctx);
+const char* sbdx_last_error(const sbdx_ctx* ctx);
+/* Stream used by all subsequent work (a cudaStream_t; NULL = legacy stream). */
+int sbdx_set_stream(sbdx_ctx* ctx, void* cuda_stream);
+/* Kernels launched by this context since creation (instrumentation). */
+unsigned long long sbdx_launch_count(const sbdx_ctx* ctx);
+
+/* Integrals. Replaces SetupIntegrals (chemistry/basic/makeintegrals.h:81-126)
+ * with exact doubles (the struct path of tpb::diag, sbdiag.h:157). eri_len
+ * must equal P*(P+1)/2 with P = L*(L+1)/2. Non-finite values -> SBDX_ERR_NUMERIC. */
+int sbdx_set_integrals(sbdx_ctx* ctx, int norb, double I0, const double* h, const double* eri,
+                       size_t eri_len);
+
+/* Sampled alpha and beta strings (the adet/bdet arguments of tpb::diag,
+ * chemistry/tpb/sbdiag.h:116-117). Strings must be unique; sorted ascending for
+ * index 0 to be the Aufbau start vector, as LoadAlphaDets leaves them
+ * (chemistry/basic/makedeterminants.h:184). All alpha strings must have the
+ * same popcount, and all beta strings likewise. */
+int sbdx_set_strings(sbdx_ctx* ctx, const uint64_t* alpha, size_t na, const uint64_t* beta, size_t nb);
+
+/* Excitation connectivity. Replaces MakeHelpers/RemakeHelpers + GenerateExcitation
+ * (chemistry/tpb/helper.h:132-197, 447-968) at world size 1. */
+int sbdx_build_connectivity(sbdx_ctx* ctx);
+/* Total entries (singles + doubles) of spin 0 (alpha) or 1 (beta). */
+int sbdx_connectivity_size(sbdx_ctx* ctx, int spin, uint64_t* n_entries);
+/* The helper lists in MakeSmartHelper's flattened layout
+ * (chemistry/tpb/helper.h:367-437): per bra string, its singles then its
+ * doubles, ascending ket index; slen/dlen: per-bra list lengths. */
+int sbdx_get_connectivity(sbdx_ctx* ctx, int spin, uint64_t* slen, uint64_t* dlen, uint64_t* idx);
+
+/* Diagonal H_II for all determinants. Replaces makeQChamDiagTerms
+ * (chemistry/tpb/qcham.h:314-366). hii: host buffer of na*nb doubles (may be
+ * NULL to only compute the device copy). */
+int sbdx_diag_terms(sbdx_ctx* ctx, double* hii);
+
+/* One H*C product. Replaces mult (chemistry/tpb/mult.h:376-632). C and S are
+ * host buffers of na*nb doubles (S is overwritten, not accumulated). */
+int sbdx_sigma(sbdx_ctx* ctx, const double* C, double* S);
+/* Same on device buffers of na*nb elements of the given precision
+ * (SBDX_FP64: double; SBDX_FP32: float storage with FP64 row accumulation),
+ * on the context stream. */
+int sbdx_sigma_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS);
+
+typedef struct {
+  int max_it;          /* outer restarts (SBD::max_it, sbdiag.h:19)            */
+  int max_nb;          /* subspace size (SBD::max_nb, sbdiag.h:20)            */
+  double eps;          /* residual-norm tolerance (SBD::eps, sbdiag.h:21)     */
+  double max_time;     /* seconds (SBD::max_time, sbdiag.h:22)                */
+  int precision;       /* SBDX_FP64: the reference algorithm; SBDX_FP32:
+                          FP32-stored subspace with FP64 defect correction    */
+  int defect_every;    /* FP32 mode: FP64 residual every k steps (default 4)  */
+  int verbose;         /* print one line per step, as davidson.h:834-846      */
+} sbdx_davidson_params;
+
+typedef struct {
+  double energy;       /* <W|H|W> after one extra FP64 sigma (sbdiag.h:250-273) */
+  double residual;     /* last residual norm                                    */
+  int n_sigma;         /* sigma products of the working precision              */
+  int n_sigma64;       /* FP64 sigma products (defect corrections + final)     */
+  int converged;       /* residual < eps                                        */
+  double seconds;      /* wall time of the solve                                */
+} sbdx_davidson_info;
+
+/* Davidson eigensolve + final energy. Replaces Davidson (max_time overload,
+ * chemistry/tpb/davidson.h:661-924), BasisInitVector (:101-140) and the energy
+ * evaluation of tpb::diag (sbdiag.h:246-273). W: host buffer of na*nb doubles;
+ * on input the start vector if init_from_W != 0, else W[0] = 1 (Hartree-Fock);
+ * on output the normalised ground-state vector. */
+int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_from_W, double* W,
+                  sbdx_davidson_info* info);
+
+/* 1-/2-RDM of a vector W (host, na*nb doubles). Replaces Correlation
+ * (chemistry/tpb/correlation.h:194-444). one: 2*L*L doubles; two: 4*L^4
+ * doubles (may be NULL to skip the 2-RDM). */
+int sbdx_rdm(sbdx_ctx* ctx, const double* W, double* one, double* two);
+
+/* Occupation density[2p+s] of W. Replaces OccupationDensity
+ * (chemistry/tpb/occupation.h:10-95) over all orbitals. */
+int sbdx_occupation(sbdx_ctx* ctx, const double* W, double* density);
+
+/* Alpha-string weights sum_b |W[a,b]|^2 (DiagonalReducedDensityMatrix,
+ * chemistry/tpb/rdmat.h:10-57), the input of CarryOverAlphaDet. */
+int sbdx_alpha_weights(sbdx_ctx* ctx, const double* W, double* weights);
+
+/* Adjoint of the energy with respect to the integrals (Hellmann-Feynman):
+ * dE/dh (L*L, one entry per unordered pair, set on both triangles) and
+ * dE/d(pq|rs) for every 8-fold packed class (eri_len doubles), computed from
+ * the RDMs of W, which the call recomputes together with the connectivity.
+ * It has no single counterpart in the reference; it contracts the reference's
+ * RDM outputs (correlation.h:194-444) the way the sample's energy check uses
+ * them (samples/selected_basis_diagonalization/main.cc:166-216). */
+int sbdx_energy_backward(sbdx_ctx* ctx, const double* W, double* dE_dh, double* dE_deri);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

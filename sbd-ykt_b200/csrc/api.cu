@@ -1,0 +1,378 @@
+// C-ABI entry points (include/sbdx.h). Validation of every host input happens
+// here, before any kernel sees it: sizes, orbital range, equal electron counts
+// per spin, finite integrals. No C++ exception crosses the boundary.
+#include "sbdx.h"
+#include "sbdx_internal.cuh"
+
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <new>
+
+struct sbdx_ctx {
+  sbdx::Ctx c;
+};
+
+namespace sbdx {
+
+bool set_cuda_err(Ctx* c, cudaError_t e, const char* what) {
+  c->err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+  return false;
+}
+
+void free_connectivity(Ctx* c);
+int build_g_table(Ctx* c);
+int davidson(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info);
+int rdm_device(Ctx* c, const double* dW, double* d_one, double* d_two);
+int occupation_device(Ctx* c, const double* dW, double* d_density);
+int alpha_weights_device(Ctx* c, const double* dW, double* d_w);
+int backward_device(Ctx* c, const double* dW, double* dE_dh, double* dE_deri);
+
+namespace {
+
+void free_vector_state(Ctx* c) {
+  cudaFree(c->d_hii); c->d_hii = nullptr; c->have_hii = false;
+  cudaFree(c->d_xt); c->d_xt = nullptr;
+  cudaFree(c->d_y); c->d_y = nullptr;
+  cudaFree(c->d_yt); c->d_yt = nullptr;
+  cudaFree(c->d_io_in); c->d_io_in = nullptr;
+  cudaFree(c->d_io_out); c->d_io_out = nullptr;
+}
+
+int ensure_io(Ctx* c) {
+  const size_t D = c->na * c->nb;
+  if (!c->d_io_in) SBDX_CUDA(c, cudaMalloc(&c->d_io_in, sizeof(double) * D));
+  if (!c->d_io_out) SBDX_CUDA(c, cudaMalloc(&c->d_io_out, sizeof(double) * D));
+  return 0;
+}
+
+int ready(Ctx* c, const char* who) {
+  if (!c->have_integrals || !c->have_strings) {
+    c->err = std::string(who) + ": set integrals and strings first";
+    return SBDX_ERR_STATE;
+  }
+  if (c->L < 64) {
+    const uint64_t lim = 1ull << c->L;
+    for (uint64_t x : c->h_a)
+      if (x >= lim) { c->err = std::string(who) + ": alpha string has bits beyond norb"; return SBDX_ERR_ARG; }
+    for (uint64_t x : c->h_b)
+      if (x >= lim) { c->err = std::string(who) + ": beta string has bits beyond norb"; return SBDX_ERR_ARG; }
+  }
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) { set_cuda_err(c, e, "cudaSetDevice"); return SBDX_ERR_CUDA; }
+  return 0;
+}
+
+template <typename F>
+int guarded(sbdx_ctx* ctx, F&& f) {
+  if (!ctx) return SBDX_ERR_ARG;
+  try {
+    return f(&ctx->c);
+  } catch (const std::bad_alloc&) {
+    ctx->c.err = "host allocation failed";
+    return SBDX_ERR_NOMEM;
+  } catch (const std::exception& ex) {
+    ctx->c.err = ex.what();
+    return SBDX_ERR_ARG;
+  } catch (...) {
+    ctx->c.err = "unknown exception";
+    return SBDX_ERR_ARG;
+  }
+}
+
+// map internal 1/2/3/5 codes (already SBDX_*), keep as is
+}  // namespace
+}  // namespace sbdx
+
+using sbdx::Ctx;
+
+extern "C" {
+
+int sbdx_ctx_create(sbdx_ctx** out, int device) {
+  if (!out) return SBDX_ERR_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return SBDX_ERR_CUDA;
+  if (cudaSetDevice(device) != cudaSuccess) return SBDX_ERR_CUDA;
+  sbdx_ctx* ctx = new (std::nothrow) sbdx_ctx();
+  if (!ctx) return SBDX_ERR_NOMEM;
+  ctx->c.device = device;
+  *out = ctx;
+  return SBDX_OK;
+}
+
+int sbdx_ctx_destroy(sbdx_ctx* ctx) {
+  if (!ctx) return SBDX_OK;
+  Ctx* c = &ctx->c;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  sbdx::free_connectivity(c);
+  sbdx::free_vector_state(c);
+  cudaFree(c->d_h); cudaFree(c->d_eri); cudaFree(c->d_eri32); cudaFree(c->d_G); cudaFree(c->d_G32);
+  cudaFree(c->d_a); cudaFree(c->d_b); cudaFree(c->d_red);
+  delete ctx;
+  return SBDX_OK;
+}
+
+const char* sbdx_last_error(const sbdx_ctx* ctx) { return ctx ? ctx->c.err.c_str() : "null context"; }
+
+unsigned long long sbdx_launch_count(const sbdx_ctx* ctx) { return ctx ? ctx->c.launches : 0ull; }
+
+int sbdx_set_stream(sbdx_ctx* ctx, void* stream) {
+  return sbdx::guarded(ctx, [&](Ctx* c) {
+    c->stream = (cudaStream_t)stream;
+    return SBDX_OK;
+  });
+}
+
+int sbdx_set_integrals(sbdx_ctx* ctx, int norb, double I0, const double* h, const double* eri, size_t eri_len) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (norb < 1 || norb > 64) { c->err = "set_integrals: norb must be in [1, 64]"; return SBDX_ERR_ARG; }
+    if (!h || !eri) { c->err = "set_integrals: null pointer"; return SBDX_ERR_ARG; }
+    const size_t npair = (size_t)norb * (norb + 1) / 2, neri = npair * (npair + 1) / 2;
+    if (eri_len != neri) {
+      c->err = "set_integrals: eri_len must be P*(P+1)/2 with P = norb*(norb+1)/2";
+      return SBDX_ERR_ARG;
+    }
+    if (!std::isfinite(I0)) { c->err = "set_integrals: non-finite I0"; return SBDX_ERR_NUMERIC; }
+    for (size_t k = 0; k < (size_t)norb * norb; ++k)
+      if (!std::isfinite(h[k])) { c->err = "set_integrals: non-finite one-electron integral"; return SBDX_ERR_NUMERIC; }
+    for (size_t k = 0; k < neri; ++k)
+      if (!std::isfinite(eri[k])) { c->err = "set_integrals: non-finite two-electron integral"; return SBDX_ERR_NUMERIC; }
+    if (cudaSetDevice(c->device) != cudaSuccess) { c->err = "cudaSetDevice failed"; return SBDX_ERR_CUDA; }
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_h); cudaFree(c->d_eri); cudaFree(c->d_eri32);
+    c->d_h = nullptr; c->d_eri = nullptr; c->d_eri32 = nullptr;
+    c->L = norb;
+    c->I0 = I0;
+    c->npair = npair;
+    c->neri = neri;
+    c->h_h.assign(h, h + (size_t)norb * norb);
+    c->h_eri.assign(eri, eri + neri);
+    std::vector<float> e32(neri);
+    for (size_t k = 0; k < neri; ++k) e32[k] = (float)eri[k];
+    SBDX_CUDA(c, cudaMalloc(&c->d_h, sizeof(double) * norb * norb));
+    SBDX_CUDA(c, cudaMalloc(&c->d_eri, sizeof(double) * neri));
+    SBDX_CUDA(c, cudaMalloc(&c->d_eri32, sizeof(float) * neri));
+    SBDX_CUDA(c, cudaMemcpy(c->d_h, h, sizeof(double) * norb * norb, cudaMemcpyHostToDevice));
+    SBDX_CUDA(c, cudaMemcpy(c->d_eri, eri, sizeof(double) * neri, cudaMemcpyHostToDevice));
+    SBDX_CUDA(c, cudaMemcpy(c->d_eri32, e32.data(), sizeof(float) * neri, cudaMemcpyHostToDevice));
+    int rc = sbdx::build_g_table(c);
+    if (rc) return rc;
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->have_integrals = true;
+    // matrix elements cached in the connectivity and the diagonal depend on the integrals
+    sbdx::free_connectivity(c);
+    cudaFree(c->d_hii); c->d_hii = nullptr; c->have_hii = false;
+    return SBDX_OK;
+  });
+}
+
+int sbdx_set_strings(sbdx_ctx* ctx, const uint64_t* alpha, size_t na, const uint64_t* beta, size_t nb) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!alpha || !beta || na == 0 || nb == 0) { c->err = "set_strings: empty string set"; return SBDX_ERR_ARG; }
+    if (na > 65535 || nb > 65535) { c->err = "set_strings: at most 65535 strings per spin"; return SBDX_ERR_ARG; }
+    const int pa = __builtin_popcountll(alpha[0]), pb = __builtin_popcountll(beta[0]);
+    for (size_t k = 0; k < na; ++k)
+      if (__builtin_popcountll(alpha[k]) != pa) { c->err = "set_strings: alpha strings differ in electron count"; return SBDX_ERR_ARG; }
+    for (size_t k = 0; k < nb; ++k)
+      if (__builtin_popcountll(beta[k]) != pb) { c->err = "set_strings: beta strings differ in electron count"; return SBDX_ERR_ARG; }
+    if (cudaSetDevice(c->device) != cudaSuccess) { c->err = "cudaSetDevice failed"; return SBDX_ERR_CUDA; }
+    cudaStreamSynchronize(c->stream);
+    sbdx::free_connectivity(c);
+    sbdx::free_vector_state(c);
+    cudaFree(c->d_a); cudaFree(c->d_b);
+    c->d_a = nullptr; c->d_b = nullptr;
+    c->na = na;
+    c->nb = nb;
+    c->h_a.assign(alpha, alpha + na);
+    c->h_b.assign(beta, beta + nb);
+    SBDX_CUDA(c, cudaMalloc(&c->d_a, sizeof(uint64_t) * na));
+    SBDX_CUDA(c, cudaMalloc(&c->d_b, sizeof(uint64_t) * nb));
+    SBDX_CUDA(c, cudaMemcpy(c->d_a, alpha, sizeof(uint64_t) * na, cudaMemcpyHostToDevice));
+    SBDX_CUDA(c, cudaMemcpy(c->d_b, beta, sizeof(uint64_t) * nb, cudaMemcpyHostToDevice));
+    c->have_strings = true;
+    return SBDX_OK;
+  });
+}
+
+int sbdx_build_connectivity(sbdx_ctx* ctx) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    int rc = sbdx::ready(c, "build_connectivity");
+    if (rc) return rc;
+    rc = sbdx::build_connectivity(c);
+    if (rc) return rc;
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SBDX_OK;
+  });
+}
+
+int sbdx_connectivity_size(sbdx_ctx* ctx, int spin, uint64_t* n_entries) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (spin != 0 && spin != 1) { c->err = "connectivity_size: spin must be 0 or 1"; return SBDX_ERR_ARG; }
+    if (!n_entries) { c->err = "connectivity_size: null pointer"; return SBDX_ERR_ARG; }
+    if (!c->have_conn) { c->err = "connectivity_size: build the connectivity first"; return SBDX_ERR_STATE; }
+    *n_entries = c->conn[spin].total;
+    return SBDX_OK;
+  });
+}
+
+int sbdx_get_connectivity(sbdx_ctx* ctx, int spin, uint64_t* slen, uint64_t* dlen, uint64_t* idx) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (spin != 0 && spin != 1) { c->err = "get_connectivity: spin must be 0 or 1"; return SBDX_ERR_ARG; }
+    if (!c->have_conn) { c->err = "get_connectivity: build the connectivity first"; return SBDX_ERR_STATE; }
+    const sbdx::Conn& cn = c->conn[spin];
+    std::vector<uint32_t> ns(cn.n), nd(cn.n), ket(cn.total);
+    SBDX_CUDA(c, cudaSetDevice(c->device));
+    SBDX_CUDA(c, cudaMemcpy(ns.data(), cn.nsing, sizeof(uint32_t) * cn.n, cudaMemcpyDeviceToHost));
+    SBDX_CUDA(c, cudaMemcpy(nd.data(), cn.ndoub, sizeof(uint32_t) * cn.n, cudaMemcpyDeviceToHost));
+    if (cn.total) SBDX_CUDA(c, cudaMemcpy(ket.data(), cn.ket, sizeof(uint32_t) * cn.total, cudaMemcpyDeviceToHost));
+    for (size_t r = 0; r < cn.n; ++r) {
+      if (slen) slen[r] = ns[r];
+      if (dlen) dlen[r] = nd[r];
+    }
+    if (idx)
+      for (size_t k = 0; k < cn.total; ++k) idx[k] = ket[k];
+    return SBDX_OK;
+  });
+}
+
+int sbdx_diag_terms(sbdx_ctx* ctx, double* hii) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    int rc = sbdx::ready(c, "diag_terms");
+    if (rc) return rc;
+    rc = sbdx::diag_terms(c);
+    if (rc) return rc;
+    if (hii) SBDX_CUDA(c, cudaMemcpyAsync(hii, c->d_hii, sizeof(double) * c->na * c->nb, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SBDX_OK;
+  });
+}
+
+int sbdx_sigma(sbdx_ctx* ctx, const double* C, double* S) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!C || !S) { c->err = "sigma: null pointer"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "sigma");
+    if (rc) return rc;
+    if ((rc = sbdx::ensure_io(c))) return rc;
+    const size_t D = c->na * c->nb;
+    SBDX_CUDA(c, cudaMemcpyAsync(c->d_io_in, C, sizeof(double) * D, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = sbdx::sigma_device(c, SBDX_FP64, c->d_io_in, c->d_io_out))) return rc;
+    SBDX_CUDA(c, cudaMemcpyAsync(S, c->d_io_out, sizeof(double) * D, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SBDX_OK;
+  });
+}
+
+int sbdx_sigma_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!dC || !dS) { c->err = "sigma_device: null pointer"; return SBDX_ERR_ARG; }
+    if (dC == dS) { c->err = "sigma_device: input and output must not alias"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "sigma_device");
+    if (rc) return rc;
+    return sbdx::sigma_device(c, precision, dC, dS);
+  });
+}
+
+int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_from_W, double* W,
+                  sbdx_davidson_info* info) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!params || !W) { c->err = "davidson: null pointer"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "davidson");
+    if (rc) return rc;
+    const size_t D = c->na * c->nb;
+    if (init_from_W)
+      for (size_t k = 0; k < D; ++k)
+        if (!std::isfinite(W[k])) { c->err = "davidson: non-finite start vector"; return SBDX_ERR_NUMERIC; }
+    if ((rc = sbdx::ensure_io(c))) return rc;
+    double* dW = (double*)c->d_io_in;
+    if (init_from_W) {
+      SBDX_CUDA(c, cudaMemcpyAsync(dW, W, sizeof(double) * D, cudaMemcpyHostToDevice, c->stream));
+    } else {
+      // BasisInitVector, init == 0 (davidson.h:130-133): W[0] = 1
+      SBDX_CUDA(c, cudaMemsetAsync(dW, 0, sizeof(double) * D, c->stream));
+      const double one = 1.0;
+      SBDX_CUDA(c, cudaMemcpyAsync(dW, &one, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
+    sbdx_davidson_info inf{};
+    rc = sbdx::davidson(c, *params, dW, inf);
+    if (rc) return rc;
+    SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * D, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (info) *info = inf;
+    return SBDX_OK;
+  });
+}
+
+int sbdx_rdm(sbdx_ctx* ctx, const double* W, double* one, double* two) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!W || !one) { c->err = "rdm: null pointer"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "rdm");
+    if (rc) return rc;
+    if ((rc = sbdx::ensure_io(c))) return rc;
+    const size_t D = c->na * c->nb, L = (size_t)c->L, L2 = L * L, L4 = L2 * L2;
+    SBDX_CUDA(c, cudaMemcpyAsync(c->d_io_in, W, sizeof(double) * D, cudaMemcpyHostToDevice, c->stream));
+    double *d_one = nullptr, *d_two = nullptr;
+    SBDX_CUDA(c, cudaMalloc(&d_one, sizeof(double) * 2 * L2));
+    if (two) {
+      cudaError_t e = cudaMalloc(&d_two, sizeof(double) * 4 * L4);
+      if (e != cudaSuccess) { cudaFree(d_one); sbdx::set_cuda_err(c, e, "cudaMalloc(2-RDM)"); return SBDX_ERR_NOMEM; }
+    }
+    rc = sbdx::rdm_device(c, (const double*)c->d_io_in, d_one, d_two);
+    if (!rc) {
+      cudaError_t e = cudaMemcpyAsync(one, d_one, sizeof(double) * 2 * L2, cudaMemcpyDeviceToHost, c->stream);
+      if (e == cudaSuccess && two) e = cudaMemcpyAsync(two, d_two, sizeof(double) * 4 * L4, cudaMemcpyDeviceToHost, c->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) { sbdx::set_cuda_err(c, e, "rdm copy-out"); rc = SBDX_ERR_CUDA; }
+    }
+    cudaFree(d_one);
+    cudaFree(d_two);
+    return rc;
+  });
+}
+
+int sbdx_occupation(sbdx_ctx* ctx, const double* W, double* density) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!W || !density) { c->err = "occupation: null pointer"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "occupation");
+    if (rc) return rc;
+    if ((rc = sbdx::ensure_io(c))) return rc;
+    const size_t D = c->na * c->nb;
+    SBDX_CUDA(c, cudaMemcpyAsync(c->d_io_in, W, sizeof(double) * D, cudaMemcpyHostToDevice, c->stream));
+    double* d = (double*)c->d_io_out;
+    if ((rc = sbdx::occupation_device(c, (const double*)c->d_io_in, d))) return rc;
+    SBDX_CUDA(c, cudaMemcpyAsync(density, d, sizeof(double) * 2 * c->L, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SBDX_OK;
+  });
+}
+
+int sbdx_alpha_weights(sbdx_ctx* ctx, const double* W, double* weights) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!W || !weights) { c->err = "alpha_weights: null pointer"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "alpha_weights");
+    if (rc) return rc;
+    if ((rc = sbdx::ensure_io(c))) return rc;
+    const size_t D = c->na * c->nb;
+    SBDX_CUDA(c, cudaMemcpyAsync(c->d_io_in, W, sizeof(double) * D, cudaMemcpyHostToDevice, c->stream));
+    double* d = (double*)c->d_io_out;
+    if ((rc = sbdx::alpha_weights_device(c, (const double*)c->d_io_in, d))) return rc;
+    SBDX_CUDA(c, cudaMemcpyAsync(weights, d, sizeof(double) * c->na, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SBDX_OK;
+  });
+}
+
+int sbdx_energy_backward(sbdx_ctx* ctx, const double* W, double* dE_dh, double* dE_deri) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!W || !dE_dh || !dE_deri) { c->err = "energy_backward: null pointer"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "energy_backward");
+    if (rc) return rc;
+    if ((rc = sbdx::ensure_io(c))) return rc;
+    const size_t D = c->na * c->nb;
+    SBDX_CUDA(c, cudaMemcpyAsync(c->d_io_in, W, sizeof(double) * D, cudaMemcpyHostToDevice, c->stream));
+    return sbdx::backward_device(c, (const double*)c->d_io_in, dE_dh, dE_deri);
+  });
+}
+
+}  // extern "C"

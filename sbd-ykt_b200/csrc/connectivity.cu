@@ -1,0 +1,213 @@
+// Excitation-connectivity builder.
+//
+// Restates GenerateExcitation (reference chemistry/tpb/helper.h:132-197): for
+// every bra string r of one spin, the ket strings k with popcount(s_r ^ s_k)
+// == 2 (single) or == 4 (double), in ascending k, singles then doubles per
+// row (the flattened layout of MakeSmartHelper, helper.h:367-437).
+//
+// B200 form: one CTA per bra row; pass 1 counts with an XOR-popcount scan, the
+// host scans the counts into row offsets, pass 2 re-scans and compacts with a
+// warp-ballot prefix so the output order is the ascending scan order. Pass 2
+// also evaluates, once per entry, everything of the matrix element that does
+// not depend on the opposite-spin string:
+//   - the same-spin part of the fermionic sign and the opposite-spin parity
+//     mask (the two halves of the reference parity(), determinants.h:228-279,
+//     on the interleaved layout alpha p -> 2p, beta p -> 2p+1);
+//   - the same-spin part of the value: OneExcite (determinants.h:423-445)
+//     without the opposite-spin Coulomb sum, or TwoExcite (:447-465).
+// The sigma kernels combine these with the opposite-spin string of each
+// determinant in O(1) (a popcount) per pair.
+#include "sbdx_internal.cuh"
+
+namespace sbdx {
+
+namespace {
+
+constexpr int kConnThreads = 256;
+
+__global__ void __launch_bounds__(kConnThreads)
+conn_count_kernel(const uint64_t* __restrict__ s, size_t n, uint32_t* __restrict__ nsing,
+                  uint32_t* __restrict__ ndoub) {
+  const size_t r = blockIdx.x;
+  const uint64_t sr = s[r];
+  uint32_t cs = 0, cd = 0;
+  for (size_t k = threadIdx.x; k < n; k += blockDim.x) {
+    int d = popc64(sr ^ s[k]);
+    cs += (d == 2);
+    cd += (d == 4);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    cs += __shfl_down_sync(0xffffffffu, cs, o);
+    cd += __shfl_down_sync(0xffffffffu, cd, o);
+  }
+  __shared__ uint32_t ws[kConnThreads / 32], wd[kConnThreads / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { ws[warp] = cs; wd[warp] = cd; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t ts = 0, td = 0;
+    for (int w = 0; w < kConnThreads / 32; ++w) { ts += ws[w]; td += wd[w]; }
+    nsing[r] = ts;
+    ndoub[r] = td;
+  }
+}
+
+// Same-spin part of <bra|H|ket> for bra string sr, ket string sk of spin `spin`.
+__device__ void make_entry(int spin, uint64_t sr, uint64_t sk, int L, const double* __restrict__ h,
+                           const double* __restrict__ eri, double& val, uint64_t& om, uint32_t& info) {
+  const uint64_t hole = sk & ~sr;  // occupied in ket only
+  const uint64_t part = sr & ~sk;  // occupied in bra only
+  if (popc64(hole) == 1) {
+    const int i = __ffsll((long long)hole) - 1, a = __ffsll((long long)part) - 1;
+    const int lo = i < a ? i : a, hi = i < a ? a : i;
+    // parity(ket, 2lo+s, 2hi+s): same-spin bits strictly between (the start
+    // bit and the [start,end) count cancel on the occupied end), plus the
+    // opposite-spin bits of the range.
+    const uint32_t neg = (uint32_t)(popc64(sk & range_mask(lo + 1, hi)) & 1);
+    om = other_range(spin, lo, hi);
+    double v = h[(size_t)a * L + i];
+    uint64_t bits = sk;
+    while (bits) {
+      const int q = __ffsll((long long)bits) - 1;
+      v += eri[eri_index(a, i, q, q)] - eri[eri_index(a, q, q, i)];
+      bits &= bits - 1;
+    }
+    val = v;
+    info = (neg << 31) | kInfoSingle | (uint32_t)i | ((uint32_t)a << 6) |
+           ((uint32_t)pair_index(a, i) << 12);
+  } else {
+    const int i = __ffsll((long long)hole) - 1;
+    const int j = __ffsll((long long)(hole & (hole - 1))) - 1;
+    const int a = __ffsll((long long)part) - 1;
+    const int b = __ffsll((long long)(part & (part - 1))) - 1;
+    int par = 0;
+    uint64_t m = 0;
+    {
+      const int lo = i < a ? i : a, hi = i < a ? a : i;
+      par += popc64(sk & range_mask(lo, hi)) + (int)((sk >> lo) & 1ull);
+      m ^= other_range(spin, lo, hi);
+    }
+    {
+      const int lo = j < b ? j : b, hi = j < b ? b : j;
+      par += popc64(sk & range_mask(lo, hi)) + (int)((sk >> lo) & 1ull);
+      m ^= other_range(spin, lo, hi);
+    }
+    if (a > j || b < i) par += 1;
+    om = m;
+    val = eri[eri_index(a, i, b, j)] - eri[eri_index(a, j, b, i)];
+    info = ((uint32_t)(par & 1) << 31) | (uint32_t)i | ((uint32_t)j << 6) | ((uint32_t)a << 12) |
+           ((uint32_t)b << 18);
+  }
+}
+
+__global__ void __launch_bounds__(kConnThreads)
+conn_fill_kernel(int spin, const uint64_t* __restrict__ s, size_t n, const uint64_t* __restrict__ off,
+                 const uint32_t* __restrict__ nsing, int L, const double* __restrict__ h,
+                 const double* __restrict__ eri, uint32_t* __restrict__ ket, double* __restrict__ val,
+                 float* __restrict__ val32, uint64_t* __restrict__ omask, uint32_t* __restrict__ info) {
+  const size_t r = blockIdx.x;
+  const uint64_t sr = s[r];
+  const uint64_t sbase0 = off[r];
+  const uint64_t dbase0 = off[r] + nsing[r];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  __shared__ uint32_t ws[kConnThreads / 32], wd[kConnThreads / 32];
+  __shared__ uint32_t s_run, d_run;
+  if (threadIdx.x == 0) { s_run = 0; d_run = 0; }
+  __syncthreads();
+  for (size_t k0 = 0; k0 < n; k0 += kConnThreads) {
+    const size_t k = k0 + threadIdx.x;
+    uint64_t sk = 0;
+    int d = 0;
+    if (k < n) { sk = s[k]; d = popc64(sr ^ sk); }
+    const bool is_s = (k < n) && d == 2, is_d = (k < n) && d == 4;
+    const unsigned bs = __ballot_sync(0xffffffffu, is_s), bd = __ballot_sync(0xffffffffu, is_d);
+    if (lane == 0) { ws[warp] = __popc(bs); wd[warp] = __popc(bd); }
+    __syncthreads();
+    uint32_t sp = 0, dp = 0, st = 0, dt = 0;
+    for (int w = 0; w < kConnThreads / 32; ++w) {
+      if (w < warp) { sp += ws[w]; dp += wd[w]; }
+      st += ws[w];
+      dt += wd[w];
+    }
+    if (is_s || is_d) {
+      const uint64_t pos = is_s ? sbase0 + s_run + sp + __popc(bs & lt)
+                                : dbase0 + d_run + dp + __popc(bd & lt);
+      double v;
+      uint64_t m;
+      uint32_t inf;
+      make_entry(spin, sr, sk, L, h, eri, v, m, inf);
+      ket[pos] = (uint32_t)k;
+      val[pos] = v;
+      val32[pos] = (float)v;
+      omask[pos] = m;
+      info[pos] = inf;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) { s_run += st; d_run += dt; }
+    __syncthreads();
+  }
+}
+
+void free_conn(Conn& c) {
+  cudaFree(c.nsing); cudaFree(c.ndoub); cudaFree(c.off); cudaFree(c.ket);
+  cudaFree(c.val); cudaFree(c.val32); cudaFree(c.omask); cudaFree(c.info);
+  c = Conn{};
+}
+
+int build_one(Ctx* c, int spin) {
+  Conn& cn = c->conn[spin];
+  free_conn(cn);
+  const size_t n = spin == 0 ? c->na : c->nb;
+  const uint64_t* s = spin == 0 ? c->d_a : c->d_b;
+  cn.n = n;
+  SBDX_CUDA(c, cudaMalloc(&cn.nsing, sizeof(uint32_t) * n));
+  SBDX_CUDA(c, cudaMalloc(&cn.ndoub, sizeof(uint32_t) * n));
+  SBDX_CUDA(c, cudaMalloc(&cn.off, sizeof(uint64_t) * (n + 1)));
+  conn_count_kernel<<<(unsigned)n, kConnThreads, 0, c->stream>>>(s, n, cn.nsing, cn.ndoub);
+  SBDX_LAUNCHED(c);
+  std::vector<uint32_t> hs(n), hd(n);
+  SBDX_CUDA(c, cudaMemcpyAsync(hs.data(), cn.nsing, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(hd.data(), cn.ndoub, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  std::vector<uint64_t> off(n + 1, 0);
+  for (size_t r = 0; r < n; ++r) off[r + 1] = off[r] + hs[r] + hd[r];
+  cn.total = off[n];
+  SBDX_CUDA(c, cudaMemcpyAsync(cn.off, off.data(), sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, c->stream));
+  const size_t t = cn.total ? cn.total : 1;
+  SBDX_CUDA(c, cudaMalloc(&cn.ket, sizeof(uint32_t) * t));
+  SBDX_CUDA(c, cudaMalloc(&cn.val, sizeof(double) * t));
+  SBDX_CUDA(c, cudaMalloc(&cn.val32, sizeof(float) * t));
+  SBDX_CUDA(c, cudaMalloc(&cn.omask, sizeof(uint64_t) * t));
+  SBDX_CUDA(c, cudaMalloc(&cn.info, sizeof(uint32_t) * t));
+  conn_fill_kernel<<<(unsigned)n, kConnThreads, 0, c->stream>>>(spin, s, n, cn.off, cn.nsing, c->L, c->d_h,
+                                                                 c->d_eri, cn.ket, cn.val, cn.val32,
+                                                                 cn.omask, cn.info);
+  SBDX_LAUNCHED(c);
+  // the host copy of `off` must stay alive until the async copy ran
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+}  // namespace
+
+void free_connectivity(Ctx* c) {
+  free_conn(c->conn[0]);
+  free_conn(c->conn[1]);
+  c->have_conn = false;
+}
+
+int build_connectivity(Ctx* c) {
+  if (!c->have_strings || !c->have_integrals) {
+    c->err = "build_connectivity: set integrals and strings first";
+    return 3;
+  }
+  int rc = build_one(c, 0);
+  if (rc) return rc;
+  rc = build_one(c, 1);
+  if (rc) return rc;
+  c->have_conn = true;
+  return 0;
+}
+
+}  // namespace sbdx

@@ -1,0 +1,564 @@
+// Davidson eigensolver on device-resident vectors.
+//
+// FP64 mode restates the reference Davidson, max_time overload
+// (chemistry/tpb/davidson.h:661-924), step by step:
+//   HC_ib = H C_ib; H[jb,ib] = <C_jb|HC_ib> (jb <= ib); Rayleigh-Ritz (dsyev
+//   on (ib+1)^2, ascending); W = sum U[k,0] C_k; R = E0 W - sum U[k,0] HC_k;
+//   normalise W and R; stop when |R| < eps; C_{ib+1} = R/(E0 - d) with the
+//   1e-12 guard; one pass of modified Gram-Schmidt; normalise; restart with
+//   C_0 = W after max_nb steps; then one more sigma for E = <W|HW>
+//   (sbdiag.h:250-273).
+// The tall-skinny products (projection <C_k|x> for all k at once, the
+// Ritz/residual combination) are single HBM passes with FP64 accumulation;
+// the (ib+1)^2 eigenproblem is solved on the host in FP64 (cyclic Jacobi,
+// ascending eigenvalues), standing in for LAPACK dsyev.
+//
+// FP32 mode ("defect correction"): the subspace holds an FP64 anchor pair
+// (W, HW), refreshed with an FP64 sigma every `defect_every` steps, plus
+// FP32-stored correction vectors C_j with FP32-storage sigma products HC_j
+// (FP64 accumulation inside the kernel). Rayleigh-Ritz, Gram-Schmidt, the
+// residual norms and the energy are FP64; convergence is decided on the exact
+// FP64 residual |HW - E W| of the anchor.
+#include "sbdx_internal.cuh"
+#include "sbdx.h"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <type_traits>
+
+namespace sbdx {
+
+namespace {
+
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocks = 4 * 148;
+constexpr int kDotChunk = 8;
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+  return t;  // valid in thread 0
+}
+
+// partial[k * gridDim.x + blk] = partial sums of <V_k, x>, k in [k0, k0+mc)
+template <typename TV, typename TX>
+__global__ void __launch_bounds__(kRedThreads)
+multidot_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restrict__ x, size_t D,
+                double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  const int k0 = blockIdx.y * kDotChunk;
+  const int mc = min(kDotChunk, m - k0);
+  double acc[kDotChunk];
+#pragma unroll
+  for (int k = 0; k < kDotChunk; ++k) acc[k] = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    const double xv = (double)x[s];
+#pragma unroll
+    for (int k = 0; k < kDotChunk; ++k)
+      if (k < mc) acc[k] = fma((double)V[(size_t)(k0 + k) * ldv + s], xv, acc[k]);
+  }
+  for (int k = 0; k < mc; ++k) {
+    const double t = block_sum(acc[k], sh);
+    if (threadIdx.x == 0) partial[(size_t)(k0 + k) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// out[k] = sum_b partial[k * nblk + b] (fixed order, deterministic)
+__global__ void finalize_kernel(const double* __restrict__ partial, int nblk, int m, double* __restrict__ out) {
+  __shared__ double sh[kRedThreads / 32];
+  for (int k = 0; k < m; ++k) {
+    double v = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) v += partial[(size_t)k * nblk + b];
+    const double t = block_sum(v, sh);
+    if (threadIdx.x == 0) out[k] = t;
+  }
+}
+
+// W = u0*W0 + sum_k u[k] C_k ;  R = E0*W - (u0*HW0 + sum_k u[k] HC_k)
+// (W0/HW0 optional FP64 anchor). partial norms of W (slot 0) and R (slot 1).
+template <typename TV>
+__global__ void __launch_bounds__(kRedThreads)
+combine_kernel(const TV* __restrict__ C, const TV* __restrict__ HC, size_t ldv, int m,
+               const double* __restrict__ u, const double* __restrict__ W0, const double* __restrict__ HW0,
+               double u0, const double* __restrict__ E0p, size_t D, double* __restrict__ W,
+               double* __restrict__ R, double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  __shared__ double su[64];
+  for (int k = threadIdx.x; k < m; k += blockDim.x) su[k] = u[k];
+  __syncthreads();
+  const double E0 = *E0p;
+  double nw = 0.0, nr = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    double w = 0.0, hw = 0.0;
+    if (W0 != nullptr) { w = u0 * W0[s]; hw = u0 * HW0[s]; }
+    for (int k = 0; k < m; ++k) {
+      w = fma((double)C[(size_t)k * ldv + s], su[k], w);
+      hw = fma((double)HC[(size_t)k * ldv + s], su[k], hw);
+    }
+    const double r = E0 * w - hw;
+    W[s] = w;
+    R[s] = r;
+    nw = fma(w, w, nw);
+    nr = fma(r, r, nr);
+  }
+  double t = block_sum(nw, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+  t = block_sum(nr, sh);
+  if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = t;
+}
+
+// v = (R / |R|) / (E0 - d) with the reference guard (davidson.h:855-862);
+// partial <V0, v> for the first Gram-Schmidt step (V0 in TV, or FP64 anchor).
+template <typename TV>
+__global__ void __launch_bounds__(kRedThreads)
+precond_kernel(const double* R, const double* __restrict__ dii, const double* __restrict__ E0p,
+               const double* __restrict__ nrm2, size_t D, double* v, const TV* __restrict__ V0,
+               const double* __restrict__ V0d, double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  const double E0 = *E0p;
+  const double inv = 1.0 / sqrt(*nrm2);
+  const double eps_reg = 1.0e-12;
+  double acc = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    const double rs = R[s] * inv;
+    const double den = E0 - dii[s];
+    const double x = fabs(den) > eps_reg ? rs / den : rs / (den - eps_reg);
+    v[s] = x;
+    const double b = V0d != nullptr ? V0d[s] : (double)V0[s];
+    acc = fma(b, x, acc);
+  }
+  const double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+// v -= olap * Vk ; partial <Vn, v> (Vn = next basis vector) or <v, v> if Vn null.
+template <typename TV>
+__global__ void __launch_bounds__(kRedThreads)
+axpy_dot_kernel(double* __restrict__ v, const TV* __restrict__ Vk, const double* __restrict__ Vkd,
+                const double* __restrict__ olap_p, const TV* __restrict__ Vn, size_t D, double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  const double olap = -(*olap_p);
+  double acc = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    const double b = Vkd != nullptr ? Vkd[s] : (double)Vk[s];
+    const double x = fma(b, olap, v[s]);
+    v[s] = x;
+    const double y = Vn != nullptr ? (double)Vn[s] : x;
+    acc = fma(y, x, acc);
+  }
+  const double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+// out = (TV)(v / sqrt(nrm2))
+template <typename TV, typename TI>
+__global__ void scale_store_kernel(const TI* v, const double* __restrict__ nrm2, size_t D, TV* out) {
+  const double inv = nrm2 != nullptr ? 1.0 / sqrt(*nrm2) : 1.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x)
+    out[s] = (TV)((double)v[s] * inv);
+}
+
+// r = HW - E W (FP64), partial |r|^2
+__global__ void __launch_bounds__(kRedThreads)
+residual_kernel(const double* __restrict__ W, const double* __restrict__ HW, const double* __restrict__ Ep,
+                size_t D, double* __restrict__ r, double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  const double E = *Ep;
+  double acc = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    const double x = E * W[s] - HW[s];
+    r[s] = x;
+    acc = fma(x, x, acc);
+  }
+  const double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+// ---- host symmetric eigensolver (stand-in for LAPACK dsyev 'V','U') ---------
+// A: n x n symmetric (upper triangle read, column-major, leading dim lda).
+// On return the columns of A are the eigenvectors, w ascending.
+void jacobi_eigen(int n, double* A, int lda, double* w) {
+  std::vector<double> a((size_t)n * n), v((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) a[i + (size_t)n * j] = i <= j ? A[i + (size_t)lda * j] : A[j + (size_t)lda * i];
+  for (int i = 0; i < n; ++i) v[i + (size_t)n * i] = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, diag = 0.0;
+    for (int j = 0; j < n; ++j) {
+      diag += a[j + (size_t)n * j] * a[j + (size_t)n * j];
+      for (int i = 0; i < j; ++i) off += a[i + (size_t)n * j] * a[i + (size_t)n * j];
+    }
+    if (off <= 1e-32 * diag || off < 1e-300) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a[p + (size_t)n * q];
+        if (apq == 0.0) continue;
+        const double theta = (a[q + (size_t)n * q] - a[p + (size_t)n * p]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
+        for (int k = 0; k < n; ++k) {
+          const double akp = a[k + (size_t)n * p], akq = a[k + (size_t)n * q];
+          a[k + (size_t)n * p] = cs * akp - sn * akq;
+          a[k + (size_t)n * q] = sn * akp + cs * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double apk = a[p + (size_t)n * k], aqk = a[q + (size_t)n * k];
+          a[p + (size_t)n * k] = cs * apk - sn * aqk;
+          a[q + (size_t)n * k] = sn * apk + cs * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = v[k + (size_t)n * p], vkq = v[k + (size_t)n * q];
+          v[k + (size_t)n * p] = cs * vkp - sn * vkq;
+          v[k + (size_t)n * q] = sn * vkp + cs * vkq;
+        }
+      }
+  }
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  for (int i = 1; i < n; ++i) {
+    const int x = ord[i];
+    int j = i - 1;
+    while (j >= 0 && a[ord[j] + (size_t)n * ord[j]] > a[x + (size_t)n * x]) { ord[j + 1] = ord[j]; --j; }
+    ord[j + 1] = x;
+  }
+  for (int k = 0; k < n; ++k) {
+    w[k] = a[ord[k] + (size_t)n * ord[k]];
+    for (int i = 0; i < n; ++i) A[i + (size_t)lda * k] = v[i + (size_t)n * ord[k]];
+  }
+}
+
+struct Work {
+  double* partial = nullptr;  // reduction partials
+  double* scal = nullptr;     // device scalars
+  double* u = nullptr;        // Ritz coefficients
+  ~Work() { cudaFree(partial); cudaFree(scal); cudaFree(u); }
+};
+
+// Device scalar slots
+enum { kE0 = 0, kNW = 1, kNR = 2, kOlap = 3, kNV = 4, kE = 5, kDots = 8 };
+
+template <typename TV, typename TX>
+int multidot(Ctx* c, Work& wk, const TV* V, size_t ldv, int m, const TX* x, size_t D, double* out) {
+  dim3 grid(kRedBlocks, (unsigned)((m + kDotChunk - 1) / kDotChunk));
+  multidot_kernel<TV, TX><<<grid, kRedThreads, 0, c->stream>>>(V, ldv, m, x, D, wk.partial);
+  SBDX_LAUNCHED(c);
+  finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, kRedBlocks, m, out);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+int finalize(Ctx* c, Work& wk, int m, double* out) {
+  finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, kRedBlocks, m, out);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+double seconds_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Expansion vector: v = precond(R); MGS against the basis [anchor?, V_0..V_{nv-1}];
+// normalised and stored into dst (TV). v is FP64 scratch (may alias R).
+template <typename TV>
+int expand(Ctx* c, Work& wk, const double* R, const double* Wd, const TV* V, int nv, size_t D, double* v, TV* dst) {
+  double* s = wk.scal;
+  // the first basis vector is the FP64 anchor when Wd != null
+  precond_kernel<TV><<<kRedBlocks, kRedThreads, 0, c->stream>>>(R, c->d_hii, s + kE0, s + kNR, D, v,
+                                                                Wd ? nullptr : V, Wd, wk.partial);
+  SBDX_LAUNCHED(c);
+  int rc = finalize(c, wk, 1, s + kOlap);
+  if (rc) return rc;
+  const int nbasis = nv + (Wd ? 1 : 0);
+  for (int k = 0; k < nbasis; ++k) {
+    const bool anchor = Wd && k == 0;
+    const int vi = Wd ? k - 1 : k;
+    const TV* vk = anchor ? nullptr : V + (size_t)vi * D;
+    const TV* vn = (k + 1 < nbasis) ? V + (size_t)(Wd ? k : k + 1) * D : nullptr;
+    axpy_dot_kernel<TV><<<kRedBlocks, kRedThreads, 0, c->stream>>>(v, vk, anchor ? Wd : nullptr, s + kOlap, vn, D,
+                                                                   wk.partial);
+    SBDX_LAUNCHED(c);
+    rc = finalize(c, wk, 1, vn ? s + kOlap : s + kNV);
+    if (rc) return rc;
+  }
+  scale_store_kernel<TV, double><<<kRedBlocks, kRedThreads, 0, c->stream>>>(v, s + kNV, D, dst);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+template <typename TV>
+int sigma_typed(Ctx* c, const TV* x, TV* y) {
+  return sigma_device(c, std::is_same<TV, double>::value ? 0 : 1, x, y);
+}
+
+// ---- FP64: the reference algorithm ------------------------------------------
+int davidson_fp64(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info) {
+  const size_t D = c->na * c->nb;
+  const int nb = p.max_nb;
+  Work wk;
+  SBDX_CUDA(c, cudaMalloc(&wk.partial, sizeof(double) * kRedBlocks * (nb + 2)));
+  SBDX_CUDA(c, cudaMalloc(&wk.scal, sizeof(double) * (kDots + nb + 8)));
+  SBDX_CUDA(c, cudaMalloc(&wk.u, sizeof(double) * (nb + 1)));
+  double *C = nullptr, *HC = nullptr, *R = nullptr;
+  SBDX_CUDA(c, cudaMalloc(&C, sizeof(double) * D * nb));
+  SBDX_CUDA(c, cudaMalloc(&HC, sizeof(double) * D * nb));
+  SBDX_CUDA(c, cudaMalloc(&R, sizeof(double) * D));
+  struct Guard { double *a, *b, *r; ~Guard() { cudaFree(a); cudaFree(b); cudaFree(r); } } g{C, HC, R};
+  double* s = wk.scal;
+  std::vector<double> H((size_t)nb * nb, 0.0), U((size_t)nb * nb), E(nb), hcol(nb + 1);
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<double> step_times;
+  bool done = false;
+  double normR = 0.0;
+  int rc = 0;
+  for (int it = 0; it < p.max_it && !done; ++it) {
+    SBDX_CUDA(c, cudaMemcpyAsync(C, dW, sizeof(double) * D, cudaMemcpyDeviceToDevice, c->stream));
+    for (int ib = 0; ib < nb; ++ib) {
+      const auto ts = std::chrono::steady_clock::now();
+      double* Cb = C + (size_t)ib * D;
+      double* HCb = HC + (size_t)ib * D;
+      if ((rc = sigma_typed<double>(c, Cb, HCb))) return rc;
+      info.n_sigma++;
+      if ((rc = multidot<double, double>(c, wk, C, D, ib + 1, HCb, D, s + kDots))) return rc;
+      SBDX_CUDA(c, cudaMemcpyAsync(hcol.data(), s + kDots, sizeof(double) * (ib + 1), cudaMemcpyDeviceToHost, c->stream));
+      SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+      for (int jb = 0; jb <= ib; ++jb) { H[jb + (size_t)nb * ib] = hcol[jb]; H[ib + (size_t)nb * jb] = hcol[jb]; }
+      for (int jb = 0; jb <= ib; ++jb)
+        for (int kb = 0; kb <= ib; ++kb) U[jb + (size_t)nb * kb] = H[jb + (size_t)nb * kb];
+      jacobi_eigen(ib + 1, U.data(), nb, E.data());
+      std::vector<double> up(ib + 2);
+      for (int k = 0; k <= ib; ++k) up[k] = U[k];
+      SBDX_CUDA(c, cudaMemcpyAsync(wk.u, up.data(), sizeof(double) * (ib + 1), cudaMemcpyHostToDevice, c->stream));
+      SBDX_CUDA(c, cudaMemcpyAsync(s + kE0, &E[0], sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      combine_kernel<double><<<kRedBlocks, kRedThreads, 0, c->stream>>>(C, HC, D, ib + 1, wk.u, nullptr, nullptr,
+                                                                        0.0, s + kE0, D, dW, R, wk.partial);
+      SBDX_LAUNCHED(c);
+      if ((rc = finalize(c, wk, 2, s + kNW))) return rc;
+      double nrm[2];
+      SBDX_CUDA(c, cudaMemcpyAsync(nrm, s + kNW, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
+      SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+      normR = std::sqrt(nrm[1]);
+      // normalise W (davidson.h:818-819)
+      scale_store_kernel<double, double><<<kRedBlocks, kRedThreads, 0, c->stream>>>(dW, s + kNW, D, dW);
+      SBDX_LAUNCHED(c);
+      if (p.verbose) {
+        std::printf(" Davidson iteration %d.%d (tol=%.6e):", it, ib, normR);
+        for (int q = 0; q < std::min(ib + 1, 4); ++q) std::printf(" %.12f", E[q]);
+        std::printf("\n");
+        std::fflush(stdout);
+      }
+      if (normR < p.eps) { done = true; info.converged = 1; break; }
+      if (ib < nb - 1) {
+        if ((rc = expand<double>(c, wk, R, nullptr, C, ib + 1, D, R, C + (size_t)(ib + 1) * D))) return rc;
+      }
+      // time guard (davidson.h:876-903)
+      SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+      step_times.push_back(seconds_since(ts));
+      double avg = 0.0;
+      for (double x : step_times) avg += x;
+      avg /= (double)step_times.size();
+      if (seconds_since(t0) + avg > p.max_time) { done = true; break; }
+    }
+  }
+  info.residual = normR;
+  // final energy <W|HW> with one more sigma (sbdiag.h:250-273)
+  if ((rc = sigma_typed<double>(c, dW, R))) return rc;
+  info.n_sigma++;
+  info.n_sigma64 = info.n_sigma;
+  if ((rc = multidot<double, double>(c, wk, dW, D, 1, R, D, s + kE))) return rc;
+  SBDX_CUDA(c, cudaMemcpyAsync(&info.energy, s + kE, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  info.seconds = seconds_since(t0);
+  return 0;
+}
+
+// ---- FP32 storage with FP64 defect correction --------------------------------
+// Generalised Rayleigh-Ritz M x = theta S x over the basis [W, C_0..C_{nv-1}]:
+// the C_j are orthonormal among themselves (MGS), the anchor W is not
+// orthogonal to them after a refresh, so S = I except row/column 0.
+bool gen_eigen(int n, const std::vector<double>& M, const std::vector<double>& S, int ld, double& theta,
+               std::vector<double>& x) {
+  std::vector<double> Lc((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    double d = S[j + (size_t)ld * j];
+    for (int k = 0; k < j; ++k) d -= Lc[j + (size_t)n * k] * Lc[j + (size_t)n * k];
+    if (!(d > 0.0)) return false;
+    d = std::sqrt(d);
+    Lc[j + (size_t)n * j] = d;
+    for (int i = j + 1; i < n; ++i) {
+      double v = S[std::min(i, j) + (size_t)ld * std::max(i, j)];
+      for (int k = 0; k < j; ++k) v -= Lc[i + (size_t)n * k] * Lc[j + (size_t)n * k];
+      Lc[i + (size_t)n * j] = v / d;
+    }
+  }
+  // A = L^-1 M L^-T
+  std::vector<double> T((size_t)n * n), A((size_t)n * n);
+  for (int col = 0; col < n; ++col)  // T = L^-1 M (forward substitution per column)
+    for (int i = 0; i < n; ++i) {
+      double v = M[std::min(i, col) + (size_t)ld * std::max(i, col)];
+      for (int k = 0; k < i; ++k) v -= Lc[i + (size_t)n * k] * T[k + (size_t)n * col];
+      T[i + (size_t)n * col] = v / Lc[i + (size_t)n * i];
+    }
+  for (int row = 0; row < n; ++row)  // A = T L^-T, i.e. A^T = L^-1 T^T
+    for (int i = 0; i < n; ++i) {
+      double v = T[row + (size_t)n * i];
+      for (int k = 0; k < i; ++k) v -= Lc[i + (size_t)n * k] * A[row + (size_t)n * k];
+      A[row + (size_t)n * i] = v / Lc[i + (size_t)n * i];
+    }
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < j; ++i) A[i + (size_t)n * j] = A[j + (size_t)n * i] = 0.5 * (A[i + (size_t)n * j] + A[j + (size_t)n * i]);
+  std::vector<double> w(n);
+  jacobi_eigen(n, A.data(), n, w.data());
+  theta = w[0];
+  x.assign(n, 0.0);
+  for (int i = n - 1; i >= 0; --i) {  // x = L^-T y
+    double v = A[i];
+    for (int k = i + 1; k < n; ++k) v -= Lc[k + (size_t)n * i] * x[k];
+    x[i] = v / Lc[i + (size_t)n * i];
+  }
+  return true;
+}
+
+int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info) {
+  const size_t D = c->na * c->nb;
+  const int nb = p.max_nb;  // FP32 correction vectors kept beside the FP64 anchor
+  const int kdef = p.defect_every > 0 ? p.defect_every : 4;
+  Work wk;
+  SBDX_CUDA(c, cudaMalloc(&wk.partial, sizeof(double) * kRedBlocks * (nb + 3)));
+  SBDX_CUDA(c, cudaMalloc(&wk.scal, sizeof(double) * (kDots + nb + 8)));
+  SBDX_CUDA(c, cudaMalloc(&wk.u, sizeof(double) * (nb + 2)));
+  float *C = nullptr, *HC = nullptr;
+  double *AW = nullptr, *Wn = nullptr, *R = nullptr;
+  SBDX_CUDA(c, cudaMalloc(&C, sizeof(float) * D * nb));
+  SBDX_CUDA(c, cudaMalloc(&HC, sizeof(float) * D * nb));
+  SBDX_CUDA(c, cudaMalloc(&AW, sizeof(double) * D * 2));  // [W | HW] anchor pair
+  SBDX_CUDA(c, cudaMalloc(&Wn, sizeof(double) * D));
+  SBDX_CUDA(c, cudaMalloc(&R, sizeof(double) * D));
+  struct Guard {
+    float *a, *b; double *c, *d, *e;
+    ~Guard() { cudaFree(a); cudaFree(b); cudaFree(c); cudaFree(d); cudaFree(e); }
+  } g{C, HC, AW, Wn, R};
+  double* W = AW;
+  double* HW = AW + D;
+  double* s = wk.scal;
+  SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * D, cudaMemcpyDeviceToDevice, c->stream));
+  const auto t0 = std::chrono::steady_clock::now();
+  int rc = 0;
+  const int ld = nb + 1;
+  std::vector<double> M((size_t)ld * ld, 0.0), S((size_t)ld * ld, 0.0), col(2 * ld + 2), x;
+  double Eanc = 0.0, normR = 0.0;
+  int nv = 0;
+  auto set_pair = [&](std::vector<double>& A, int i, int j, double v) {
+    A[i + (size_t)ld * j] = v;
+    A[j + (size_t)ld * i] = v;
+  };
+  auto refresh = [&]() -> int {
+    // exact anchor (defect correction): HW = H W in FP64, E = <W|HW>, R = E W - HW
+    int r2 = sigma_typed<double>(c, W, HW);
+    if (r2) return r2;
+    info.n_sigma64++;
+    if ((r2 = multidot<double, double>(c, wk, W, D, 1, HW, D, s + kE))) return r2;
+    residual_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, s + kE, D, R, wk.partial);
+    SBDX_LAUNCHED(c);
+    if ((r2 = finalize(c, wk, 1, s + kNR))) return r2;
+    SBDX_CUDA(c, cudaMemcpyAsync(s + kE0, s + kE, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    double h2[2];
+    SBDX_CUDA(c, cudaMemcpyAsync(&h2[0], s + kE, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaMemcpyAsync(&h2[1], s + kNR, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    Eanc = h2[0];
+    normR = std::sqrt(h2[1]);
+    set_pair(M, 0, 0, Eanc);
+    set_pair(S, 0, 0, 1.0);
+    if (nv > 0) {  // anchor row against the kept corrections: <C_j|W>, <C_j|HW>
+      if ((r2 = multidot<float, double>(c, wk, C, D, nv, W, D, s + kDots))) return r2;
+      if ((r2 = multidot<float, double>(c, wk, C, D, nv, HW, D, s + kDots + nv))) return r2;
+      SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kDots, sizeof(double) * 2 * nv, cudaMemcpyDeviceToHost, c->stream));
+      SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+      for (int j = 0; j < nv; ++j) { set_pair(S, 0, j + 1, col[j]); set_pair(M, 0, j + 1, col[nv + j]); }
+    }
+    return 0;
+  };
+  if ((rc = refresh())) return rc;
+  int steps = 0;
+  const int max_steps = p.max_it * p.max_nb;
+  while (true) {
+    if (p.verbose) {
+      std::printf(" Davidson defect step %d (exact tol=%.6e): %.12f\n", steps, normR, Eanc);
+      std::fflush(stdout);
+    }
+    if (normR < p.eps) { info.converged = 1; break; }
+    if (steps >= max_steps || seconds_since(t0) > p.max_time) break;
+    if (nv == nb) nv = 0;  // thick restart with the anchor only
+    // expansion from the exact FP64 residual (kE0 = E, kNR = |R|^2)
+    if ((rc = expand<float>(c, wk, R, W, C, nv, D, R, C + (size_t)nv * D))) return rc;
+    ++nv;
+    for (int inner = 0; inner < kdef; ++inner) {
+      const int j = nv - 1;  // newest correction
+      float* Cb = C + (size_t)j * D;
+      float* HCb = HC + (size_t)j * D;
+      if ((rc = sigma_typed<float>(c, Cb, HCb))) return rc;
+      info.n_sigma++;
+      ++steps;
+      // <C_k|HC_j> (k <= j) and <W|C_j>, <HW|C_j>
+      if ((rc = multidot<float, float>(c, wk, C, D, nv, HCb, D, s + kDots))) return rc;
+      if ((rc = multidot<double, float>(c, wk, AW, D, 2, Cb, D, s + kDots + nv))) return rc;
+      SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kDots, sizeof(double) * (nv + 2), cudaMemcpyDeviceToHost, c->stream));
+      SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+      for (int k = 0; k < nv; ++k) {
+        set_pair(M, k + 1, j + 1, col[k]);
+        set_pair(S, k + 1, j + 1, k == j ? 1.0 : 0.0);
+      }
+      set_pair(S, 0, j + 1, col[nv]);
+      set_pair(M, 0, j + 1, col[nv + 1]);
+      const int n = nv + 1;
+      double theta = 0.0;
+      if (!gen_eigen(n, M, S, ld, theta, x)) {
+        c->err = "davidson (FP32): projected overlap matrix is not positive definite";
+        return 5;
+      }
+      SBDX_CUDA(c, cudaMemcpyAsync(wk.u, x.data() + 1, sizeof(double) * nv, cudaMemcpyHostToDevice, c->stream));
+      SBDX_CUDA(c, cudaMemcpyAsync(s + kE0, &theta, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      combine_kernel<float><<<kRedBlocks, kRedThreads, 0, c->stream>>>(C, HC, D, nv, wk.u, W, HW, x[0], s + kE0, D,
+                                                                       Wn, R, wk.partial);
+      SBDX_LAUNCHED(c);
+      if ((rc = finalize(c, wk, 2, s + kNW))) return rc;
+      if (inner == kdef - 1 || nv == nb) break;
+      if ((rc = expand<float>(c, wk, R, W, C, nv, D, R, C + (size_t)nv * D))) return rc;
+      ++nv;
+    }
+    // W <- normalised Ritz vector, then the exact FP64 refresh
+    scale_store_kernel<double, double><<<kRedBlocks, kRedThreads, 0, c->stream>>>(Wn, s + kNW, D, W);
+    SBDX_LAUNCHED(c);
+    if ((rc = refresh())) return rc;
+  }
+  SBDX_CUDA(c, cudaMemcpyAsync(dW, W, sizeof(double) * D, cudaMemcpyDeviceToDevice, c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  info.residual = normR;
+  info.energy = Eanc;
+  info.seconds = seconds_since(t0);
+  return 0;
+}
+
+}  // namespace
+
+int davidson(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info) {
+  if (p.max_nb < 1 || p.max_nb > 60 || p.max_it < 1) {
+    c->err = "davidson: max_nb must be in [1, 60] and max_it >= 1";
+    return 1;
+  }
+  if (!c->have_conn) { int rc = build_connectivity(c); if (rc) return rc; }
+  if (!c->have_hii) { int rc = diag_terms(c); if (rc) return rc; }
+  if (p.precision == 0) return davidson_fp64(c, p, dW, info);
+  if (p.precision == 1) return davidson_mixed(c, p, dW, info);
+  c->err = "davidson: precision must be SBDX_FP64 or SBDX_FP32";
+  return 1;
+}
+
+}  // namespace sbdx

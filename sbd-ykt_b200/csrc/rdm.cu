@@ -1,0 +1,467 @@
+// 1-/2-particle reduced density matrices, occupation density, alpha-string
+// weights and the energy adjoint.
+//
+// Restates Correlation (reference chemistry/tpb/correlation.h:194-444) with
+// ZeroDiffCorrelation (:15-44), OneDiffCorrelation (:49-86) and
+// TwoDiffCorrelation (:91-130): the same element indices and signs, summed in
+// a different order. The reference accumulates every (bra, ket) pair into a
+// per-thread copy of the 4*L^4 array; here the sums are regrouped so that
+// global atomics are per connectivity entry, not per determinant pair:
+//   - diagonal: per bra row, the row weight sum_c W^2 and the opposite-spin
+//     occupation profile sum_c W^2 n_q(c) (one CTA per row), then an L x L
+//     finalize;
+//   - same-spin singles/doubles: one warp per connectivity entry (r -> k)
+//     reduces sum_c W[r,c] W[k,c] (-1)^{opposite-spin parity} over the
+//     opposite-spin index c (and, for singles, its n_q-weighted profile);
+//     the beta task runs on W^T;
+//   - alpha-single x beta-single: one CTA per bra alpha row stages W[ja, :]
+//     in shared memory and folds all (ib, jb) pairs of each beta excitation
+//     pattern (i_b, a_b) into an L x L shared accumulator before flushing.
+// Layout: one[s*L^2 + p + L q], two[(s + 2t)*L^4 + i + L j + L^2 k + L^3 l].
+#include "sbdx_internal.cuh"
+
+namespace sbdx {
+
+int ensure_sigma_scratch(Ctx* c);
+
+namespace {
+
+constexpr int kRowThreads = 256;
+
+// Reference parity(det, start, end) (determinants.h:228-279) on the
+// interleaved determinant of (alpha, beta): returns the sign bit (1 = -1).
+__device__ __forceinline__ uint32_t ref_parity_bit(uint64_t a, uint64_t b, int start, int end) {
+  const uint64_t ma = range_mask((start + 1) >> 1, (end + 1) >> 1);
+  const uint64_t mb = range_mask(start >> 1, end >> 1);
+  const uint64_t sw = (start & 1) ? b : a;
+  return (uint32_t)(popc64(a & ma) + popc64(b & mb) + (int)((sw >> (start >> 1)) & 1ull)) & 1u;
+}
+
+// Row weights and occupation profiles of one orientation of W (rows x cols):
+// wrow[r] = sum_c W^2; P[p][q] += wrow[r] for p, q in s_row[r];
+// X[p][q] += sum_c W[r,c]^2 n_q(s_col[c]) for p in s_row[r] (if X != null).
+__global__ void __launch_bounds__(kRowThreads)
+row_weight_kernel(const double* __restrict__ W, size_t rows, size_t cols, const uint64_t* __restrict__ s_row,
+                  const uint64_t* __restrict__ s_col, int L, double* __restrict__ wrow, double* __restrict__ P,
+                  double* __restrict__ X) {
+  __shared__ double vq[64];
+  __shared__ double red[kRowThreads / 32];
+  const size_t r = blockIdx.x;
+  for (int q = threadIdx.x; q < 64; q += blockDim.x) vq[q] = 0.0;
+  __syncthreads();
+  double s = 0.0;
+  for (size_t c = threadIdx.x; c < cols; c += blockDim.x) {
+    const double w = W[r * cols + c];
+    const double w2 = w * w;
+    s += w2;
+    if (X != nullptr && w2 != 0.0) {
+      uint64_t bits = s_col[c];
+      while (bits) {
+        const int q = __ffsll((long long)bits) - 1;
+        bits &= bits - 1;
+        atomicAdd(&vq[q], w2);
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kRowThreads / 32; ++w) t += red[w];
+    red[0] = t;
+    wrow[r] = t;
+  }
+  __syncthreads();
+  const double tot = red[0];
+  const uint64_t own = s_row[r];
+  // P: pairs of own orbitals; X: own orbital x opposite-spin profile
+  for (int t = threadIdx.x; t < L * L; t += blockDim.x) {
+    const int p = t / L, q = t % L;
+    if ((own >> p) & 1ull) {
+      if ((own >> q) & 1ull) atomicAdd(&P[t], tot);
+      if (X != nullptr && vq[q] != 0.0) atomicAdd(&X[t], vq[q]);
+    }
+  }
+}
+
+// Diagonal (ZeroDiffCorrelation) contributions from P_alpha, P_beta, X.
+__global__ void diag_finalize_kernel(int L, const double* __restrict__ Pa, const double* __restrict__ Pb,
+                                     const double* __restrict__ X, double* __restrict__ one, double* __restrict__ two) {
+  const size_t L2 = (size_t)L * L, L3 = L2 * L, L4 = L3 * L;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= L * L) return;
+  const int p = t / L, q = t % L;
+  const size_t d = (size_t)p + L * q + L2 * p + L3 * q;   // [p, q, p, q]
+  const size_t x = (size_t)p + L * q + L2 * q + L3 * p;   // [p, q, q, p]
+  if (p == q) {
+    one[(size_t)p + L * p] += Pa[t];
+    one[L2 + (size_t)p + L * p] += Pb[t];
+  } else {
+    two[0 * L4 + d] += Pa[t];
+    two[0 * L4 + x] -= Pa[t];
+    two[3 * L4 + d] += Pb[t];
+    two[3 * L4 + x] -= Pb[t];
+  }
+  // opposite spins: alpha p, beta q -> block 2 at [p,q,p,q], block 1 at [q,p,q,p]
+  const double v = X[t];
+  two[2 * L4 + d] += v;
+  two[1 * L4 + (size_t)q + L * p + L2 * q + L3 * p] += v;
+}
+
+__device__ __forceinline__ size_t find_row(const uint64_t* off, size_t n, uint64_t e) {
+  size_t lo = 0, hi = n;  // off[lo] <= e < off[hi]
+  while (hi - lo > 1) {
+    const size_t mid = (lo + hi) >> 1;
+    if (off[mid] <= e) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Same-spin singles and doubles of spin `spin`, one warp per entry.
+__global__ void __launch_bounds__(256)
+rdm_same_kernel(int spin, const double* __restrict__ W, size_t rows, size_t cols, const uint64_t* __restrict__ s_row,
+                const uint64_t* __restrict__ s_col, const uint64_t* __restrict__ off, const uint32_t* __restrict__ ket,
+                const uint64_t* __restrict__ omask, const uint32_t* __restrict__ info, size_t total, int L,
+                double* __restrict__ one, double* __restrict__ two) {
+  __shared__ double vq_all[8][64];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t e = (size_t)blockIdx.x * 8 + warp;
+  double* vq = vq_all[warp];
+  for (int q = lane; q < 64; q += 32) vq[q] = 0.0;
+  __syncwarp();
+  if (e >= total) return;
+  const size_t r = find_row(off, rows, e);
+  const size_t k = ket[e];
+  const uint32_t inf = info[e];
+  const uint64_t om = omask[e];
+  const uint64_t sr = s_row[r];
+  const bool single = (inf & kInfoSingle) != 0;
+  uint32_t sbit;
+  int oi = 0, oa = 0, i_e = 0, j_e = 0, a_e = 0, b_e = 0;
+  if (single) {
+    sbit = inf >> 31;
+    i_e = (int)(inf & 63u);
+    a_e = (int)((inf >> 6) & 63u);
+    oi = a_e;  // bra-only orbital
+    oa = i_e;  // ket-only orbital
+  } else {
+    i_e = (int)(inf & 63u); j_e = (int)((inf >> 6) & 63u);
+    a_e = (int)((inf >> 12) & 63u); b_e = (int)((inf >> 18) & 63u);
+    // TwoDiffCorrelation sign on the bra: I = a_e, J = b_e (bra-only), A = i_e,
+    // B = j_e (ket-only); same-spin part here, opposite-spin part via omask.
+    int par = 0;
+    {
+      const int lo = a_e < i_e ? a_e : i_e, hi = a_e < i_e ? i_e : a_e;
+      par += popc64(sr & range_mask(lo, hi)) + (int)((sr >> lo) & 1ull);
+    }
+    {
+      const int lo = b_e < j_e ? b_e : j_e, hi = b_e < j_e ? j_e : b_e;
+      par += popc64(sr & range_mask(lo, hi)) + (int)((sr >> lo) & 1ull);
+    }
+    if (i_e > b_e || j_e < a_e) par += 1;
+    sbit = (uint32_t)(par & 1);
+  }
+  double s = 0.0;
+  const double* wr = W + r * cols;
+  const double* wk = W + k * cols;
+  for (size_t c = lane; c < cols; c += 32) {
+    const double x = wr[c] * wk[c];
+    if (x == 0.0) continue;
+    const uint64_t o = s_col[c];
+    const uint32_t neg = (sbit ^ (uint32_t)popc64(o & om)) & 1u;
+    const double t = neg ? -x : x;
+    s += t;
+    if (single) {
+      uint64_t bits = o;
+      while (bits) {
+        const int q = __ffsll((long long)bits) - 1;
+        bits &= bits - 1;
+        atomicAdd(&vq[q], t);
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  s = __shfl_sync(0xffffffffu, s, 0);
+  __syncwarp();
+  const size_t L2 = (size_t)L * L, L3 = L2 * L, L4 = L3 * L;
+  const int ss = 3 * spin;           // same-spin block
+  const int so = spin + 2 * (1 - spin), os = (1 - spin) + 2 * spin;
+  if (single) {
+    if (lane == 0) atomicAdd(&one[(size_t)spin * L2 + oi + (size_t)L * oa], s);
+    // same-spin occupied orbitals of the bra (including oi itself, whose
+    // four terms cancel exactly as in the reference)
+    uint64_t bits = sr;
+    int n = 0;
+    while (bits) {
+      const int oj = __ffsll((long long)bits) - 1;
+      bits &= bits - 1;
+      if ((n++ & 31) == lane) {
+        atomicAdd(&two[ss * L4 + oa + (size_t)L * oj + L2 * oi + L3 * oj], s);
+        atomicAdd(&two[ss * L4 + oj + (size_t)L * oa + L2 * oj + L3 * oi], s);
+        atomicAdd(&two[ss * L4 + oa + (size_t)L * oj + L2 * oj + L3 * oi], -s);
+        atomicAdd(&two[ss * L4 + oj + (size_t)L * oa + L2 * oi + L3 * oj], -s);
+      }
+    }
+    for (int q = lane; q < L; q += 32) {
+      const double v = vq[q];
+      if (v != 0.0) {
+        atomicAdd(&two[so * L4 + oa + (size_t)L * q + L2 * oi + L3 * q], v);
+        atomicAdd(&two[os * L4 + q + (size_t)L * oa + L2 * q + L3 * oi], v);
+      }
+    }
+  } else if (lane == 0 && s != 0.0) {
+    // oi = a_e, oj = b_e (bra-only); oa = i_e, ob = j_e (ket-only); same spin
+    atomicAdd(&two[ss * L4 + i_e + (size_t)L * j_e + L2 * (a_e + (size_t)L * b_e)], s);
+    atomicAdd(&two[ss * L4 + j_e + (size_t)L * i_e + L2 * (b_e + (size_t)L * a_e)], s);
+    atomicAdd(&two[ss * L4 + i_e + (size_t)L * j_e + L2 * (b_e + (size_t)L * a_e)], -s);
+    atomicAdd(&two[ss * L4 + j_e + (size_t)L * i_e + L2 * (a_e + (size_t)L * b_e)], -s);
+  }
+}
+
+// Alpha single x beta single pairs (task type 0). One CTA per bra alpha row.
+__global__ void __launch_bounds__(512)
+rdm_ab_kernel(const double* __restrict__ W, size_t nb, const uint64_t* __restrict__ astr,
+              const uint64_t* __restrict__ bstr, const uint64_t* __restrict__ a_off,
+              const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
+              const uint32_t* __restrict__ a_info, const uint64_t* __restrict__ b_off,
+              const uint32_t* __restrict__ b_nsing, const uint32_t* __restrict__ b_ket,
+              const uint32_t* __restrict__ b_info, int L, double* __restrict__ two) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* acc = reinterpret_cast<double*>(smem);  // [L*L] by (i_b, a_b)
+  double* ws = acc + (size_t)L * L;               // [nb]
+  const size_t ia = blockIdx.x;
+  const uint64_t alpha_bra = astr[ia];
+  const double* wbra = W + ia * nb;
+  const size_t L2 = (size_t)L * L, L3 = L2 * L, L4 = L3 * L;
+  const uint32_t ns = a_nsing[ia];
+  for (uint32_t k = 0; k < ns; ++k) {
+    const uint64_t e = a_off[ia] + k;
+    const size_t ja = a_ket[e];
+    const uint32_t inf = a_info[e];
+    const int ia_h = (int)(inf & 63u);          // alpha ket-only orbital i_a
+    const int ia_p = (int)((inf >> 6) & 63u);   // alpha bra-only orbital a_a
+    __syncthreads();
+    for (int t = threadIdx.x; t < L * L; t += blockDim.x) acc[t] = 0.0;
+    for (size_t t = threadIdx.x; t < nb; t += blockDim.x) ws[t] = W[ja * nb + t];
+    __syncthreads();
+    for (size_t ib = threadIdx.x; ib < nb; ib += blockDim.x) {
+      const double wi = wbra[ib];
+      if (wi == 0.0) continue;
+      const uint64_t beta_bra = bstr[ib];
+      const uint64_t m0 = b_off[ib], m1 = m0 + b_nsing[ib];
+      for (uint64_t m = m0; m < m1; ++m) {
+        const double wj = ws[b_ket[m]];
+        if (wj == 0.0) continue;
+        const uint32_t i2 = b_info[m];
+        const int ib_h = (int)(i2 & 63u), ib_p = (int)((i2 >> 6) & 63u);
+        // c = bra-only {2 a_a, 2 a_b + 1}, d = ket-only {2 i_a, 2 i_b + 1}
+        const int c0 = 2 * ia_p, c1 = 2 * ib_p + 1, d0 = 2 * ia_h, d1 = 2 * ib_h + 1;
+        const int I = c0 < c1 ? c0 : c1, J = c0 < c1 ? c1 : c0;
+        const int A = d0 < d1 ? d0 : d1, B = d0 < d1 ? d1 : d0;
+        const uint32_t par = ref_parity_bit(alpha_bra, beta_bra, I < A ? I : A, I < A ? A : I) ^
+                             ref_parity_bit(alpha_bra, beta_bra, J < B ? J : B, J < B ? B : J);
+        const double v = wi * wj;
+        atomicAdd(&acc[ib_h * L + ib_p], par ? -v : v);
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < L * L; t += blockDim.x) {
+      const double v0 = acc[t];
+      if (v0 == 0.0) continue;
+      const int ib_h = t / L, ib_p = t % L;
+      const int c0 = 2 * ia_p, c1 = 2 * ib_p + 1, d0 = 2 * ia_h, d1 = 2 * ib_h + 1;
+      const int I = c0 < c1 ? c0 : c1, J = c0 < c1 ? c1 : c0;
+      const int A = d0 < d1 ? d0 : d1, B = d0 < d1 ? d1 : d0;
+      const double sg = (A > J || B < I) ? -v0 : v0;
+      const int oi = I >> 1, si = I & 1, oa = A >> 1, sa = A & 1, oj = J >> 1, sj = J & 1, ob = B >> 1;
+      if (si == sa) {
+        atomicAdd(&two[(si + 2 * sj) * L4 + oa + (size_t)L * ob + L2 * (oi + (size_t)L * oj)], sg);
+        atomicAdd(&two[(sj + 2 * si) * L4 + ob + (size_t)L * oa + L2 * (oj + (size_t)L * oi)], sg);
+      } else {
+        atomicAdd(&two[(si + 2 * sj) * L4 + oa + (size_t)L * ob + L2 * (oj + (size_t)L * oi)], -sg);
+        atomicAdd(&two[(sj + 2 * si) * L4 + ob + (size_t)L * oa + L2 * (oi + (size_t)L * oj)], -sg);
+      }
+    }
+  }
+}
+
+template <typename T>
+__global__ void transpose_d_kernel(const T* __restrict__ in, size_t rows, size_t cols, T* __restrict__ out) {
+  __shared__ T tile[32][33];
+  const size_t c0 = (size_t)blockIdx.x * 32, r0 = (size_t)blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const size_t r = r0 + k, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) tile[k][threadIdx.x] = in[r * cols + c];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const size_t c = c0 + k, r = r0 + threadIdx.x;
+    if (r < rows && c < cols) out[c * rows + r] = tile[threadIdx.x][k];
+  }
+}
+
+// dE/dh and dE/d(pq|rs) from the RDMs: E = I0 + sum_pq h_pq g_pq
+//   + 1/2 sum_{io,jo,ia,ja} (io ia|jo ja) sum_s G_s[io + L jo + L^2 ia + L^3 ja]
+// (sample main.cc:166-216). One thread per 8-fold class sums its distinct
+// index permutations.
+__global__ void backward_eri_kernel(int L, const double* __restrict__ two, double* __restrict__ g) {
+  const size_t npair = (size_t)L * (L + 1) / 2;
+  const size_t neri = npair * (npair + 1) / 2;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= neri) return;
+  // decode t -> (pq, rs) with pq >= rs, then pq -> (p >= q), rs -> (r >= s)
+  size_t pq = (size_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while (pq * (pq + 1) / 2 > t) --pq;
+  while ((pq + 1) * (pq + 2) / 2 <= t) ++pq;
+  const size_t rs = t - pq * (pq + 1) / 2;
+  auto split = [](size_t x, int& a, int& b) {
+    size_t p = (size_t)((sqrt(8.0 * (double)x + 1.0) - 1.0) * 0.5);
+    while (p * (p + 1) / 2 > x) --p;
+    while ((p + 1) * (p + 2) / 2 <= x) ++p;
+    a = (int)p;
+    b = (int)(x - p * (p + 1) / 2);
+  };
+  int p, q, r, s;
+  split(pq, p, q);
+  split(rs, r, s);
+  const size_t L2 = (size_t)L * L, L3 = L2 * L, L4 = L3 * L;
+  // the 8 index orders (io, ia | jo, ja); keep distinct ones
+  int cand[8][4] = {{p, q, r, s}, {q, p, r, s}, {p, q, s, r}, {q, p, s, r},
+                    {r, s, p, q}, {s, r, p, q}, {r, s, q, p}, {s, r, q, p}};
+  double sum = 0.0;
+  for (int k = 0; k < 8; ++k) {
+    bool dup = false;
+    for (int m = 0; m < k; ++m)
+      if (cand[m][0] == cand[k][0] && cand[m][1] == cand[k][1] && cand[m][2] == cand[k][2] && cand[m][3] == cand[k][3])
+        dup = true;
+    if (dup) continue;
+    const int io = cand[k][0], ia = cand[k][1], jo = cand[k][2], ja = cand[k][3];
+    const size_t idx = (size_t)io + L * (size_t)jo + L2 * ia + L3 * ja;
+    sum += 0.5 * (two[idx] + two[L4 + idx] + two[2 * L4 + idx] + two[3 * L4 + idx]);
+  }
+  g[t] = sum;
+}
+
+struct Scratch {
+  double* p = nullptr;
+  ~Scratch() { cudaFree(p); }
+};
+
+}  // namespace
+
+// Row weights of both orientations: wa[na], wb[nb]; P_a, P_b, X (L*L each).
+static int weights(Ctx* c, const double* dW, double* wa, double* wb, double* Pa, double* Pb, double* X, double* Wt) {
+  const size_t na = c->na, nb = c->nb;
+  row_weight_kernel<<<(unsigned)na, kRowThreads, 0, c->stream>>>(dW, na, nb, c->d_a, c->d_b, c->L, wa, Pa, X);
+  SBDX_LAUNCHED(c);
+  if (wb) {
+    dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((na + 31) / 32));
+    transpose_d_kernel<double><<<grid, dim3(32, 8), 0, c->stream>>>(dW, na, nb, Wt);
+    SBDX_LAUNCHED(c);
+    row_weight_kernel<<<(unsigned)nb, kRowThreads, 0, c->stream>>>(Wt, nb, na, c->d_b, c->d_a, c->L, wb, Pb, nullptr);
+    SBDX_LAUNCHED(c);
+  }
+  return 0;
+}
+
+int rdm_device(Ctx* c, const double* dW, double* d_one, double* d_two) {
+  if (!c->have_conn) { int rc = build_connectivity(c); if (rc) return rc; }
+  int rc = ensure_sigma_scratch(c);
+  if (rc) return rc;
+  const size_t na = c->na, nb = c->nb, L = (size_t)c->L, L2 = L * L, L4 = L2 * L2;
+  Scratch sc;
+  SBDX_CUDA(c, cudaMalloc(&sc.p, sizeof(double) * (na + nb + 3 * L2 + (d_two ? 0 : 4 * L4))));
+  double* wa = sc.p;
+  double* wb = wa + na;
+  double* Pa = wb + nb;
+  double* Pb = Pa + L2;
+  double* X = Pb + L2;
+  double* two = d_two ? d_two : X + L2;  // the 1-RDM alone still needs a 2-RDM sink
+  SBDX_CUDA(c, cudaMemsetAsync(Pa, 0, sizeof(double) * 3 * L2, c->stream));
+  SBDX_CUDA(c, cudaMemsetAsync(d_one, 0, sizeof(double) * 2 * L2, c->stream));
+  SBDX_CUDA(c, cudaMemsetAsync(two, 0, sizeof(double) * 4 * L4, c->stream));
+  double* Wt = reinterpret_cast<double*>(c->d_xt);
+  if ((rc = weights(c, dW, wa, wb, Pa, Pb, X, Wt))) return rc;
+  diag_finalize_kernel<<<(unsigned)((L2 + 255) / 256), 256, 0, c->stream>>>(c->L, Pa, Pb, X, d_one, two);
+  SBDX_LAUNCHED(c);
+  for (int spin = 0; spin < 2; ++spin) {
+    const Conn& cn = c->conn[spin];
+    if (cn.total == 0) continue;
+    const double* Wm = spin == 0 ? dW : Wt;
+    const size_t rows = spin == 0 ? na : nb, cols = spin == 0 ? nb : na;
+    rdm_same_kernel<<<(unsigned)((cn.total + 7) / 8), 256, 0, c->stream>>>(
+        spin, Wm, rows, cols, spin == 0 ? c->d_a : c->d_b, spin == 0 ? c->d_b : c->d_a, cn.off, cn.ket, cn.omask,
+        cn.info, cn.total, c->L, d_one, two);
+    SBDX_LAUNCHED(c);
+  }
+  {
+    const size_t smem = sizeof(double) * (L2 + nb);
+    if (smem > 220 * 1024) { c->err = "rdm: beta dimension too large for the shared-memory row"; return 1; }
+    SBDX_CUDA(c, cudaFuncSetAttribute(rdm_ab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const Conn& ca = c->conn[0];
+    const Conn& cb = c->conn[1];
+    rdm_ab_kernel<<<(unsigned)na, 512, smem, c->stream>>>(dW, nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket, ca.info,
+                                                           cb.off, cb.nsing, cb.ket, cb.info, c->L, two);
+    SBDX_LAUNCHED(c);
+  }
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int occupation_device(Ctx* c, const double* dW, double* d_density) {
+  int rc = ensure_sigma_scratch(c);
+  if (rc) return rc;
+  const size_t na = c->na, nb = c->nb, L = (size_t)c->L, L2 = L * L;
+  Scratch sc;
+  SBDX_CUDA(c, cudaMalloc(&sc.p, sizeof(double) * (na + nb + 3 * L2)));
+  double *wa = sc.p, *wb = wa + na, *Pa = wb + nb, *Pb = Pa + L2, *X = Pb + L2;
+  SBDX_CUDA(c, cudaMemsetAsync(Pa, 0, sizeof(double) * 3 * L2, c->stream));
+  if ((rc = weights(c, dW, wa, wb, Pa, Pb, nullptr, reinterpret_cast<double*>(c->d_xt)))) return rc;
+  // density[2p] = Pa[p][p], density[2p+1] = Pb[p][p]
+  std::vector<double> pa(L2), pb(L2), dens(2 * L);
+  SBDX_CUDA(c, cudaMemcpyAsync(pa.data(), Pa, sizeof(double) * L2, cudaMemcpyDeviceToHost, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(pb.data(), Pb, sizeof(double) * L2, cudaMemcpyDeviceToHost, c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (size_t p = 0; p < L; ++p) { dens[2 * p] = pa[p * L + p]; dens[2 * p + 1] = pb[p * L + p]; }
+  (void)X;
+  SBDX_CUDA(c, cudaMemcpyAsync(d_density, dens.data(), sizeof(double) * 2 * L, cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int alpha_weights_device(Ctx* c, const double* dW, double* d_w) {
+  const size_t L2 = (size_t)c->L * c->L;
+  Scratch sc;
+  SBDX_CUDA(c, cudaMalloc(&sc.p, sizeof(double) * L2));
+  SBDX_CUDA(c, cudaMemsetAsync(sc.p, 0, sizeof(double) * L2, c->stream));
+  return weights(c, dW, d_w, nullptr, sc.p, nullptr, nullptr, nullptr);
+}
+
+int backward_device(Ctx* c, const double* dW, double* dE_dh, double* dE_deri) {
+  // the connectivity is rebuilt from the strings; nothing of the forward solve is kept
+  free_connectivity(c);
+  int rc = build_connectivity(c);
+  if (rc) return rc;
+  const size_t L = (size_t)c->L, L2 = L * L, L4 = L2 * L2;
+  Scratch sc;
+  SBDX_CUDA(c, cudaMalloc(&sc.p, sizeof(double) * (2 * L2 + 4 * L4 + c->neri)));
+  double *one = sc.p, *two = one + 2 * L2, *g = two + 4 * L4;
+  if ((rc = rdm_device(c, dW, one, two))) return rc;
+  backward_eri_kernel<<<(unsigned)((c->neri + 255) / 256), 256, 0, c->stream>>>(c->L, two, g);
+  SBDX_LAUNCHED(c);
+  std::vector<double> h1(2 * L2);
+  SBDX_CUDA(c, cudaMemcpyAsync(h1.data(), one, sizeof(double) * 2 * L2, cudaMemcpyDeviceToHost, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(dE_deri, g, sizeof(double) * c->neri, cudaMemcpyDeviceToHost, c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  // one FCIDUMP entry (p, q) sets h[p][q] and h[q][p] (makeintegrals.h:108-112)
+  for (size_t p = 0; p < L; ++p)
+    for (size_t q = 0; q < L; ++q) {
+      const double gpq = h1[p + L * q] + h1[L2 + p + L * q];
+      const double gqp = h1[q + L * p] + h1[L2 + q + L * p];
+      dE_dh[p * L + q] = p == q ? gpq : gpq + gqp;
+    }
+  return 0;
+}
+
+}  // namespace sbdx

@@ -1,0 +1,145 @@
+// Internal definitions of the sbdx CUDA library (not part of the C-ABI).
+//
+// Data layout in HBM (one context = one Hamiltonian + one alpha x beta basis):
+//   strings      uint64 per spin string, bit p = spatial orbital p (L <= 64)
+//   vectors      D = na*nb elements, alpha-major: index ia*nb + ib, the same
+//                order as the reference (chemistry/tpb/mult.h:487-488)
+//   integrals    h: L*L FP64; eri: 8-fold packed (pq|rs) FP64 (+FP32 copy);
+//                G: (pq|jj) table [npair x L] for the opposite-spin Coulomb
+//                term of single excitations
+//   connectivity per spin: CSR over bra strings, each row = singles (ascending
+//                ket) then doubles (ascending ket), the order of the
+//                reference helper lists (chemistry/tpb/helper.h:132-197,
+//                367-437). Per entry: ket index, the same-spin part of the
+//                matrix element (FP64 and FP32), the opposite-spin sign mask
+//                and a packed info word (see below).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+
+namespace sbdx {
+
+// ---- info word of a connectivity entry --------------------------------------
+//  bit 31      : same-spin sign is negative
+//  bit 30      : single excitation (else double)
+//  singles     : bits 0-5 hole i (occupied in ket), 6-11 particle a (occupied
+//                in bra), 12-23 packed pair index pq(a,i)
+//  doubles     : bits 0-5 i, 6-11 j (ket holes, i<j), 12-17 a, 18-23 b
+//                (bra particles, a<b)
+constexpr uint32_t kInfoNeg = 1u << 31;
+constexpr uint32_t kInfoSingle = 1u << 30;
+
+struct Conn {
+  size_t n = 0;          // number of bra strings
+  size_t total = 0;      // number of entries
+  uint32_t* nsing = nullptr;  // [n]
+  uint32_t* ndoub = nullptr;  // [n]
+  uint64_t* off = nullptr;    // [n+1] row starts
+  uint32_t* ket = nullptr;    // [total]
+  double* val = nullptr;      // [total] same-spin part of H_IJ (FP64)
+  float* val32 = nullptr;     // [total] FP32 copy
+  uint64_t* omask = nullptr;  // [total] opposite-spin parity mask
+  uint32_t* info = nullptr;   // [total]
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // integrals
+  int L = 0;
+  double I0 = 0.0;
+  size_t npair = 0, neri = 0;
+  double* d_h = nullptr;
+  double* d_eri = nullptr;
+  float* d_eri32 = nullptr;
+  double* d_G = nullptr;
+  float* d_G32 = nullptr;
+  std::vector<double> h_h, h_eri;  // host copies (backward / diag host helpers)
+  bool have_integrals = false;
+  // strings
+  size_t na = 0, nb = 0;
+  uint64_t* d_a = nullptr;
+  uint64_t* d_b = nullptr;
+  std::vector<uint64_t> h_a, h_b;
+  bool have_strings = false;
+  // connectivity (0 = alpha, 1 = beta)
+  Conn conn[2];
+  bool have_conn = false;
+  // diagonal
+  double* d_hii = nullptr;
+  bool have_hii = false;
+  // sigma scratch (sized for D): transposed input, FP64 partial outputs
+  void* d_xt = nullptr;     // D elements of the widest type used (8 B)
+  double* d_y = nullptr;    // D FP64: alpha-major partial sigma
+  double* d_yt = nullptr;   // D FP64: beta-major partial sigma
+  void* d_io_in = nullptr;  // D FP64 staging for host-buffer entry points
+  void* d_io_out = nullptr;
+  // reductions
+  double* d_red = nullptr;  // partial sums
+  size_t red_cap = 0;
+  // launch statistics (kernels launched by this context since reset)
+  unsigned long long launches = 0;
+};
+
+// ---- error handling -----------------------------------------------------------
+bool set_cuda_err(Ctx* c, cudaError_t e, const char* what);
+#define SBDX_CUDA(c, call)                                   \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) {                                 \
+      set_cuda_err((c), e_, #call);                          \
+      return 2;                                              \
+    }                                                        \
+  } while (0)
+#define SBDX_LAUNCHED(c)                                      \
+  do {                                                        \
+    ++(c)->launches;                                          \
+    cudaError_t e_ = cudaGetLastError();                      \
+    if (e_ != cudaSuccess) { set_cuda_err((c), e_, "kernel launch"); return 2; } \
+  } while (0)
+
+// ---- device helpers ------------------------------------------------------------
+__host__ __device__ __forceinline__ uint64_t range_mask(int lo, int hi) {
+  // bits [lo, hi) for 0 <= lo <= hi <= 64
+  uint64_t h = hi >= 64 ? ~0ull : ((1ull << hi) - 1ull);
+  uint64_t l = lo >= 64 ? ~0ull : ((1ull << lo) - 1ull);
+  return h & ~l;
+}
+
+__host__ __device__ __forceinline__ int pair_index(int p, int q) {
+  return p > q ? p * (p + 1) / 2 + q : q * (q + 1) / 2 + p;
+}
+
+__host__ __device__ __forceinline__ size_t pair2_index(size_t pq, size_t rs) {
+  return pq > rs ? pq * (pq + 1) / 2 + rs : rs * (rs + 1) / 2 + pq;
+}
+
+__host__ __device__ __forceinline__ size_t eri_index(int p, int q, int r, int s) {
+  return pair2_index((size_t)pair_index(p, q), (size_t)pair_index(r, s));
+}
+
+__device__ __forceinline__ int popc64(uint64_t x) { return __popcll(x); }
+
+// Opposite-spin parity mask of one occupied-range term of the reference
+// parity() (chemistry/basic/determinants.h:228-279) for a same-spin pair of
+// spatial orbitals x < y of spin `spin`: the opposite-spin orbitals whose
+// spin-orbital index lies in [2x+spin, 2y+spin).
+__host__ __device__ __forceinline__ uint64_t other_range(int spin, int x, int y) {
+  return spin == 0 ? range_mask(x, y) : range_mask(x + 1, y + 1);
+}
+
+// ---- internal entry points shared between translation units ------------------
+int build_connectivity(Ctx* c);
+void free_connectivity(Ctx* c);
+int build_g_table(Ctx* c);
+int diag_terms(Ctx* c);
+// sigma: X (na x nb, type by precision: 0 = FP64, 1 = FP32) -> S (same type)
+int sigma_device(Ctx* c, int precision, const void* X, void* S);
+int ensure_sigma_scratch(Ctx* c);
+int ensure_reduction(Ctx* c, size_t n);
+
+}  // namespace sbdx

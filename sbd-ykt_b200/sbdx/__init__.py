@@ -1,0 +1,204 @@
+"""Python binding of the sbdx C-ABI (include/sbdx.h) over the in-tree CUDA
+library libsbdx.so (sm_100a).
+
+This is the thin layer the tests, the benchmark and the autograd check use; the
+drop-in for C++ callers of the reference is the header API in
+cpp/include/sbd/sbd.h. There is no CPU fallback: if the CUDA library is not
+built, importing a Context raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import synth  # noqa: F401
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "libsbdx.so")
+
+SBDX_OK = 0
+SBDX_FP64 = 0
+SBDX_FP32 = 1
+ERRORS = {1: "SBDX_ERR_ARG", 2: "SBDX_ERR_CUDA", 3: "SBDX_ERR_STATE", 4: "SBDX_ERR_NOMEM", 5: "SBDX_ERR_NUMERIC"}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_up = ctypes.POINTER(ctypes.c_uint64)
+
+EXPORTS = [
+    "sbdx_ctx_create", "sbdx_ctx_destroy", "sbdx_last_error", "sbdx_set_stream", "sbdx_launch_count",
+    "sbdx_set_integrals", "sbdx_set_strings", "sbdx_build_connectivity", "sbdx_connectivity_size",
+    "sbdx_get_connectivity", "sbdx_diag_terms", "sbdx_sigma", "sbdx_sigma_device", "sbdx_davidson",
+    "sbdx_rdm", "sbdx_occupation", "sbdx_alpha_weights", "sbdx_energy_backward",
+]
+
+
+class DavidsonParams(ctypes.Structure):
+    _fields_ = [("max_it", ctypes.c_int), ("max_nb", ctypes.c_int), ("eps", ctypes.c_double),
+                ("max_time", ctypes.c_double), ("precision", ctypes.c_int), ("defect_every", ctypes.c_int),
+                ("verbose", ctypes.c_int)]
+
+
+class DavidsonInfo(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("residual", ctypes.c_double), ("n_sigma", ctypes.c_int),
+                ("n_sigma64", ctypes.c_int), ("converged", ctypes.c_int), ("seconds", ctypes.c_double)]
+
+
+class SbdxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libsbdx.so and declare the C-ABI signatures. Raises when missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"sbdx CUDA library not built: {path} (run __graft_entry__.build())")
+    lib = ctypes.CDLL(path)
+    lib.sbdx_last_error.restype = ctypes.c_char_p
+    lib.sbdx_launch_count.restype = ctypes.c_ulonglong
+    lib.sbdx_ctx_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]
+    for name in EXPORTS:
+        fn = getattr(lib, name)
+        if name not in ("sbdx_last_error", "sbdx_launch_count"):
+            fn.restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _u(a):
+    return a.ctypes.data_as(_up)
+
+
+class Context:
+    """One Hamiltonian + one alpha x beta basis on one GPU."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.sbdx_ctx_create(ctypes.byref(h), device)
+        if rc != SBDX_OK:
+            raise SbdxError(rc, "context creation failed (no CUDA device?)")
+        self.h = h
+        self.L = 0
+        self.na = self.nb = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sbdx_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc != SBDX_OK:
+            raise SbdxError(rc, self.lib.sbdx_last_error(self.h).decode())
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.sbdx_launch_count(self.h))
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self.lib.sbdx_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
+
+    def set_integrals(self, L, I0, h, eri):
+        h = np.ascontiguousarray(h, dtype=np.float64).reshape(-1)
+        eri = np.ascontiguousarray(eri, dtype=np.float64)
+        self._check(self.lib.sbdx_set_integrals(self.h, ctypes.c_int(L), ctypes.c_double(I0), _d(h), _d(eri),
+                                                ctypes.c_size_t(len(eri))))
+        self.L = L
+
+    def set_strings(self, alpha, beta):
+        a = np.ascontiguousarray(alpha, dtype=np.uint64)
+        b = np.ascontiguousarray(beta, dtype=np.uint64)
+        self._check(self.lib.sbdx_set_strings(self.h, _u(a), ctypes.c_size_t(len(a)), _u(b), ctypes.c_size_t(len(b))))
+        self.na, self.nb = len(a), len(b)
+
+    def load(self, prob):
+        self.set_integrals(prob.L, prob.I0, prob.h, prob.eri)
+        self.set_strings(prob.alpha, prob.beta)
+        return self
+
+    def build_connectivity(self):
+        self._check(self.lib.sbdx_build_connectivity(self.h))
+
+    def connectivity(self, spin):
+        n = ctypes.c_uint64(0)
+        self._check(self.lib.sbdx_connectivity_size(self.h, ctypes.c_int(spin), ctypes.byref(n)))
+        rows = self.na if spin == 0 else self.nb
+        sl = np.zeros(rows, np.uint64)
+        dl = np.zeros(rows, np.uint64)
+        idx = np.zeros(max(n.value, 1), np.uint64)
+        self._check(self.lib.sbdx_get_connectivity(self.h, ctypes.c_int(spin), _u(sl), _u(dl), _u(idx)))
+        return sl, dl, idx[: n.value]
+
+    def diag_terms(self):
+        out = np.zeros(self.na * self.nb)
+        self._check(self.lib.sbdx_diag_terms(self.h, _d(out)))
+        return out
+
+    def sigma(self, C):
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        S = np.empty_like(C)
+        self._check(self.lib.sbdx_sigma(self.h, _d(C), _d(S)))
+        return S
+
+    def sigma_device(self, precision, c_ptr: int, s_ptr: int):
+        self._check(self.lib.sbdx_sigma_device(self.h, ctypes.c_int(precision), ctypes.c_void_p(c_ptr),
+                                               ctypes.c_void_p(s_ptr)))
+
+    def davidson(self, max_it=1, max_nb=10, eps=1e-4, max_time=86400.0, precision=SBDX_FP64, defect_every=4,
+                 verbose=0, W=None):
+        p = DavidsonParams(max_it, max_nb, eps, max_time, precision, defect_every, verbose)
+        D = self.na * self.nb
+        init = 1 if W is not None else 0
+        W = np.zeros(D) if W is None else np.ascontiguousarray(W, dtype=np.float64).copy()
+        info = DavidsonInfo()
+        self._check(self.lib.sbdx_davidson(self.h, ctypes.byref(p), ctypes.c_int(init), _d(W), ctypes.byref(info)))
+        return info, W
+
+    def rdm(self, W, two=True):
+        L = self.L
+        one = np.zeros(2 * L * L)
+        tw = np.zeros(4 * L ** 4) if two else None
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        self._check(self.lib.sbdx_rdm(self.h, _d(W), _d(one), _d(tw) if two else None))
+        return one, tw
+
+    def occupation(self, W):
+        out = np.zeros(2 * self.L)
+        self._check(self.lib.sbdx_occupation(self.h, _d(np.ascontiguousarray(W, dtype=np.float64)), _d(out)))
+        return out
+
+    def alpha_weights(self, W):
+        out = np.zeros(self.na)
+        self._check(self.lib.sbdx_alpha_weights(self.h, _d(np.ascontiguousarray(W, dtype=np.float64)), _d(out)))
+        return out
+
+    def energy_backward(self, W):
+        L = self.L
+        dh = np.zeros(L * L)
+        deri = np.zeros(synth.neri(L))
+        self._check(self.lib.sbdx_energy_backward(self.h, _d(np.ascontiguousarray(W, dtype=np.float64)), _d(dh), _d(deri)))
+        return dh, deri

@@ -1,0 +1,116 @@
+"""Parity of the CUDA path (through the C-ABI) with the oracle on seeded inputs.
+
+Tolerances: connectivity bit-exact; diagonal and FP64 sigma within 1e-12
+relative to max |value|; FP64 Davidson energy within 1e-9 Ha; RDMs within
+1e-8 max-abs; FP32-storage sigma within 2e-6 relative.
+"""
+import numpy as np
+import pytest
+
+import sbdx
+from sbdx import synth
+from oracle import Port
+
+pytestmark = pytest.mark.gpu
+
+PROBLEMS = [
+    (10, 3, 2, 40, 30, 7),     # unequal alpha/beta electron counts
+    (12, 4, 4, 120, 90, 11),
+    (16, 3, 5, 60, 200, 13),
+    (24, 5, 5, 150, 150, 17),
+    (40, 6, 6, 120, 140, 19),
+]
+
+
+@pytest.fixture(scope="module")
+def port():
+    return Port()
+
+
+def _prob(spec):
+    L, na_el, nb_el, Na, Nb, seed = spec
+    return synth.random_problem(L, na_el, nb_el, Na, Nb, seed=seed)
+
+
+@pytest.mark.parametrize("spec", PROBLEMS)
+def test_connectivity_bit_exact(spec, port):
+    prob = _prob(spec)
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        ctx.build_connectivity()
+        for spin, s in ((0, prob.alpha), (1, prob.beta)):
+            sl, dl, idx = ctx.connectivity(spin)
+            rsl, rdl, ridx = port.connectivity(s)
+            assert np.array_equal(sl, rsl) and np.array_equal(dl, rdl)
+            assert np.array_equal(idx, ridx)
+
+
+@pytest.mark.parametrize("spec", PROBLEMS)
+def test_diag_and_sigma_fp64(spec, port):
+    prob = _prob(spec)
+    rng = np.random.default_rng(1)
+    C = rng.standard_normal(prob.D)
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        hii = ctx.diag_terms()
+        ref_h = port.diag_terms(prob)
+        assert np.abs(hii - ref_h).max() <= 1e-12 * np.abs(ref_h).max()
+        S = ctx.sigma(C)
+        ref = port.sigma(prob, C)
+        assert np.abs(S - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_sigma_fp32_storage(port):
+    torch = pytest.importorskip("torch")
+    prob = _prob(PROBLEMS[3])
+    rng = np.random.default_rng(2)
+    C = rng.standard_normal(prob.D)
+    ref = port.sigma(prob, C.astype(np.float32).astype(np.float64))
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        dC = torch.tensor(C, dtype=torch.float32, device="cuda")
+        dS = torch.empty_like(dC)
+        ctx.sigma_device(sbdx.SBDX_FP32, dC.data_ptr(), dS.data_ptr())
+        torch.cuda.synchronize()
+        S = dS.double().cpu().numpy()
+    assert np.abs(S - ref).max() <= 2e-6 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("spec", PROBLEMS[1:4])
+def test_davidson_fp64_energy(spec, port):
+    prob = _prob(spec)
+    E_ref, W_ref, nsig = port.davidson(prob, max_it=6, max_nb=10, eps=1e-9)
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        info, W = ctx.davidson(max_it=6, max_nb=10, eps=1e-9)
+    assert abs(info.energy - E_ref) < 1e-9
+    assert abs(abs(np.dot(W, W_ref)) - 1.0) < 1e-8
+
+
+@pytest.mark.parametrize("spec", PROBLEMS[1:4])
+def test_davidson_mixed_matches_fp64(spec, port):
+    prob = _prob(spec)
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        i64, W64 = ctx.davidson(max_it=10, max_nb=12, eps=1e-8)
+        i32, W32 = ctx.davidson(max_it=10, max_nb=12, eps=1e-8, precision=sbdx.SBDX_FP32)
+    assert i32.converged == 1
+    assert abs(i32.energy - i64.energy) < 1e-8
+
+
+@pytest.mark.parametrize("spec", PROBLEMS[:4])
+def test_rdm_matches_oracle(spec, port):
+    prob = _prob(spec)
+    E, W, _ = port.davidson(prob, max_it=4, max_nb=10, eps=1e-8)
+    one_r, two_r = port.rdm(prob, W)
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        one, two = ctx.rdm(W)
+        dens = ctx.occupation(W)
+        wa = ctx.alpha_weights(W)
+    assert np.abs(one - one_r).max() < 1e-8
+    assert np.abs(two - two_r).max() < 1e-8
+    assert np.abs(dens - port.occupation(prob, W)).max() < 1e-12
+    Wm = W.reshape(prob.na, prob.nb)
+    assert np.abs(wa - (Wm ** 2).sum(1)).max() < 1e-12
+    assert abs(port.rdm_energy(prob, one, two) - E) < 1e-9
