@@ -303,7 +303,7 @@ int davidson_fp64(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davids
   const int nb = p.max_nb;
   Work wk;
   SBDX_CUDA(c, cudaMalloc(&wk.partial, sizeof(double) * kRedBlocks * (nb + 2)));
-  SBDX_CUDA(c, cudaMalloc(&wk.scal, sizeof(double) * (kDots + nb + 8)));
+  SBDX_CUDA(c, cudaMalloc(&wk.scal, sizeof(double) * (kDots + 2 * nb + 16)));
   SBDX_CUDA(c, cudaMalloc(&wk.u, sizeof(double) * (nb + 1)));
   double *C = nullptr, *HC = nullptr, *R = nullptr;
   SBDX_CUDA(c, cudaMalloc(&C, sizeof(double) * D * nb));
@@ -431,7 +431,7 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
   const int kdef = p.defect_every > 0 ? p.defect_every : 4;
   Work wk;
   SBDX_CUDA(c, cudaMalloc(&wk.partial, sizeof(double) * kRedBlocks * (nb + 3)));
-  SBDX_CUDA(c, cudaMalloc(&wk.scal, sizeof(double) * (kDots + nb + 8)));
+  SBDX_CUDA(c, cudaMalloc(&wk.scal, sizeof(double) * (kDots + 2 * nb + 16)));
   SBDX_CUDA(c, cudaMalloc(&wk.u, sizeof(double) * (nb + 2)));
   float *C = nullptr, *HC = nullptr;
   double *AW = nullptr, *Wn = nullptr, *R = nullptr;
