@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Benchmark of the sbd tpb selected-CI hot path on B200.
+
+Metric (the reference's headline for this path): H*v det-pairs/s, plus the
+Davidson time to a 1e-8 residual in FP64 and in the mixed (FP32-storage,
+FP64 defect-correction) form, on the plain-FP64 drop-in workload: L = 58
+orbitals, 7 alpha + 7 beta electrons, 8000 x 8000 sampled strings (64M
+determinants, 512 MB per FP64 vector), seeded synthetic integrals and strings.
+
+One step = one sigma (S = H C) over the whole workload. `value` times K steps
+with C resident in HBM (CUDA events on the launching stream, max over ranks);
+C (512 MB) is larger than the 126 MB L2, so no flush is needed between steps.
+`e2e` times the same product through the C-ABI call sbdx_sigma with pinned
+host buffers, the host->device copy of C and the device->host copy of S inside
+every step. The roofline uses the algorithmic bytes of one sigma,
+B = P*s_c + D*(2*s_c + s_h) + 4*(connectivity entries) + 8*(na + nb), against
+the measured HBM copy bandwidth. The CPU baseline is the reference's own
+OpenMP mult (compiled in oracle/_ref) on a bounded sample of bra alpha rows.
+
+Multi-GPU: the path is run at MPI world size 1; --gpus N runs N independent
+replicas (one process per GPU) and reports the whole-job det-pairs/s.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "sbd-ykt_b200"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "H·v det-pairs/s and Davidson s to 1e-8 Ha, mixed vs FP64, 1 B200"
+UNIT = "det-pairs/s"
+WORKLOAD = "cfg2"
+WORKLOAD_DESC = "plain FP64 drop-in: L=58, 7a+7b electrons, 8000x8000 strings (64M dets), K=96 integrals"
+REF_CLI = os.path.join(ROOT, "oracle", "_ref", "sbd_ref_cli")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-davidson", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU-baseline sample duration")
+    ap.add_argument("--davidson-tol", type=float, default=1e-8)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.fh = None
+
+    def start(self):
+        try:
+            self.fh = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.flush()
+        with open(self.fh.name) as f:
+            rows = [r.strip().split(", ") for r in f if r.strip()]
+        os.unlink(self.fh.name)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax = max(smax, float(r[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_index(local: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x for x in vis.split(",") if x.strip()]
+        if local < len(ids) and ids[local].strip().isdigit():
+            return int(ids[local])
+    return local
+
+
+def cpu_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_sample(prob, target_s: float, reps: int, threads: int):
+    """Run the reference's own mult on bra alpha rows [0, rows) with rows sized
+    so one run takes about target_s seconds. Returns per-run (seconds, pairs)."""
+    from sbdx import synth
+
+    if not os.path.exists(REF_CLI):
+        return None, "reference CPU build not present (oracle/_ref)"
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "problem.bin")
+        synth.write_problem_bin(path, prob)
+
+        def run(rows, n):
+            out = subprocess.run([REF_CLI, "sigma-sample", path, str(rows), str(n), str(threads)], check=True,
+                                 capture_output=True, text=True).stdout
+            return [json.loads(line) for line in out.splitlines() if line.startswith("{")]
+
+        cal = run(1, 1)[0]
+        rows = max(1, min(prob.na, int(target_s / max(cal["seconds"], 1e-6))))
+        res = run(rows, reps)
+    return res, rows
+
+
+def roofline_bytes(prob, dp, s_c: int, s_h: int = 8) -> float:
+    conn = dp["Sa"] + dp["Da"] + dp["Sb"] + dp["Db"]
+    return dp["offdiag"] * s_c + prob.D * (2 * s_c + s_h) + 4 * conn + 8 * (prob.na + prob.nb)
+
+
+def traffic_per_sigma(workload: str):
+    """DRAM bytes of one sigma from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"sigma_{workload}_dram.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_sigma")
+    return None
+
+
+def load_workload(name: str):
+    """'cfg2' or 'cfg2@0.6' (string counts scaled, for small profiling cases)."""
+    from sbdx import synth
+
+    if "@" in name:
+        base, scale = name.split("@", 1)
+        return synth.config(base, float(scale))
+    return synth.config(name)
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    prob = load_workload(args.workload)
+    threads = cpu_cores()
+    res, rows = reference_sample(prob, target_s=2.0, reps=args.warmup + args.steps, threads=threads)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": rows}))
+        return 0
+    timed = res[args.warmup:]
+    secs = sum(r["seconds"] for r in timed)
+    pairs = sum(r["pairs"] for r in timed)
+    value = pairs / secs
+    sample = f"reference mult (chemistry/tpb/mult.h) on bra alpha rows [0,{rows}) of {prob.na}, all beta rows"
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / len(timed),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": WORKLOAD_DESC, "parallelism": "replicas",
+                   "sample_rows": rows},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    import sbdx
+    from sbdx import synth
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    prob = load_workload(args.workload)
+    ctx = sbdx.Context(local)
+    ctx.load(prob)
+    ctx.build_connectivity()
+    sa, da, _ = ctx.connectivity(0)
+    sb, db, _ = ctx.connectivity(1)
+    dp = synth.det_pairs(sa, da, sb, db)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    D = prob.D
+    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    C = torch.randn(D, dtype=torch.float64, device="cuda", generator=gen)
+    S = torch.empty_like(C)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident FP64 sigma (value) --------------------------------------
+    for _ in range(args.warmup):
+        ctx.sigma_device(sbdx.SBDX_FP64, C.data_ptr(), S.data_ptr())
+    barrier()
+    sampler = ClockSampler(gpu_index(local))
+    sampler.start()
+    launches0 = ctx.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.sigma_device(sbdx.SBDX_FP64, C.data_ptr(), S.data_ptr())
+    e1.record(stream)
+    barrier()
+    clocks = sampler.stop()
+    launches = ctx.launches - launches0
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    value = world * dp["total"] / (ms * 1e-3)
+
+    # ---- per-phase durations (events between the sigma's kernels) ---------------
+    ctx.set_profiling(True)
+    nprof = max(2, min(args.steps, 5))
+    for _ in range(nprof):
+        ctx.sigma_device(sbdx.SBDX_FP64, C.data_ptr(), S.data_ptr())
+    ncalls, phases = ctx.phase_times()
+    ctx.set_profiling(False)
+    phases = {k: v / ncalls for k, v in phases.items()}
+    dominant = max(phases, key=phases.get)
+
+    # ---- FP32-storage sigma ---------------------------------------------------
+    C32, S32 = C.float(), torch.empty(D, dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        ctx.sigma_device(sbdx.SBDX_FP32, C32.data_ptr(), S32.data_ptr())
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.sigma_device(sbdx.SBDX_FP32, C32.data_ptr(), S32.data_ptr())
+    e1.record(stream)
+    barrier()
+    ms32 = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    del C32, S32
+
+    # ---- end to end through the C-ABI with pinned host buffers --------------------
+    hC = C.cpu().pin_memory()
+    hS = torch.empty(D, dtype=torch.float64).pin_memory()
+    ctx.sigma_host_ptr(hC.data_ptr(), hS.data_ptr())
+    barrier()
+    n_e2e = max(2, min(args.steps, 5))
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(n_e2e):
+        ctx.sigma_host_ptr(hC.data_ptr(), hS.data_ptr())
+    e1.record(stream)
+    barrier()
+    wall_e2e = (time.perf_counter() - t0) / n_e2e
+    ms_e2e = max_over_ranks(max(e0.elapsed_time(e1) / n_e2e, 1e3 * wall_e2e))
+    e2e_value = world * dp["total"] / (ms_e2e * 1e-3)
+    del hC, hS
+
+    # ---- Davidson to 1e-8: FP64 vs mixed -------------------------------------------
+    dav = None
+    if not args.no_davidson:
+        del S
+        torch.cuda.empty_cache()
+        i64, _ = ctx.davidson(max_it=100, max_nb=12, eps=args.davidson_tol)
+        i32, _ = ctx.davidson(max_it=100, max_nb=12, eps=args.davidson_tol, precision=sbdx.SBDX_FP32)
+        dav = {"tol": args.davidson_tol, "max_nb": 12,
+               "fp64": {"seconds": i64.seconds, "sigmas": i64.n_sigma, "energy": i64.energy, "residual": i64.residual,
+                        "converged": bool(i64.converged)},
+               "mixed": {"seconds": i32.seconds, "sigmas_fp32": i32.n_sigma, "sigmas_fp64": i32.n_sigma64,
+                         "energy": i32.energy, "residual": i32.residual, "converged": bool(i32.converged),
+                         "dE_vs_fp64": i32.energy - i64.energy},
+               "speedup_mixed_vs_fp64": i64.seconds / i32.seconds if i32.seconds > 0 else None}
+
+    # ---- CPU baseline (reference OpenMP mult, bounded sample, rank 0, N=1) -------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = cpu_cores()
+        res, rows = reference_sample(prob, target_s=args.cpu_seconds, reps=1, threads=threads)
+        if res is not None:
+            r = res[0]
+            cpu = {"value": r["pairs"] / r["seconds"], "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"reference mult (chemistry/tpb/mult.h) on bra alpha rows [0,{rows}) of {prob.na}, "
+                             f"all beta rows: {r['pairs']:.3e} det-pairs in {r['seconds']:.2f} s"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference", "sample": rows}
+
+    hbm, peak_kind = peaks()
+    B = roofline_bytes(prob, dp, 8)
+    achieved = B / (ms * 1e-3) / 1e9
+    traffic = traffic_per_sigma(args.workload)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded integrals and string samples of the stated law)",
+        "config": {"workload": args.workload, "desc": WORKLOAD_DESC, "dets": D, "na": prob.na, "nb": prob.nb,
+                   "norb": prob.L, "det_pairs_per_sigma": dp["total"], "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (C = 512 MB), no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "kernel": "sigma (5 launches: alpha same-spin, transpose, beta same-spin, "
+                     "alpha-beta, combine)", "algorithmic_bytes_per_sigma": B, "peak_kind": peak_kind,
+                     "dominant_phase": dominant, "phase_ms": phases},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * D, "d2h_bytes_per_step": 8 * D,
+                "ms_per_step": ms_e2e},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "fp32_sigma": {"value": world * dp["total"] / (ms32 * 1e-3), "ms_per_step": ms32},
+        "davidson": dav,
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    return run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -53,6 +53,14 @@ const char* sbdx_last_error(const sbdx_ctx* ctx);
 int sbdx_set_stream(sbdx_ctx* ctx, void* cuda_stream);
 /* Kernels launched by this context since creation (instrumentation). */
 unsigned long long sbdx_launch_count(const sbdx_ctx* ctx);
+/* Instrumentation with no reference counterpart (the reference prints wall
+ * timers, sbdiag.h:171-262): when on, every sigma records CUDA events between
+ * its five phases (alpha same-spin, transpose, beta same-spin, alpha-beta,
+ * combine) and accumulates their durations; this adds one host sync per sigma.
+ * sbdx_phase_times copies up to n accumulated milliseconds and returns the
+ * number of sigma calls timed; on == 0 also resets the accumulators. */
+int sbdx_set_profiling(sbdx_ctx* ctx, int on);
+long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n);
 
 /* Integrals. Replaces SetupIntegrals (chemistry/basic/makeintegrals.h:81-126)
  * with exact doubles (the struct path of tpb::diag, sbdiag.h:157). eri_len

@@ -6,8 +6,8 @@
  * Reads a problem written by sbdx.synth.write_problem_bin (header: L, nelec,
  * na, nb as int64; I0; h[L*L]; eri[packed]; alpha strings; beta strings), runs
  * the reference's own sigma (mult.h:376-632) restricted to bra alpha rows
- * [0, rows) `reps` times, and prints one JSON line per run with the seconds and
- * the number of off-diagonal det-pairs evaluated.
+ * [0, rows) `reps` times (helpers built once), and prints one JSON line per
+ * run with the seconds and the number of off-diagonal det-pairs evaluated.
  */
 #include <cstdio>
 #include <cstdint>
@@ -17,10 +17,11 @@
 #include <string>
 #include <omp.h>
 
-extern "C" double ref_sigma_sample(int L, int nelec, double I0, const double* h, const double* eri,
-                                   int bit_length, const uint64_t* astr, size_t na,
-                                   const uint64_t* bstr, size_t nb, const double* C, double* S,
-                                   size_t rows, int threads, double* pairs);
+extern "C" double ref_sigma_sample_multi(int L, int nelec, double I0, const double* h,
+                                         const double* eri, int bit_length, const uint64_t* astr,
+                                         size_t na, const uint64_t* bstr, size_t nb, const double* C,
+                                         double* S, size_t rows, int threads, int reps,
+                                         double* seconds, double* pairs);
 
 int main(int argc, char** argv) {
   if (argc < 6 || std::string(argv[1]) != "sigma-sample") {
@@ -53,13 +54,13 @@ int main(int argc, char** argv) {
     s ^= s << 13; s ^= s >> 7; s ^= s << 17;
     C[i] = (double)(s >> 11) * (1.0 / 9007199254740992.0) - 0.5;
   }
-  for (int r = 0; r < reps; ++r) {
-    double pairs = 0;
-    double t = ref_sigma_sample(L, nelec, I0, h.data(), eri.data(), 20, a.data(), na, b.data(), nb,
-                                C.data(), nullptr, rows, threads, &pairs);
-    std::printf("{\"seconds\": %.6f, \"pairs\": %.0f, \"rows\": %zu, \"threads\": %d}\n", t, pairs,
-                rows, threads);
-    std::fflush(stdout);
-  }
+  std::vector<double> secs(reps > 0 ? reps : 1);
+  double pairs = 0;
+  ref_sigma_sample_multi(L, nelec, I0, h.data(), eri.data(), 20, a.data(), na, b.data(), nb, C.data(),
+                         nullptr, rows, threads, reps, secs.data(), &pairs);
+  for (int r = 0; r < reps; ++r)
+    std::printf("{\"seconds\": %.6f, \"pairs\": %.0f, \"rows\": %zu, \"threads\": %d}\n", secs[r],
+                pairs, rows, threads);
+  std::fflush(stdout);
   return 0;
 }

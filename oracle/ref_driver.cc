@@ -179,12 +179,13 @@ void ref_sigma(int L, int nelec, double I0, const double* h, const double* eri, 
 /* A bounded sample of the reference sigma for CPU-baseline timing: the
  * reference mult over helpers whose bra alpha range is restricted to
  * [0, rows) (ket ranges stay full), exactly the per-task loops of
- * mult.h:453-610. Returns seconds of the mult call; *pairs receives the
- * number of off-diagonal det-pairs the sample evaluated. */
-double ref_sigma_sample(int L, int nelec, double I0, const double* h, const double* eri,
-                        int bit_length, const uint64_t* astr, size_t na, const uint64_t* bstr,
-                        size_t nb, const double* C, double* S, size_t rows, int threads,
-                        double* pairs) {
+ * mult.h:453-610. The helpers are built once; mult runs `reps` times and
+ * seconds[r] receives the duration of run r. *pairs receives the number of
+ * off-diagonal det-pairs one run evaluates. Returns the mean seconds. */
+double ref_sigma_sample_multi(int L, int nelec, double I0, const double* h, const double* eri,
+                              int bit_length, const uint64_t* astr, size_t na, const uint64_t* bstr,
+                              size_t nb, const double* C, double* S, size_t rows, int threads,
+                              int reps, double* seconds, double* pairs) {
   if (threads > 0) omp_set_num_threads(threads);
   Ham H = setup(L, nelec, I0, h, eri);
   size_t bl = (size_t)bit_length;
@@ -213,12 +214,27 @@ double ref_sigma_sample(int L, int nelec, double I0, const double* h, const doub
   // the diagonal loop of mult runs over T.size() == na*nb, so hii and Wb are full size
   std::vector<double> hii(na * nb, 0.0);
   std::vector<double> Wk(C, C + na * nb), Wb(na * nb, 0.0);
-  auto t0 = std::chrono::high_resolution_clock::now();
-  sbd::mult(hii, Wk, Wb, a, b, bl, (size_t)L, 1, 1, helper, H.I0, H.I1, H.I2, 0, 0, 0);
-  auto t1 = std::chrono::high_resolution_clock::now();
+  double total = 0.0;
+  for (int r = 0; r < reps; ++r) {
+    std::fill(Wb.begin(), Wb.end(), 0.0);
+    auto t0 = std::chrono::high_resolution_clock::now();
+    sbd::mult(hii, Wk, Wb, a, b, bl, (size_t)L, 1, 1, helper, H.I0, H.I1, H.I2, 0, 0, 0);
+    auto t1 = std::chrono::high_resolution_clock::now();
+    double dt = std::chrono::duration<double>(t1 - t0).count();
+    if (seconds) seconds[r] = dt;
+    total += dt;
+  }
   if (S) std::memcpy(S, Wb.data(), sizeof(double) * rows * nb);
   sbd::FreeHelpers(helper);
-  return std::chrono::duration<double>(t1 - t0).count();
+  return reps > 0 ? total / reps : 0.0;
+}
+
+double ref_sigma_sample(int L, int nelec, double I0, const double* h, const double* eri,
+                        int bit_length, const uint64_t* astr, size_t na, const uint64_t* bstr,
+                        size_t nb, const double* C, double* S, size_t rows, int threads,
+                        double* pairs) {
+  return ref_sigma_sample_multi(L, nelec, I0, h, eri, bit_length, astr, na, bstr, nb, C, S, rows,
+                                threads, 1, nullptr, pairs);
 }
 
 /* 1-/2-RDM of a given vector W by the reference Correlation

@@ -110,6 +110,8 @@ int sbdx_ctx_destroy(sbdx_ctx* ctx) {
   sbdx::free_vector_state(c);
   cudaFree(c->d_h); cudaFree(c->d_eri); cudaFree(c->d_eri32); cudaFree(c->d_G); cudaFree(c->d_G32);
   cudaFree(c->d_a); cudaFree(c->d_b); cudaFree(c->d_red);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
   delete ctx;
   return SBDX_OK;
 }
@@ -117,6 +119,24 @@ int sbdx_ctx_destroy(sbdx_ctx* ctx) {
 const char* sbdx_last_error(const sbdx_ctx* ctx) { return ctx ? ctx->c.err.c_str() : "null context"; }
 
 unsigned long long sbdx_launch_count(const sbdx_ctx* ctx) { return ctx ? ctx->c.launches : 0ull; }
+
+int sbdx_set_profiling(sbdx_ctx* ctx, int on) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    SBDX_CUDA(c, cudaSetDevice(c->device));
+    if (on && !c->ev[0])
+      for (auto& e : c->ev) SBDX_CUDA(c, cudaEventCreate(&e));
+    for (double& x : c->phase_ms) x = 0.0;
+    c->phase_calls = 0;
+    c->profiling = on != 0;
+    return SBDX_OK;
+  });
+}
+
+long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n) {
+  if (!ctx || !ms) return -1;
+  for (int k = 0; k < n && k < sbdx::kSigmaPhases; ++k) ms[k] = ctx->c.phase_ms[k];
+  return (long long)ctx->c.phase_calls;
+}
 
 int sbdx_set_stream(sbdx_ctx* ctx, void* stream) {
   return sbdx::guarded(ctx, [&](Ctx* c) {

@@ -83,7 +83,14 @@ struct Ctx {
   size_t red_cap = 0;
   // launch statistics (kernels launched by this context since reset)
   unsigned long long launches = 0;
+  // optional per-phase timing of the sigma (CUDA events on the context stream)
+  bool profiling = false;
+  cudaEvent_t ev[8] = {};
+  double phase_ms[8] = {};
+  unsigned long long phase_calls = 0;
 };
+
+constexpr int kSigmaPhases = 5;  // alpha same-spin, transpose, beta same-spin, alpha-beta, combine
 
 // ---- error handling -----------------------------------------------------------
 bool set_cuda_err(Ctx* c, cudaError_t e, const char* what);

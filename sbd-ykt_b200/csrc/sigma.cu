@@ -207,6 +207,10 @@ int run_sigma(Ctx* c, const T* X, T* S) {
   const V* G = std::is_same<T, double>::value ? (const V*)c->d_G : (const V*)c->d_G32;
   const V* eri = std::is_same<T, double>::value ? (const V*)c->d_eri : (const V*)c->d_eri32;
   T* xt = reinterpret_cast<T*>(c->d_xt);
+  auto mark = [&](int k) {
+    if (c->profiling) cudaEventRecord(c->ev[k], c->stream);
+  };
+  mark(0);
   // 1. alpha excitations + diagonal -> Y
   {
     dim3 grid((unsigned)((nb + kSameThreads - 1) / kSameThreads), (unsigned)na);
@@ -214,12 +218,14 @@ int run_sigma(Ctx* c, const T* X, T* S) {
                                                                ca.info, G, c->L, c->d_hii, c->d_y);
     SBDX_LAUNCHED(c);
   }
+  mark(1);
   // 2. C -> C^T
   {
     dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((na + 31) / 32));
     transpose_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(X, na, nb, xt);
     SBDX_LAUNCHED(c);
   }
+  mark(2);
   // 3. beta excitations on C^T -> Yt
   {
     dim3 grid((unsigned)((na + kSameThreads - 1) / kSameThreads), (unsigned)nb);
@@ -227,6 +233,7 @@ int run_sigma(Ctx* c, const T* X, T* S) {
                                                                cb.info, G, c->L, nullptr, c->d_yt);
     SBDX_LAUNCHED(c);
   }
+  mark(3);
   // 4. alpha single x beta single -> Y +=
   {
     const size_t budget = 200 * 1024;
@@ -247,11 +254,22 @@ int run_sigma(Ctx* c, const T* X, T* S) {
                                                               cb.info, eri, (int)c->npair, (int)tile, c->d_y);
     SBDX_LAUNCHED(c);
   }
+  mark(4);
   // 5. S = Y + Yt^T
   {
     dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((na + 31) / 32));
     combine_transpose_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(c->d_y, c->d_yt, na, nb, S);
     SBDX_LAUNCHED(c);
+  }
+  mark(5);
+  if (c->profiling) {
+    SBDX_CUDA(c, cudaEventSynchronize(c->ev[5]));
+    for (int k = 0; k < kSigmaPhases; ++k) {
+      float ms = 0.f;
+      SBDX_CUDA(c, cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]));
+      c->phase_ms[k] += ms;
+    }
+    ++c->phase_calls;
   }
   return 0;
 }

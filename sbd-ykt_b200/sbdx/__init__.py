@@ -30,8 +30,10 @@ EXPORTS = [
     "sbdx_ctx_create", "sbdx_ctx_destroy", "sbdx_last_error", "sbdx_set_stream", "sbdx_launch_count",
     "sbdx_set_integrals", "sbdx_set_strings", "sbdx_build_connectivity", "sbdx_connectivity_size",
     "sbdx_get_connectivity", "sbdx_diag_terms", "sbdx_sigma", "sbdx_sigma_device", "sbdx_davidson",
-    "sbdx_rdm", "sbdx_occupation", "sbdx_alpha_weights", "sbdx_energy_backward",
+    "sbdx_rdm", "sbdx_occupation", "sbdx_alpha_weights", "sbdx_energy_backward", "sbdx_set_profiling",
+    "sbdx_phase_times",
 ]
+PHASES = ["alpha_same_spin", "transpose", "beta_same_spin", "alpha_beta", "combine"]
 
 
 class DavidsonParams(ctypes.Structure):
@@ -67,8 +69,9 @@ def load_library(path: str = LIB_PATH):
     lib.sbdx_ctx_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]
     for name in EXPORTS:
         fn = getattr(lib, name)
-        if name not in ("sbdx_last_error", "sbdx_launch_count"):
+        if name not in ("sbdx_last_error", "sbdx_launch_count", "sbdx_phase_times"):
             fn.restype = ctypes.c_int
+    lib.sbdx_phase_times.restype = ctypes.c_longlong
     _lib = lib
     return lib
 
@@ -119,6 +122,14 @@ class Context:
     def launches(self) -> int:
         return int(self.lib.sbdx_launch_count(self.h))
 
+    def set_profiling(self, on: bool):
+        self._check(self.lib.sbdx_set_profiling(self.h, ctypes.c_int(1 if on else 0)))
+
+    def phase_times(self):
+        ms = np.zeros(len(PHASES))
+        n = self.lib.sbdx_phase_times(self.h, _d(ms), ctypes.c_int(len(PHASES)))
+        return int(n), dict(zip(PHASES, ms.tolist()))
+
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.sbdx_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
 
@@ -163,6 +174,11 @@ class Context:
         S = np.empty_like(C)
         self._check(self.lib.sbdx_sigma(self.h, _d(C), _d(S)))
         return S
+
+    def sigma_host_ptr(self, c_ptr: int, s_ptr: int):
+        """sbdx_sigma on raw host pointers (e.g. pinned torch tensors)."""
+        self._check(self.lib.sbdx_sigma(self.h, ctypes.cast(ctypes.c_void_p(c_ptr), _dp),
+                                        ctypes.cast(ctypes.c_void_p(s_ptr), _dp)))
 
     def sigma_device(self, precision, c_ptr: int, s_ptr: int):
         self._check(self.lib.sbdx_sigma_device(self.h, ctypes.c_int(precision), ctypes.c_void_p(c_ptr),
