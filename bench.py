@@ -232,6 +232,7 @@ def run_ours(args, rank, world, local):
     ctx = sbdx.Context(local)
     ctx.load(prob)
     ctx.build_connectivity()
+    tune = ctx.autotune()
     sa, da, _ = ctx.connectivity(0)
     sb, db, _ = ctx.connectivity(1)
     dp = synth.det_pairs(sa, da, sb, db)
@@ -351,6 +352,7 @@ def run_ours(args, rank, world, local):
         "data": "synthetic (seeded integrals and string samples of the stated law)",
         "config": {"workload": args.workload, "desc": WORKLOAD_DESC, "dets": D, "na": prob.na, "nb": prob.nb,
                    "norb": prob.L, "det_pairs_per_sigma": dp["total"], "parallelism": f"replicas x{world}",
+                   "tuning": {"same_vec": tune[0], "ab_rows": tune[1]},
                    "l2": "inputs larger than L2 (C = 512 MB), no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "kernel": "sigma (5 launches: alpha same-spin, transpose, beta same-spin, "

@@ -61,6 +61,14 @@ unsigned long long sbdx_launch_count(const sbdx_ctx* ctx);
  * number of sigma calls timed; on == 0 also resets the accumulators. */
 int sbdx_set_profiling(sbdx_ctx* ctx, int on);
 long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n);
+/* Launch shapes of the sigma kernels (no reference counterpart): columns per
+ * thread of the same-spin kernel (1, 2 or 4) and ket rows staged per pass of
+ * the alpha-beta kernel (1-4); 0 selects the built-in default. Shapes that do
+ * not fit the problem (alignment, shared memory) are narrowed automatically. */
+int sbdx_set_tuning(sbdx_ctx* ctx, int same_vec, int ab_rows);
+/* Times the candidate shapes on the current problem (a few sigma products on
+ * scratch vectors, FP64 and FP32) and keeps the fastest; writes the choice. */
+int sbdx_autotune(sbdx_ctx* ctx, int* same_vec, int* ab_rows);
 
 /* Integrals. Replaces SetupIntegrals (chemistry/basic/makeintegrals.h:81-126)
  * with exact doubles (the struct path of tpb::diag, sbdiag.h:157). eri_len

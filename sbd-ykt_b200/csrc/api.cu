@@ -27,6 +27,7 @@ int rdm_device(Ctx* c, const double* dW, double* d_one, double* d_two);
 int occupation_device(Ctx* c, const double* dW, double* d_density);
 int alpha_weights_device(Ctx* c, const double* dW, double* d_w);
 int backward_device(Ctx* c, const double* dW, double* dE_dh, double* dE_deri);
+int autotune(Ctx* c);
 
 namespace {
 
@@ -136,6 +137,30 @@ long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n) {
   if (!ctx || !ms) return -1;
   for (int k = 0; k < n && k < sbdx::kSigmaPhases; ++k) ms[k] = ctx->c.phase_ms[k];
   return (long long)ctx->c.phase_calls;
+}
+
+int sbdx_set_tuning(sbdx_ctx* ctx, int same_vec, int ab_rows) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (same_vec < 0 || same_vec > 4 || same_vec == 3 || ab_rows < 0 || ab_rows > 4) {
+      c->err = "set_tuning: same_vec in {0,1,2,4}, ab_rows in [0,4]";
+      return SBDX_ERR_ARG;
+    }
+    c->tune.same_vec = same_vec;
+    c->tune.ab_rows = ab_rows;
+    return SBDX_OK;
+  });
+}
+
+int sbdx_autotune(sbdx_ctx* ctx, int* same_vec, int* ab_rows) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    int rc = sbdx::ready(c, "autotune");
+    if (rc) return rc;
+    rc = sbdx::autotune(c);
+    if (rc) return rc;
+    if (same_vec) *same_vec = c->tune.same_vec;
+    if (ab_rows) *ab_rows = c->tune.ab_rows;
+    return SBDX_OK;
+  });
 }
 
 int sbdx_set_stream(sbdx_ctx* ctx, void* stream) {

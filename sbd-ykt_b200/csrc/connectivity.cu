@@ -19,6 +19,8 @@
 // determinant in O(1) (a popcount) per pair.
 #include "sbdx_internal.cuh"
 
+#include <algorithm>
+
 namespace sbdx {
 
 namespace {
@@ -104,7 +106,8 @@ __global__ void __launch_bounds__(kConnThreads)
 conn_fill_kernel(int spin, const uint64_t* __restrict__ s, size_t n, const uint64_t* __restrict__ off,
                  const uint32_t* __restrict__ nsing, int L, const double* __restrict__ h,
                  const double* __restrict__ eri, uint32_t* __restrict__ ket, double* __restrict__ val,
-                 float* __restrict__ val32, uint64_t* __restrict__ omask, uint32_t* __restrict__ info) {
+                 float* __restrict__ val32, uint64_t* __restrict__ omask, uint32_t* __restrict__ info,
+                 uint64_t* __restrict__ srec) {
   const size_t r = blockIdx.x;
   const uint64_t sr = s[r];
   const uint64_t sbase0 = off[r];
@@ -142,6 +145,12 @@ conn_fill_kernel(int spin, const uint64_t* __restrict__ s, size_t n, const uint6
       val32[pos] = (float)v;
       omask[pos] = m;
       info[pos] = inf;
+      if (is_s) {
+        const uint32_t i = inf & 63u, a = (inf >> 6) & 63u;
+        const uint64_t lo = i < a ? i : a, hi = i < a ? a : i;
+        srec[pos] = (uint64_t)k | ((uint64_t)((inf >> 12) & 0xfffu) << 16) | (lo << 28) | (hi << 34) |
+                    ((uint64_t)(inf >> 31) << 40);
+      }
     }
     __syncthreads();
     if (threadIdx.x == 0) { s_run += st; d_run += dt; }
@@ -152,6 +161,7 @@ conn_fill_kernel(int spin, const uint64_t* __restrict__ s, size_t n, const uint6
 void free_conn(Conn& c) {
   cudaFree(c.nsing); cudaFree(c.ndoub); cudaFree(c.off); cudaFree(c.ket);
   cudaFree(c.val); cudaFree(c.val32); cudaFree(c.omask); cudaFree(c.info);
+  cudaFree(c.srec); cudaFree(c.order);
   c = Conn{};
 }
 
@@ -180,10 +190,18 @@ int build_one(Ctx* c, int spin) {
   SBDX_CUDA(c, cudaMalloc(&cn.val32, sizeof(float) * t));
   SBDX_CUDA(c, cudaMalloc(&cn.omask, sizeof(uint64_t) * t));
   SBDX_CUDA(c, cudaMalloc(&cn.info, sizeof(uint32_t) * t));
+  SBDX_CUDA(c, cudaMalloc(&cn.srec, sizeof(uint64_t) * t));
+  SBDX_CUDA(c, cudaMalloc(&cn.order, sizeof(uint32_t) * n));
   conn_fill_kernel<<<(unsigned)n, kConnThreads, 0, c->stream>>>(spin, s, n, cn.off, cn.nsing, c->L, c->d_h,
                                                                  c->d_eri, cn.ket, cn.val, cn.val32,
-                                                                 cn.omask, cn.info);
+                                                                 cn.omask, cn.info, cn.srec);
   SBDX_LAUNCHED(c);
+  // bra strings ordered by their number of singles (longest first), so the
+  // threads of one warp in the alpha-beta kernels walk lists of similar length
+  std::vector<uint32_t> order(n);
+  for (size_t r = 0; r < n; ++r) order[r] = (uint32_t)r;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return hs[x] > hs[y]; });
+  SBDX_CUDA(c, cudaMemcpyAsync(cn.order, order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream));
   // the host copy of `off` must stay alive until the async copy ran
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
   return 0;

@@ -43,6 +43,11 @@ struct Conn {
   float* val32 = nullptr;     // [total] FP32 copy
   uint64_t* omask = nullptr;  // [total] opposite-spin parity mask
   uint32_t* info = nullptr;   // [total]
+  // compact record of single excitations (doubles slots unused), read by the
+  // alpha-beta kernels: bits 0-15 ket, 16-27 pair index pq(a,i), 28-33 lo,
+  // 34-39 hi (lo = min(i,a), hi = max(i,a)), bit 40 same-spin sign
+  uint64_t* srec = nullptr;   // [total]
+  uint32_t* order = nullptr;  // [n] bra strings sorted by singles count (desc)
 };
 
 struct Ctx {
@@ -83,6 +88,11 @@ struct Ctx {
   size_t red_cap = 0;
   // launch statistics (kernels launched by this context since reset)
   unsigned long long launches = 0;
+  // launch shapes of the sigma kernels (0 = heuristic default)
+  struct {
+    int same_vec = 0;  // columns per thread in the same-spin kernel (1, 2, 4)
+    int ab_rows = 0;   // ket rows staged per pass in the alpha-beta kernel (1-4)
+  } tune;
   // optional per-phase timing of the sigma (CUDA events on the context stream)
   bool profiling = false;
   cudaEvent_t ev[8] = {};
@@ -131,6 +141,17 @@ __host__ __device__ __forceinline__ size_t eri_index(int p, int q, int r, int s)
 
 __device__ __forceinline__ int popc64(uint64_t x) { return __popcll(x); }
 
+// Flip the sign of v when bit 0 of neg is set.
+__device__ __forceinline__ double flip_sign(double v, uint32_t neg) {
+  return __longlong_as_double(__double_as_longlong(v) ^ ((unsigned long long)(neg & 1u) << 63));
+}
+
+// Prefix parity word: bit x = parity of popcount(s & bits[0..x]).
+__device__ __forceinline__ uint64_t prefix_parity(uint64_t s) {
+  s ^= s << 1; s ^= s << 2; s ^= s << 4; s ^= s << 8; s ^= s << 16; s ^= s << 32;
+  return s;
+}
+
 // Opposite-spin parity mask of one occupied-range term of the reference
 // parity() (chemistry/basic/determinants.h:228-279) for a same-spin pair of
 // spatial orbitals x < y of spin `spin`: the opposite-spin orbitals whose
@@ -148,5 +169,6 @@ int diag_terms(Ctx* c);
 int sigma_device(Ctx* c, int precision, const void* X, void* S);
 int ensure_sigma_scratch(Ctx* c);
 int ensure_reduction(Ctx* c, size_t n);
+int autotune(Ctx* c);
 
 }  // namespace sbdx

@@ -27,6 +27,7 @@
 // FP32 mode reads FP32 vectors and FP32 matrix elements.
 #include "sbdx_internal.cuh"
 
+#include <cstdint>
 #include <type_traits>
 
 namespace sbdx {
@@ -34,32 +35,79 @@ namespace sbdx {
 namespace {
 
 constexpr int kSameThreads = 256;
-constexpr int kAbThreads = 512;
 
 template <typename T> struct Prec;
 template <> struct Prec<double> { using V = double; };
 template <> struct Prec<float> { using V = float; };
 
-template <typename T>
+// ---- v2 kernels ----------------------------------------------------------------
+
+template <typename T, int VEC> struct VecIO;
+template <> struct VecIO<double, 1> {
+  static __device__ __forceinline__ void load(const double* p, double* o) { o[0] = __ldg(p); }
+};
+template <> struct VecIO<double, 2> {
+  static __device__ __forceinline__ void load(const double* p, double* o) {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+    o[0] = v.x; o[1] = v.y;
+  }
+};
+template <> struct VecIO<double, 4> {
+  static __device__ __forceinline__ void load(const double* p, double* o) {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 w = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    o[0] = v.x; o[1] = v.y; o[2] = w.x; o[3] = w.y;
+  }
+};
+template <> struct VecIO<float, 1> {
+  static __device__ __forceinline__ void load(const float* p, double* o) { o[0] = (double)__ldg(p); }
+};
+template <> struct VecIO<float, 2> {
+  static __device__ __forceinline__ void load(const float* p, double* o) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    o[0] = v.x; o[1] = v.y;
+  }
+};
+template <> struct VecIO<float, 4> {
+  static __device__ __forceinline__ void load(const float* p, double* o) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+  }
+};
+
+// Same-spin excitations, VEC consecutive columns per thread. Grid: x = bra
+// row (fastest, so the CTAs resident at one time share one column strip of the
+// ket rows and the strip stays in L2), y = column strip of kSameThreads*VEC.
+// Requires ncol % VEC == 0 (the host picks VEC accordingly).
+template <typename T, int VEC>
 __global__ void __launch_bounds__(kSameThreads)
-sigma_same_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __restrict__ other,
-                  const uint64_t* __restrict__ off, const uint32_t* __restrict__ ket,
-                  const typename Prec<T>::V* __restrict__ val, const uint64_t* __restrict__ omask,
-                  const uint32_t* __restrict__ info, const typename Prec<T>::V* __restrict__ G, int L,
-                  const double* __restrict__ hii, double* __restrict__ Y) {
+sigma_same_v2_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __restrict__ other,
+                     const uint64_t* __restrict__ off, const uint32_t* __restrict__ nsing,
+                     const uint32_t* __restrict__ ket, const typename Prec<T>::V* __restrict__ val,
+                     const uint64_t* __restrict__ omask, const uint32_t* __restrict__ info,
+                     const typename Prec<T>::V* __restrict__ G, int L, const double* __restrict__ hii,
+                     double* __restrict__ Y) {
   using V = typename Prec<T>::V;
-  const size_t r = blockIdx.y;
-  const size_t c = (size_t)blockIdx.x * kSameThreads + threadIdx.x;
-  const bool active = c < ncol;
-  const uint64_t o = active ? other[c] : 0ull;
-  double acc = 0.0;
-  if (hii != nullptr && active) acc = hii[r * ncol + c] * (double)X[r * ncol + c];
+  const size_t r = blockIdx.x;
+  const size_t c0 = ((size_t)blockIdx.y * kSameThreads + threadIdx.x) * VEC;
+  const bool active = c0 < ncol;
+  uint64_t o[VEC];
+  double acc[VEC];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) { o[v] = active ? other[c0 + v] : 0ull; acc[v] = 0.0; }
+  if (hii != nullptr && active) {
+    double x[VEC];
+    VecIO<T, VEC>::load(X + r * ncol + c0, x);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = hii[r * ncol + c0 + v] * x[v];
+  }
   __shared__ uint32_t s_ket[kSameThreads], s_info[kSameThreads];
   __shared__ uint64_t s_om[kSameThreads];
   __shared__ V s_val[kSameThreads];
-  const uint64_t beg = off[r], end = off[r + 1];
+  const uint64_t beg = off[r], end = off[r + 1], send = beg + nsing[r];
   for (uint64_t base = beg; base < end; base += kSameThreads) {
     const int cnt = (int)min((uint64_t)kSameThreads, end - base);
+    const int nsb = send > base ? (int)min((uint64_t)cnt, send - base) : 0;
     __syncthreads();
     if ((int)threadIdx.x < cnt) {
       const uint64_t e = base + threadIdx.x;
@@ -69,83 +117,145 @@ sigma_same_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __restri
       s_val[threadIdx.x] = val[e];
     }
     __syncthreads();
-    if (active) {
-#pragma unroll 4
-      for (int e = 0; e < cnt; ++e) {
-        const uint32_t inf = s_info[e];
-        double hv = (double)s_val[e];
-        if (inf & kInfoSingle) {
-          // opposite-spin Coulomb term of OneExcite: sum_{q in other} (ai|qq)
-          const V* g = G + (size_t)((inf >> 12) & 0xfffu) * L;
-          uint64_t bits = o;
-          while (bits) {
-            const int q = __ffsll((long long)bits) - 1;
-            bits &= bits - 1;
-            hv += (double)g[q];
-          }
+    if (!active) continue;
+    // singles: value + opposite-spin Coulomb sum_{q in other} (ai|qq)
+    for (int e = 0; e < nsb; ++e) {
+      const uint32_t inf = s_info[e];
+      const double hv0 = (double)s_val[e];
+      const uint64_t om = s_om[e];
+      const V* g = G + (size_t)((inf >> 12) & 0xfffu) * L;
+      double x[VEC];
+      VecIO<T, VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        double hv = hv0;
+        uint64_t bits = o[v];
+        while (bits) {
+          const int q = __ffsll((long long)bits) - 1;
+          bits &= bits - 1;
+          hv += (double)g[q];
         }
-        const uint32_t neg = ((uint32_t)popc64(o & s_om[e]) ^ (inf >> 31)) & 1u;
-        const double x = (double)X[(size_t)s_ket[e] * ncol + c];
-        acc = fma(neg ? -hv : hv, x, acc);
+        const uint32_t neg = (uint32_t)popc64(o[v] & om) ^ (inf >> 31);
+        acc[v] = fma(flip_sign(hv, neg), x[v], acc[v]);
       }
     }
+    // doubles: one popcount per pair
+#pragma unroll 2
+    for (int e = nsb; e < cnt; ++e) {
+      const uint32_t sgn = s_info[e] >> 31;
+      const double hv = (double)s_val[e];
+      const uint64_t om = s_om[e];
+      double x[VEC];
+      VecIO<T, VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) acc[v] = fma(flip_sign(hv, (uint32_t)popc64(o[v] & om) ^ sgn), x[v], acc[v]);
+    }
   }
-  if (active) Y[r * ncol + c] = acc;
+  if (active) {
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) Y[r * ncol + c0 + v] = acc[v];
+  }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kAbThreads)
-sigma_ab_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restrict__ astr,
-                const uint64_t* __restrict__ bstr, const uint64_t* __restrict__ a_off,
-                const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
-                const uint32_t* __restrict__ a_info, const uint64_t* __restrict__ a_omask,
-                const uint64_t* __restrict__ b_off, const uint32_t* __restrict__ b_nsing,
-                const uint32_t* __restrict__ b_ket, const uint32_t* __restrict__ b_info,
-                const typename Prec<T>::V* __restrict__ eri, int npair, int ib_tile,
-                double* __restrict__ Y) {
+constexpr int kAb2Threads = 1024;
+constexpr int kAb2Slots = 8;  // beta strings per thread per CTA (register accumulators)
+
+// Alpha single x beta single, v2. One CTA per (bra alpha row ia, chunk of the
+// beta order). R ket rows C[ja, :] of the alpha singles of ia and their
+// integral rows (ai|..) are staged in shared memory per pass; each thread owns
+// up to kAb2Slots bra beta strings (taken from the list-length order) and
+// walks their beta-single records once per pass, applying each record to all
+// R staged rows. Sign: alpha factor s_a (-1)^{|beta(ib) & [lo_a,hi_a)|} per
+// (thread, row) and beta factor s_b (-1)^{|alpha(ja) & (lo_b,hi_b]|} per pair,
+// the latter from the prefix-parity word of alpha(ja).
+template <typename T, int R>
+__global__ void __launch_bounds__(kAb2Threads, 1)
+sigma_ab_v2_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restrict__ astr,
+                   const uint64_t* __restrict__ bstr, const uint64_t* __restrict__ a_off,
+                   const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
+                   const uint32_t* __restrict__ a_info, const uint64_t* __restrict__ a_omask,
+                   const uint64_t* __restrict__ b_off, const uint32_t* __restrict__ b_nsing,
+                   const uint64_t* __restrict__ b_rec, const uint32_t* __restrict__ b_order,
+                   const typename Prec<T>::V* __restrict__ eri, int npair, size_t xstride,
+                   double* __restrict__ Y) {
   using V = typename Prec<T>::V;
   extern __shared__ __align__(16) unsigned char smem[];
-  double* acc = reinterpret_cast<double*>(smem);                       // [ib_tile]
-  T* xs = reinterpret_cast<T*>(smem + sizeof(double) * ib_tile);        // [nb]
-  V* erow = reinterpret_cast<V*>(reinterpret_cast<unsigned char*>(xs) +
-                                 ((sizeof(T) * nb + 15) & ~(size_t)15));  // [npair]
+  T* xs = reinterpret_cast<T*>(smem);                                  // [R][xstride]
+  V* erow = reinterpret_cast<V*>(smem + sizeof(T) * xstride * R);     // [R][npair]
+  __shared__ uint64_t s_P[R], s_M[R];
+  __shared__ uint32_t s_sa[R];
   const size_t ia = blockIdx.x;
-  const size_t ib0 = (size_t)blockIdx.y * ib_tile;
-  const size_t ib1 = min(nb, ib0 + (size_t)ib_tile);
-  for (size_t t = threadIdx.x; t < ib1 - ib0; t += kAbThreads) acc[t] = 0.0;
+  const size_t chunk0 = (size_t)blockIdx.y * kAb2Threads * kAb2Slots;
+  double acc[kAb2Slots];
+#pragma unroll
+  for (int k = 0; k < kAb2Slots; ++k) acc[k] = 0.0;
   const uint64_t e0 = a_off[ia];
-  const uint32_t ns = a_nsing[ia];
-  for (uint32_t k = 0; k < ns; ++k) {
-    const uint64_t e = e0 + k;
-    const size_t ja = a_ket[e];
-    const uint32_t inf = a_info[e];
-    const uint64_t ma = a_omask[e];
-    const size_t pq = (inf >> 12) & 0xfffu;
+  const int ns = (int)a_nsing[ia];
+  for (int k0 = 0; k0 < ns; k0 += R) {
+    const int nr = min(R, ns - k0);
     __syncthreads();
-    const T* xrow = X + ja * nb;
-    for (size_t t = threadIdx.x; t < nb; t += kAbThreads) xs[t] = xrow[t];
-    for (int t = threadIdx.x; t < npair; t += kAbThreads) erow[t] = eri[pair2_index(pq, (size_t)t)];
+    if ((int)threadIdx.x < nr) {
+      const uint64_t e = e0 + k0 + threadIdx.x;
+      const uint32_t inf = a_info[e];
+      s_P[threadIdx.x] = prefix_parity(astr[a_ket[e]]);
+      s_M[threadIdx.x] = a_omask[e];
+      s_sa[threadIdx.x] = inf >> 31;
+    }
+    for (int rr = 0; rr < nr; ++rr) {
+      const uint64_t e = e0 + k0 + rr;
+      const T* xrow = X + (size_t)a_ket[e] * nb;
+      T* dst = xs + (size_t)rr * xstride;
+      for (size_t t = threadIdx.x; t < nb; t += kAb2Threads) dst[t] = xrow[t];
+      const size_t pq = (a_info[e] >> 12) & 0xfffu;
+      V* er = erow + (size_t)rr * npair;
+      for (int t = threadIdx.x; t < npair; t += kAb2Threads) er[t] = eri[pair2_index(pq, (size_t)t)];
+    }
     __syncthreads();
-    const uint64_t aj = astr[ja];
-    const uint32_t sa = inf >> 31;
-    for (size_t ib = ib0 + threadIdx.x; ib < ib1; ib += kAbThreads) {
-      const uint32_t base = sa ^ ((uint32_t)popc64(bstr[ib] & ma) & 1u);
+    uint64_t P[R], M[R];
+    uint32_t sa[R];
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+      P[rr] = rr < nr ? s_P[rr] : 0ull;
+      M[rr] = rr < nr ? s_M[rr] : 0ull;
+      sa[rr] = rr < nr ? s_sa[rr] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kAb2Slots; ++k) {
+      const size_t idx = chunk0 + (size_t)k * kAb2Threads + threadIdx.x;
+      if (idx >= nb) continue;
+      const uint32_t ib = b_order[idx];
+      const uint64_t bI = bstr[ib];
+      uint32_t base[R];
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) base[rr] = sa[rr] ^ (uint32_t)popc64(bI & M[rr]);
       const uint64_t m0 = b_off[ib], m1 = m0 + b_nsing[ib];
-      double s = 0.0;
+      double s = acc[k];
       for (uint64_t m = m0; m < m1; ++m) {
-        const uint32_t jb = b_ket[m];
-        const uint32_t i2 = b_info[m];
-        const int j = (int)(i2 & 63u), b = (int)((i2 >> 6) & 63u);
-        const int lo = j < b ? j : b, hi = j < b ? b : j;
-        const uint32_t neg = (base ^ (i2 >> 31) ^ (uint32_t)popc64(aj & range_mask(lo + 1, hi + 1))) & 1u;
-        const double v = (double)erow[(i2 >> 12) & 0xfffu];
-        s = fma(neg ? -v : v, (double)xs[jb], s);
+        const uint64_t rec = __ldg(b_rec + m);
+        const uint32_t jb = (uint32_t)(rec & 0xffffu);
+        const uint32_t pq = (uint32_t)((rec >> 16) & 0xfffu);
+        const uint32_t lo = (uint32_t)((rec >> 28) & 63u), hi = (uint32_t)((rec >> 34) & 63u);
+        const uint32_t sb = (uint32_t)(rec >> 40);
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) {
+          if (rr < nr) {
+            const uint32_t par = base[rr] ^ sb ^ (uint32_t)((P[rr] >> hi) ^ (P[rr] >> lo));
+            const double v = (double)erow[(size_t)rr * npair + pq];
+            s = fma(flip_sign(v, par), (double)xs[(size_t)rr * xstride + jb], s);
+          }
+        }
       }
-      acc[ib - ib0] += s;
+      acc[k] = s;
     }
   }
-  __syncthreads();
-  for (size_t t = threadIdx.x; t < ib1 - ib0; t += kAbThreads) Y[ia * nb + ib0 + t] += acc[t];
+#pragma unroll
+  for (int k = 0; k < kAb2Slots; ++k) {
+    const size_t idx = chunk0 + (size_t)k * kAb2Threads + threadIdx.x;
+    if (idx < nb) {
+      const uint32_t ib = b_order[idx];
+      Y[ia * nb + ib] += acc[k];
+    }
+  }
 }
 
 template <typename T>
@@ -192,8 +302,70 @@ __global__ void g_table_kernel(const double* __restrict__ eri, int L, size_t npa
   G32[t] = (float)v;
 }
 
-size_t ab_smem_bytes(size_t nb, size_t tsz, size_t vsz, size_t npair, size_t tile) {
-  return sizeof(double) * tile + ((tsz * nb + 15) & ~(size_t)15) + vsz * npair;
+template <typename T, int VEC>
+int launch_same(Ctx* c, const T* X, size_t nrow, size_t ncol, const uint64_t* other, const Conn& cn,
+                const typename Prec<T>::V* val, const typename Prec<T>::V* G, const double* hii, double* Y) {
+  dim3 grid((unsigned)nrow, (unsigned)((ncol + (size_t)kSameThreads * VEC - 1) / ((size_t)kSameThreads * VEC)));
+  sigma_same_v2_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, other, cn.off, cn.nsing, cn.ket, val,
+                                                                      cn.omask, cn.info, G, c->L, hii, Y);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+template <typename T>
+int run_same(Ctx* c, const T* X, size_t nrow, size_t ncol, const uint64_t* other, const Conn& cn,
+             const typename Prec<T>::V* val, const typename Prec<T>::V* G, const double* hii, double* Y) {
+  // widest vector that divides the row length and keeps 16-byte alignment
+  constexpr int kWide = sizeof(T) == 8 ? 2 : 4;
+  const bool aligned = (reinterpret_cast<uintptr_t>(X) % 16) == 0;
+  int vec = c->tune.same_vec > 0 ? c->tune.same_vec : kWide;
+  while (vec > 1 && (!aligned || ncol % vec != 0)) vec >>= 1;
+  if (vec >= 4) return launch_same<T, 4>(c, X, nrow, ncol, other, cn, val, G, hii, Y);
+  if (vec == 2) return launch_same<T, 2>(c, X, nrow, ncol, other, cn, val, G, hii, Y);
+  return launch_same<T, 1>(c, X, nrow, ncol, other, cn, val, G, hii, Y);
+}
+
+size_t ab2_smem_bytes(size_t nb, size_t tsz, size_t vsz, size_t npair, int R, size_t* stride) {
+  const size_t per = 16 / tsz;
+  const size_t xstride = (nb + per - 1) / per * per;
+  if (stride) *stride = xstride;
+  return (size_t)R * (tsz * xstride + vsz * npair);
+}
+
+template <typename T, int R>
+int launch_ab2(Ctx* c, const T* X, size_t smem, size_t xstride) {
+  using V = typename Prec<T>::V;
+  const Conn& ca = c->conn[0];
+  const Conn& cb = c->conn[1];
+  const V* eri = std::is_same<T, double>::value ? (const V*)c->d_eri : (const V*)c->d_eri32;
+  SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v2_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t per_cta = (size_t)kAb2Threads * kAb2Slots;
+  dim3 grid((unsigned)c->na, (unsigned)((c->nb + per_cta - 1) / per_cta));
+  sigma_ab_v2_kernel<T, R><<<grid, kAb2Threads, smem, c->stream>>>(
+      X, c->nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket, ca.info, ca.omask, cb.off, cb.nsing, cb.srec, cb.order, eri,
+      (int)c->npair, xstride, c->d_y);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+template <typename T>
+int run_ab(Ctx* c, const T* X) {
+  using V = typename Prec<T>::V;
+  const size_t budget = 220 * 1024;
+  int R = c->tune.ab_rows > 0 ? c->tune.ab_rows : 4;
+  size_t stride = 0, smem = 0;
+  for (; R >= 1; --R) {
+    smem = ab2_smem_bytes(c->nb, sizeof(T), sizeof(V), c->npair, R, &stride);
+    if (smem <= budget) break;
+  }
+  if (R >= 1) {
+    if (R >= 4) return launch_ab2<T, 4>(c, X, smem, stride);
+    if (R == 3) return launch_ab2<T, 3>(c, X, smem, stride);
+    if (R == 2) return launch_ab2<T, 2>(c, X, smem, stride);
+    return launch_ab2<T, 1>(c, X, smem, stride);
+  }
+  c->err = "sigma: beta dimension too large for one shared-memory ket row";
+  return 1;
 }
 
 template <typename T>
@@ -205,19 +377,14 @@ int run_sigma(Ctx* c, const T* X, T* S) {
   const V* valA = std::is_same<T, double>::value ? (const V*)ca.val : (const V*)ca.val32;
   const V* valB = std::is_same<T, double>::value ? (const V*)cb.val : (const V*)cb.val32;
   const V* G = std::is_same<T, double>::value ? (const V*)c->d_G : (const V*)c->d_G32;
-  const V* eri = std::is_same<T, double>::value ? (const V*)c->d_eri : (const V*)c->d_eri32;
   T* xt = reinterpret_cast<T*>(c->d_xt);
   auto mark = [&](int k) {
     if (c->profiling) cudaEventRecord(c->ev[k], c->stream);
   };
+  int rc = 0;
   mark(0);
   // 1. alpha excitations + diagonal -> Y
-  {
-    dim3 grid((unsigned)((nb + kSameThreads - 1) / kSameThreads), (unsigned)na);
-    sigma_same_kernel<T><<<grid, kSameThreads, 0, c->stream>>>(X, nb, c->d_b, ca.off, ca.ket, valA, ca.omask,
-                                                               ca.info, G, c->L, c->d_hii, c->d_y);
-    SBDX_LAUNCHED(c);
-  }
+  if ((rc = run_same<T>(c, X, na, nb, c->d_b, ca, valA, G, c->d_hii, c->d_y))) return rc;
   mark(1);
   // 2. C -> C^T
   {
@@ -227,33 +394,10 @@ int run_sigma(Ctx* c, const T* X, T* S) {
   }
   mark(2);
   // 3. beta excitations on C^T -> Yt
-  {
-    dim3 grid((unsigned)((na + kSameThreads - 1) / kSameThreads), (unsigned)nb);
-    sigma_same_kernel<T><<<grid, kSameThreads, 0, c->stream>>>(xt, na, c->d_a, cb.off, cb.ket, valB, cb.omask,
-                                                               cb.info, G, c->L, nullptr, c->d_yt);
-    SBDX_LAUNCHED(c);
-  }
+  if ((rc = run_same<T>(c, xt, nb, na, c->d_a, cb, valB, G, nullptr, c->d_yt))) return rc;
   mark(3);
   // 4. alpha single x beta single -> Y +=
-  {
-    const size_t budget = 200 * 1024;
-    const size_t fixed = ab_smem_bytes(nb, sizeof(T), sizeof(V), c->npair, 0);
-    if (fixed + 8 * 32 > budget) {
-      c->err = "sigma: beta dimension too large for the shared-memory ket row";
-      return 1;
-    }
-    size_t tile = (budget - fixed) / sizeof(double);
-    if (tile > nb) tile = nb;
-    const unsigned ntile = (unsigned)((nb + tile - 1) / tile);
-    tile = (nb + ntile - 1) / ntile;
-    const size_t smem = ab_smem_bytes(nb, sizeof(T), sizeof(V), c->npair, tile);
-    SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((unsigned)na, ntile);
-    sigma_ab_kernel<T><<<grid, kAbThreads, smem, c->stream>>>(X, nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket,
-                                                              ca.info, ca.omask, cb.off, cb.nsing, cb.ket,
-                                                              cb.info, eri, (int)c->npair, (int)tile, c->d_y);
-    SBDX_LAUNCHED(c);
-  }
+  if ((rc = run_ab<T>(c, X))) return rc;
   mark(4);
   // 5. S = Y + Yt^T
   {
@@ -294,6 +438,63 @@ int ensure_sigma_scratch(Ctx* c) {
   if (!c->d_xt) SBDX_CUDA(c, cudaMalloc(&c->d_xt, sizeof(double) * D));
   if (!c->d_y) SBDX_CUDA(c, cudaMalloc(&c->d_y, sizeof(double) * D));
   if (!c->d_yt) SBDX_CUDA(c, cudaMalloc(&c->d_yt, sizeof(double) * D));
+  return 0;
+}
+
+// Autotuner: time every candidate (same_vec, ab_rows) on the current problem
+// with CUDA events (one warm-up and two timed FP64 sigmas each, on scratch
+// vectors) and keep the fastest. The same-spin and alpha-beta choices are
+// independent kernels, so they are tuned separately through the phase timers.
+int autotune(Ctx* c) {
+  int rc = 0;
+  if (!c->have_conn && (rc = build_connectivity(c))) return rc;
+  if (!c->have_hii && (rc = diag_terms(c))) return rc;
+  if ((rc = ensure_sigma_scratch(c))) return rc;
+  const size_t D = c->na * c->nb;
+  double *X = nullptr, *S = nullptr;
+  SBDX_CUDA(c, cudaMallocAsync(&X, sizeof(double) * D, c->stream));
+  SBDX_CUDA(c, cudaMallocAsync(&S, sizeof(double) * D, c->stream));
+  SBDX_CUDA(c, cudaMemsetAsync(X, 0, sizeof(double) * D, c->stream));
+  const bool prof0 = c->profiling;
+  const auto saved = c->tune;
+  if (!c->ev[0])
+    for (auto& e : c->ev) SBDX_CUDA(c, cudaEventCreate(&e));
+  c->profiling = true;
+  auto measure = [&](int vec, int rows, double* same_ms, double* ab_ms) -> int {
+    c->tune.same_vec = vec;
+    c->tune.ab_rows = rows;
+    int r2 = run_sigma<double>(c, X, S);
+    if (r2) return r2;
+    for (double& x : c->phase_ms) x = 0.0;
+    c->phase_calls = 0;
+    for (int k = 0; k < 2; ++k)
+      if ((r2 = run_sigma<double>(c, X, S))) return r2;
+    *same_ms = c->phase_ms[0] + c->phase_ms[2];
+    *ab_ms = c->phase_ms[3];
+    return 0;
+  };
+  int best_vec = 1, best_rows = 1;
+  double best_same = 1e300, best_ab = 1e300;
+  const int vecs[3] = {1, 2, 4};
+  for (int v : vecs) {
+    double sm = 0, ab = 0;
+    if ((rc = measure(v, 1, &sm, &ab))) break;
+    if (sm < best_same) { best_same = sm; best_vec = v; }
+  }
+  for (int rows = 1; rc == 0 && rows <= 4; ++rows) {
+    double sm = 0, ab = 0;
+    if ((rc = measure(best_vec, rows, &sm, &ab))) break;
+    if (ab < best_ab) { best_ab = ab; best_rows = rows; }
+  }
+  c->profiling = prof0;
+  for (double& x : c->phase_ms) x = 0.0;
+  c->phase_calls = 0;
+  cudaFreeAsync(X, c->stream);
+  cudaFreeAsync(S, c->stream);
+  if (rc) { c->tune = saved; return rc; }
+  c->tune.same_vec = best_vec;
+  c->tune.ab_rows = best_rows;
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
   return 0;
 }
 

@@ -31,7 +31,7 @@ EXPORTS = [
     "sbdx_set_integrals", "sbdx_set_strings", "sbdx_build_connectivity", "sbdx_connectivity_size",
     "sbdx_get_connectivity", "sbdx_diag_terms", "sbdx_sigma", "sbdx_sigma_device", "sbdx_davidson",
     "sbdx_rdm", "sbdx_occupation", "sbdx_alpha_weights", "sbdx_energy_backward", "sbdx_set_profiling",
-    "sbdx_phase_times",
+    "sbdx_phase_times", "sbdx_set_tuning", "sbdx_autotune",
 ]
 PHASES = ["alpha_same_spin", "transpose", "beta_same_spin", "alpha_beta", "combine"]
 
@@ -129,6 +129,14 @@ class Context:
         ms = np.zeros(len(PHASES))
         n = self.lib.sbdx_phase_times(self.h, _d(ms), ctypes.c_int(len(PHASES)))
         return int(n), dict(zip(PHASES, ms.tolist()))
+
+    def set_tuning(self, same_vec: int = 0, ab_rows: int = 0):
+        self._check(self.lib.sbdx_set_tuning(self.h, ctypes.c_int(same_vec), ctypes.c_int(ab_rows)))
+
+    def autotune(self):
+        v, r = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(self.lib.sbdx_autotune(self.h, ctypes.byref(v), ctypes.byref(r)))
+        return v.value, r.value
 
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.sbdx_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
