@@ -61,14 +61,20 @@ unsigned long long sbdx_launch_count(const sbdx_ctx* ctx);
  * number of sigma calls timed; on == 0 also resets the accumulators. */
 int sbdx_set_profiling(sbdx_ctx* ctx, int on);
 long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n);
-/* Launch shapes of the sigma kernels (no reference counterpart): columns per
- * thread of the same-spin kernel (1, 2 or 4) and ket rows staged per pass of
- * the alpha-beta kernel (1-4); 0 selects the built-in default. Shapes that do
- * not fit the problem (alignment, shared memory) are narrowed automatically. */
-int sbdx_set_tuning(sbdx_ctx* ctx, int same_vec, int ab_rows);
-/* Times the candidate shapes on the current problem (a few sigma products on
- * scratch vectors, FP64 and FP32) and keeps the fastest; writes the choice. */
-int sbdx_autotune(sbdx_ctx* ctx, int* same_vec, int* ab_rows);
+/* Launch shapes of the sigma kernels (no reference counterpart), applied to
+ * both precisions; 0 selects the built-in default.
+ *   same_code: 1/2/4/8 = columns per thread of the prefix-parity-table
+ *              same-spin kernel, 11/12/14 = 1/2/4 columns of the popcount one;
+ *   ab_code:   10*variant + staged ket rows (1-4) of the alpha-beta kernel,
+ *              variant 0 = L1 gathers, 1 = shared-memory staging, 2 =
+ *              double-buffered TMA staging, 3 = staging with two 512-thread
+ *              CTAs per SM, 4 = staging with SELL-32 beta records.
+ * Shapes that do not fit the problem (alignment, shared memory) are narrowed. */
+int sbdx_set_tuning(sbdx_ctx* ctx, int same_code, int ab_code);
+/* Autotuner: times the candidate codes on the current problem (a few sigma
+ * products on scratch vectors, for FP64 and for FP32 separately) and keeps the
+ * fastest; writes the FP64 choice. */
+int sbdx_autotune(sbdx_ctx* ctx, int* same_code, int* ab_code);
 
 /* Integrals. Replaces SetupIntegrals (chemistry/basic/makeintegrals.h:81-126)
  * with exact doubles (the struct path of tpb::diag, sbdiag.h:157). eri_len

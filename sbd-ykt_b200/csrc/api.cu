@@ -20,6 +20,17 @@ bool set_cuda_err(Ctx* c, cudaError_t e, const char* what) {
   return false;
 }
 
+int check_device_error(Ctx* c) {
+  int h = 0;
+  SBDX_CUDA(c, cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (h == 0) return 0;
+  SBDX_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+  c->err = "device watchdog: a bulk-copy completion wait timed out in the alpha-beta sigma kernel (code " +
+           std::to_string(h) + ")";
+  return SBDX_ERR_CUDA;
+}
+
 void free_connectivity(Ctx* c);
 int build_g_table(Ctx* c);
 int davidson(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info);
@@ -98,6 +109,10 @@ int sbdx_ctx_create(sbdx_ctx** out, int device) {
   sbdx_ctx* ctx = new (std::nothrow) sbdx_ctx();
   if (!ctx) return SBDX_ERR_NOMEM;
   ctx->c.device = device;
+  if (cudaMalloc(&ctx->c.d_err, sizeof(int)) != cudaSuccess || cudaMemset(ctx->c.d_err, 0, sizeof(int)) != cudaSuccess) {
+    delete ctx;
+    return SBDX_ERR_CUDA;
+  }
   *out = ctx;
   return SBDX_OK;
 }
@@ -110,6 +125,7 @@ int sbdx_ctx_destroy(sbdx_ctx* ctx) {
   sbdx::free_connectivity(c);
   sbdx::free_vector_state(c);
   cudaFree(c->d_h); cudaFree(c->d_eri); cudaFree(c->d_eri32); cudaFree(c->d_G); cudaFree(c->d_G32);
+  cudaFree(c->d_V); cudaFree(c->d_V32); cudaFree(c->d_err);
   cudaFree(c->d_a); cudaFree(c->d_b); cudaFree(c->d_red);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -139,14 +155,20 @@ long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n) {
   return (long long)ctx->c.phase_calls;
 }
 
-int sbdx_set_tuning(sbdx_ctx* ctx, int same_vec, int ab_rows) {
+int sbdx_set_tuning(sbdx_ctx* ctx, int same_code, int ab_code) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {
-    if (same_vec < 0 || same_vec > 4 || same_vec == 3 || ab_rows < 0 || ab_rows > 4) {
-      c->err = "set_tuning: same_vec in {0,1,2,4}, ab_rows in [0,4]";
+    const int v = same_code % 10;
+    const bool same_ok = same_code == 0 || ((same_code < 10 && (v == 1 || v == 2 || v == 4 || v == 8)) ||
+                                            (same_code > 10 && same_code < 20 && (v == 1 || v == 2 || v == 4)));
+    const bool ab_ok = ab_code == 0 || (ab_code > 0 && ab_code < 50 && ab_code % 10 >= 1 && ab_code % 10 <= 4);
+    if (!same_ok || !ab_ok) {
+      c->err = "set_tuning: same_code in {0,1,2,4,8,11,12,14}, ab_code = 10*variant + rows with variant 0-4, rows 1-4";
       return SBDX_ERR_ARG;
     }
-    c->tune.same_vec = same_vec;
-    c->tune.ab_rows = ab_rows;
+    for (auto& t : c->tune) {
+      t.same_code = same_code;
+      t.ab_code = ab_code;
+    }
     return SBDX_OK;
   });
 }
@@ -157,8 +179,8 @@ int sbdx_autotune(sbdx_ctx* ctx, int* same_vec, int* ab_rows) {
     if (rc) return rc;
     rc = sbdx::autotune(c);
     if (rc) return rc;
-    if (same_vec) *same_vec = c->tune.same_vec;
-    if (ab_rows) *ab_rows = c->tune.ab_rows;
+    if (same_vec) *same_vec = c->tune[0].same_code;
+    if (ab_rows) *ab_rows = c->tune[0].ab_code;
     return SBDX_OK;
   });
 }
@@ -304,8 +326,7 @@ int sbdx_sigma(sbdx_ctx* ctx, const double* C, double* S) {
     SBDX_CUDA(c, cudaMemcpyAsync(c->d_io_in, C, sizeof(double) * D, cudaMemcpyHostToDevice, c->stream));
     if ((rc = sbdx::sigma_device(c, SBDX_FP64, c->d_io_in, c->d_io_out))) return rc;
     SBDX_CUDA(c, cudaMemcpyAsync(S, c->d_io_out, sizeof(double) * D, cudaMemcpyDeviceToHost, c->stream));
-    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
-    return SBDX_OK;
+    return sbdx::check_device_error(c);
   });
 }
 
@@ -342,6 +363,7 @@ int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_fr
     sbdx_davidson_info inf{};
     rc = sbdx::davidson(c, *params, dW, inf);
     if (rc) return rc;
+    if ((rc = sbdx::check_device_error(c))) return rc;
     SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * D, cudaMemcpyDeviceToHost, c->stream));
     SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
     if (info) *info = inf;

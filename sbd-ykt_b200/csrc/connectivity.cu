@@ -107,7 +107,7 @@ conn_fill_kernel(int spin, const uint64_t* __restrict__ s, size_t n, const uint6
                  const uint32_t* __restrict__ nsing, int L, const double* __restrict__ h,
                  const double* __restrict__ eri, uint32_t* __restrict__ ket, double* __restrict__ val,
                  float* __restrict__ val32, uint64_t* __restrict__ omask, uint32_t* __restrict__ info,
-                 uint64_t* __restrict__ srec) {
+                 uint64_t* __restrict__ srec, uint32_t* __restrict__ spos) {
   const size_t r = blockIdx.x;
   const uint64_t sr = s[r];
   const uint64_t sbase0 = off[r];
@@ -145,6 +145,24 @@ conn_fill_kernel(int spin, const uint64_t* __restrict__ s, size_t n, const uint6
       val32[pos] = (float)v;
       omask[pos] = m;
       info[pos] = inf;
+      {
+        // boundaries of the opposite-spin ranges: [lo,hi) for alpha
+        // excitations, (lo,hi] = [lo+1,hi+1) for beta excitations
+        uint32_t p[4] = {0, 0, 0, 0};
+        const uint32_t sh = (uint32_t)spin;
+        if (is_s) {
+          const uint32_t i = inf & 63u, a = (inf >> 6) & 63u;
+          p[0] = (i < a ? i : a) + sh;
+          p[1] = (i < a ? a : i) + sh;
+        } else {
+          const uint32_t i = inf & 63u, j = (inf >> 6) & 63u, a = (inf >> 12) & 63u, b = (inf >> 18) & 63u;
+          p[0] = (i < a ? i : a) + sh;
+          p[1] = (i < a ? a : i) + sh;
+          p[2] = (j < b ? j : b) + sh;
+          p[3] = (j < b ? b : j) + sh;
+        }
+        spos[pos] = p[0] | (p[1] << 7) | (p[2] << 14) | (p[3] << 21) | (inf & (kInfoNeg | kInfoSingle));
+      }
       if (is_s) {
         const uint32_t i = inf & 63u, a = (inf >> 6) & 63u;
         const uint64_t lo = i < a ? i : a, hi = i < a ? a : i;
@@ -161,7 +179,8 @@ conn_fill_kernel(int spin, const uint64_t* __restrict__ s, size_t n, const uint6
 void free_conn(Conn& c) {
   cudaFree(c.nsing); cudaFree(c.ndoub); cudaFree(c.off); cudaFree(c.ket);
   cudaFree(c.val); cudaFree(c.val32); cudaFree(c.omask); cudaFree(c.info);
-  cudaFree(c.srec); cudaFree(c.order);
+  cudaFree(c.srec); cudaFree(c.order); cudaFree(c.spos);
+  cudaFree(c.sell); cudaFree(c.soff); cudaFree(c.slen);
   c = Conn{};
 }
 
@@ -191,10 +210,11 @@ int build_one(Ctx* c, int spin) {
   SBDX_CUDA(c, cudaMalloc(&cn.omask, sizeof(uint64_t) * t));
   SBDX_CUDA(c, cudaMalloc(&cn.info, sizeof(uint32_t) * t));
   SBDX_CUDA(c, cudaMalloc(&cn.srec, sizeof(uint64_t) * t));
+  SBDX_CUDA(c, cudaMalloc(&cn.spos, sizeof(uint32_t) * t));
   SBDX_CUDA(c, cudaMalloc(&cn.order, sizeof(uint32_t) * n));
   conn_fill_kernel<<<(unsigned)n, kConnThreads, 0, c->stream>>>(spin, s, n, cn.off, cn.nsing, c->L, c->d_h,
                                                                  c->d_eri, cn.ket, cn.val, cn.val32,
-                                                                 cn.omask, cn.info, cn.srec);
+                                                                 cn.omask, cn.info, cn.srec, cn.spos);
   SBDX_LAUNCHED(c);
   // bra strings ordered by their number of singles (longest first), so the
   // threads of one warp in the alpha-beta kernels walk lists of similar length
@@ -202,6 +222,37 @@ int build_one(Ctx* c, int spin) {
   for (size_t r = 0; r < n; ++r) order[r] = (uint32_t)r;
   std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return hs[x] > hs[y]; });
   SBDX_CUDA(c, cudaMemcpyAsync(cn.order, order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream));
+  // SELL-32 copy of the single-excitation records in list-length order
+  {
+    std::vector<uint64_t> rec(cn.total ? cn.total : 1);
+    if (cn.total)
+      SBDX_CUDA(c, cudaMemcpyAsync(rec.data(), cn.srec, sizeof(uint64_t) * cn.total, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    const size_t ns = (n + 31) / 32;
+    std::vector<uint64_t> soff(ns + 1, 0);
+    std::vector<uint32_t> slen(ns, 0);
+    for (size_t sl = 0; sl < ns; ++sl) {
+      uint32_t mx = 0;
+      for (size_t l = 0; l < 32 && sl * 32 + l < n; ++l) mx = std::max(mx, hs[order[sl * 32 + l]]);
+      slen[sl] = mx;
+      soff[sl + 1] = soff[sl] + 32ull * mx;
+    }
+    const uint64_t kPad = 1ull << 41;
+    std::vector<uint64_t> sell(soff[ns] ? soff[ns] : 1, kPad);
+    for (size_t sl = 0; sl < ns; ++sl)
+      for (size_t l = 0; l < 32 && sl * 32 + l < n; ++l) {
+        const uint32_t r = order[sl * 32 + l];
+        for (uint32_t m = 0; m < hs[r]; ++m) sell[soff[sl] + 32ull * m + l] = rec[off[r] + m];
+      }
+    cn.nslice = ns;
+    SBDX_CUDA(c, cudaMalloc(&cn.sell, sizeof(uint64_t) * sell.size()));
+    SBDX_CUDA(c, cudaMalloc(&cn.soff, sizeof(uint64_t) * (ns + 1)));
+    SBDX_CUDA(c, cudaMalloc(&cn.slen, sizeof(uint32_t) * (ns ? ns : 1)));
+    SBDX_CUDA(c, cudaMemcpyAsync(cn.sell, sell.data(), sizeof(uint64_t) * sell.size(), cudaMemcpyHostToDevice, c->stream));
+    SBDX_CUDA(c, cudaMemcpyAsync(cn.soff, soff.data(), sizeof(uint64_t) * (ns + 1), cudaMemcpyHostToDevice, c->stream));
+    if (ns) SBDX_CUDA(c, cudaMemcpyAsync(cn.slen, slen.data(), sizeof(uint32_t) * ns, cudaMemcpyHostToDevice, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
   // the host copy of `off` must stay alive until the async copy ran
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
   return 0;

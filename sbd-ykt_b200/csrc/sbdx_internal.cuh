@@ -47,7 +47,30 @@ struct Conn {
   // alpha-beta kernels: bits 0-15 ket, 16-27 pair index pq(a,i), 28-33 lo,
   // 34-39 hi (lo = min(i,a), hi = max(i,a)), bit 40 same-spin sign
   uint64_t* srec = nullptr;   // [total]
+  // opposite-spin sign as boundaries of prefix parities: four 7-bit fields
+  // (bits 0-6, 7-13, 14-20, 21-27) hold positions x (0..64) with
+  // sign = xor_k parity(other & bits[0, x_k)); bit 31 is the same-spin sign,
+  // bit 30 marks a single
+  uint32_t* spos = nullptr;   // [total]
   uint32_t* order = nullptr;  // [n] bra strings sorted by singles count (desc)
+  // single-excitation records in SELL-32 layout over `order`: slice s covers
+  // order[32s .. 32s+31]; record m of lane l sits at sell[soff[s] + 32m + l];
+  // shorter lists are padded with records that have bit 41 set (no contribution)
+  uint64_t* sell = nullptr;   // [soff[nslice]]
+  uint64_t* soff = nullptr;   // [nslice + 1]
+  uint32_t* slen = nullptr;   // [nslice] records per lane of each slice
+  size_t nslice = 0;
+};
+
+// Launch shape of the sigma kernels. Codes (also the C-ABI encoding):
+//   same-spin: 1/2/4/8 = columns per thread of the prefix-parity-table kernel,
+//              11/12/14 = 1/2/4 columns of the popcount kernel
+//   alpha-beta: 10*variant + staged rows; variant 1 = shared-memory staging,
+//              2 = double-buffered TMA staging, 3 = staging with 512-thread CTAs,
+//              4 = staging with SELL-32 records, 0 = L1 gathers (rows 1-4)
+struct Tune {
+  int same_code = 0;  // 0 = built-in default for the precision
+  int ab_code = 0;
 };
 
 struct Ctx {
@@ -63,6 +86,10 @@ struct Ctx {
   float* d_eri32 = nullptr;
   double* d_G = nullptr;
   float* d_G32 = nullptr;
+  double* d_V = nullptr;    // unpacked (pq|rs) [npair x vstride], row pq contiguous
+  float* d_V32 = nullptr;   // same in FP32, row stride vstride32
+  size_t vstride = 0, vstride32 = 0;  // row strides padded to 16 bytes
+  int* d_err = nullptr;     // device error word (watchdog timeouts), 0 = ok
   std::vector<double> h_h, h_eri;  // host copies (backward / diag host helpers)
   bool have_integrals = false;
   // strings
@@ -88,11 +115,8 @@ struct Ctx {
   size_t red_cap = 0;
   // launch statistics (kernels launched by this context since reset)
   unsigned long long launches = 0;
-  // launch shapes of the sigma kernels (0 = heuristic default)
-  struct {
-    int same_vec = 0;  // columns per thread in the same-spin kernel (1, 2, 4)
-    int ab_rows = 0;   // ket rows staged per pass in the alpha-beta kernel (1-4)
-  } tune;
+  // launch shapes of the sigma kernels per precision (index 0 = FP64, 1 = FP32)
+  Tune tune[2];
   // optional per-phase timing of the sigma (CUDA events on the context stream)
   bool profiling = false;
   cudaEvent_t ev[8] = {};
@@ -141,9 +165,14 @@ __host__ __device__ __forceinline__ size_t eri_index(int p, int q, int r, int s)
 
 __device__ __forceinline__ int popc64(uint64_t x) { return __popcll(x); }
 
-// Flip the sign of v when bit 0 of neg is set.
+// Flip the sign of v when bit 0 of neg is set (only the high word changes).
 __device__ __forceinline__ double flip_sign(double v, uint32_t neg) {
-  return __longlong_as_double(__double_as_longlong(v) ^ ((unsigned long long)(neg & 1u) << 63));
+  return __hiloint2double(__double2hiint(v) ^ (int)(neg << 31), __double2loint(v));
+}
+
+// Parity bit of popcount(a & b) for 64-bit words split in 32-bit halves.
+__device__ __forceinline__ uint32_t and_parity(uint32_t alo, uint32_t ahi, uint32_t blo, uint32_t bhi) {
+  return (uint32_t)(__popc(alo & blo) + __popc(ahi & bhi));
 }
 
 // Prefix parity word: bit x = parity of popcount(s & bits[0..x]).
@@ -170,5 +199,11 @@ int sigma_device(Ctx* c, int precision, const void* X, void* S);
 int ensure_sigma_scratch(Ctx* c);
 int ensure_reduction(Ctx* c, size_t n);
 int autotune(Ctx* c);
+// Returns 0, or sets c->err and returns SBDX_ERR_CUDA when a kernel recorded a
+// watchdog timeout in the device error word (which is then cleared).
+int check_device_error(Ctx* c);
+
+// Device error codes written to Ctx::d_err.
+constexpr int kErrWatchdogAb = 1;  // alpha-beta kernel: TMA completion wait timed out
 
 }  // namespace sbdx

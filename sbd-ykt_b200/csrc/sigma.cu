@@ -92,9 +92,15 @@ sigma_same_v2_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __res
   const size_t c0 = ((size_t)blockIdx.y * kSameThreads + threadIdx.x) * VEC;
   const bool active = c0 < ncol;
   uint64_t o[VEC];
+  uint32_t olo[VEC], ohi[VEC];
   double acc[VEC];
 #pragma unroll
-  for (int v = 0; v < VEC; ++v) { o[v] = active ? other[c0 + v] : 0ull; acc[v] = 0.0; }
+  for (int v = 0; v < VEC; ++v) {
+    o[v] = active ? other[c0 + v] : 0ull;
+    olo[v] = (uint32_t)o[v];
+    ohi[v] = (uint32_t)(o[v] >> 32);
+    acc[v] = 0.0;
+  }
   if (hii != nullptr && active) {
     double x[VEC];
     VecIO<T, VEC>::load(X + r * ncol + c0, x);
@@ -145,10 +151,131 @@ sigma_same_v2_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __res
       const uint32_t sgn = s_info[e] >> 31;
       const double hv = (double)s_val[e];
       const uint64_t om = s_om[e];
+      const uint32_t omlo = (uint32_t)om, omhi = (uint32_t)(om >> 32);
       double x[VEC];
       VecIO<T, VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
 #pragma unroll
-      for (int v = 0; v < VEC; ++v) acc[v] = fma(flip_sign(hv, (uint32_t)popc64(o[v] & om) ^ sgn), x[v], acc[v]);
+      for (int v = 0; v < VEC; ++v)
+        acc[v] = fma(flip_sign(hv, and_parity(olo[v], ohi[v], omlo, omhi) + sgn), x[v], acc[v]);
+    }
+  }
+  if (active) {
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) Y[r * ncol + c0 + v] = acc[v];
+  }
+}
+
+template <> struct VecIO<double, 8> {
+  static __device__ __forceinline__ void load(const double* p, double* o) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double2 v = __ldg(q + k);
+      o[2 * k] = v.x; o[2 * k + 1] = v.y;
+    }
+  }
+};
+template <> struct VecIO<float, 8> {
+  static __device__ __forceinline__ void load(const float* p, double* o) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    const float4 w = __ldg(reinterpret_cast<const float4*>(p) + 1);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; o[4] = w.x; o[5] = w.y; o[6] = w.z; o[7] = w.w;
+  }
+};
+
+constexpr int kParityRows = 65;  // prefix-parity positions 0..64
+
+// Same-spin excitations, v4. As v2 (VEC consecutive columns per thread,
+// rows-fastest grid) but the opposite-spin sign of an entry is read from a
+// per-thread table of prefix parities in shared memory: tab[x][t] bit v =
+// parity(other[c0+v] & bits[0,x)); an entry's sign for all VEC columns is the
+// xor of four table bytes at its boundary positions (spos). No popcount in
+// the inner loop.
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kSameThreads)
+sigma_same_v4_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __restrict__ other,
+                     const uint64_t* __restrict__ off, const uint32_t* __restrict__ nsing,
+                     const uint32_t* __restrict__ ket, const typename Prec<T>::V* __restrict__ val,
+                     const uint32_t* __restrict__ spos, const uint32_t* __restrict__ info,
+                     const typename Prec<T>::V* __restrict__ G, int L, const double* __restrict__ hii,
+                     double* __restrict__ Y) {
+  static_assert(VEC <= 8, "one byte of parity bits per thread");
+  using V = typename Prec<T>::V;
+  __shared__ uint8_t tab[kParityRows][kSameThreads];
+  __shared__ uint32_t s_ket[kSameThreads], s_pos[kSameThreads];
+  __shared__ V s_val[kSameThreads];
+  const size_t r = blockIdx.x;
+  const size_t c0 = ((size_t)blockIdx.y * kSameThreads + threadIdx.x) * VEC;
+  const bool active = c0 < ncol;
+  uint64_t o[VEC];
+  double acc[VEC];
+  {
+    uint64_t P[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      o[v] = active ? other[c0 + v] : 0ull;
+      P[v] = prefix_parity(o[v]);
+      acc[v] = 0.0;
+    }
+    tab[0][threadIdx.x] = 0;
+    for (int x = 1; x < kParityRows; ++x) {
+      uint32_t b = 0;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) b |= (uint32_t)((P[v] >> (x - 1)) & 1ull) << v;
+      tab[x][threadIdx.x] = (uint8_t)b;
+    }
+  }
+  if (hii != nullptr && active) {
+    double x[VEC];
+    VecIO<T, VEC>::load(X + r * ncol + c0, x);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = hii[r * ncol + c0 + v] * x[v];
+  }
+  const uint64_t beg = off[r], end = off[r + 1], send = beg + nsing[r];
+  const unsigned t = threadIdx.x;
+  for (uint64_t base = beg; base < end; base += kSameThreads) {
+    const int cnt = (int)min((uint64_t)kSameThreads, end - base);
+    const int nsb = send > base ? (int)min((uint64_t)cnt, send - base) : 0;
+    __syncthreads();
+    if ((int)t < cnt) {
+      const uint64_t e = base + t;
+      s_ket[t] = ket[e];
+      s_pos[t] = spos[e];
+      s_val[t] = val[e];
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (int e = 0; e < nsb; ++e) {
+      const uint32_t ps = s_pos[e];
+      const uint32_t neg = (uint32_t)tab[ps & 127u][t] ^ (uint32_t)tab[(ps >> 7) & 127u][t] ^ ((ps >> 31) ? 0xffu : 0u);
+      const uint32_t inf = info[base + e];
+      const V* g = G + (size_t)((inf >> 12) & 0xfffu) * L;
+      const double hv0 = (double)s_val[e];
+      double x[VEC];
+      VecIO<T, VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        double hv = hv0;
+        uint64_t bits = o[v];
+        while (bits) {
+          const int q = __ffsll((long long)bits) - 1;
+          bits &= bits - 1;
+          hv += (double)g[q];
+        }
+        acc[v] = fma(flip_sign(hv, neg >> v), x[v], acc[v]);
+      }
+    }
+#pragma unroll 2
+    for (int e = nsb; e < cnt; ++e) {
+      const uint32_t ps = s_pos[e];
+      const uint32_t neg = (uint32_t)tab[ps & 127u][t] ^ (uint32_t)tab[(ps >> 7) & 127u][t] ^
+                           (uint32_t)tab[(ps >> 14) & 127u][t] ^ (uint32_t)tab[(ps >> 21) & 127u][t] ^
+                           ((ps >> 31) ? 0xffu : 0u);
+      const double hv = (double)s_val[e];
+      double x[VEC];
+      VecIO<T, VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) acc[v] = fma(flip_sign(hv, neg >> v), x[v], acc[v]);
     }
   }
   if (active) {
@@ -160,6 +287,14 @@ sigma_same_v2_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __res
 constexpr int kAb2Threads = 1024;
 constexpr int kAb2Slots = 8;  // beta strings per thread per CTA (register accumulators)
 
+// Slot k of thread t takes position k*nthreads + t of the list-length order on
+// even k and k*nthreads + (nthreads-1-t) on odd k, so every thread's lists add
+// up to about the same length (a plain stride gives warp 0 the longest list of
+// every slot).
+__device__ __forceinline__ size_t snake_index(size_t chunk0, int k, int nthreads, int t) {
+  return chunk0 + (size_t)k * nthreads + (size_t)((k & 1) ? (nthreads - 1 - t) : t);
+}
+
 // Alpha single x beta single, v2. One CTA per (bra alpha row ia, chunk of the
 // beta order). R ket rows C[ja, :] of the alpha singles of ia and their
 // integral rows (ai|..) are staged in shared memory per pass; each thread owns
@@ -168,8 +303,8 @@ constexpr int kAb2Slots = 8;  // beta strings per thread per CTA (register accum
 // R staged rows. Sign: alpha factor s_a (-1)^{|beta(ib) & [lo_a,hi_a)|} per
 // (thread, row) and beta factor s_b (-1)^{|alpha(ja) & (lo_b,hi_b]|} per pair,
 // the latter from the prefix-parity word of alpha(ja).
-template <typename T, int R>
-__global__ void __launch_bounds__(kAb2Threads, 1)
+template <typename T, int R, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT)
 sigma_ab_v2_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restrict__ astr,
                    const uint64_t* __restrict__ bstr, const uint64_t* __restrict__ a_off,
                    const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
@@ -179,16 +314,17 @@ sigma_ab_v2_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
                    const typename Prec<T>::V* __restrict__ eri, int npair, size_t xstride,
                    double* __restrict__ Y) {
   using V = typename Prec<T>::V;
+  constexpr int kSlots = 8192 / NT;
   extern __shared__ __align__(16) unsigned char smem[];
   T* xs = reinterpret_cast<T*>(smem);                                  // [R][xstride]
   V* erow = reinterpret_cast<V*>(smem + sizeof(T) * xstride * R);     // [R][npair]
   __shared__ uint64_t s_P[R], s_M[R];
   __shared__ uint32_t s_sa[R];
   const size_t ia = blockIdx.x;
-  const size_t chunk0 = (size_t)blockIdx.y * kAb2Threads * kAb2Slots;
-  double acc[kAb2Slots];
+  const size_t chunk0 = (size_t)blockIdx.y * NT * kSlots;
+  double acc[kSlots];
 #pragma unroll
-  for (int k = 0; k < kAb2Slots; ++k) acc[k] = 0.0;
+  for (int k = 0; k < kSlots; ++k) acc[k] = 0.0;
   const uint64_t e0 = a_off[ia];
   const int ns = (int)a_nsing[ia];
   for (int k0 = 0; k0 < ns; k0 += R) {
@@ -205,10 +341,10 @@ sigma_ab_v2_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
       const uint64_t e = e0 + k0 + rr;
       const T* xrow = X + (size_t)a_ket[e] * nb;
       T* dst = xs + (size_t)rr * xstride;
-      for (size_t t = threadIdx.x; t < nb; t += kAb2Threads) dst[t] = xrow[t];
+      for (size_t t = threadIdx.x; t < nb; t += NT) dst[t] = xrow[t];
       const size_t pq = (a_info[e] >> 12) & 0xfffu;
       V* er = erow + (size_t)rr * npair;
-      for (int t = threadIdx.x; t < npair; t += kAb2Threads) er[t] = eri[pair2_index(pq, (size_t)t)];
+      for (int t = threadIdx.x; t < npair; t += NT) er[t] = eri[pair2_index(pq, (size_t)t)];
     }
     __syncthreads();
     uint64_t P[R], M[R];
@@ -220,8 +356,8 @@ sigma_ab_v2_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
       sa[rr] = rr < nr ? s_sa[rr] : 0u;
     }
 #pragma unroll
-    for (int k = 0; k < kAb2Slots; ++k) {
-      const size_t idx = chunk0 + (size_t)k * kAb2Threads + threadIdx.x;
+    for (int k = 0; k < kSlots; ++k) {
+      const size_t idx = snake_index(chunk0, k, NT, threadIdx.x);
       if (idx >= nb) continue;
       const uint32_t ib = b_order[idx];
       const uint64_t bI = bstr[ib];
@@ -230,8 +366,10 @@ sigma_ab_v2_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
       for (int rr = 0; rr < R; ++rr) base[rr] = sa[rr] ^ (uint32_t)popc64(bI & M[rr]);
       const uint64_t m0 = b_off[ib], m1 = m0 + b_nsing[ib];
       double s = acc[k];
+      uint64_t next = m0 < m1 ? __ldg(b_rec + m0) : 0ull;
       for (uint64_t m = m0; m < m1; ++m) {
-        const uint64_t rec = __ldg(b_rec + m);
+        const uint64_t rec = next;
+        if (m + 1 < m1) next = __ldg(b_rec + m + 1);
         const uint32_t jb = (uint32_t)(rec & 0xffffu);
         const uint32_t pq = (uint32_t)((rec >> 16) & 0xfffu);
         const uint32_t lo = (uint32_t)((rec >> 28) & 63u), hi = (uint32_t)((rec >> 34) & 63u);
@@ -249,13 +387,385 @@ sigma_ab_v2_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
     }
   }
 #pragma unroll
-  for (int k = 0; k < kAb2Slots; ++k) {
-    const size_t idx = chunk0 + (size_t)k * kAb2Threads + threadIdx.x;
+  for (int k = 0; k < kSlots; ++k) {
+    const size_t idx = snake_index(chunk0, k, NT, threadIdx.x);
     if (idx < nb) {
       const uint32_t ib = b_order[idx];
       Y[ia * nb + ib] += acc[k];
     }
   }
+}
+
+// Alpha single x beta single, v5: the v2 staging scheme with the beta-single
+// records read in SELL-32 layout. Warp w of the CTA owns slices w, 63-w,
+// 64+w, ... (a snake over the length-sorted slices, so warps get equal work);
+// lane l of a slice owns bra beta string order[32s+l]. Every record load of a
+// warp is one contiguous 256-byte read; padded records contribute zero.
+template <typename T, int R, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT)
+sigma_ab_v5_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restrict__ astr,
+                   const uint64_t* __restrict__ bstr, const uint64_t* __restrict__ a_off,
+                   const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
+                   const uint32_t* __restrict__ a_info, const uint64_t* __restrict__ a_omask,
+                   const uint64_t* __restrict__ sell, const uint64_t* __restrict__ soff,
+                   const uint32_t* __restrict__ slen, size_t nslice, const uint32_t* __restrict__ b_order,
+                   const typename Prec<T>::V* __restrict__ eri, int npair, size_t xstride,
+                   double* __restrict__ Y) {
+  using V = typename Prec<T>::V;
+  constexpr int kWarps = NT / 32;
+  constexpr int kSlices = 8192 / NT;  // slices per warp per CTA (32*kWarps*kSlices = 8192 strings)
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* xs = reinterpret_cast<T*>(smem);
+  V* erow = reinterpret_cast<V*>(smem + sizeof(T) * xstride * R);
+  __shared__ uint64_t s_P[R], s_M[R];
+  __shared__ uint32_t s_sa[R];
+  const size_t ia = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t slice0 = (size_t)blockIdx.y * kWarps * kSlices;
+  auto slice_of = [&](int k) -> size_t {
+    return slice0 + (size_t)k * kWarps + ((k & 1) ? (kWarps - 1 - warp) : warp);
+  };
+  uint64_t bI[kSlices];
+  double acc[kSlices];
+#pragma unroll
+  for (int k = 0; k < kSlices; ++k) {
+    const size_t sl = slice_of(k);
+    const size_t pos = sl * 32 + lane;
+    bI[k] = (sl < nslice && pos < nb) ? bstr[b_order[pos]] : 0ull;
+    acc[k] = 0.0;
+  }
+  const uint64_t e0 = a_off[ia];
+  const int ns = (int)a_nsing[ia];
+  for (int k0 = 0; k0 < ns; k0 += R) {
+    const int nr = min(R, ns - k0);
+    __syncthreads();
+    if ((int)threadIdx.x < nr) {
+      const uint64_t e = e0 + k0 + threadIdx.x;
+      s_P[threadIdx.x] = prefix_parity(astr[a_ket[e]]);
+      s_M[threadIdx.x] = a_omask[e];
+      s_sa[threadIdx.x] = a_info[e] >> 31;
+    }
+    for (int rr = 0; rr < nr; ++rr) {
+      const uint64_t e = e0 + k0 + rr;
+      const T* xrow = X + (size_t)a_ket[e] * nb;
+      T* dst = xs + (size_t)rr * xstride;
+      for (size_t t = threadIdx.x; t < nb; t += NT) dst[t] = xrow[t];
+      const size_t pq = (a_info[e] >> 12) & 0xfffu;
+      V* er = erow + (size_t)rr * npair;
+      for (int t = threadIdx.x; t < npair; t += NT) er[t] = eri[pair2_index(pq, (size_t)t)];
+    }
+    __syncthreads();
+    uint64_t P[R], M[R];
+    uint32_t sa[R];
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+      P[rr] = rr < nr ? s_P[rr] : 0ull;
+      M[rr] = rr < nr ? s_M[rr] : 0ull;
+      sa[rr] = rr < nr ? s_sa[rr] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kSlices; ++k) {
+      const size_t sl = slice_of(k);
+      if (sl >= nslice) continue;
+      uint32_t base[R];
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) base[rr] = sa[rr] ^ (uint32_t)popc64(bI[k] & M[rr]);
+      const uint32_t len = slen[sl];
+      const uint64_t* rp = sell + soff[sl] + lane;
+      double s = acc[k];
+      uint64_t next = len ? __ldg(rp) : 0ull;
+      for (uint32_t m = 0; m < len; ++m) {
+        const uint64_t rec = next;
+        if (m + 1 < len) next = __ldg(rp + 32ull * (m + 1));
+        const uint32_t jb = (uint32_t)(rec & 0xffffu);
+        const uint32_t pq = (uint32_t)((rec >> 16) & 0xfffu);
+        const uint32_t lo = (uint32_t)((rec >> 28) & 63u), hi = (uint32_t)((rec >> 34) & 63u);
+        const uint32_t sb = (uint32_t)(rec >> 40);
+        const bool pad = (rec >> 41) & 1ull;
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) {
+          if (rr < nr) {
+            const uint32_t par = base[rr] ^ sb ^ (uint32_t)((P[rr] >> hi) ^ (P[rr] >> lo));
+            const double v = pad ? 0.0 : (double)erow[(size_t)rr * npair + pq];
+            s = fma(flip_sign(v, par), (double)xs[(size_t)rr * xstride + jb], s);
+          }
+        }
+      }
+      acc[k] = s;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kSlices; ++k) {
+    const size_t sl = slice_of(k);
+    const size_t pos = sl * 32 + lane;
+    if (sl < nslice && pos < nb) Y[ia * nb + b_order[pos]] += acc[k];
+  }
+}
+
+// ---- double-buffered TMA staging ---------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait: gives up when the phase has not completed after `limit_ns`
+// nanoseconds of the global timer (or 2^26 polls, whichever comes first).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < (1u << 26); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 255u && global_ns() - t0 > limit_ns) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+constexpr uint64_t kWaitLimit = 2000000000ull;  // 2 s
+
+// Alpha single x beta single, v4: as v2, with the R ket rows and integral
+// rows of the next group of alpha singles loaded by TMA (cp.async.bulk, one
+// issuing thread) into the second of two shared-memory buffers while the
+// current group is computed. Requires 16-byte aligned rows (nb*sizeof(T) % 16
+// == 0 and a 16-byte aligned X); the host checks this.
+template <typename T, int R>
+__global__ void __launch_bounds__(kAb2Threads, 1)
+sigma_ab_v4_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restrict__ astr,
+                   const uint64_t* __restrict__ bstr, const uint64_t* __restrict__ a_off,
+                   const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
+                   const uint32_t* __restrict__ a_info, const uint64_t* __restrict__ a_omask,
+                   const uint64_t* __restrict__ b_off, const uint32_t* __restrict__ b_nsing,
+                   const uint64_t* __restrict__ b_rec, const uint32_t* __restrict__ b_order,
+                   const typename Prec<T>::V* __restrict__ Vtab, size_t vstride, int* __restrict__ err,
+                   double* __restrict__ Y) {
+  using V = typename Prec<T>::V;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const size_t xbytes = sizeof(T) * nb, vbytes = sizeof(V) * vstride;
+  const size_t bufbytes = (size_t)R * (xbytes + vbytes);
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int s_abort;
+  const size_t ia = blockIdx.x;
+  const size_t chunk0 = (size_t)blockIdx.y * kAb2Threads * kAb2Slots;
+  const uint64_t e0 = a_off[ia];
+  const int ns = (int)a_nsing[ia];
+  const int ngroups = (ns + R - 1) / R;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_abort = 0;
+  }
+  __syncthreads();
+  auto issue = [&](int g) {  // thread 0 only
+    const int b = g & 1;
+    const int nr = min(R, ns - g * R);
+    unsigned char* buf = smem + (size_t)b * bufbytes;
+    mbar_arrive_expect_tx(&bar[b], (uint32_t)(nr * (xbytes + vbytes)));
+    for (int rr = 0; rr < nr; ++rr) {
+      const uint64_t e = e0 + (uint64_t)g * R + rr;
+      const size_t ja = a_ket[e];
+      const size_t pq = (a_info[e] >> 12) & 0xfffu;
+      tma_load_1d(buf + (size_t)rr * xbytes, X + ja * nb, (uint32_t)xbytes, &bar[b]);
+      tma_load_1d(buf + (size_t)R * xbytes + (size_t)rr * vbytes, Vtab + pq * vstride, (uint32_t)vbytes, &bar[b]);
+    }
+  };
+  if (threadIdx.x == 0) {
+    if (ngroups > 0) issue(0);
+    if (ngroups > 1) issue(1);
+  }
+  double acc[kAb2Slots];
+#pragma unroll
+  for (int k = 0; k < kAb2Slots; ++k) acc[k] = 0.0;
+  for (int g = 0; g < ngroups; ++g) {
+    const int b = g & 1;
+    const int nr = min(R, ns - g * R);
+    if (!mbar_wait_bounded(&bar[b], (uint32_t)((g >> 1) & 1), kWaitLimit)) {
+      atomicExch(err, kErrWatchdogAb);
+      s_abort = 1;
+    }
+    __syncthreads();
+    if (s_abort) break;
+    const T* xs = reinterpret_cast<const T*>(smem + (size_t)b * bufbytes);
+    const V* erow = reinterpret_cast<const V*>(smem + (size_t)b * bufbytes + (size_t)R * xbytes);
+    uint64_t P[R], M[R];
+    uint32_t sa[R];
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+      const uint64_t e = e0 + (uint64_t)g * R + (rr < nr ? rr : 0);
+      const uint32_t inf = __ldg(a_info + e);
+      P[rr] = prefix_parity(__ldg(astr + __ldg(a_ket + e)));
+      M[rr] = __ldg(a_omask + e);
+      sa[rr] = inf >> 31;
+    }
+#pragma unroll
+    for (int k = 0; k < kAb2Slots; ++k) {
+      const size_t idx = snake_index(chunk0, k, kAb2Threads, threadIdx.x);
+      if (idx >= nb) continue;
+      const uint32_t ib = __ldg(b_order + idx);
+      const uint64_t bI = __ldg(bstr + ib);
+      uint32_t base[R];
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) base[rr] = sa[rr] ^ (uint32_t)popc64(bI & M[rr]);
+      const uint64_t m0 = __ldg(b_off + ib), m1 = m0 + __ldg(b_nsing + ib);
+      double s = acc[k];
+      uint64_t next = m0 < m1 ? __ldg(b_rec + m0) : 0ull;
+      for (uint64_t m = m0; m < m1; ++m) {
+        const uint64_t rec = next;
+        if (m + 1 < m1) next = __ldg(b_rec + m + 1);
+        const uint32_t jb = (uint32_t)(rec & 0xffffu);
+        const uint32_t pq = (uint32_t)((rec >> 16) & 0xfffu);
+        const uint32_t lo = (uint32_t)((rec >> 28) & 63u), hi = (uint32_t)((rec >> 34) & 63u);
+        const uint32_t sb = (uint32_t)(rec >> 40);
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) {
+          if (rr < nr) {
+            const uint32_t par = base[rr] ^ sb ^ (uint32_t)((P[rr] >> hi) ^ (P[rr] >> lo));
+            const double v = (double)erow[(size_t)rr * vstride + pq];
+            s = fma(flip_sign(v, par), (double)xs[(size_t)rr * nb + jb], s);
+          }
+        }
+      }
+      acc[k] = s;
+    }
+    __syncthreads();  // buffer b is free again
+    if (threadIdx.x == 0 && g + 2 < ngroups) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(g + 2);
+    }
+  }
+  if (s_abort) {
+    // leave no bulk copy in flight into this CTA's shared memory
+    if (threadIdx.x == 0)
+      for (int b = 0; b < 2; ++b) mbar_wait_bounded(&bar[b], 0u, kWaitLimit);
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < kAb2Slots; ++k) {
+    const size_t idx = snake_index(chunk0, k, kAb2Threads, threadIdx.x);
+    if (idx < nb) Y[ia * nb + b_order[idx]] += acc[k];
+  }
+}
+
+constexpr int kAb3Threads = 256;
+constexpr int kAb3Slots = 8;
+
+// Alpha single x beta single, v3: no shared-memory staging and no barriers.
+// One CTA per (bra alpha row ia, chunk of kAb3Threads*kAb3Slots beta strings
+// of the list-length order). Each thread walks the alpha singles of ia in
+// groups of R and, for each of its bra beta strings, the beta-single records;
+// the ket values C[ja, jb] and the integrals (ai|bj) (row pq(a,i) of the
+// unpacked table) are gathered through L1, where the R rows shared by the CTA
+// stay resident.
+template <typename T, int R>
+__global__ void __launch_bounds__(kAb3Threads)
+sigma_ab_v3_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restrict__ astr,
+                   const uint64_t* __restrict__ bstr, const uint64_t* __restrict__ a_off,
+                   const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
+                   const uint32_t* __restrict__ a_info, const uint64_t* __restrict__ a_omask,
+                   const uint64_t* __restrict__ b_off, const uint32_t* __restrict__ b_nsing,
+                   const uint64_t* __restrict__ b_rec, const uint32_t* __restrict__ b_order,
+                   const typename Prec<T>::V* __restrict__ V, int npair, double* __restrict__ Y) {
+  using VT = typename Prec<T>::V;
+  const size_t ia = blockIdx.x;
+  const size_t chunk0 = (size_t)blockIdx.y * kAb3Threads * kAb3Slots;
+  uint32_t ibs[kAb3Slots];
+  uint32_t bIlo[kAb3Slots], bIhi[kAb3Slots];
+  double acc[kAb3Slots];
+#pragma unroll
+  for (int k = 0; k < kAb3Slots; ++k) {
+    const size_t idx = chunk0 + (size_t)k * kAb3Threads + threadIdx.x;
+    ibs[k] = idx < nb ? b_order[idx] : 0xffffffffu;
+    const uint64_t b = idx < nb ? bstr[ibs[k]] : 0ull;
+    bIlo[k] = (uint32_t)b;
+    bIhi[k] = (uint32_t)(b >> 32);
+    acc[k] = 0.0;
+  }
+  const uint64_t e0 = a_off[ia];
+  const int ns = (int)a_nsing[ia];
+  for (int k0 = 0; k0 < ns; k0 += R) {
+    const int nr = min(R, ns - k0);
+    const T* xr[R];
+    const VT* vr[R];
+    uint64_t P[R];
+    uint32_t Mlo[R], Mhi[R], sa[R];
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+      const uint64_t e = e0 + k0 + (rr < nr ? rr : 0);
+      const uint32_t inf = __ldg(a_info + e);
+      const uint32_t ja = __ldg(a_ket + e);
+      const uint64_t m = __ldg(a_omask + e);
+      xr[rr] = X + (size_t)ja * nb;
+      vr[rr] = V + (size_t)((inf >> 12) & 0xfffu) * (size_t)npair;
+      P[rr] = prefix_parity(__ldg(astr + ja));
+      Mlo[rr] = (uint32_t)m;
+      Mhi[rr] = (uint32_t)(m >> 32);
+      sa[rr] = inf >> 31;
+    }
+#pragma unroll
+    for (int k = 0; k < kAb3Slots; ++k) {
+      if (ibs[k] == 0xffffffffu) continue;
+      const uint32_t ib = ibs[k];
+      uint32_t base[R];
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) base[rr] = sa[rr] + and_parity(bIlo[k], bIhi[k], Mlo[rr], Mhi[rr]);
+      const uint64_t m0 = __ldg(b_off + ib), m1 = m0 + __ldg(b_nsing + ib);
+      double s = acc[k];
+      uint64_t next = m0 < m1 ? __ldg(b_rec + m0) : 0ull;
+      for (uint64_t m = m0; m < m1; ++m) {
+        const uint64_t rec = next;
+        if (m + 1 < m1) next = __ldg(b_rec + m + 1);
+        const uint32_t jb = (uint32_t)(rec & 0xffffu);
+        const uint32_t pq = (uint32_t)((rec >> 16) & 0xfffu);
+        const uint32_t lo = (uint32_t)((rec >> 28) & 63u), hi = (uint32_t)((rec >> 34) & 63u);
+        const uint32_t sb = (uint32_t)(rec >> 40);
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) {
+          if (rr < nr) {
+            const uint32_t par = base[rr] + sb + (uint32_t)((P[rr] >> hi) ^ (P[rr] >> lo));
+            const double v = (double)__ldg(vr[rr] + pq);
+            s = fma(flip_sign(v, par), (double)__ldg(xr[rr] + jb), s);
+          }
+        }
+      }
+      acc[k] = s;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kAb3Slots; ++k)
+    if (ibs[k] != 0xffffffffu) Y[ia * nb + ibs[k]] += acc[k];
+}
+
+__global__ void unpack_eri_kernel(const double* __restrict__ eri, size_t npair, size_t vs, size_t vs32,
+                                  double* __restrict__ V, float* __restrict__ V32) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npair * npair) return;
+  const size_t r = t / npair, q = t % npair;
+  const double v = eri[pair2_index(r, q)];
+  V[r * vs + q] = v;
+  V32[r * vs32 + q] = (float)v;
 }
 
 template <typename T>
@@ -304,10 +814,16 @@ __global__ void g_table_kernel(const double* __restrict__ eri, int L, size_t npa
 
 template <typename T, int VEC>
 int launch_same(Ctx* c, const T* X, size_t nrow, size_t ncol, const uint64_t* other, const Conn& cn,
-                const typename Prec<T>::V* val, const typename Prec<T>::V* G, const double* hii, double* Y) {
+                const typename Prec<T>::V* val, const typename Prec<T>::V* G, const double* hii, double* Y,
+                int kind) {
   dim3 grid((unsigned)nrow, (unsigned)((ncol + (size_t)kSameThreads * VEC - 1) / ((size_t)kSameThreads * VEC)));
-  sigma_same_v2_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, other, cn.off, cn.nsing, cn.ket, val,
-                                                                      cn.omask, cn.info, G, c->L, hii, Y);
+  if (kind == 1) {
+    sigma_same_v2_kernel<T, VEC <= 4 ? VEC : 4><<<grid, kSameThreads, 0, c->stream>>>(
+        X, ncol, other, cn.off, cn.nsing, cn.ket, val, cn.omask, cn.info, G, c->L, hii, Y);
+  } else {
+    sigma_same_v4_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, other, cn.off, cn.nsing, cn.ket, val,
+                                                                        cn.spos, cn.info, G, c->L, hii, Y);
+  }
   SBDX_LAUNCHED(c);
   return 0;
 }
@@ -315,14 +831,18 @@ int launch_same(Ctx* c, const T* X, size_t nrow, size_t ncol, const uint64_t* ot
 template <typename T>
 int run_same(Ctx* c, const T* X, size_t nrow, size_t ncol, const uint64_t* other, const Conn& cn,
              const typename Prec<T>::V* val, const typename Prec<T>::V* G, const double* hii, double* Y) {
-  // widest vector that divides the row length and keeps 16-byte alignment
-  constexpr int kWide = sizeof(T) == 8 ? 2 : 4;
+  // default: popcount kernel x4 for FP64, parity-table kernel x8 for FP32;
+  // narrowed to the widest vector that divides the row and keeps 16-byte alignment
+  const int code0 = c->tune[sizeof(T) == 8 ? 0 : 1].same_code;
+  const int code = code0 > 0 ? code0 : (sizeof(T) == 8 ? 14 : 8);
+  const int kind = code >= 10 ? 1 : 0;
+  int vec = code % 10;
   const bool aligned = (reinterpret_cast<uintptr_t>(X) % 16) == 0;
-  int vec = c->tune.same_vec > 0 ? c->tune.same_vec : kWide;
   while (vec > 1 && (!aligned || ncol % vec != 0)) vec >>= 1;
-  if (vec >= 4) return launch_same<T, 4>(c, X, nrow, ncol, other, cn, val, G, hii, Y);
-  if (vec == 2) return launch_same<T, 2>(c, X, nrow, ncol, other, cn, val, G, hii, Y);
-  return launch_same<T, 1>(c, X, nrow, ncol, other, cn, val, G, hii, Y);
+  if (vec >= 8 && kind == 0) return launch_same<T, 8>(c, X, nrow, ncol, other, cn, val, G, hii, Y, kind);
+  if (vec >= 4) return launch_same<T, 4>(c, X, nrow, ncol, other, cn, val, G, hii, Y, kind);
+  if (vec == 2) return launch_same<T, 2>(c, X, nrow, ncol, other, cn, val, G, hii, Y, kind);
+  return launch_same<T, 1>(c, X, nrow, ncol, other, cn, val, G, hii, Y, kind);
 }
 
 size_t ab2_smem_bytes(size_t nb, size_t tsz, size_t vsz, size_t npair, int R, size_t* stride) {
@@ -333,17 +853,101 @@ size_t ab2_smem_bytes(size_t nb, size_t tsz, size_t vsz, size_t npair, int R, si
 }
 
 template <typename T, int R>
-int launch_ab2(Ctx* c, const T* X, size_t smem, size_t xstride) {
+int launch_ab2(Ctx* c, const T* X, size_t smem, size_t xstride, int threads) {
   using V = typename Prec<T>::V;
   const Conn& ca = c->conn[0];
   const Conn& cb = c->conn[1];
   const V* eri = std::is_same<T, double>::value ? (const V*)c->d_eri : (const V*)c->d_eri32;
-  SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v2_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const size_t per_cta = (size_t)kAb2Threads * kAb2Slots;
+  const size_t per_cta = 8192;
   dim3 grid((unsigned)c->na, (unsigned)((c->nb + per_cta - 1) / per_cta));
-  sigma_ab_v2_kernel<T, R><<<grid, kAb2Threads, smem, c->stream>>>(
+  if (threads == 512) {
+    SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v2_kernel<T, R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    sigma_ab_v2_kernel<T, R, 512><<<grid, 512, smem, c->stream>>>(
+        X, c->nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket, ca.info, ca.omask, cb.off, cb.nsing, cb.srec, cb.order,
+        eri, (int)c->npair, xstride, c->d_y);
+    SBDX_LAUNCHED(c);
+    return 0;
+  }
+  SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v2_kernel<T, R, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  sigma_ab_v2_kernel<T, R, 1024><<<grid, 1024, smem, c->stream>>>(
       X, c->nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket, ca.info, ca.omask, cb.off, cb.nsing, cb.srec, cb.order, eri,
       (int)c->npair, xstride, c->d_y);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+template <typename T, int R>
+int launch_ab3(Ctx* c, const T* X) {
+  using V = typename Prec<T>::V;
+  const Conn& ca = c->conn[0];
+  const Conn& cb = c->conn[1];
+  const V* Vt = std::is_same<T, double>::value ? (const V*)c->d_V : (const V*)c->d_V32;
+  const size_t vs = std::is_same<T, double>::value ? c->vstride : c->vstride32;
+  const size_t per_cta = (size_t)kAb3Threads * kAb3Slots;
+  dim3 grid((unsigned)c->na, (unsigned)((c->nb + per_cta - 1) / per_cta));
+  sigma_ab_v3_kernel<T, R><<<grid, kAb3Threads, 0, c->stream>>>(
+      X, c->nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket, ca.info, ca.omask, cb.off, cb.nsing, cb.srec, cb.order, Vt,
+      (int)vs, c->d_y);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+template <typename T, int R>
+int launch_ab4(Ctx* c, const T* X, size_t smem) {
+  using V = typename Prec<T>::V;
+  const Conn& ca = c->conn[0];
+  const Conn& cb = c->conn[1];
+  const V* Vt = std::is_same<T, double>::value ? (const V*)c->d_V : (const V*)c->d_V32;
+  const size_t vs = std::is_same<T, double>::value ? c->vstride : c->vstride32;
+  SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v4_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t per_cta = (size_t)kAb2Threads * kAb2Slots;
+  dim3 grid((unsigned)c->na, (unsigned)((c->nb + per_cta - 1) / per_cta));
+  sigma_ab_v4_kernel<T, R><<<grid, kAb2Threads, smem, c->stream>>>(
+      X, c->nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket, ca.info, ca.omask, cb.off, cb.nsing, cb.srec, cb.order, Vt,
+      vs, c->d_err, c->d_y);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+// Double-buffered TMA variant when rows are 16-byte aligned and two buffers of
+// at least one row fit; returns 1 (not launched) otherwise.
+template <typename T>
+int try_ab4(Ctx* c, const T* X, int rows_req) {
+  using V = typename Prec<T>::V;
+  const size_t xbytes = sizeof(T) * c->nb;
+  const size_t vs = std::is_same<T, double>::value ? c->vstride : c->vstride32;
+  const size_t vbytes = sizeof(V) * vs;
+  if (xbytes % 16 != 0 || (reinterpret_cast<uintptr_t>(X) % 16) != 0) return 1;
+  const size_t budget = 200 * 1024;
+  int R = rows_req > 0 ? rows_req : 4;
+  for (; R >= 1; --R)
+    if (2 * (size_t)R * (xbytes + vbytes) <= budget) break;
+  if (R < 1) return 1;
+  const size_t smem = 2 * (size_t)R * (xbytes + vbytes);
+  int rc;
+  if (R >= 4) rc = launch_ab4<T, 4>(c, X, smem);
+  else if (R == 3) rc = launch_ab4<T, 3>(c, X, smem);
+  else if (R == 2) rc = launch_ab4<T, 2>(c, X, smem);
+  else rc = launch_ab4<T, 1>(c, X, smem);
+  return rc ? -rc : 0;
+}
+
+template <typename T, int R>
+int launch_ab5(Ctx* c, const T* X, size_t smem, size_t xstride) {
+  using V = typename Prec<T>::V;
+  const Conn& ca = c->conn[0];
+  const Conn& cb = c->conn[1];
+  const V* eri = std::is_same<T, double>::value ? (const V*)c->d_eri : (const V*)c->d_eri32;
+  constexpr int NT = 1024;
+  SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v5_kernel<T, R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  const size_t slices_per_cta = 8192 / 32;
+  dim3 grid((unsigned)c->na, (unsigned)((cb.nslice + slices_per_cta - 1) / slices_per_cta));
+  sigma_ab_v5_kernel<T, R, NT><<<grid, NT, smem, c->stream>>>(
+      X, c->nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket, ca.info, ca.omask, cb.sell, cb.soff, cb.slen, cb.nslice,
+      cb.order, eri, (int)c->npair, xstride, c->d_y);
   SBDX_LAUNCHED(c);
   return 0;
 }
@@ -351,21 +955,42 @@ int launch_ab2(Ctx* c, const T* X, size_t smem, size_t xstride) {
 template <typename T>
 int run_ab(Ctx* c, const T* X) {
   using V = typename Prec<T>::V;
-  const size_t budget = 220 * 1024;
-  int R = c->tune.ab_rows > 0 ? c->tune.ab_rows : 4;
+  const int code0 = c->tune[sizeof(T) == 8 ? 0 : 1].ab_code;
+  const int code = code0 > 0 ? code0 : (sizeof(T) == 8 ? 42 : 13);
+  const int variant = code / 10;
+  const int rows = code % 10 > 0 ? code % 10 : 2;
+  if (variant == 2) {  // double-buffered TMA staging, when rows are 16-byte aligned
+    const int rc = try_ab4<T>(c, X, rows);
+    if (rc <= 0) return -rc;
+  }
+  if (variant == 0) {
+    if (rows >= 4) return launch_ab3<T, 4>(c, X);
+    if (rows == 3) return launch_ab3<T, 3>(c, X);
+    if (rows == 2) return launch_ab3<T, 2>(c, X);
+    return launch_ab3<T, 1>(c, X);
+  }
+  const int threads = variant == 3 ? 512 : 1024;
+  const size_t budget = threads == 512 ? 110 * 1024 : 220 * 1024;
+  int R = rows;
   size_t stride = 0, smem = 0;
   for (; R >= 1; --R) {
     smem = ab2_smem_bytes(c->nb, sizeof(T), sizeof(V), c->npair, R, &stride);
     if (smem <= budget) break;
   }
-  if (R >= 1) {
-    if (R >= 4) return launch_ab2<T, 4>(c, X, smem, stride);
-    if (R == 3) return launch_ab2<T, 3>(c, X, smem, stride);
-    if (R == 2) return launch_ab2<T, 2>(c, X, smem, stride);
-    return launch_ab2<T, 1>(c, X, smem, stride);
+  if (R < 1) {
+    c->err = "sigma: beta dimension too large for one shared-memory ket row";
+    return 1;
   }
-  c->err = "sigma: beta dimension too large for one shared-memory ket row";
-  return 1;
+  if (variant == 4) {
+    if (R >= 4) return launch_ab5<T, 4>(c, X, smem, stride);
+    if (R == 3) return launch_ab5<T, 3>(c, X, smem, stride);
+    if (R == 2) return launch_ab5<T, 2>(c, X, smem, stride);
+    return launch_ab5<T, 1>(c, X, smem, stride);
+  }
+  if (R >= 4) return launch_ab2<T, 4>(c, X, smem, stride, threads);
+  if (R == 3) return launch_ab2<T, 3>(c, X, smem, stride, threads);
+  if (R == 2) return launch_ab2<T, 2>(c, X, smem, stride, threads);
+  return launch_ab2<T, 1>(c, X, smem, stride, threads);
 }
 
 template <typename T>
@@ -430,6 +1055,20 @@ int build_g_table(Ctx* c) {
   SBDX_CUDA(c, cudaMalloc(&c->d_G32, sizeof(float) * n));
   g_table_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->d_eri, c->L, c->npair, c->d_G, c->d_G32);
   SBDX_LAUNCHED(c);
+  const size_t nv = c->npair * c->npair;
+  c->vstride = (c->npair + 1) / 2 * 2;
+  c->vstride32 = (c->npair + 3) / 4 * 4;
+  cudaFree(c->d_V);
+  cudaFree(c->d_V32);
+  c->d_V = nullptr;
+  c->d_V32 = nullptr;
+  SBDX_CUDA(c, cudaMalloc(&c->d_V, sizeof(double) * c->npair * c->vstride));
+  SBDX_CUDA(c, cudaMalloc(&c->d_V32, sizeof(float) * c->npair * c->vstride32));
+  SBDX_CUDA(c, cudaMemsetAsync(c->d_V, 0, sizeof(double) * c->npair * c->vstride, c->stream));
+  SBDX_CUDA(c, cudaMemsetAsync(c->d_V32, 0, sizeof(float) * c->npair * c->vstride32, c->stream));
+  unpack_eri_kernel<<<(unsigned)((nv + 255) / 256), 256, 0, c->stream>>>(c->d_eri, c->npair, c->vstride,
+                                                                           c->vstride32, c->d_V, c->d_V32);
+  SBDX_LAUNCHED(c);
   return 0;
 }
 
@@ -441,59 +1080,66 @@ int ensure_sigma_scratch(Ctx* c) {
   return 0;
 }
 
-// Autotuner: time every candidate (same_vec, ab_rows) on the current problem
-// with CUDA events (one warm-up and two timed FP64 sigmas each, on scratch
-// vectors) and keep the fastest. The same-spin and alpha-beta choices are
-// independent kernels, so they are tuned separately through the phase timers.
+// Autotuner: for each precision, time the candidate kernel variants and launch
+// shapes on the current problem (one warm-up and two timed sigmas each, CUDA
+// events between the phases, scratch input vectors) and keep the fastest
+// same-spin and alpha-beta choice separately.
 int autotune(Ctx* c) {
   int rc = 0;
   if (!c->have_conn && (rc = build_connectivity(c))) return rc;
   if (!c->have_hii && (rc = diag_terms(c))) return rc;
   if ((rc = ensure_sigma_scratch(c))) return rc;
   const size_t D = c->na * c->nb;
-  double *X = nullptr, *S = nullptr;
+  void *X = nullptr, *S = nullptr;
   SBDX_CUDA(c, cudaMallocAsync(&X, sizeof(double) * D, c->stream));
   SBDX_CUDA(c, cudaMallocAsync(&S, sizeof(double) * D, c->stream));
   SBDX_CUDA(c, cudaMemsetAsync(X, 0, sizeof(double) * D, c->stream));
   const bool prof0 = c->profiling;
-  const auto saved = c->tune;
   if (!c->ev[0])
     for (auto& e : c->ev) SBDX_CUDA(c, cudaEventCreate(&e));
   c->profiling = true;
-  auto measure = [&](int vec, int rows, double* same_ms, double* ab_ms) -> int {
-    c->tune.same_vec = vec;
-    c->tune.ab_rows = rows;
-    int r2 = run_sigma<double>(c, X, S);
-    if (r2) return r2;
-    for (double& x : c->phase_ms) x = 0.0;
-    c->phase_calls = 0;
-    for (int k = 0; k < 2; ++k)
-      if ((r2 = run_sigma<double>(c, X, S))) return r2;
-    *same_ms = c->phase_ms[0] + c->phase_ms[2];
-    *ab_ms = c->phase_ms[3];
-    return 0;
-  };
-  int best_vec = 1, best_rows = 1;
-  double best_same = 1e300, best_ab = 1e300;
-  const int vecs[3] = {1, 2, 4};
-  for (int v : vecs) {
-    double sm = 0, ab = 0;
-    if ((rc = measure(v, 1, &sm, &ab))) break;
-    if (sm < best_same) { best_same = sm; best_vec = v; }
-  }
-  for (int rows = 1; rc == 0 && rows <= 4; ++rows) {
-    double sm = 0, ab = 0;
-    if ((rc = measure(best_vec, rows, &sm, &ab))) break;
-    if (ab < best_ab) { best_ab = ab; best_rows = rows; }
+  const int same_cand[] = {14, 12, 11, 8, 4, 2, 1};
+  const int ab_cand[] = {42, 43, 41, 44, 12, 13, 14, 11, 22, 21, 32, 31};
+  for (int prec = 0; prec < 2 && rc == 0; ++prec) {
+    const Tune saved = c->tune[prec];
+    auto measure = [&](int same, int ab, double* same_ms, double* ab_ms) -> int {
+      c->tune[prec].same_code = same;
+      c->tune[prec].ab_code = ab;
+      int r2 = prec == 0 ? run_sigma<double>(c, (const double*)X, (double*)S)
+                         : run_sigma<float>(c, (const float*)X, (float*)S);
+      if (r2) return r2;
+      for (double& x : c->phase_ms) x = 0.0;
+      c->phase_calls = 0;
+      for (int k = 0; k < 2 && r2 == 0; ++k)
+        r2 = prec == 0 ? run_sigma<double>(c, (const double*)X, (double*)S)
+                       : run_sigma<float>(c, (const float*)X, (float*)S);
+      *same_ms = c->phase_ms[0] + c->phase_ms[2];
+      *ab_ms = c->phase_ms[3];
+      return r2;
+    };
+    int best_same = 0, best_ab = 0;
+    double t_same = 1e300, t_ab = 1e300;
+    for (int sc : same_cand) {
+      double sm = 0, ab = 0;
+      if ((rc = measure(sc, 42, &sm, &ab))) break;
+      if (sm < t_same) { t_same = sm; best_same = sc; }
+    }
+    for (int ac : ab_cand) {
+      if (rc) break;
+      double sm = 0, ab = 0;
+      if ((rc = measure(best_same, ac, &sm, &ab))) break;
+      if (ab < t_ab) { t_ab = ab; best_ab = ac; }
+    }
+    if (rc) { c->tune[prec] = saved; break; }
+    c->tune[prec].same_code = best_same;
+    c->tune[prec].ab_code = best_ab;
   }
   c->profiling = prof0;
   for (double& x : c->phase_ms) x = 0.0;
   c->phase_calls = 0;
   cudaFreeAsync(X, c->stream);
   cudaFreeAsync(S, c->stream);
-  if (rc) { c->tune = saved; return rc; }
-  c->tune.same_vec = best_vec;
-  c->tune.ab_rows = best_rows;
+  if (rc) return rc;
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
   return 0;
 }

@@ -1,0 +1,120 @@
+"""Generate the golden fixtures of the parity tests from the compiled reference.
+
+Run in a container where the reference tree is mounted and oracle/_ref has
+been built (make -C oracle ref):
+
+    python tests/golden/make_golden.py
+
+Every array in the fixtures is an output of the UNMODIFIED reference headers
+(walkup/sbd-ykt), driven through oracle/ref_driver.cc:
+  * small_*.npz : seeded synthetic problems -- connectivity lists
+                  (GenerateExcitation/MakeSmartHelper), matrix elements of
+                  sampled determinant pairs (Hij), diagonal (makeQChamDiagTerms),
+                  one sigma (mult), Davidson energy and vector, 1-/2-RDM
+                  (Correlation), and the tpb::diag outputs (energy, density,
+                  carry-over strings) on the struct path;
+  * h2o_1em3.npz / n2_1em3.npz : the reference's own known-answer inputs
+                  (data/h2o, data/n2 with the 1e-3 string files) as parsed by
+                  LoadFCIDump/LoadAlphaDets, the integrals after the file path's
+                  text round trip, and the energies of both entry points.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [os.path.join(ROOT, "oracle"), os.path.join(ROOT, "sbd-ykt_b200")]
+
+from oracle import Ref  # noqa: E402
+from sbdx import synth  # noqa: E402
+
+REF = "/root/reference"
+
+SMALL = {
+    # name: (L, n_alpha, n_beta, Na, Nb, seed)
+    "small_a": (10, 3, 2, 40, 30, 7),
+    "small_b": (14, 4, 4, 90, 70, 21),
+    "small_c": (20, 3, 5, 50, 120, 33),
+}
+
+
+def small(ref: Ref, name, spec):
+    L, na_el, nb_el, Na, Nb, seed = spec
+    prob = synth.random_problem(L, na_el, nb_el, Na, Nb, seed=seed)
+    (asl, adl, bsl, bdl), flat = ref.connectivity(prob.alpha, prob.beta, L)
+    rng = np.random.default_rng(seed)
+    n = 4000
+    ia = rng.integers(0, prob.na, n)
+    ib = rng.integers(0, prob.nb, n)
+    ja = rng.integers(0, prob.na, n)
+    jb = rng.integers(0, prob.nb, n)
+    ja[: n // 3] = ia[: n // 3]
+    jb[n // 3: 2 * n // 3] = ib[n // 3: 2 * n // 3]
+    hij, od = ref.hij(prob, prob.alpha[ia], prob.beta[ib], prob.alpha[ja], prob.beta[jb])
+    hii = ref.diag_terms(prob)
+    C = rng.standard_normal(prob.D)
+    S = ref.sigma(prob, C)
+    E, W = ref.davidson(prob, max_it=6, max_nb=10, eps=1e-10)
+    one, two = ref.rdm(prob, W)
+    d = ref.tpb_diag(prob, max_it=6, max_nb=10, eps=1e-10, do_rdm=0, ratio=0.0, threshold=0.01)
+    d2 = ref.tpb_diag(prob, max_it=6, max_nb=10, eps=1e-10, do_rdm=0, ratio=0.5, threshold=0.01)
+    extra = {"two": two} if L <= 14 else {}  # the 4*L^4 2-RDM only for the small orbital counts
+    np.savez_compressed(
+        os.path.join(HERE, f"{name}.npz"), L=L, nelec=prob.nelec, I0=prob.I0, h=prob.h, eri=prob.eri,
+        alpha=prob.alpha, beta=prob.beta, a_slen=asl, a_dlen=adl, b_slen=bsl, b_dlen=bdl, conn_flat=flat,
+        pair_ia=ia, pair_ib=ib, pair_ja=ja, pair_jb=jb, hij=hij, orb_diff=od, hii=hii, C=C, S=S, E=E, W=W,
+        one=one, diag_energy=d["energy"], diag_density=d["density"], diag_carry=d["carryover"],
+        diag_carry_ratio=d2["carryover"], **extra)
+    print(name, prob.na, prob.nb, "E", E)
+
+
+def kat(ref: Ref, mol, fcidump, adet, L):
+    La, N, I0r, hr, erir = ref.fcidump_roundtrip(fcidump)
+    assert La == L
+    alpha = ref.load_alpha_dets(adet, L)
+    # exact doubles as written in the file (no round trip), for the struct path
+    h = np.zeros((L, L))
+    eri = np.zeros(len(erir))
+    I0 = 0.0
+    with open(fcidump) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) != 5 or "&" in line or "=" in line:
+                continue
+            try:
+                v = float(parts[0])
+                i, j, k, l = (int(x) for x in parts[1:])
+            except ValueError:
+                continue
+            if i == j == k == l == 0:
+                I0 = v
+            elif k == 0 and l == 0:
+                h[i - 1, j - 1] = h[j - 1, i - 1] = v
+            else:
+                eri[synth.eri_index(i - 1, j - 1, k - 1, l - 1)] = v
+    file_path = ref.tpb_diag_files(fcidump, adet, L, max_it=10, max_nb=10, eps=1e-8, do_rdm=1)
+    prob = synth.Problem(L=L, nelec=N, I0=I0, h=h.reshape(-1), eri=eri, alpha=alpha, beta=alpha.copy())
+    struct = ref.tpb_diag(prob, max_it=10, max_nb=10, eps=1e-8, do_rdm=0)
+    np.savez_compressed(
+        os.path.join(HERE, f"{mol}_1em3.npz"), L=L, nelec=N, I0=I0, h=h.reshape(-1), eri=eri, alpha=alpha,
+        I0_rt=I0r, h_rt=hr, eri_rt=erir, E_file=file_path["energy"], density_file=file_path["density"],
+        carry_file=file_path["carryover"], one_file=file_path["one"], E_struct=struct["energy"])
+    print(mol, len(alpha), "E_file", file_path["energy"], "E_struct", struct["energy"])
+
+
+def main():
+    if not Ref.available():
+        raise SystemExit("oracle/_ref/libsbdref.so missing: run make -C oracle ref")
+    ref = Ref()
+    for name, spec in SMALL.items():
+        small(ref, name, spec)
+    kat(ref, "h2o", f"{REF}/data/h2o/fcidump.txt", f"{REF}/data/h2o/h2o-1em3-alpha.txt", 24)
+    kat(ref, "n2", f"{REF}/data/n2/fcidump.txt", f"{REF}/data/n2/1em3-alpha.txt", 18)
+
+
+if __name__ == "__main__":
+    main()
