@@ -1,0 +1,72 @@
+"""CUDA path (C-ABI) against the reference's golden outputs (tests/golden).
+
+Connectivity bit-exact; diagonal and sigma within 1e-12 relative; Davidson
+energy within 1e-9 Ha; 1-/2-RDM within 1e-8; density within 1e-8; carry-over
+strings as a set.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import sbdx
+from sbdx import synth
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def load(name):
+    g = dict(np.load(os.path.join(GOLD, f"{name}.npz")))
+    prob = synth.Problem(L=int(g["L"]), nelec=int(g["nelec"]), I0=float(g["I0"]), h=g["h"], eri=g["eri"],
+                         alpha=g["alpha"].astype(np.uint64), beta=g["beta"].astype(np.uint64))
+    return prob, g
+
+
+@pytest.mark.parametrize("name", ["small_a", "small_b", "small_c"])
+def test_cuda_matches_reference_golden(name):
+    prob, g = load(name)
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        ctx.build_connectivity()
+        sa, da, ia = ctx.connectivity(0)
+        sb, db, ib = ctx.connectivity(1)
+        assert np.array_equal(sa, g["a_slen"]) and np.array_equal(da, g["a_dlen"])
+        assert np.array_equal(sb, g["b_slen"]) and np.array_equal(db, g["b_dlen"])
+        assert np.array_equal(np.concatenate([ia, ib]), g["conn_flat"])
+        hii = ctx.diag_terms()
+        assert np.abs(hii - g["hii"]).max() <= 1e-12 * np.abs(g["hii"]).max()
+        S = ctx.sigma(g["C"])
+        assert np.abs(S - g["S"]).max() <= 1e-12 * np.abs(g["S"]).max()
+        info, W = ctx.davidson(max_it=6, max_nb=10, eps=1e-10)
+        assert abs(info.energy - float(g["E"])) < 1e-9
+        one, two = ctx.rdm(g["W"], two="two" in g)
+        assert np.abs(one - g["one"]).max() < 1e-8
+        if "two" in g:
+            assert np.abs(two - g["two"]).max() < 1e-8
+        dens = ctx.occupation(W)
+        assert np.abs(dens - g["diag_density"]).max() < 1e-8
+        wa = ctx.alpha_weights(W)
+    order = np.argsort(-wa, kind="stable")
+    cum = np.cumsum(wa[order])
+    kept = min(int(np.searchsorted(cum, 1.0 - 0.01, side="right")) + 1, len(wa))
+    assert set(prob.alpha[order[:kept]].tolist()) == set(g["diag_carry"].tolist())
+
+
+@pytest.mark.parametrize("mol", ["h2o", "n2"])
+def test_known_answer_energies_cabi(mol):
+    g = dict(np.load(os.path.join(GOLD, f"{mol}_1em3.npz")))
+    a = g["alpha"].astype(np.uint64)
+    L = int(g["L"])
+    file_prob = synth.Problem(L=L, nelec=int(g["nelec"]), I0=float(g["I0_rt"]), h=g["h_rt"], eri=g["eri_rt"],
+                              alpha=a, beta=a)
+    with sbdx.Context(0) as ctx:
+        ctx.load(file_prob)
+        info, W = ctx.davidson(max_it=10, max_nb=10, eps=1e-8)
+        assert abs(info.energy - float(g["E_file"])) < 1e-9
+        assert np.abs(ctx.occupation(W) - g["density_file"]).max() < 1e-8
+        one, _ = ctx.rdm(W, two=False)
+        assert np.abs(one - g["one_file"]).max() < 1e-8
+        ctx.set_integrals(L, float(g["I0"]), g["h"], g["eri"])
+        info2, _ = ctx.davidson(max_it=10, max_nb=10, eps=1e-8)
+        assert abs(info2.energy - float(g["E_struct"])) < 1e-9
