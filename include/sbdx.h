@@ -104,6 +104,35 @@ int sbdx_get_connectivity(sbdx_ctx* ctx, int spin, uint64_t* slen, uint64_t* dle
  * NULL to only compute the device copy). */
 int sbdx_diag_terms(sbdx_ctx* ctx, double* hii);
 
+/* Diagonal H_II computed without any device allocation. This entry point has no
+ * counterpart in the reference; it returns the same values as sbdx_diag_terms.
+ *
+ * For callers that must not have a library allocate or free device memory:
+ * code whose device memory all comes from its own pre-sized pool or framework
+ * allocator, and code that records its stream into a replayable sequence where
+ * a cudaMalloc/cudaFree would either be refused or synchronise the device.
+ * No context is used: every input is a device pointer the caller owns.
+ *   d_h     L*L FP64, row-major;  d_eri  8-fold packed (pq|rs) FP64
+ *   d_alpha na uint64 strings;    d_beta nb uint64 strings (bits >= norb ignored)
+ *   d_hii   na*nb FP64 output, alpha-major (index ia*nb + ib)
+ *   stream  cudaStream_t to launch on (NULL = legacy default stream)
+ * The intermediate per-string energies and beta Coulomb rows live in one
+ * fixed file-scope device array of 524288 doubles (4 MiB) per GPU; a call needs
+ * na + nb + nb*norb <= 524288 and na <= 65535, else it returns SBDX_ERR_ARG
+ * with a message in errbuf and launches nothing. Nothing has to start at zero:
+ * each call writes every scratch word before reading it.
+ * The first call on each device (with that device current) looks up the
+ * array's device address with cudaGetSymbolAddress, which may initialise the
+ * CUDA context; make that first call before any stream capture begins.
+ * All calls on one device share the array: calls that can overlap (on
+ * different streams, or from several host threads) race and give wrong
+ * results; serialise them on one stream. Asynchronous: synchronise the stream
+ * before reading d_hii. errbuf (may be NULL) receives a NUL-terminated
+ * message of at most errlen bytes when the status is not SBDX_OK. */
+int sbdx_diag_terms_noalloc(int norb, double I0, const double* d_h, const double* d_eri,
+                            const uint64_t* d_alpha, size_t na, const uint64_t* d_beta, size_t nb,
+                            double* d_hii, void* stream, char* errbuf, size_t errlen);
+
 /* One H*C product. Replaces mult (chemistry/tpb/mult.h:376-632). C and S are
  * host buffers of na*nb doubles (S is overwritten, not accumulated). */
 int sbdx_sigma(sbdx_ctx* ctx, const double* C, double* S);

@@ -226,3 +226,21 @@ class Context:
         deri = np.zeros(synth.neri(L))
         self._check(self.lib.sbdx_energy_backward(self.h, _d(np.ascontiguousarray(W, dtype=np.float64)), _d(dh), _d(deri)))
         return dh, deri
+
+
+def diag_terms_noalloc(norb: int, I0: float, h_ptr: int, eri_ptr: int, alpha_ptr: int, na: int, beta_ptr: int,
+                       nb: int, hii_ptr: int, stream_ptr: int = 0):
+    """sbdx_diag_terms_noalloc on caller-owned device pointers (no context, no
+    device allocation). Launches asynchronously on `stream_ptr`; the library
+    keeps one fixed 4 MiB scratch array per GPU, so calls must not overlap.
+    Raises SbdxError with the library's message on a non-zero status."""
+    lib = load_library()
+    fn = lib.sbdx_diag_terms_noalloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                   ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p,
+                   ctypes.c_char_p, ctypes.c_size_t]
+    buf = ctypes.create_string_buffer(256)
+    rc = fn(norb, I0, h_ptr, eri_ptr, alpha_ptr, na, beta_ptr, nb, hii_ptr, stream_ptr, buf, len(buf))
+    if rc != SBDX_OK:
+        raise SbdxError(rc, buf.value.decode())
