@@ -56,6 +56,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU-baseline sample duration")
     ap.add_argument("--davidson-tol", type=float, default=1e-8)
+    ap.add_argument("--tune", default=None, metavar="SAME,AB",
+                    help="fixed sigma launch codes for both precisions instead of the autotuner (profiling runs)")
     return ap.parse_args()
 
 
@@ -232,7 +234,11 @@ def run_ours(args, rank, world, local):
     ctx = sbdx.Context(local)
     ctx.load(prob)
     ctx.build_connectivity()
-    tune = ctx.autotune()
+    if args.tune:
+        tune = tuple(int(x) for x in args.tune.split(","))
+        ctx.set_tuning(*tune)
+    else:
+        tune = ctx.autotune()
     sa, da, _ = ctx.connectivity(0)
     sb, db, _ = ctx.connectivity(1)
     dp = synth.det_pairs(sa, da, sb, db)

@@ -18,8 +18,11 @@
 // The sigma kernels combine these with the opposite-spin string of each
 // determinant in O(1) (a popcount) per pair.
 #include "sbdx_internal.cuh"
+#include "sbdx.h"
 
 #include <algorithm>
+#include <cstdint>
+#include <vector>
 
 namespace sbdx {
 
@@ -181,7 +184,105 @@ void free_conn(Conn& c) {
   cudaFree(c.val); cudaFree(c.val32); cudaFree(c.omask); cudaFree(c.info);
   cudaFree(c.srec); cudaFree(c.order); cudaFree(c.spos);
   cudaFree(c.sell); cudaFree(c.soff); cudaFree(c.slen);
+  cudaFree(c.bsell); cudaFree(c.bsoff); cudaFree(c.bslen); cudaFree(c.vrow);
+  cudaFree(c.split_row); cudaFree(c.split_slot);
   c = Conn{};
+}
+
+// Balanced SELL-32 of the single records (see Conn::bsell). The cap starts at
+// twice the mean list length (at least 16), so that no lane of a warp walks a
+// list much longer than the others, and doubles until the partial-sum slots
+// fit the kernel's shared-memory budget. The slices per warp are the smallest
+// of 8, 12, 16 that cover the virtual rows in the fewest CTAs.
+int build_balanced_sell(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const std::vector<uint64_t>& off,
+                        const std::vector<uint32_t>& order, const std::vector<uint64_t>& rec) {
+  const size_t n = cn.n;
+  uint64_t total = 0;
+  uint32_t mx = 0;
+  for (size_t r = 0; r < n; ++r) { total += hs[r]; mx = std::max(mx, hs[r]); }
+  uint32_t cap = std::max<uint32_t>(16, 2 * (uint32_t)((total + n - 1) / n));
+  std::vector<uint32_t> parts(n);
+  int nslot = 0;
+  for (;;) {
+    nslot = 0;
+    for (size_t r = 0; r < n; ++r) {
+      parts[r] = hs[r] == 0 ? 0 : (hs[r] + cap - 1) / cap;
+      if (parts[r] > 1) nslot += (int)parts[r];
+    }
+    if (nslot <= kMaxSplitSlots || cap >= mx) break;
+    cap *= 2;
+  }
+  if (nslot > kMaxSplitSlots) {
+    c->err = "build_connectivity: too many split beta lists";
+    return SBDX_ERR_ARG;
+  }
+  // virtual rows: (bra string, first record, length, slot + 1 or 0)
+  struct VRow { uint32_t r; uint64_t beg; uint32_t len; uint32_t slot1; };
+  std::vector<VRow> vr;
+  std::vector<uint32_t> split_row, split_slot(1, 0);
+  for (uint32_t r : order) {
+    if (parts[r] <= 1) continue;
+    const uint32_t p = parts[r], base = hs[r] / p, rem = hs[r] % p;
+    uint64_t beg = off[r];
+    for (uint32_t j = 0; j < p; ++j) {
+      const uint32_t len = base + (j < rem ? 1u : 0u);
+      vr.push_back({r, beg, len, split_slot.back() + j + 1});
+      beg += len;
+    }
+    split_row.push_back(r);
+    split_slot.push_back(split_slot.back() + p);
+  }
+  for (uint32_t r : order)  // longest first
+    if (parts[r] == 1) vr.push_back({r, off[r], hs[r], 0});
+  const size_t nv = vr.size();
+  int ks = 8;
+  {
+    size_t best = SIZE_MAX;
+    for (int cand : {8, 12, 16}) {
+      const size_t chunks = (nv + 1024 * (size_t)cand - 1) / (1024 * (size_t)cand);
+      if (chunks < best) { best = chunks; ks = cand; }
+    }
+  }
+  const size_t ns = (nv + 31) / 32;
+  std::vector<uint64_t> soff(ns + 1, 0);
+  std::vector<uint32_t> slen(ns ? ns : 1, 0);
+  for (size_t sl = 0; sl < ns; ++sl) {
+    uint32_t m = 0;
+    for (size_t l = 0; l < 32 && sl * 32 + l < nv; ++l) m = std::max(m, vr[sl * 32 + l].len);
+    slen[sl] = m;
+    soff[sl + 1] = soff[sl] + 32ull * m;
+  }
+  const uint64_t kPad = 1ull << 41;
+  std::vector<uint64_t> sell(soff[ns] ? soff[ns] : 1, kPad);
+  std::vector<uint32_t> vrow(nv ? nv : 1, 0);
+  for (size_t v = 0; v < nv; ++v) {
+    const size_t sl = v / 32, l = v % 32;
+    for (uint32_t m = 0; m < vr[v].len; ++m) sell[soff[sl] + 32ull * m + l] = rec[vr[v].beg + m];
+    vrow[v] = vr[v].r | (vr[v].slot1 << 16);
+  }
+  cn.bnslice = ns;
+  cn.nv = nv;
+  cn.nsplit = (int)split_row.size();
+  cn.nslot = (int)split_slot.back();
+  cn.cap = (int)cap;
+  cn.slices_per_warp = ks;
+  if (split_row.empty()) split_row.push_back(0);
+  SBDX_CUDA(c, cudaMalloc(&cn.bsell, sizeof(uint64_t) * sell.size()));
+  SBDX_CUDA(c, cudaMalloc(&cn.bsoff, sizeof(uint64_t) * (ns + 1)));
+  SBDX_CUDA(c, cudaMalloc(&cn.bslen, sizeof(uint32_t) * slen.size()));
+  SBDX_CUDA(c, cudaMalloc(&cn.vrow, sizeof(uint32_t) * vrow.size()));
+  SBDX_CUDA(c, cudaMalloc(&cn.split_row, sizeof(uint32_t) * split_row.size()));
+  SBDX_CUDA(c, cudaMalloc(&cn.split_slot, sizeof(uint32_t) * split_slot.size()));
+  SBDX_CUDA(c, cudaMemcpyAsync(cn.bsell, sell.data(), sizeof(uint64_t) * sell.size(), cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(cn.bsoff, soff.data(), sizeof(uint64_t) * (ns + 1), cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(cn.bslen, slen.data(), sizeof(uint32_t) * slen.size(), cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(cn.vrow, vrow.data(), sizeof(uint32_t) * vrow.size(), cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(cn.split_row, split_row.data(), sizeof(uint32_t) * split_row.size(),
+                               cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(cn.split_slot, split_slot.data(), sizeof(uint32_t) * split_slot.size(),
+                               cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // host vectors die at return
+  return 0;
 }
 
 int build_one(Ctx* c, int spin) {
@@ -252,6 +353,10 @@ int build_one(Ctx* c, int spin) {
     SBDX_CUDA(c, cudaMemcpyAsync(cn.soff, soff.data(), sizeof(uint64_t) * (ns + 1), cudaMemcpyHostToDevice, c->stream));
     if (ns) SBDX_CUDA(c, cudaMemcpyAsync(cn.slen, slen.data(), sizeof(uint32_t) * ns, cudaMemcpyHostToDevice, c->stream));
     SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (spin == 1) {
+      const int rc = build_balanced_sell(c, cn, hs, off, order, rec);
+      if (rc) return rc;
+    }
   }
   // the host copy of `off` must stay alive until the async copy ran
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -263,6 +368,9 @@ int build_one(Ctx* c, int spin) {
 void free_connectivity(Ctx* c) {
   free_conn(c->conn[0]);
   free_conn(c->conn[1]);
+  cudaFree(c->d_Da); cudaFree(c->d_Db); cudaFree(c->d_Da32); cudaFree(c->d_Db32);
+  c->d_Da = c->d_Db = nullptr;
+  c->d_Da32 = c->d_Db32 = nullptr;
   c->have_conn = false;
 }
 
@@ -274,6 +382,8 @@ int build_connectivity(Ctx* c) {
   int rc = build_one(c, 0);
   if (rc) return rc;
   rc = build_one(c, 1);
+  if (rc) return rc;
+  rc = build_coulomb_tables(c);
   if (rc) return rc;
   c->have_conn = true;
   return 0;

@@ -60,7 +60,27 @@ struct Conn {
   uint64_t* soff = nullptr;   // [nslice + 1]
   uint32_t* slen = nullptr;   // [nslice] records per lane of each slice
   size_t nslice = 0;
+  // balanced SELL-32 of the single-excitation records (beta spin only), read
+  // by the alpha-first alpha-beta kernel. A bra string with more than `cap`
+  // singles is split into equal parts ("virtual rows") of at most `cap`
+  // records; the split parts come first, then the unsplit rows longest first.
+  // vrow[v]: bits 0-15 bra string, bits 16-31 = 1 + partial-sum slot of a
+  // split part (0 for an unsplit row). The parts of split string s occupy
+  // slots split_slot[s] .. split_slot[s+1]-1 and are summed in that order.
+  uint64_t* bsell = nullptr;      // [bsoff[bnslice]]
+  uint64_t* bsoff = nullptr;      // [bnslice + 1]
+  uint32_t* bslen = nullptr;      // [bnslice]
+  uint32_t* vrow = nullptr;       // [nv]
+  uint32_t* split_row = nullptr;  // [nsplit]
+  uint32_t* split_slot = nullptr; // [nsplit + 1]
+  size_t bnslice = 0, nv = 0;
+  int nsplit = 0, nslot = 0, cap = 0;
+  int slices_per_warp = 8;        // 8, 12 or 16: virtual rows per CTA = 1024 * this
 };
+
+// Largest number of partial-sum slots of split rows (shared memory of the
+// alpha-first alpha-beta kernel: 8 bytes each).
+constexpr int kMaxSplitSlots = 2048;
 
 // Launch shape of the sigma kernels. Codes (also the C-ABI encoding):
 //   same-spin: 1/2/4/8 = columns per thread of the prefix-parity-table kernel,
@@ -104,8 +124,16 @@ struct Ctx {
   // diagonal
   double* d_hii = nullptr;
   bool have_hii = false;
+  // opposite-spin Coulomb term of single excitations in the alpha-first
+  // sigma: Db[pq * db_stride + ib] = sum_{q in beta(ib)} (pq|qq) (alpha
+  // singles), Da[pq * da_stride + ia] = sum_{p in alpha(ia)} (pq|pp) (beta
+  // singles); FP64 and FP32 copies; built with the connectivity
+  double *d_Da = nullptr, *d_Db = nullptr;
+  float *d_Da32 = nullptr, *d_Db32 = nullptr;
+  size_t da_stride = 0, db_stride = 0;
   // sigma scratch (sized for D): transposed input, FP64 partial outputs
   void* d_xt = nullptr;     // D elements of the widest type used (8 B)
+  void* d_xp = nullptr;     // D elements (8 B): phi o C, the input in the alpha-first basis
   double* d_y = nullptr;    // D FP64: alpha-major partial sigma
   double* d_yt = nullptr;   // D FP64: beta-major partial sigma
   void* d_io_in = nullptr;  // D FP64 staging for host-buffer entry points
@@ -181,6 +209,18 @@ __device__ __forceinline__ uint64_t prefix_parity(uint64_t s) {
   return s;
 }
 
+// Sign of determinant (alpha, beta) of the reference's interleaved ordering
+// (alpha p -> spin orbital 2p, beta p -> 2p+1) relative to the alpha-first
+// ordering (all alpha spin orbitals before all beta ones): the parity of the
+// number of pairs (alpha p, beta q) with q < p, which is
+// parity(beta & prefix_parity(alpha)) up to the basis-wide constant
+// (-1)^{n_alpha n_beta}. Returns 1 for a minus sign. With C' = phi o C, every
+// sign of H in the alpha-first basis is a pure same-spin sign, and
+// H C = phi o (H' C').
+__device__ __forceinline__ uint32_t basis_phase(uint64_t alpha_prefix_parity, uint64_t beta) {
+  return (uint32_t)__popcll(beta & alpha_prefix_parity) & 1u;
+}
+
 // Opposite-spin parity mask of one occupied-range term of the reference
 // parity() (chemistry/basic/determinants.h:228-279) for a same-spin pair of
 // spatial orbitals x < y of spin `spin`: the opposite-spin orbitals whose
@@ -193,6 +233,7 @@ __host__ __device__ __forceinline__ uint64_t other_range(int spin, int x, int y)
 int build_connectivity(Ctx* c);
 void free_connectivity(Ctx* c);
 int build_g_table(Ctx* c);
+int build_coulomb_tables(Ctx* c);
 int diag_terms(Ctx* c);
 // sigma: X (na x nb, type by precision: 0 = FP64, 1 = FP32) -> S (same type)
 int sigma_device(Ctx* c, int precision, const void* X, void* S);

@@ -993,8 +993,409 @@ int run_ab(Ctx* c, const T* X) {
   return launch_ab2<T, 1>(c, X, smem, stride, threads);
 }
 
+// ---- alpha-first sigma (v6) -----------------------------------------------------
+//
+// The sigma is evaluated in the alpha-first determinant ordering: with the
+// +-1 basis phase phi (basis_phase), H C = phi o (H' (phi o C)) where every
+// sign of H' is a pure same-spin sign. So the same-spin kernels need no
+// opposite-spin parity per pair, and the alpha-beta sign is the product of the
+// two same-spin signs stored with the connectivity. The opposite-spin Coulomb
+// term of a single excitation, sum_{q in other} (pq|qq), is read from the
+// per-string Coulomb tables (Ctx::d_Da / d_Db) instead of being summed per pair.
+//   0. Xp = phi o X and Xpt = (phi o X)^T            (phase_split_kernel)
+//   1. alpha same-spin + diagonal on Xp -> Y          (sigma_same_v6_kernel)
+//   2. beta same-spin on Xpt -> Yt                    (sigma_same_v6_kernel)
+//   3. alpha single x beta single on Xp -> Y +=       (sigma_ab_v6_kernel)
+//   4. S = phi o (Y + Yt^T)                           (combine_phase_kernel)
+
 template <typename T>
-int run_sigma(Ctx* c, const T* X, T* S) {
+__global__ void phase_split_kernel(const T* __restrict__ X, size_t na, size_t nb, const uint64_t* __restrict__ astr,
+                                   const uint64_t* __restrict__ bstr, T* __restrict__ Xp, T* __restrict__ Xpt) {
+  __shared__ T tile[32][33];
+  __shared__ uint64_t s_pa[32], s_b[32];
+  const size_t ib0 = (size_t)blockIdx.x * 32, ia0 = (size_t)blockIdx.y * 32;
+  const int tx = threadIdx.x;
+  if (threadIdx.y == 0) {
+    s_pa[tx] = ia0 + tx < na ? prefix_parity(astr[ia0 + tx]) : 0ull;
+    s_b[tx] = ib0 + tx < nb ? bstr[ib0 + tx] : 0ull;
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const size_t ia = ia0 + k, ib = ib0 + tx;
+    if (ia < na && ib < nb) {
+      T v = X[ia * nb + ib];
+      if (basis_phase(s_pa[k], s_b[tx])) v = -v;
+      Xp[ia * nb + ib] = v;
+      tile[k][tx] = v;
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const size_t ib = ib0 + k, ia = ia0 + tx;
+    if (ia < na && ib < nb) Xpt[ib * na + ia] = tile[tx][k];
+  }
+}
+
+// S[ia, ib] = phi(ia, ib) (Y[ia, ib] + Yt[ib, ia]), stored in T.
+template <typename T>
+__global__ void combine_phase_kernel(const double* __restrict__ Y, const double* __restrict__ Yt, size_t na,
+                                     size_t nb, const uint64_t* __restrict__ astr, const uint64_t* __restrict__ bstr,
+                                     T* __restrict__ S) {
+  __shared__ double tile[32][33];
+  __shared__ uint64_t s_pa[32], s_b[32];
+  const size_t ib0 = (size_t)blockIdx.x * 32, ia0 = (size_t)blockIdx.y * 32;
+  const int tx = threadIdx.x;
+  if (threadIdx.y == 0) {
+    s_pa[tx] = ia0 + tx < na ? prefix_parity(astr[ia0 + tx]) : 0ull;
+    s_b[tx] = ib0 + tx < nb ? bstr[ib0 + tx] : 0ull;
+  }
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const size_t ib = ib0 + k, ia = ia0 + tx;
+    if (ib < nb && ia < na) tile[tx][k] = Yt[ib * na + ia];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const size_t ia = ia0 + k, ib = ib0 + tx;
+    if (ia < na && ib < nb) {
+      const double y = Y[ia * nb + ib] + tile[k][tx];
+      S[ia * nb + ib] = (T)(basis_phase(s_pa[k], s_b[tx]) ? -y : y);
+    }
+  }
+}
+
+// D[pq * stride + k] = sum over the orbitals q < L of string k of (pq|qq).
+__global__ void coulomb_table_kernel(const double* __restrict__ G, int L, const uint64_t* __restrict__ s, size_t n,
+                                     size_t stride, double* __restrict__ D, float* __restrict__ D32) {
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t pq = blockIdx.y;
+  if (k >= n) return;
+  const double* g = G + pq * (size_t)L;
+  uint64_t bits = s[k] & range_mask(0, L);
+  double v = 0.0;
+  while (bits) {
+    const int q = __ffsll((long long)bits) - 1;
+    bits &= bits - 1;
+    v += g[q];
+  }
+  D[pq * stride + k] = v;
+  D32[pq * stride + k] = (float)v;
+}
+
+// Same-spin excitations in the alpha-first basis, VEC consecutive columns per
+// thread; grid x = bra row (fastest: the resident CTAs share one column strip
+// of the ket rows, which stays in L2), y = column strip. A CTA stages the
+// entries of its row (ket, signed value, signed pair index) in shared memory;
+// per pair a double costs one FMA and a single one add (the Coulomb table
+// element of its column) and one FMA. Requires ncol % VEC == 0.
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kSameThreads)
+sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __restrict__ off,
+                     const uint32_t* __restrict__ nsing, const uint32_t* __restrict__ ket,
+                     const typename Prec<T>::V* __restrict__ val, const uint32_t* __restrict__ info,
+                     const typename Prec<T>::V* __restrict__ Dt, size_t dstride, const double* __restrict__ hii,
+                     double* __restrict__ Y) {
+  __shared__ uint32_t s_ket[kSameThreads], s_pq[kSameThreads];
+  __shared__ double s_val[kSameThreads];
+  const size_t r = blockIdx.x;
+  const size_t c0 = ((size_t)blockIdx.y * kSameThreads + threadIdx.x) * VEC;
+  const bool active = c0 < ncol;
+  double acc[VEC];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) acc[v] = 0.0;
+  if (hii != nullptr && active) {
+    double x[VEC];
+    VecIO<T, VEC>::load(X + r * ncol + c0, x);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = hii[r * ncol + c0 + v] * x[v];
+  }
+  const uint64_t beg = off[r], end = off[r + 1], send = beg + nsing[r];
+  const unsigned t = threadIdx.x;
+  for (uint64_t base = beg; base < end; base += kSameThreads) {
+    const int cnt = (int)min((uint64_t)kSameThreads, end - base);
+    const int nsb = send > base ? (int)min((uint64_t)cnt, send - base) : 0;
+    __syncthreads();
+    if ((int)t < cnt) {
+      const uint64_t e = base + t;
+      const uint32_t inf = info[e];
+      const double v = (double)val[e];
+      s_ket[t] = ket[e];
+      s_val[t] = (inf >> 31) ? -v : v;
+      s_pq[t] = ((inf >> 12) & 0xfffu) | (inf & kInfoNeg);
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (int e = 0; e < nsb; ++e) {
+      const uint32_t pqs = s_pq[e];
+      const double hv = s_val[e];
+      double x[VEC], d[VEC];
+      VecIO<T, VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+      VecIO<T, VEC>::load(Dt + (size_t)(pqs & 0xfffu) * dstride + c0, d);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) acc[v] = fma(hv + flip_sign(d[v], pqs >> 31), x[v], acc[v]);
+    }
+#pragma unroll 4
+    for (int e = nsb; e < cnt; ++e) {
+      const double hv = s_val[e];
+      double x[VEC];
+      VecIO<T, VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) acc[v] = fma(hv, x[v], acc[v]);
+    }
+  }
+  if (active) {
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) Y[r * ncol + c0 + v] = acc[v];
+  }
+}
+
+constexpr int kAb6Threads = 1024;
+
+// Alpha single x beta single in the alpha-first basis, balanced. One CTA per
+// (bra alpha row ia, chunk of 1024*KS virtual rows of the balanced beta SELL).
+// Per group of R alpha singles ja of ia: the ket rows Xp[ja, :] and the
+// integral rows (ai|..) of the unpacked table are copied to shared memory with
+// 16-byte loads; lane l of a warp owns virtual row 32s+l of slice s and walks
+// its records (contiguous 256-byte warp reads), applying each to the R staged
+// rows: sign = s_alpha(ia,ja) xor s_beta(ib,jb), both from the connectivity.
+// Warp w owns slices w, 2*32-1-w, 2*32+w, ... (a snake over the length-sorted
+// slices). Unsplit virtual rows add their sum to Y directly; split parts park
+// theirs in shared memory and are added in slot order (deterministic). All
+// split parts lie in chunk 0.
+template <typename T, int R, int KS>
+__global__ void __launch_bounds__(kAb6Threads, 1)
+sigma_ab_v6_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restrict__ a_off,
+                   const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
+                   const uint32_t* __restrict__ a_info, const uint64_t* __restrict__ sell,
+                   const uint64_t* __restrict__ soff, const uint32_t* __restrict__ slen, size_t nslice,
+                   const uint32_t* __restrict__ vrow, size_t nv, const uint32_t* __restrict__ split_row,
+                   const uint32_t* __restrict__ split_slot, int nsplit,
+                   const typename Prec<T>::V* __restrict__ Vt, size_t vstride, size_t xstride,
+                   double* __restrict__ Y) {
+  using V = typename Prec<T>::V;
+  constexpr int kWarps = kAb6Threads / 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* xs = reinterpret_cast<T*>(smem);                                               // [R][xstride]
+  V* erow = reinterpret_cast<V*>(smem + sizeof(T) * xstride * R);                   // [R][vstride]
+  double* part = reinterpret_cast<double*>(smem + sizeof(T) * xstride * R + sizeof(V) * vstride * R);
+  __shared__ uint32_t s_sa[R];
+  const size_t ia = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t slice0 = (size_t)blockIdx.y * kWarps * KS;
+  auto slice_of = [&](int k) -> size_t {
+    return slice0 + (size_t)k * kWarps + ((k & 1) ? (kWarps - 1 - warp) : warp);
+  };
+  double acc[KS];
+#pragma unroll
+  for (int k = 0; k < KS; ++k) acc[k] = 0.0;
+  const uint64_t e0 = a_off[ia];
+  const int ns = (int)a_nsing[ia];
+  const size_t xv = nb * sizeof(T) / 16;        // 16-byte vectors of a ket row (xstride covers the tail)
+  const size_t ev = vstride * sizeof(V) / 16;   // 16-byte vectors of an integral row
+  for (int k0 = 0; k0 < ns; k0 += R) {
+    const int nr = min(R, ns - k0);
+    __syncthreads();
+    if ((int)threadIdx.x < nr) s_sa[threadIdx.x] = a_info[e0 + k0 + threadIdx.x] >> 31;
+    for (int rr = 0; rr < nr; ++rr) {
+      const uint64_t e = e0 + k0 + rr;
+      const T* src = Xp + (size_t)a_ket[e] * nb;
+      T* dst = xs + (size_t)rr * xstride;
+      if ((nb * sizeof(T)) % 16 == 0) {
+        const uint4* s4 = reinterpret_cast<const uint4*>(src);
+        uint4* d4 = reinterpret_cast<uint4*>(dst);
+        for (size_t t = threadIdx.x; t < xv; t += kAb6Threads) d4[t] = __ldg(s4 + t);
+      } else {
+        for (size_t t = threadIdx.x; t < nb; t += kAb6Threads) dst[t] = src[t];
+      }
+      const uint4* v4 = reinterpret_cast<const uint4*>(Vt + (size_t)((a_info[e] >> 12) & 0xfffu) * vstride);
+      uint4* ed = reinterpret_cast<uint4*>(erow + (size_t)rr * vstride);
+      for (size_t t = threadIdx.x; t < ev; t += kAb6Threads) ed[t] = __ldg(v4 + t);
+    }
+    __syncthreads();
+    uint32_t sa[R];
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) sa[rr] = rr < nr ? s_sa[rr] : 0u;
+#pragma unroll
+    for (int k = 0; k < KS; ++k) {
+      const size_t sl = slice_of(k);
+      if (sl >= nslice) continue;
+      const uint32_t len = slen[sl];
+      const uint64_t* rp = sell + soff[sl] + lane;
+      double s = acc[k];
+      uint64_t next = len ? __ldg(rp) : 0ull;
+      for (uint32_t m = 0; m < len; ++m) {
+        const uint64_t rec = next;
+        if (m + 1 < len) next = __ldg(rp + 32ull * (m + 1));
+        const uint32_t jb = (uint32_t)(rec & 0xffffu);
+        const uint32_t pq = (uint32_t)((rec >> 16) & 0xfffu);
+        const uint32_t sb = (uint32_t)(rec >> 40) & 1u;
+        const bool pad = (rec >> 41) & 1ull;
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) {
+          if (rr < nr) {
+            const double v = pad ? 0.0 : (double)erow[(size_t)rr * vstride + pq];
+            s = fma(flip_sign(v, sa[rr] ^ sb), (double)xs[(size_t)rr * xstride + jb], s);
+          }
+        }
+      }
+      acc[k] = s;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < KS; ++k) {
+    const size_t sl = slice_of(k);
+    const size_t pos = sl * 32 + lane;
+    if (sl < nslice && pos < nv) {
+      const uint32_t w = vrow[pos];
+      const uint32_t slot1 = w >> 16;
+      if (slot1 == 0) Y[ia * nb + (w & 0xffffu)] += acc[k];
+      else part[slot1 - 1] = acc[k];
+    }
+  }
+  if (blockIdx.y == 0 && nsplit > 0) {
+    __syncthreads();
+    for (int s = threadIdx.x; s < nsplit; s += kAb6Threads) {
+      double t = 0.0;
+      for (uint32_t j = split_slot[s]; j < split_slot[s + 1]; ++j) t += part[j];
+      Y[ia * nb + split_row[s]] += t;
+    }
+  }
+}
+
+template <typename T, int VEC>
+int launch_same_v6(Ctx* c, const T* X, size_t nrow, size_t ncol, const Conn& cn, const typename Prec<T>::V* val,
+                   const typename Prec<T>::V* Dt, size_t dstride, const double* hii, double* Y) {
+  dim3 grid((unsigned)nrow, (unsigned)((ncol + (size_t)kSameThreads * VEC - 1) / ((size_t)kSameThreads * VEC)));
+  sigma_same_v6_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, cn.off, cn.nsing, cn.ket, val, cn.info,
+                                                                     Dt, dstride, hii, Y);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+// v6 same-spin codes: 21, 22, 24, 28 = 1, 2, 4, 8 columns per thread, narrowed
+// to the widest vector that divides the row and keeps 16-byte alignment.
+template <typename T>
+int run_same_v6(Ctx* c, int code, const T* X, size_t nrow, size_t ncol, const Conn& cn,
+                const typename Prec<T>::V* val, const typename Prec<T>::V* Dt, size_t dstride, const double* hii,
+                double* Y) {
+  int vec = code % 10;
+  const bool aligned = (reinterpret_cast<uintptr_t>(X) % 16) == 0;
+  while (vec > 1 && (!aligned || ncol % vec != 0)) vec >>= 1;
+  if (vec >= 8) return launch_same_v6<T, 8>(c, X, nrow, ncol, cn, val, Dt, dstride, hii, Y);
+  if (vec >= 4) return launch_same_v6<T, 4>(c, X, nrow, ncol, cn, val, Dt, dstride, hii, Y);
+  if (vec == 2) return launch_same_v6<T, 2>(c, X, nrow, ncol, cn, val, Dt, dstride, hii, Y);
+  return launch_same_v6<T, 1>(c, X, nrow, ncol, cn, val, Dt, dstride, hii, Y);
+}
+
+template <typename T, int R, int KS>
+int launch_ab_v6(Ctx* c, const T* Xp, size_t smem, size_t xstride) {
+  using V = typename Prec<T>::V;
+  const Conn& ca = c->conn[0];
+  const Conn& cb = c->conn[1];
+  const bool f64 = std::is_same<T, double>::value;
+  const V* Vt = f64 ? (const V*)c->d_V : (const V*)c->d_V32;
+  const size_t vs = f64 ? c->vstride : c->vstride32;
+  SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v6_kernel<T, R, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  const size_t per_cta = (size_t)(kAb6Threads / 32) * KS;  // slices
+  dim3 grid((unsigned)c->na, (unsigned)((cb.bnslice + per_cta - 1) / per_cta));
+  if (grid.y == 0) grid.y = 1;
+  sigma_ab_v6_kernel<T, R, KS><<<grid, kAb6Threads, smem, c->stream>>>(
+      Xp, c->nb, ca.off, ca.nsing, ca.ket, ca.info, cb.bsell, cb.bsoff, cb.bslen, cb.bnslice, cb.vrow, cb.nv,
+      cb.split_row, cb.split_slot, cb.nsplit, Vt, vs, xstride, c->d_y);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+template <typename T, int R>
+int launch_ab_v6_ks(Ctx* c, const T* Xp, size_t smem, size_t xstride) {
+  const int ks = c->conn[1].slices_per_warp;
+  if (ks >= 16) return launch_ab_v6<T, R, 16>(c, Xp, smem, xstride);
+  if (ks >= 12) return launch_ab_v6<T, R, 12>(c, Xp, smem, xstride);
+  return launch_ab_v6<T, R, 8>(c, Xp, smem, xstride);
+}
+
+// v6 alpha-beta codes: 61-64 = 1-4 staged alpha singles per group, narrowed
+// until the ket rows, integral rows and split slots fit in shared memory.
+template <typename T>
+int run_ab_v6(Ctx* c, int code, const T* Xp) {
+  using V = typename Prec<T>::V;
+  const bool f64 = std::is_same<T, double>::value;
+  const size_t vs = f64 ? c->vstride : c->vstride32;
+  const size_t per = 16 / sizeof(T);
+  const size_t xstride = (c->nb + per - 1) / per * per;
+  const size_t budget = 227 * 1024 - 1024;  // dynamic part; the static part is a few bytes
+  const size_t extra = sizeof(double) * (size_t)c->conn[1].nslot;
+  int R = code % 10 > 0 ? code % 10 : 2;
+  size_t smem = 0;
+  for (; R >= 1; --R) {
+    smem = (size_t)R * (sizeof(T) * xstride + sizeof(V) * vs) + extra;
+    if (smem <= budget) break;
+  }
+  if (R < 1) {
+    c->err = "sigma: beta dimension too large for one shared-memory ket row";
+    return 1;
+  }
+  if (R >= 4) return launch_ab_v6_ks<T, 4>(c, Xp, smem, xstride);
+  if (R == 3) return launch_ab_v6_ks<T, 3>(c, Xp, smem, xstride);
+  if (R == 2) return launch_ab_v6_ks<T, 2>(c, Xp, smem, xstride);
+  return launch_ab_v6_ks<T, 1>(c, Xp, smem, xstride);
+}
+
+bool is_v6(const Tune& t) { return t.same_code > 20 && t.same_code < 30 && t.ab_code > 60 && t.ab_code < 70; }
+
+template <typename T>
+int run_sigma_v6(Ctx* c, const Tune& tune, const T* X, T* S) {
+  using V = typename Prec<T>::V;
+  const size_t na = c->na, nb = c->nb;
+  const bool f64 = std::is_same<T, double>::value;
+  const Conn& ca = c->conn[0];
+  const Conn& cb = c->conn[1];
+  const V* valA = f64 ? (const V*)ca.val : (const V*)ca.val32;
+  const V* valB = f64 ? (const V*)cb.val : (const V*)cb.val32;
+  const V* Db = f64 ? (const V*)c->d_Db : (const V*)c->d_Db32;
+  const V* Da = f64 ? (const V*)c->d_Da : (const V*)c->d_Da32;
+  T* xp = reinterpret_cast<T*>(c->d_xp);
+  T* xpt = reinterpret_cast<T*>(c->d_xt);
+  auto mark = [&](int k) {
+    if (c->profiling) cudaEventRecord(c->ev[k], c->stream);
+  };
+  int rc = 0;
+  mark(0);
+  {
+    dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((na + 31) / 32));
+    phase_split_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(X, na, nb, c->d_a, c->d_b, xp, xpt);
+    SBDX_LAUNCHED(c);
+  }
+  mark(1);
+  if ((rc = run_same_v6<T>(c, tune.same_code, xp, na, nb, ca, valA, Db, c->db_stride, c->d_hii, c->d_y))) return rc;
+  mark(2);
+  if ((rc = run_same_v6<T>(c, tune.same_code, xpt, nb, na, cb, valB, Da, c->da_stride, nullptr, c->d_yt))) return rc;
+  mark(3);
+  if ((rc = run_ab_v6<T>(c, tune.ab_code, xp))) return rc;
+  mark(4);
+  {
+    dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((na + 31) / 32));
+    combine_phase_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(c->d_y, c->d_yt, na, nb, c->d_a, c->d_b, S);
+    SBDX_LAUNCHED(c);
+  }
+  mark(5);
+  if (c->profiling) {
+    // reported in the phase order alpha same-spin, transpose (here the phase
+    // split), beta same-spin, alpha-beta, combine
+    const int from[kSigmaPhases] = {1, 0, 2, 3, 4};
+    SBDX_CUDA(c, cudaEventSynchronize(c->ev[5]));
+    for (int k = 0; k < kSigmaPhases; ++k) {
+      float ms = 0.f;
+      SBDX_CUDA(c, cudaEventElapsedTime(&ms, c->ev[from[k]], c->ev[from[k] + 1]));
+      c->phase_ms[k] += ms;
+    }
+    ++c->phase_calls;
+  }
+  return 0;
+}
+
+template <typename T>
+int run_sigma_v5(Ctx* c, const T* X, T* S) {
   using V = typename Prec<T>::V;
   const size_t na = c->na, nb = c->nb;
   const Conn& ca = c->conn[0];
@@ -1043,7 +1444,53 @@ int run_sigma(Ctx* c, const T* X, T* S) {
   return 0;
 }
 
+// Default launch codes: the alpha-first (v6) kernels.
+constexpr Tune kDefaultTune[2] = {{24, 62}, {28, 64}};
+
+Tune effective_tune(const Ctx* c, bool f64) {
+  Tune t = c->tune[f64 ? 0 : 1];
+  const Tune& d = kDefaultTune[f64 ? 0 : 1];
+  const bool v6 = (t.same_code > 20 && t.same_code < 30) || (t.ab_code > 60 && t.ab_code < 70) ||
+                  (t.same_code == 0 && t.ab_code == 0);
+  if (v6) {
+    if (t.same_code == 0) t.same_code = d.same_code;
+    if (t.ab_code == 0) t.ab_code = d.ab_code;
+  }
+  return t;
+}
+
+template <typename T>
+int run_sigma(Ctx* c, const T* X, T* S) {
+  const Tune t = effective_tune(c, std::is_same<T, double>::value);
+  if (is_v6(t)) return run_sigma_v6<T>(c, t, X, S);
+  return run_sigma_v5<T>(c, X, S);
+}
+
 }  // namespace
+
+int build_coulomb_tables(Ctx* c) {
+  cudaFree(c->d_Da); cudaFree(c->d_Db); cudaFree(c->d_Da32); cudaFree(c->d_Db32);
+  c->d_Da = c->d_Db = nullptr;
+  c->d_Da32 = c->d_Db32 = nullptr;
+  c->da_stride = (c->na + 7) / 8 * 8;
+  c->db_stride = (c->nb + 7) / 8 * 8;
+  const size_t na_el = c->npair * c->da_stride, nb_el = c->npair * c->db_stride;
+  SBDX_CUDA(c, cudaMalloc(&c->d_Da, sizeof(double) * na_el));
+  SBDX_CUDA(c, cudaMalloc(&c->d_Db, sizeof(double) * nb_el));
+  SBDX_CUDA(c, cudaMalloc(&c->d_Da32, sizeof(float) * na_el));
+  SBDX_CUDA(c, cudaMalloc(&c->d_Db32, sizeof(float) * nb_el));
+  SBDX_CUDA(c, cudaMemsetAsync(c->d_Da, 0, sizeof(double) * na_el, c->stream));
+  SBDX_CUDA(c, cudaMemsetAsync(c->d_Db, 0, sizeof(double) * nb_el, c->stream));
+  SBDX_CUDA(c, cudaMemsetAsync(c->d_Da32, 0, sizeof(float) * na_el, c->stream));
+  SBDX_CUDA(c, cudaMemsetAsync(c->d_Db32, 0, sizeof(float) * nb_el, c->stream));
+  dim3 ga((unsigned)((c->na + 255) / 256), (unsigned)c->npair);
+  coulomb_table_kernel<<<ga, 256, 0, c->stream>>>(c->d_G, c->L, c->d_a, c->na, c->da_stride, c->d_Da, c->d_Da32);
+  SBDX_LAUNCHED(c);
+  dim3 gb((unsigned)((c->nb + 255) / 256), (unsigned)c->npair);
+  coulomb_table_kernel<<<gb, 256, 0, c->stream>>>(c->d_G, c->L, c->d_b, c->nb, c->db_stride, c->d_Db, c->d_Db32);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
 
 int build_g_table(Ctx* c) {
   const size_t n = c->npair * (size_t)c->L;
@@ -1075,6 +1522,7 @@ int build_g_table(Ctx* c) {
 int ensure_sigma_scratch(Ctx* c) {
   const size_t D = c->na * c->nb;
   if (!c->d_xt) SBDX_CUDA(c, cudaMalloc(&c->d_xt, sizeof(double) * D));
+  if (!c->d_xp) SBDX_CUDA(c, cudaMalloc(&c->d_xp, sizeof(double) * D));
   if (!c->d_y) SBDX_CUDA(c, cudaMalloc(&c->d_y, sizeof(double) * D));
   if (!c->d_yt) SBDX_CUDA(c, cudaMalloc(&c->d_yt, sizeof(double) * D));
   return 0;
@@ -1098,8 +1546,8 @@ int autotune(Ctx* c) {
   if (!c->ev[0])
     for (auto& e : c->ev) SBDX_CUDA(c, cudaEventCreate(&e));
   c->profiling = true;
-  const int same_cand[] = {14, 12, 11, 8, 4, 2, 1};
-  const int ab_cand[] = {42, 43, 41, 44, 12, 13, 14, 11, 22, 21, 32, 31};
+  const int same_cand[] = {24, 28, 22};
+  const int ab_cand[] = {62, 61, 63, 64};
   for (int prec = 0; prec < 2 && rc == 0; ++prec) {
     const Tune saved = c->tune[prec];
     auto measure = [&](int same, int ab, double* same_ms, double* ab_ms) -> int {
@@ -1121,7 +1569,7 @@ int autotune(Ctx* c) {
     double t_same = 1e300, t_ab = 1e300;
     for (int sc : same_cand) {
       double sm = 0, ab = 0;
-      if ((rc = measure(sc, 42, &sm, &ab))) break;
+      if ((rc = measure(sc, ab_cand[0], &sm, &ab))) break;
       if (sm < t_same) { t_same = sm; best_same = sc; }
     }
     for (int ac : ab_cand) {

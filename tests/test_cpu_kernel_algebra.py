@@ -133,3 +133,69 @@ def test_kernel_algebra_equals_reference_rules(spec):
         if n_checked > 6000:
             break
     assert n_checked > 500
+
+
+def basis_phase(alpha_s, beta_s):
+    """phi(alpha, beta) of the alpha-first ordering: the parity of the number of
+    (alpha p, beta q) pairs with q < p, up to the basis-wide constant
+    (-1)^{n_alpha n_beta}; equal to parity(beta & prefix_parity(alpha))."""
+    return popc(beta_s & prefix_parity(alpha_s)) & 1
+
+
+def separated_element(prob, spin_pairs):
+    """H_IJ in the alpha-first ordering, where every sign is a pure same-spin
+    sign: ((spin, bra, ket), ...) for the excited spins, plus the opposite-spin
+    string of a same-spin excitation for the single's Coulomb term."""
+    if len(spin_pairs) == 2:  # alpha single x beta single
+        (_, ia_s, ja_s), (_, ib_s, jb_s) = spin_pairs
+        ea = entry(prob, 0, ia_s, ja_s)
+        eb = entry(prob, 1, ib_s, jb_s)
+        v = eri(prob, ea["a"], ea["i"], eb["a"], eb["i"])
+        return -v if ea["neg"] ^ eb["neg"] else v
+    ((spin, sr, sk, other),) = spin_pairs
+    e = entry(prob, spin, sr, sk)
+    v = e["val"]
+    if e["single"]:  # the opposite-spin Coulomb table entry D[pq(a,i)][other]
+        v += sum(eri(prob, e["a"], e["i"], q, q) for q in range(prob.L) if (other >> q) & 1)
+    return -v if e["neg"] else v
+
+
+@pytest.mark.parametrize("spec", [(8, 3, 2, 40, 25, 3), (12, 4, 4, 60, 60, 5), (16, 2, 5, 30, 80, 9),
+                                  (64, 3, 3, 40, 40, 11)])
+def test_alpha_first_basis_factorises_signs(spec):
+    """H_int[I,J] = phi(I) phi(J) H_sep[I,J]: the interleaved matrix elements of
+    the reference are the alpha-first ones conjugated by the +-1 basis phase,
+    and in the alpha-first basis the opposite-spin string enters no sign."""
+    L, na_el, nb_el, Na, Nb, seed = spec
+    prob = synth.random_problem(L, na_el, nb_el, Na, Nb, seed=seed)
+    port = Port()
+    a = [int(x) for x in prob.alpha]
+    b = [int(x) for x in prob.beta]
+    rng = np.random.default_rng(seed + 100)
+    n_checked = 0
+
+    def check(x, y, z, w, pairs):
+        nonlocal n_checked
+        ref = port.hij(prob, a[x], b[y], a[z], b[w])
+        flip = basis_phase(a[x], b[y]) ^ basis_phase(a[z], b[w])
+        sep = separated_element(prob, pairs)
+        assert abs((-sep if flip else sep) - ref) <= 1e-12
+        n_checked += 1
+
+    for _ in range(300):
+        x, y = int(rng.integers(prob.na)), int(rng.integers(prob.nb))
+        for z in range(prob.na):
+            if popc(a[x] ^ a[z]) in (2, 4):
+                check(x, y, z, y, [(0, a[x], a[z], b[y])])
+        for w in range(prob.nb):
+            if popc(b[y] ^ b[w]) in (2, 4):
+                check(x, y, x, w, [(1, b[y], b[w], a[x])])
+        for z in range(prob.na):
+            if popc(a[x] ^ a[z]) != 2:
+                continue
+            for w in range(prob.nb):
+                if popc(b[y] ^ b[w]) == 2:
+                    check(x, y, z, w, [(0, a[x], a[z]), (1, b[y], b[w])])
+        if n_checked > 6000:
+            break
+    assert n_checked > 500

@@ -60,6 +60,39 @@ def test_diag_and_sigma_fp64(spec, port):
         assert np.abs(S - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+# Workloads whose beta single-excitation lists are very uneven (near-Aufbau
+# strings connect to many more strings than the mean), so the balanced
+# alpha-beta layout splits lists; the last one needs two CTAs per alpha row.
+SKEWED = [("cfg4", 0.25, None), ("cfg1", 1.0, None), ("wide", 20, 17000)]
+_SKEWED_CACHE = {}
+
+
+def _skewed(name, scale, nb):
+    if name == "wide":  # few alpha strings x 17000 beta strings (L=20, 6 electrons)
+        I0, h, eri = synth.make_integrals(20, 8, seed=91)
+        return synth.Problem(L=20, nelec=12, I0=I0, h=h, eri=eri, alpha=synth.sample_strings(20, 6, scale, 92),
+                             beta=synth.sample_strings(20, 6, nb, 93))
+    return synth.config(name, scale)
+
+
+@pytest.mark.parametrize("name,scale,nb", SKEWED)
+@pytest.mark.parametrize("tuning", [(0, 0), (21, 61), (28, 64), (14, 42)])
+def test_sigma_split_lists_and_orderings(name, scale, nb, tuning, port):
+    """Default (alpha-first, balanced) and explicit launch codes, including the
+    interleaved kernels, against the oracle."""
+    key = (name, scale, nb)
+    if key not in _SKEWED_CACHE:
+        prob = _skewed(name, scale, nb)
+        C = np.random.default_rng(3).standard_normal(prob.D)
+        _SKEWED_CACHE[key] = (prob, C, port.sigma(prob, C))
+    prob, C, ref = _SKEWED_CACHE[key]
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        ctx.set_tuning(*tuning)
+        S = ctx.sigma(C)
+    assert np.abs(S - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
 def test_sigma_fp32_storage(port):
     torch = pytest.importorskip("torch")
     prob = _prob(PROBLEMS[3])
