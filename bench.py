@@ -12,9 +12,12 @@ with C resident in HBM (CUDA events on the launching stream, max over ranks);
 C (512 MB) is larger than the 126 MB L2, so no flush is needed between steps.
 `e2e` times the same product through the C-ABI call sbdx_sigma with pinned
 host buffers, the host->device copy of C and the device->host copy of S inside
-every step. The roofline uses the algorithmic bytes of one sigma,
-B = P*s_c + D*(2*s_c + s_h) + 4*(connectivity entries) + 8*(na + nb), against
-the measured HBM copy bandwidth. The CPU baseline is the reference's own
+every step. `roofline` describes the dominant kernel of the sigma (the
+alpha-beta kernel): its algorithmic bytes per launch, one vector gather per
+alpha-single x beta-single pair plus the read-modify-write of the partial
+sigma (P_ab*s_c + 16*D), over its CUDA-event time, against the measured HBM
+copy bandwidth; `roofline.sigma` gives the same for the whole sigma with
+B = P*s_c + D*(2*s_c + s_h) + 4*(connectivity entries) + 8*(na + nb). The CPU baseline is the reference's own
 OpenMP mult (compiled in oracle/_ref) on a bounded sample of bra alpha rows.
 
 Multi-GPU: the path is run at MPI world size 1; --gpus N runs N independent
@@ -171,12 +174,36 @@ def roofline_bytes(prob, dp, s_c: int, s_h: int = 8) -> float:
     return dp["offdiag"] * s_c + prob.D * (2 * s_c + s_h) + 4 * conn + 8 * (prob.na + prob.nb)
 
 
-def traffic_per_sigma(workload: str):
-    """DRAM bytes of one sigma from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", f"sigma_{workload}_dram.json")
+# CUDA kernel of each sigma phase (alpha-first path) and its ncu summary file
+PHASE_KERNELS = {"alpha_same_spin": "sigma_same_v6", "transpose": "phase_split", "beta_same_spin": "sigma_same_v6",
+                 "alpha_beta": "sigma_ab_v6", "combine": "combine_phase"}
+
+
+def phase_bytes(prob, dp, s_c: int) -> dict:
+    """Algorithmic bytes of each sigma phase: one vector gather per nonzero of
+    its part of H (the matrix is never stored), plus the streams every
+    element of the phase reads or writes once."""
+    D = prob.D
+    na, nb = prob.na, prob.nb
+    return {
+        "transpose": 3.0 * D * s_c,                                            # read C, write phi o C and its transpose
+        "alpha_same_spin": nb * (dp["Sa"] + dp["Da"]) * s_c + D * (s_c + 16),  # + own row, hii, Y
+        "beta_same_spin": na * (dp["Sb"] + dp["Db"]) * s_c + D * 8,           # + Yt
+        "alpha_beta": dp["alpha_beta"] * s_c + 16.0 * D,                       # + Y read-modify-write
+        "combine": D * (16.0 + s_c),                                           # Y, Yt -> S
+    }
+
+
+def traffic_per_launch(kernel: str, workload: str):
+    """DRAM bytes of one launch of `kernel` on `workload` from the committed
+    ncu summary profiles/<kernel>_<workload>.md (line 'dram_bytes_per_launch: N')."""
+    import re
+
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     if os.path.exists(path):
-        with open(path) as f:
-            return json.load(f).get("dram_bytes_per_sigma")
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+        if m:
+            return float(m.group(1))
     return None
 
 
@@ -301,6 +328,12 @@ def run_ours(args, rank, world, local):
     e1.record(stream)
     barrier()
     ms32 = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    ctx.set_profiling(True)
+    for _ in range(nprof):
+        ctx.sigma_device(sbdx.SBDX_FP32, C32.data_ptr(), S32.data_ptr())
+    ncalls32, phases32 = ctx.phase_times()
+    ctx.set_profiling(False)
+    phases32 = {k: v / ncalls32 for k, v in phases32.items()}
     del C32, S32
 
     # ---- end to end through the C-ABI with pinned host buffers --------------------
@@ -350,8 +383,19 @@ def run_ours(args, rank, world, local):
 
     hbm, peak_kind = peaks()
     B = roofline_bytes(prob, dp, 8)
-    achieved = B / (ms * 1e-3) / 1e9
-    traffic = traffic_per_sigma(args.workload)
+    pb = phase_bytes(prob, dp, 8)
+    pb32 = phase_bytes(prob, dp, 4)
+    kern = PHASE_KERNELS[dominant]
+    achieved = pb[dominant] / (phases[dominant] * 1e-3) / 1e9
+    roofline = {
+        "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+        "traffic": traffic_per_launch(kern, args.workload), "kernel": kern, "phase": dominant,
+        "algorithmic_bytes_per_launch": pb[dominant], "ms_per_launch": phases[dominant], "peak_kind": peak_kind,
+        "phases": {k: {"ms": phases[k], "bytes": pb[k], "gbs": pb[k] / (phases[k] * 1e-3) / 1e9,
+                       "frac": pb[k] / (phases[k] * 1e-3) / 1e9 / hbm} for k in phases},
+        "sigma": {"algorithmic_bytes": B, "ms": ms, "gbs": B / (ms * 1e-3) / 1e9,
+                  "frac": B / (ms * 1e-3) / 1e9 / hbm},
+    }
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -359,16 +403,16 @@ def run_ours(args, rank, world, local):
         "config": {"workload": args.workload, "desc": WORKLOAD_DESC, "dets": D, "na": prob.na, "nb": prob.nb,
                    "norb": prob.L, "det_pairs_per_sigma": dp["total"], "parallelism": f"replicas x{world}",
                    "tuning": {"same_vec": tune[0], "ab_rows": tune[1]},
-                   "l2": "inputs larger than L2 (C = 512 MB), no flush"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "kernel": "sigma (5 launches: alpha same-spin, transpose, beta same-spin, "
-                     "alpha-beta, combine)", "algorithmic_bytes_per_sigma": B, "peak_kind": peak_kind,
-                     "dominant_phase": dominant, "phase_ms": phases},
+                   "l2": f"inputs larger than L2 (C = {8 * D / 1e6:.0f} MB > 126 MB), no flush"
+                         if 8 * D > 126e6 else "C fits in L2: timings include L2 reuse"},
+        "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * D, "d2h_bytes_per_step": 8 * D,
                 "ms_per_step": ms_e2e},
         "gpu_launches": launches,
         "clocks": clocks,
-        "fp32_sigma": {"value": world * dp["total"] / (ms32 * 1e-3), "ms_per_step": ms32},
+        "fp32_sigma": {"value": world * dp["total"] / (ms32 * 1e-3), "ms_per_step": ms32,
+                       "phases": {k: {"ms": phases32[k], "gbs": pb32[k] / (phases32[k] * 1e-3) / 1e9}
+                                  for k in phases32}},
         "davidson": dav,
         "cpu_baseline": cpu,
     }

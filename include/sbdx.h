@@ -62,7 +62,13 @@ unsigned long long sbdx_launch_count(const sbdx_ctx* ctx);
 int sbdx_set_profiling(sbdx_ctx* ctx, int on);
 long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n);
 /* Launch shapes of the sigma kernels (no reference counterpart), applied to
- * both precisions; 0 selects the built-in default.
+ * both precisions; 0 selects the built-in default (alpha-first kernels).
+ * Alpha-first kernels (the sigma evaluated in the alpha-before-beta
+ * determinant ordering, conjugated by the +-1 basis phase):
+ *   same_code: 21/22/24/28 = 1/2/4/8 columns per thread;
+ *   ab_code:   61-64 = 1-4 staged ket rows of the balanced alpha-beta kernel.
+ * Interleaved-ordering kernels (kept for comparison; both codes must then
+ * come from this family):
  *   same_code: 1/2/4/8 = columns per thread of the prefix-parity-table
  *              same-spin kernel, 11/12/14 = 1/2/4 columns of the popcount one;
  *   ab_code:   10*variant + staged ket rows (1-4) of the alpha-beta kernel,
@@ -148,7 +154,8 @@ typedef struct {
   double max_time;     /* seconds (SBD::max_time, sbdiag.h:22)                */
   int precision;       /* SBDX_FP64: the reference algorithm; SBDX_FP32:
                           FP32-stored subspace with FP64 defect correction    */
-  int defect_every;    /* FP32 mode: FP64 residual every k steps (default 4)  */
+  int defect_every;    /* FP32 mode: 0 = exact FP64 refresh when the estimated
+                          residual fell 1e4-fold (default); k > 0 = every k steps */
   int verbose;         /* print one line per step, as davidson.h:834-846      */
 } sbdx_davidson_params;
 

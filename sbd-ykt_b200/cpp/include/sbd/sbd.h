@@ -462,7 +462,7 @@ void diag(const Comm& /*comm*/, const SBD& sbd_data, const FCIDump& fcidump,
   p.eps = sbd_data.eps;
   p.max_time = sbd_data.max_time;
   p.precision = (prec && std::string(prec) == "fp32") ? SBDX_FP32 : SBDX_FP64;
-  p.defect_every = 4;
+  p.defect_every = 0;
   p.verbose = detail::env_int("SBDX_VERBOSE", 1);
   sbdx_davidson_info info{};
   ctx.check(sbdx_davidson(ctx.h, &p, init_from_W, W.data(), &info));

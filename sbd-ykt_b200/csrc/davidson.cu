@@ -14,11 +14,14 @@
 // ascending eigenvalues), standing in for LAPACK dsyev.
 //
 // FP32 mode ("defect correction"): the subspace holds an FP64 anchor pair
-// (W, HW), refreshed with an FP64 sigma every `defect_every` steps, plus
-// FP32-stored correction vectors C_j with FP32-storage sigma products HC_j
-// (FP64 accumulation inside the kernel). Rayleigh-Ritz, Gram-Schmidt, the
-// residual norms and the energy are FP64; convergence is decided on the exact
-// FP64 residual |HW - E W| of the anchor.
+// (W, HW), the current Ritz vector, plus up to 2*max_nb FP32-stored
+// correction vectors C_j with FP32-storage sigma products HC_j (FP64
+// accumulation inside the kernel). The anchor is refreshed with an exact FP64
+// sigma when the estimated residual has dropped 1e4-fold (or every
+// `defect_every` steps when that is set). Expansion uses Olsen's correction of
+// the diagonal preconditioner; a full subspace keeps its newest third.
+// Rayleigh-Ritz, Gram-Schmidt, the residual norms and the energy are FP64;
+// convergence is decided on the exact FP64 residual |HW - E W| of the anchor.
 #include "sbdx_internal.cuh"
 #include "sbdx.h"
 
@@ -242,7 +245,7 @@ struct Work {
 };
 
 // Device scalar slots
-enum { kE0 = 0, kNW = 1, kNR = 2, kOlap = 3, kNV = 4, kE = 5, kDots = 8 };
+enum { kE0 = 0, kNW = 1, kNR = 2, kOlap = 3, kNV = 4, kE = 5, kAB = 6, kDots = 8 };
 
 template <typename TV, typename TX>
 int multidot(Ctx* c, Work& wk, const TV* V, size_t ldv, int m, const TX* x, size_t D, double* out) {
@@ -378,6 +381,148 @@ int davidson_fp64(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davids
   return 0;
 }
 
+// W <- u0*W + sum_k u[k] C_k ; HW <- u0*HW + sum_k u[k] HC_k (in place, FP64);
+// R = theta*W - HW. Partial |W|^2 (slot 0) and |R|^2 (slot 1).
+template <typename TV>
+__global__ void __launch_bounds__(kRedThreads)
+update_anchor_kernel(const TV* __restrict__ C, const TV* __restrict__ HC, size_t ldv, int m,
+                     const double* __restrict__ u, double u0, const double* __restrict__ thetap, size_t D,
+                     double* __restrict__ W, double* __restrict__ HW, double* __restrict__ R,
+                     double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  __shared__ double su[64];
+  for (int k = threadIdx.x; k < m; k += blockDim.x) su[k] = u[k];
+  __syncthreads();
+  const double th = *thetap;
+  double nw = 0.0, nr = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    double w = u0 * W[s], hw = u0 * HW[s];
+    for (int k = 0; k < m; ++k) {
+      w = fma((double)C[(size_t)k * ldv + s], su[k], w);
+      hw = fma((double)HC[(size_t)k * ldv + s], su[k], hw);
+    }
+    const double r = th * w - hw;
+    W[s] = w;
+    HW[s] = hw;
+    R[s] = r;
+    nw = fma(w, w, nw);
+    nr = fma(r, r, nr);
+  }
+  double t = block_sum(nw, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+  t = block_sum(nr, sh);
+  if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = t;
+}
+
+// W, HW, R *= 1/sqrt(nw2)
+__global__ void scale3_kernel(double* W, double* HW, double* R, const double* __restrict__ nw2, size_t D) {
+  const double inv = 1.0 / sqrt(*nw2);
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    W[s] *= inv;
+    HW[s] *= inv;
+    R[s] *= inv;
+  }
+}
+
+__device__ __forceinline__ double precond_inv(double E0, double d) {
+  const double den = E0 - d;
+  return fabs(den) > 1.0e-12 ? 1.0 / den : 1.0 / (den - 1.0e-12);
+}
+
+// Olsen's corrected preconditioner, pass 1: v = P R/|R| with
+// P = (E0 - diag)^-1 (reference guard); partials <W, v> and <W, P W>.
+__global__ void __launch_bounds__(kRedThreads)
+olsen_precond_kernel(const double* __restrict__ R, const double* __restrict__ W, const double* __restrict__ dii,
+                     const double* __restrict__ E0p, const double* __restrict__ nr2, size_t D, double* __restrict__ v,
+                     double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  const double E0 = *E0p;
+  const double inv = 1.0 / sqrt(*nr2);
+  double a = 0.0, b = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    const double p = precond_inv(E0, dii[s]);
+    const double x = R[s] * inv * p;
+    const double w = W[s];
+    v[s] = x;
+    a = fma(w, x, a);
+    b = fma(w * w, p, b);
+  }
+  double t = block_sum(a, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+  t = block_sum(b, sh);
+  if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = t;
+}
+
+// Pass 2: v -= (a/b) P W, so that v is orthogonal to W; partial <W, v> (about
+// zero) for the anchor step of the following Gram-Schmidt pass.
+__global__ void __launch_bounds__(kRedThreads)
+olsen_apply_kernel(double* __restrict__ v, const double* __restrict__ W, const double* __restrict__ dii,
+                   const double* __restrict__ E0p, const double* __restrict__ ab, size_t D,
+                   double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  const double E0 = *E0p;
+  const double eps = ab[1] != 0.0 ? ab[0] / ab[1] : 0.0;
+  double acc = 0.0, nn = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    const double w = W[s];
+    const double x = v[s] - eps * precond_inv(E0, dii[s]) * w;
+    v[s] = x;
+    acc = fma(w, x, acc);
+    nn = fma(x, x, nn);
+  }
+  double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+  t = block_sum(nn, sh);
+  if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = t;
+}
+
+// Expansion vector of the mixed solver: Olsen-corrected preconditioned
+// residual (orthogonal to the anchor W), modified Gram-Schmidt against the
+// anchor and the nv corrections (a second pass when the first removed more than
+// three quarters of the norm), normalised and stored in FP32. Returns 0, or -1
+// when what is left is negligible (the subspace already holds the direction).
+int expand_olsen(Ctx* c, Work& wk, const double* R, const double* W, const float* V, int nv, size_t D, double* v,
+                 float* dst) {
+  double* s = wk.scal;
+  olsen_precond_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(R, W, c->d_hii, s + kE0, s + kNR, D, v,
+                                                                  wk.partial);
+  SBDX_LAUNCHED(c);
+  int rc = finalize(c, wk, 2, s + kAB);
+  if (rc) return rc;
+  // v -= eps P W, then <W, v> for the anchor step of Gram-Schmidt and |v|^2
+  olsen_apply_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(v, W, c->d_hii, s + kE0, s + kAB, D, wk.partial);
+  SBDX_LAUNCHED(c);
+  if ((rc = finalize(c, wk, 2, s + kOlap))) return rc;  // kOlap, kNV
+  double before = 0.0;
+  SBDX_CUDA(c, cudaMemcpyAsync(&before, s + kNV, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  const int nbasis = nv + 1;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) {  // restart the sweep: <W, v>
+      multidot_kernel<double, double><<<dim3(kRedBlocks, 1), kRedThreads, 0, c->stream>>>(W, D, 1, v, D, wk.partial);
+      SBDX_LAUNCHED(c);
+      if ((rc = finalize(c, wk, 1, s + kOlap))) return rc;
+    }
+    for (int k = 0; k < nbasis; ++k) {
+      const bool anchor = k == 0;
+      const float* vk = anchor ? nullptr : V + (size_t)(k - 1) * D;
+      const float* vn = (k + 1 < nbasis) ? V + (size_t)k * D : nullptr;
+      axpy_dot_kernel<float><<<kRedBlocks, kRedThreads, 0, c->stream>>>(v, vk, anchor ? W : nullptr, s + kOlap, vn,
+                                                                        D, wk.partial);
+      SBDX_LAUNCHED(c);
+      if ((rc = finalize(c, wk, 1, vn ? s + kOlap : s + kNV))) return rc;
+    }
+    double after = 0.0;
+    SBDX_CUDA(c, cudaMemcpyAsync(&after, s + kNV, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (!(after > 1e-24 * before)) return -1;
+    if (after > 0.0625 * before) break;
+    before = after;
+  }
+  scale_store_kernel<float, double><<<kRedBlocks, kRedThreads, 0, c->stream>>>(v, s + kNV, D, dst);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
 // ---- FP32 storage with FP64 defect correction --------------------------------
 // Generalised Rayleigh-Ritz M x = theta S x over the basis [W, C_0..C_{nv-1}]:
 // the C_j are orthonormal among themselves (MGS), the anchor W is not
@@ -425,33 +570,48 @@ bool gen_eigen(int n, const std::vector<double>& M, const std::vector<double>& S
   return true;
 }
 
+// Mixed precision (defect correction). The subspace is an FP64 anchor pair
+// (W, HW), always the current Ritz vector and its product, plus up to
+// nc = 2*max_nb FP32 corrections C_j with FP32-storage products HC_j (the
+// same bytes as max_nb FP64 vectors). Each step: expand with the
+// Olsen-corrected preconditioned residual, one FP32 sigma, generalised
+// Rayleigh-Ritz in FP64, then the anchor becomes the new Ritz vector (its
+// projected row is x^T M, x^T S on the host; HW accumulates FP32 products).
+// The anchor is refreshed with an exact FP64 sigma (HW, E = <W|HW>, R) when
+// the estimated residual has dropped by kRefreshDrop since the last exact
+// one, or falls below eps, or every `defect_every` steps when that is set;
+// convergence is decided on the exact FP64 residual only. On a full subspace
+// the newest third of the corrections is kept (thick restart).
+constexpr double kRefreshDrop = 1e-4;
+
 int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info) {
   const size_t D = c->na * c->nb;
-  const int nb = p.max_nb;  // FP32 correction vectors kept beside the FP64 anchor
-  const int kdef = p.defect_every > 0 ? p.defect_every : 4;
+  const int nc = std::min(2 * p.max_nb, 60);  // FP32 correction vectors
+  const int keep = nc >= 3 ? nc / 3 : 0;
+  const int period = p.defect_every > 0 ? p.defect_every : 0;
   Work wk;
-  SBDX_CUDA(c, cudaMalloc(&wk.partial, sizeof(double) * kRedBlocks * (nb + 3)));
-  SBDX_CUDA(c, cudaMalloc(&wk.scal, sizeof(double) * (kDots + 2 * nb + 16)));
-  SBDX_CUDA(c, cudaMalloc(&wk.u, sizeof(double) * (nb + 2)));
+  SBDX_CUDA(c, cudaMalloc(&wk.partial, sizeof(double) * kRedBlocks * (nc + 3)));
+  SBDX_CUDA(c, cudaMalloc(&wk.scal, sizeof(double) * (kDots + 2 * nc + 16)));
+  SBDX_CUDA(c, cudaMalloc(&wk.u, sizeof(double) * (nc + 2)));
   float *C = nullptr, *HC = nullptr;
-  double *AW = nullptr, *Wn = nullptr, *R = nullptr;
-  SBDX_CUDA(c, cudaMalloc(&C, sizeof(float) * D * nb));
-  SBDX_CUDA(c, cudaMalloc(&HC, sizeof(float) * D * nb));
+  double *AW = nullptr, *R = nullptr, *V = nullptr;
+  SBDX_CUDA(c, cudaMalloc(&C, sizeof(float) * D * nc));
+  SBDX_CUDA(c, cudaMalloc(&HC, sizeof(float) * D * nc));
   SBDX_CUDA(c, cudaMalloc(&AW, sizeof(double) * D * 2));  // [W | HW] anchor pair
-  SBDX_CUDA(c, cudaMalloc(&Wn, sizeof(double) * D));
   SBDX_CUDA(c, cudaMalloc(&R, sizeof(double) * D));
+  SBDX_CUDA(c, cudaMalloc(&V, sizeof(double) * D));
   struct Guard {
     float *a, *b; double *c, *d, *e;
     ~Guard() { cudaFree(a); cudaFree(b); cudaFree(c); cudaFree(d); cudaFree(e); }
-  } g{C, HC, AW, Wn, R};
+  } g{C, HC, AW, R, V};
   double* W = AW;
   double* HW = AW + D;
   double* s = wk.scal;
   SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * D, cudaMemcpyDeviceToDevice, c->stream));
   const auto t0 = std::chrono::steady_clock::now();
   int rc = 0;
-  const int ld = nb + 1;
-  std::vector<double> M((size_t)ld * ld, 0.0), S((size_t)ld * ld, 0.0), col(2 * ld + 2), x;
+  const int ld = nc + 1;
+  std::vector<double> M((size_t)ld * ld, 0.0), S((size_t)ld * ld, 0.0), col(2 * ld + 2), x, row(2 * ld);
   double Eanc = 0.0, normR = 0.0;
   int nv = 0;
   auto set_pair = [&](std::vector<double>& A, int i, int j, double v) {
@@ -459,7 +619,7 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
     A[j + (size_t)ld * i] = v;
   };
   auto refresh = [&]() -> int {
-    // exact anchor (defect correction): HW = H W in FP64, E = <W|HW>, R = E W - HW
+    // exact anchor: HW = H W in FP64, E = <W|HW>, R = E W - HW (W has unit norm)
     int r2 = sigma_typed<double>(c, W, HW);
     if (r2) return r2;
     info.n_sigma64++;
@@ -476,17 +636,18 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
     normR = std::sqrt(h2[1]);
     set_pair(M, 0, 0, Eanc);
     set_pair(S, 0, 0, 1.0);
-    if (nv > 0) {  // anchor row against the kept corrections: <C_j|W>, <C_j|HW>
-      if ((r2 = multidot<float, double>(c, wk, C, D, nv, W, D, s + kDots))) return r2;
-      if ((r2 = multidot<float, double>(c, wk, C, D, nv, HW, D, s + kDots + nv))) return r2;
-      SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kDots, sizeof(double) * 2 * nv, cudaMemcpyDeviceToHost, c->stream));
+    if (nv > 0) {  // <HW|C_j> changed with the exact HW (<W|C_j> did not)
+      if ((r2 = multidot<float, double>(c, wk, C, D, nv, HW, D, s + kDots))) return r2;
+      SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kDots, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
       SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
-      for (int j = 0; j < nv; ++j) { set_pair(S, 0, j + 1, col[j]); set_pair(M, 0, j + 1, col[nv + j]); }
+      for (int j = 0; j < nv; ++j) set_pair(M, 0, j + 1, col[j]);
     }
     return 0;
   };
   if ((rc = refresh())) return rc;
-  int steps = 0;
+  double r_ref = normR;
+  int steps = 0, since = 0;
+  bool stalled = false;
   const int max_steps = p.max_it * p.max_nb;
   while (true) {
     if (p.verbose) {
@@ -494,26 +655,50 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
       std::fflush(stdout);
     }
     if (normR < p.eps) { info.converged = 1; break; }
-    if (steps >= max_steps || seconds_since(t0) > p.max_time) break;
-    if (nv == nb) nv = 0;  // thick restart with the anchor only
-    // expansion from the exact FP64 residual (kE0 = E, kNR = |R|^2)
-    if ((rc = expand<float>(c, wk, R, W, C, nv, D, R, C + (size_t)nv * D))) return rc;
-    ++nv;
-    for (int inner = 0; inner < kdef; ++inner) {
-      const int j = nv - 1;  // newest correction
+    if (steps >= max_steps || seconds_since(t0) > p.max_time || stalled) break;
+    bool exact = false;
+    while (!exact) {
+      if (nv == nc) {  // thick restart: keep the newest corrections beside the anchor
+        const int drop = nc - keep;
+        if (keep > 0) {
+          SBDX_CUDA(c, cudaMemcpyAsync(C, C + (size_t)drop * D, sizeof(float) * D * keep, cudaMemcpyDeviceToDevice,
+                                       c->stream));
+          SBDX_CUDA(c, cudaMemcpyAsync(HC, HC + (size_t)drop * D, sizeof(float) * D * keep,
+                                       cudaMemcpyDeviceToDevice, c->stream));
+        }
+        for (int i = 0; i <= keep; ++i)
+          for (int j = 0; j <= keep; ++j) {
+            const int si = i == 0 ? 0 : i + drop, sj = j == 0 ? 0 : j + drop;
+            M[i + (size_t)ld * j] = M[si + (size_t)ld * sj];
+            S[i + (size_t)ld * j] = S[si + (size_t)ld * sj];
+          }
+        nv = keep;
+      }
+      rc = expand_olsen(c, wk, R, W, C, nv, D, V, C + (size_t)nv * D);
+      if (rc > 0) return rc;
+      if (rc < 0) {  // no new direction: refresh, or stop if that changes nothing
+        rc = 0;
+        if (since == 0) { stalled = true; break; }
+        exact = true;
+        break;
+      }
+      const int j = nv++;
       float* Cb = C + (size_t)j * D;
       float* HCb = HC + (size_t)j * D;
       if ((rc = sigma_typed<float>(c, Cb, HCb))) return rc;
       info.n_sigma++;
       ++steps;
-      // <C_k|HC_j> (k <= j) and <W|C_j>, <HW|C_j>
+      ++since;
+      // <C_k|HC_j>, <C_k|C_j> (k <= j), <W|C_j>, <HW|C_j>
       if ((rc = multidot<float, float>(c, wk, C, D, nv, HCb, D, s + kDots))) return rc;
       if ((rc = multidot<double, float>(c, wk, AW, D, 2, Cb, D, s + kDots + nv))) return rc;
-      SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kDots, sizeof(double) * (nv + 2), cudaMemcpyDeviceToHost, c->stream));
+      if ((rc = multidot<float, float>(c, wk, C, D, nv, Cb, D, s + kDots + nv + 2))) return rc;
+      SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kDots, sizeof(double) * (2 * nv + 2), cudaMemcpyDeviceToHost,
+                                   c->stream));
       SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
       for (int k = 0; k < nv; ++k) {
         set_pair(M, k + 1, j + 1, col[k]);
-        set_pair(S, k + 1, j + 1, k == j ? 1.0 : 0.0);
+        set_pair(S, k + 1, j + 1, col[nv + 2 + k]);
       }
       set_pair(S, 0, j + 1, col[nv]);
       set_pair(M, 0, j + 1, col[nv + 1]);
@@ -523,20 +708,48 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
         c->err = "davidson (FP32): projected overlap matrix is not positive definite";
         return 5;
       }
+      // the anchor becomes the Ritz vector: W <- x0 W + sum x_k C_k (same for HW)
       SBDX_CUDA(c, cudaMemcpyAsync(wk.u, x.data() + 1, sizeof(double) * nv, cudaMemcpyHostToDevice, c->stream));
       SBDX_CUDA(c, cudaMemcpyAsync(s + kE0, &theta, sizeof(double), cudaMemcpyHostToDevice, c->stream));
-      combine_kernel<float><<<kRedBlocks, kRedThreads, 0, c->stream>>>(C, HC, D, nv, wk.u, W, HW, x[0], s + kE0, D,
-                                                                       Wn, R, wk.partial);
+      update_anchor_kernel<float><<<kRedBlocks, kRedThreads, 0, c->stream>>>(C, HC, D, nv, wk.u, x[0], s + kE0, D,
+                                                                             W, HW, R, wk.partial);
       SBDX_LAUNCHED(c);
       if ((rc = finalize(c, wk, 2, s + kNW))) return rc;
-      if (inner == kdef - 1 || nv == nb) break;
-      if ((rc = expand<float>(c, wk, R, W, C, nv, D, R, C + (size_t)nv * D))) return rc;
-      ++nv;
+      scale3_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, R, s + kNW, D);
+      SBDX_LAUNCHED(c);
+      double nrm[2];
+      SBDX_CUDA(c, cudaMemcpyAsync(nrm, s + kNW, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
+      SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+      const double nw = std::sqrt(nrm[0]);
+      const double r_est = std::sqrt(nrm[1]) / nw;
+      // projected row of the new anchor (divided by its norm like the vectors)
+      for (int k = 0; k < n; ++k) {
+        double sm = 0.0, ss = 0.0;
+        for (int i = 0; i < n; ++i) {
+          sm += x[i] * M[std::min(i, k) + (size_t)ld * std::max(i, k)];
+          ss += x[i] * S[std::min(i, k) + (size_t)ld * std::max(i, k)];
+        }
+        row[k] = sm / nw;
+        row[ld + k] = ss / nw;
+      }
+      for (int k = 1; k < n; ++k) { set_pair(M, 0, k, row[k]); set_pair(S, 0, k, row[ld + k]); }
+      set_pair(M, 0, 0, theta / (nw * nw));
+      set_pair(S, 0, 0, 1.0);
+      // R/|R| is what the next expansion uses; kNR must hold |R|^2 of the scaled R
+      const double nr2 = r_est * r_est;
+      SBDX_CUDA(c, cudaMemcpyAsync(s + kNR, &nr2, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      Eanc = theta;
+      if (p.verbose) {
+        std::printf("   step %d: theta=%.12f est.res=%.3e\n", steps, theta, r_est);
+        std::fflush(stdout);
+      }
+      const bool due = period > 0 ? since >= period : (r_est < kRefreshDrop * r_ref || r_est < p.eps);
+      if (due || steps >= max_steps || seconds_since(t0) > p.max_time) exact = true;
     }
-    // W <- normalised Ritz vector, then the exact FP64 refresh
-    scale_store_kernel<double, double><<<kRedBlocks, kRedThreads, 0, c->stream>>>(Wn, s + kNW, D, W);
-    SBDX_LAUNCHED(c);
+    if (stalled) break;
     if ((rc = refresh())) return rc;
+    r_ref = normR;
+    since = 0;
   }
   SBDX_CUDA(c, cudaMemcpyAsync(dW, W, sizeof(double) * D, cudaMemcpyDeviceToDevice, c->stream));
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));

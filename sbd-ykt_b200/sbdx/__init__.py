@@ -192,7 +192,7 @@ class Context:
         self._check(self.lib.sbdx_sigma_device(self.h, ctypes.c_int(precision), ctypes.c_void_p(c_ptr),
                                                ctypes.c_void_p(s_ptr)))
 
-    def davidson(self, max_it=1, max_nb=10, eps=1e-4, max_time=86400.0, precision=SBDX_FP64, defect_every=4,
+    def davidson(self, max_it=1, max_nb=10, eps=1e-4, max_time=86400.0, precision=SBDX_FP64, defect_every=0,
                  verbose=0, W=None):
         p = DavidsonParams(max_it, max_nb, eps, max_time, precision, defect_every, verbose)
         D = self.na * self.nb
