@@ -66,7 +66,10 @@ long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n);
  * Alpha-first kernels (the sigma evaluated in the alpha-before-beta
  * determinant ordering, conjugated by the +-1 basis phase):
  *   same_code: 21/22/24/28 = 1/2/4/8 columns per thread;
- *   ab_code:   61-64 = 1-4 staged ket rows of the balanced alpha-beta kernel.
+ *   ab_code:   61-64 = 1-4 staged ket rows of the balanced alpha-beta kernel,
+ *              71 = the same with the rows packed in 16-byte elements (2 FP64
+ *              or 4 FP32 rows per group; falls back to 62/64 when nb is too
+ *              large for the packs to fit in shared memory).
  * Interleaved-ordering kernels (kept for comparison; both codes must then
  * come from this family):
  *   same_code: 1/2/4/8 = columns per thread of the prefix-parity-table

@@ -159,18 +159,18 @@ long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n) {
 int sbdx_set_tuning(sbdx_ctx* ctx, int same_code, int ab_code) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {
     const int v = same_code % 10;
-    const bool same_v6 = same_code > 20 && same_code < 30, ab_v6 = ab_code > 60 && ab_code < 70;
+    const bool same_v6 = same_code > 20 && same_code < 30, ab_v6 = (ab_code > 60 && ab_code < 70) || ab_code == 71;
     const bool same_ok = same_code == 0 || ((same_code < 10 && (v == 1 || v == 2 || v == 4 || v == 8)) ||
                                             (same_code > 10 && same_code < 20 && (v == 1 || v == 2 || v == 4)) ||
                                             (same_v6 && (v == 1 || v == 2 || v == 4 || v == 8)));
     const bool ab_ok = ab_code == 0 || (ab_code > 0 && ab_code < 50 && ab_code % 10 >= 1 && ab_code % 10 <= 4) ||
-                       (ab_v6 && ab_code % 10 >= 1 && ab_code % 10 <= 4);
+                       (ab_v6 && ab_code % 10 >= 1 && ab_code % 10 <= 4);  // 71 included
     // the alpha-first codes (2x, 6x) evaluate the whole sigma in another
     // determinant ordering and cannot be mixed with the interleaved ones
     const bool mixed = (same_v6 && ab_code != 0 && !ab_v6) || (ab_v6 && same_code != 0 && !same_v6) ||
                        (same_code != 0 && !same_v6 && ab_code == 0) || (ab_code != 0 && !ab_v6 && same_code == 0);
     if (!same_ok || !ab_ok || mixed) {
-      c->err = "set_tuning: alpha-first codes same in {21,22,24,28} with ab in {61..64}, or interleaved codes "
+      c->err = "set_tuning: alpha-first codes same in {21,22,24,28} with ab in {61..64, 71}, or interleaved codes "
                "same in {1,2,4,8,11,12,14} with ab = 10*variant + rows (variant 0-4, rows 1-4); 0 = default";
       return SBDX_ERR_ARG;
     }

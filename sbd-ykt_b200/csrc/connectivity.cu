@@ -255,10 +255,43 @@ int build_balanced_sell(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const
   const uint64_t kPad = 1ull << 41;
   std::vector<uint64_t> sell(soff[ns] ? soff[ns] : 1, kPad);
   std::vector<uint32_t> vrow(nv ? nv : 1, 0);
-  for (size_t v = 0; v < nv; ++v) {
-    const size_t sl = v / 32, l = v % 32;
-    for (uint32_t m = 0; m < vr[v].len; ++m) sell[soff[sl] + 32ull * m + l] = rec[vr[v].beg + m];
-    vrow[v] = vr[v].r | (vr[v].slot1 << 16);
+  // Record order inside each virtual row is free (it only changes the order of
+  // the sum). Per slice, step m and quarter-warp (8 lanes, one 128-byte
+  // shared-memory wavefront of 16-byte loads), pick for every lane the record
+  // whose ket index and pair index fall in the least used of the 8 bank slots
+  // (index mod 8), most constrained lane first: fewer bank conflicts on the
+  // two shared-memory loads of each record.
+  std::vector<std::vector<uint64_t>> left(32);
+  for (size_t sl = 0; sl < ns; ++sl) {
+    const size_t l_end = std::min<size_t>(32, nv - sl * 32);
+    for (size_t l = 0; l < l_end; ++l) {
+      const VRow& w = vr[sl * 32 + l];
+      left[l].assign(rec.begin() + w.beg, rec.begin() + w.beg + w.len);
+      vrow[sl * 32 + l] = w.r | (w.slot1 << 16);
+    }
+    for (uint32_t m = 0; m < slen[sl]; ++m)
+      for (size_t q = 0; q * 8 < l_end; ++q) {
+        int cj[8] = {0}, cp[8] = {0};
+        size_t lanes[8];
+        size_t nl = 0;
+        for (size_t l = q * 8; l < std::min(l_end, q * 8 + 8); ++l)
+          if (!left[l].empty()) lanes[nl++] = l;
+        std::sort(lanes, lanes + nl, [&](size_t x, size_t y) { return left[x].size() < left[y].size(); });
+        for (size_t i = 0; i < nl; ++i) {
+          std::vector<uint64_t>& lst = left[lanes[i]];
+          size_t best = 0;
+          int bc = 1 << 30;
+          for (size_t t = 0; t < lst.size(); ++t) {
+            const int c = cj[lst[t] & 7u] + cp[(lst[t] >> 16) & 7u];
+            if (c < bc) { bc = c; best = t; }
+          }
+          const uint64_t r = lst[best];
+          lst.erase(lst.begin() + (std::ptrdiff_t)best);
+          ++cj[r & 7u];
+          ++cp[(r >> 16) & 7u];
+          sell[soff[sl] + 32ull * m + lanes[i]] = r;
+        }
+      }
   }
   cn.bnslice = ns;
   cn.nv = nv;

@@ -414,16 +414,6 @@ update_anchor_kernel(const TV* __restrict__ C, const TV* __restrict__ HC, size_t
   if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = t;
 }
 
-// W, HW, R *= 1/sqrt(nw2)
-__global__ void scale3_kernel(double* W, double* HW, double* R, const double* __restrict__ nw2, size_t D) {
-  const double inv = 1.0 / sqrt(*nw2);
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
-    W[s] *= inv;
-    HW[s] *= inv;
-    R[s] *= inv;
-  }
-}
-
 __device__ __forceinline__ double precond_inv(double E0, double d) {
   const double den = E0 - d;
   return fabs(den) > 1.0e-12 ? 1.0 / den : 1.0 / (den - 1.0e-12);
@@ -476,41 +466,82 @@ olsen_apply_kernel(double* __restrict__ v, const double* __restrict__ W, const d
   if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = t;
 }
 
+// partial[(2k + i) * gridDim.x + blk] = partial sums of <V_k, x_i>, i = 0, 1,
+// k in [k0, k0+mc): two projections with one read of V.
+template <typename TV, typename TX>
+__global__ void __launch_bounds__(kRedThreads)
+multidot2_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restrict__ x0, const TX* __restrict__ x1,
+                 size_t D, double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  const int k0 = blockIdx.y * kDotChunk;
+  const int mc = min(kDotChunk, m - k0);
+  double a0[kDotChunk], a1[kDotChunk];
+#pragma unroll
+  for (int k = 0; k < kDotChunk; ++k) a0[k] = a1[k] = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    const double y0 = (double)x0[s], y1 = (double)x1[s];
+#pragma unroll
+    for (int k = 0; k < kDotChunk; ++k)
+      if (k < mc) {
+        const double v = (double)V[(size_t)(k0 + k) * ldv + s];
+        a0[k] = fma(v, y0, a0[k]);
+        a1[k] = fma(v, y1, a1[k]);
+      }
+  }
+  for (int k = 0; k < mc; ++k) {
+    double t = block_sum(a0[k], sh);
+    if (threadIdx.x == 0) partial[(size_t)(2 * (k0 + k)) * gridDim.x + blockIdx.x] = t;
+    t = block_sum(a1[k], sh);
+    if (threadIdx.x == 0) partial[(size_t)(2 * (k0 + k) + 1) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// Classical Gram-Schmidt update: v -= o[0] W + sum_k o[k+1] V_k; partial |v|^2.
+template <typename TV>
+__global__ void __launch_bounds__(kRedThreads)
+gs_subtract_kernel(double* __restrict__ v, const double* __restrict__ W, const TV* __restrict__ V, size_t ldv, int m,
+                   const double* __restrict__ o, size_t D, double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  __shared__ double so[65];
+  for (int k = threadIdx.x; k <= m; k += blockDim.x) so[k] = o[k];
+  __syncthreads();
+  double nn = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    double x = fma(-so[0], W[s], v[s]);
+    for (int k = 0; k < m; ++k) x = fma(-so[k + 1], (double)V[(size_t)k * ldv + s], x);
+    v[s] = x;
+    nn = fma(x, x, nn);
+  }
+  const double t = block_sum(nn, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
 // Expansion vector of the mixed solver: Olsen-corrected preconditioned
-// residual (orthogonal to the anchor W), modified Gram-Schmidt against the
-// anchor and the nv corrections (a second pass when the first removed more than
-// three quarters of the norm), normalised and stored in FP32. Returns 0, or -1
-// when what is left is negligible (the subspace already holds the direction).
+// residual (orthogonal to the anchor W), classical Gram-Schmidt against the
+// anchor and the nv corrections (all projections in one reduction, one update
+// pass; repeated once when the first pass removed more than three quarters of
+// the norm), normalised and stored in FP32. `o` is device scratch for nv + 1
+// doubles. Returns 0, or -1 when what is left is negligible (the subspace
+// already holds the direction).
 int expand_olsen(Ctx* c, Work& wk, const double* R, const double* W, const float* V, int nv, size_t D, double* v,
-                 float* dst) {
+                 double* o, float* dst) {
   double* s = wk.scal;
   olsen_precond_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(R, W, c->d_hii, s + kE0, s + kNR, D, v,
                                                                   wk.partial);
   SBDX_LAUNCHED(c);
   int rc = finalize(c, wk, 2, s + kAB);
   if (rc) return rc;
-  // v -= eps P W, then <W, v> for the anchor step of Gram-Schmidt and |v|^2
   olsen_apply_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(v, W, c->d_hii, s + kE0, s + kAB, D, wk.partial);
   SBDX_LAUNCHED(c);
-  if ((rc = finalize(c, wk, 2, s + kOlap))) return rc;  // kOlap, kNV
+  if ((rc = finalize(c, wk, 2, s + kOlap))) return rc;  // kOlap = <W, v>, kNV = |v|^2
   double before = 0.0;
   SBDX_CUDA(c, cudaMemcpyAsync(&before, s + kNV, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  const int nbasis = nv + 1;
   for (int pass = 0; pass < 2; ++pass) {
-    if (pass == 1) {  // restart the sweep: <W, v>
-      multidot_kernel<double, double><<<dim3(kRedBlocks, 1), kRedThreads, 0, c->stream>>>(W, D, 1, v, D, wk.partial);
-      SBDX_LAUNCHED(c);
-      if ((rc = finalize(c, wk, 1, s + kOlap))) return rc;
-    }
-    for (int k = 0; k < nbasis; ++k) {
-      const bool anchor = k == 0;
-      const float* vk = anchor ? nullptr : V + (size_t)(k - 1) * D;
-      const float* vn = (k + 1 < nbasis) ? V + (size_t)k * D : nullptr;
-      axpy_dot_kernel<float><<<kRedBlocks, kRedThreads, 0, c->stream>>>(v, vk, anchor ? W : nullptr, s + kOlap, vn,
-                                                                        D, wk.partial);
-      SBDX_LAUNCHED(c);
-      if ((rc = finalize(c, wk, 1, vn ? s + kOlap : s + kNV))) return rc;
-    }
+    if ((rc = multidot<double, double>(c, wk, W, D, 1, v, D, o))) return rc;
+    if (nv > 0 && (rc = multidot<float, double>(c, wk, V, D, nv, v, D, o + 1))) return rc;
+    gs_subtract_kernel<float><<<kRedBlocks, kRedThreads, 0, c->stream>>>(v, W, V, D, nv, o, D, wk.partial);
+    SBDX_LAUNCHED(c);
+    if ((rc = finalize(c, wk, 1, s + kNV))) return rc;
     double after = 0.0;
     SBDX_CUDA(c, cudaMemcpyAsync(&after, s + kNV, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -590,7 +621,7 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
   const int keep = nc >= 3 ? nc / 3 : 0;
   const int period = p.defect_every > 0 ? p.defect_every : 0;
   Work wk;
-  SBDX_CUDA(c, cudaMalloc(&wk.partial, sizeof(double) * kRedBlocks * (nc + 3)));
+  SBDX_CUDA(c, cudaMalloc(&wk.partial, sizeof(double) * kRedBlocks * (2 * nc + 4)));  // multidot2: 2 per vector
   SBDX_CUDA(c, cudaMalloc(&wk.scal, sizeof(double) * (kDots + 2 * nc + 16)));
   SBDX_CUDA(c, cudaMalloc(&wk.u, sizeof(double) * (nc + 2)));
   float *C = nullptr, *HC = nullptr;
@@ -674,7 +705,7 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
           }
         nv = keep;
       }
-      rc = expand_olsen(c, wk, R, W, C, nv, D, V, C + (size_t)nv * D);
+      rc = expand_olsen(c, wk, R, W, C, nv, D, V, wk.u, C + (size_t)nv * D);
       if (rc > 0) return rc;
       if (rc < 0) {  // no new direction: refresh, or stop if that changes nothing
         rc = 0;
@@ -689,19 +720,23 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
       info.n_sigma++;
       ++steps;
       ++since;
-      // <C_k|HC_j>, <C_k|C_j> (k <= j), <W|C_j>, <HW|C_j>
-      if ((rc = multidot<float, float>(c, wk, C, D, nv, HCb, D, s + kDots))) return rc;
-      if ((rc = multidot<double, float>(c, wk, AW, D, 2, Cb, D, s + kDots + nv))) return rc;
-      if ((rc = multidot<float, float>(c, wk, C, D, nv, Cb, D, s + kDots + nv + 2))) return rc;
+      // (<C_k|HC_j>, <C_k|C_j>) for k <= j with one read of C; <W|C_j>, <HW|C_j>
+      {
+        dim3 grid(kRedBlocks, (unsigned)((nv + kDotChunk - 1) / kDotChunk));
+        multidot2_kernel<float, float><<<grid, kRedThreads, 0, c->stream>>>(C, D, nv, HCb, Cb, D, wk.partial);
+        SBDX_LAUNCHED(c);
+        if ((rc = finalize(c, wk, 2 * nv, s + kDots))) return rc;
+      }
+      if ((rc = multidot<double, float>(c, wk, AW, D, 2, Cb, D, s + kDots + 2 * nv))) return rc;
       SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kDots, sizeof(double) * (2 * nv + 2), cudaMemcpyDeviceToHost,
                                    c->stream));
       SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
       for (int k = 0; k < nv; ++k) {
-        set_pair(M, k + 1, j + 1, col[k]);
-        set_pair(S, k + 1, j + 1, col[nv + 2 + k]);
+        set_pair(M, k + 1, j + 1, col[2 * k]);
+        set_pair(S, k + 1, j + 1, col[2 * k + 1]);
       }
-      set_pair(S, 0, j + 1, col[nv]);
-      set_pair(M, 0, j + 1, col[nv + 1]);
+      set_pair(S, 0, j + 1, col[2 * nv]);
+      set_pair(M, 0, j + 1, col[2 * nv + 1]);
       const int n = nv + 1;
       double theta = 0.0;
       if (!gen_eigen(n, M, S, ld, theta, x)) {
@@ -714,30 +749,30 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
       update_anchor_kernel<float><<<kRedBlocks, kRedThreads, 0, c->stream>>>(C, HC, D, nv, wk.u, x[0], s + kE0, D,
                                                                              W, HW, R, wk.partial);
       SBDX_LAUNCHED(c);
+      // |W|^2 (kNW) and |R|^2 (kNR). x is S-normalised and S holds the exact dots
+      // of the stored vectors, so the new anchor has unit norm to rounding.
       if ((rc = finalize(c, wk, 2, s + kNW))) return rc;
-      scale3_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, R, s + kNW, D);
-      SBDX_LAUNCHED(c);
       double nrm[2];
       SBDX_CUDA(c, cudaMemcpyAsync(nrm, s + kNW, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
       SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
-      const double nw = std::sqrt(nrm[0]);
-      const double r_est = std::sqrt(nrm[1]) / nw;
-      // projected row of the new anchor (divided by its norm like the vectors)
+      const double r_est = std::sqrt(nrm[1]);
+      if (std::fabs(nrm[0] - 1.0) > 1e-6) {
+        c->err = "davidson (FP32): Ritz vector lost its normalisation";
+        return 5;
+      }
+      // projected row of the new anchor: x^T M, x^T S
       for (int k = 0; k < n; ++k) {
         double sm = 0.0, ss = 0.0;
         for (int i = 0; i < n; ++i) {
           sm += x[i] * M[std::min(i, k) + (size_t)ld * std::max(i, k)];
           ss += x[i] * S[std::min(i, k) + (size_t)ld * std::max(i, k)];
         }
-        row[k] = sm / nw;
-        row[ld + k] = ss / nw;
+        row[k] = sm;
+        row[ld + k] = ss;
       }
       for (int k = 1; k < n; ++k) { set_pair(M, 0, k, row[k]); set_pair(S, 0, k, row[ld + k]); }
-      set_pair(M, 0, 0, theta / (nw * nw));
+      set_pair(M, 0, 0, theta);
       set_pair(S, 0, 0, 1.0);
-      // R/|R| is what the next expansion uses; kNR must hold |R|^2 of the scaled R
-      const double nr2 = r_est * r_est;
-      SBDX_CUDA(c, cudaMemcpyAsync(s + kNR, &nr2, sizeof(double), cudaMemcpyHostToDevice, c->stream));
       Eanc = theta;
       if (p.verbose) {
         std::printf("   step %d: theta=%.12f est.res=%.3e\n", steps, theta, r_est);

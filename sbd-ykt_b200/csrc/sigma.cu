@@ -1261,6 +1261,159 @@ sigma_ab_v6_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
   }
 }
 
+// 16-byte packs of the staged rows of the alpha-beta kernel v7: element e of
+// the pack of ket index jb is C'[ja_e, jb] (and of pair index pq, the signed
+// integral s_alpha(ja_e) (a_e i_e|pq)).
+template <typename T> struct RowPack;
+template <> struct RowPack<double> {
+  using P = double2;
+  static constexpr int kRows = 2;
+  static __device__ __forceinline__ void set(P& p, int e, double v) { if (e == 0) p.x = v; else p.y = v; }
+  static __device__ __forceinline__ double dot(const P& a, const P& b) { return fma(a.x, b.x, a.y * b.y); }
+};
+template <> struct RowPack<float> {
+  using P = float4;
+  static constexpr int kRows = 4;
+  static __device__ __forceinline__ void set(P& p, int e, float v) {
+    if (e == 0) p.x = v; else if (e == 1) p.y = v; else if (e == 2) p.z = v; else p.w = v;
+  }
+  static __device__ __forceinline__ double dot(const P& a, const P& b) {
+    return fma((double)a.x, (double)b.x,
+               fma((double)a.y, (double)b.y, fma((double)a.z, (double)b.z, (double)a.w * (double)b.w)));
+  }
+};
+
+// Alpha single x beta single, v7: as v6 (balanced SELL-32, alpha-first signs,
+// split rows, one CTA per (bra alpha row, chunk)), with the staged rows
+// interleaved into 16-byte packs (2 FP64 or 4 FP32 rows per group): a record
+// costs two 128-bit shared loads (ket pack, integral pack) for all rows of
+// the group, and the alpha sign is applied to the integrals when they are
+// staged, so the per-record sign is the beta one only.
+template <typename T, int KS>
+__global__ void __launch_bounds__(kAb6Threads, 1)
+sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restrict__ a_off,
+                   const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
+                   const uint32_t* __restrict__ a_info, const uint64_t* __restrict__ sell,
+                   const uint64_t* __restrict__ soff, const uint32_t* __restrict__ slen, size_t nslice,
+                   const uint32_t* __restrict__ vrow, size_t nv, const uint32_t* __restrict__ split_row,
+                   const uint32_t* __restrict__ split_slot, int nsplit, const T* __restrict__ Vt, size_t vstride,
+                   int npair, double* __restrict__ Y) {
+  using RP = RowPack<T>;
+  using P = typename RP::P;
+  constexpr int VR = RP::kRows;
+  constexpr int kWarps = kAb6Threads / 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  P* xs = reinterpret_cast<P*>(smem);   // [nb]
+  P* er = xs + nb;                      // [npair]
+  double* part = reinterpret_cast<double*>(er + npair);
+  const size_t ia = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t slice0 = (size_t)blockIdx.y * kWarps * KS;
+  auto slice_of = [&](int k) -> size_t {
+    return slice0 + (size_t)k * kWarps + ((k & 1) ? (kWarps - 1 - warp) : warp);
+  };
+  double acc[KS];
+#pragma unroll
+  for (int k = 0; k < KS; ++k) acc[k] = 0.0;
+  const uint64_t e0 = a_off[ia];
+  const int ns = (int)a_nsing[ia];
+  for (int k0 = 0; k0 < ns; k0 += VR) {
+    const int nr = min(VR, ns - k0);
+    const T* xrow[VR];
+    const T* vrow_p[VR];
+    bool neg[VR];
+#pragma unroll
+    for (int e = 0; e < VR; ++e) {
+      const uint64_t ent = e0 + k0 + (e < nr ? e : 0);
+      const uint32_t inf = a_info[ent];
+      xrow[e] = Xp + (size_t)a_ket[ent] * nb;
+      vrow_p[e] = Vt + (size_t)((inf >> 12) & 0xfffu) * vstride;
+      neg[e] = (inf >> 31) != 0;
+    }
+    __syncthreads();
+    for (size_t t = threadIdx.x; t < nb; t += kAb6Threads) {
+      P p;
+#pragma unroll
+      for (int e = 0; e < VR; ++e) RP::set(p, e, e < nr ? __ldg(xrow[e] + t) : (T)0);
+      xs[t] = p;
+    }
+    for (int t = threadIdx.x; t < npair; t += kAb6Threads) {
+      P p;
+#pragma unroll
+      for (int e = 0; e < VR; ++e) {
+        const T v = e < nr ? __ldg(vrow_p[e] + t) : (T)0;
+        RP::set(p, e, neg[e] ? -v : v);
+      }
+      er[t] = p;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < KS; ++k) {
+      const size_t sl = slice_of(k);
+      if (sl >= nslice) continue;
+      const uint32_t len = slen[sl];
+      const uint64_t* rp = sell + soff[sl] + lane;
+      double s = acc[k];
+      uint64_t next = len ? __ldg(rp) : 0ull;
+      for (uint32_t m = 0; m < len; ++m) {
+        const uint64_t rec = next;
+        if (m + 1 < len) next = __ldg(rp + 32ull * (m + 1));
+        const P x = xs[rec & 0xffffu];
+        const P ev = er[(rec >> 16) & 0xfffu];
+        double d = RP::dot(ev, x);
+        d = ((rec >> 41) & 1ull) ? 0.0 : d;
+        s += flip_sign(d, (uint32_t)(rec >> 40) & 1u);
+      }
+      acc[k] = s;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < KS; ++k) {
+    const size_t sl = slice_of(k);
+    const size_t pos = sl * 32 + lane;
+    if (sl < nslice && pos < nv) {
+      const uint32_t w = vrow[pos];
+      const uint32_t slot1 = w >> 16;
+      if (slot1 == 0) Y[ia * nb + (w & 0xffffu)] += acc[k];
+      else part[slot1 - 1] = acc[k];
+    }
+  }
+  if (blockIdx.y == 0 && nsplit > 0) {
+    __syncthreads();
+    for (int s = threadIdx.x; s < nsplit; s += kAb6Threads) {
+      double t = 0.0;
+      for (uint32_t j = split_slot[s]; j < split_slot[s + 1]; ++j) t += part[j];
+      Y[ia * nb + split_row[s]] += t;
+    }
+  }
+}
+
+// Shared memory of v7: nb + npair 16-byte packs plus the split slots.
+size_t ab7_smem_bytes(const Ctx* c) {
+  return 16 * (c->nb + c->npair) + sizeof(double) * (size_t)c->conn[1].nslot;
+}
+constexpr size_t kAbSmemBudget = 227 * 1024 - 1024;
+
+template <typename T, int KS>
+int launch_ab_v7(Ctx* c, const T* Xp) {
+  const Conn& ca = c->conn[0];
+  const Conn& cb = c->conn[1];
+  const bool f64 = std::is_same<T, double>::value;
+  const T* Vt = f64 ? (const T*)c->d_V : (const T*)c->d_V32;
+  const size_t vs = f64 ? c->vstride : c->vstride32;
+  const size_t smem = ab7_smem_bytes(c);
+  SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v7_kernel<T, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  const size_t per_cta = (size_t)(kAb6Threads / 32) * KS;
+  dim3 grid((unsigned)c->na, (unsigned)((cb.bnslice + per_cta - 1) / per_cta));
+  if (grid.y == 0) grid.y = 1;
+  sigma_ab_v7_kernel<T, KS><<<grid, kAb6Threads, smem, c->stream>>>(
+      Xp, c->nb, ca.off, ca.nsing, ca.ket, ca.info, cb.bsell, cb.bsoff, cb.bslen, cb.bnslice, cb.vrow, cb.nv,
+      cb.split_row, cb.split_slot, cb.nsplit, Vt, vs, (int)c->npair, c->d_y);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
 template <typename T, int VEC>
 int launch_same_v6(Ctx* c, const T* X, size_t nrow, size_t ncol, const Conn& cn, const typename Prec<T>::V* val,
                    const typename Prec<T>::V* Dt, size_t dstride, const double* hii, double* Y) {
@@ -1319,6 +1472,15 @@ int launch_ab_v6_ks(Ctx* c, const T* Xp, size_t smem, size_t xstride) {
 template <typename T>
 int run_ab_v6(Ctx* c, int code, const T* Xp) {
   using V = typename Prec<T>::V;
+  if (code / 10 == 7) {  // 71: packed rows, when nb + npair packs fit in shared memory
+    if (ab7_smem_bytes(c) <= kAbSmemBudget) {
+      const int ks = c->conn[1].slices_per_warp;
+      if (ks >= 16) return launch_ab_v7<T, 16>(c, Xp);
+      if (ks >= 12) return launch_ab_v7<T, 12>(c, Xp);
+      return launch_ab_v7<T, 8>(c, Xp);
+    }
+    code = std::is_same<T, double>::value ? 62 : 64;
+  }
   const bool f64 = std::is_same<T, double>::value;
   const size_t vs = f64 ? c->vstride : c->vstride32;
   const size_t per = 16 / sizeof(T);
@@ -1341,7 +1503,9 @@ int run_ab_v6(Ctx* c, int code, const T* Xp) {
   return launch_ab_v6_ks<T, 1>(c, Xp, smem, xstride);
 }
 
-bool is_v6(const Tune& t) { return t.same_code > 20 && t.same_code < 30 && t.ab_code > 60 && t.ab_code < 70; }
+bool is_v6(const Tune& t) {
+  return t.same_code > 20 && t.same_code < 30 && ((t.ab_code > 60 && t.ab_code < 70) || t.ab_code == 71);
+}
 
 template <typename T>
 int run_sigma_v6(Ctx* c, const Tune& tune, const T* X, T* S) {
@@ -1445,13 +1609,13 @@ int run_sigma_v5(Ctx* c, const T* X, T* S) {
 }
 
 // Default launch codes: the alpha-first (v6) kernels.
-constexpr Tune kDefaultTune[2] = {{24, 62}, {28, 64}};
+constexpr Tune kDefaultTune[2] = {{24, 71}, {28, 71}};
 
 Tune effective_tune(const Ctx* c, bool f64) {
   Tune t = c->tune[f64 ? 0 : 1];
   const Tune& d = kDefaultTune[f64 ? 0 : 1];
   const bool v6 = (t.same_code > 20 && t.same_code < 30) || (t.ab_code > 60 && t.ab_code < 70) ||
-                  (t.same_code == 0 && t.ab_code == 0);
+                  t.ab_code == 71 || (t.same_code == 0 && t.ab_code == 0);
   if (v6) {
     if (t.same_code == 0) t.same_code = d.same_code;
     if (t.ab_code == 0) t.ab_code = d.ab_code;
@@ -1547,7 +1711,7 @@ int autotune(Ctx* c) {
     for (auto& e : c->ev) SBDX_CUDA(c, cudaEventCreate(&e));
   c->profiling = true;
   const int same_cand[] = {24, 28, 22};
-  const int ab_cand[] = {62, 61, 63, 64};
+  const int ab_cand[] = {71, 62, 61, 63, 64};
   for (int prec = 0; prec < 2 && rc == 0; ++prec) {
     const Tune saved = c->tune[prec];
     auto measure = [&](int same, int ab, double* same_ms, double* ab_ms) -> int {

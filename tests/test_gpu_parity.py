@@ -76,7 +76,7 @@ def _skewed(name, scale, nb):
 
 
 @pytest.mark.parametrize("name,scale,nb", SKEWED)
-@pytest.mark.parametrize("tuning", [(0, 0), (21, 61), (28, 64), (14, 42)])
+@pytest.mark.parametrize("tuning", [(0, 0), (21, 61), (28, 64), (24, 71), (14, 42)])
 def test_sigma_split_lists_and_orderings(name, scale, nb, tuning, port):
     """Default (alpha-first, balanced) and explicit launch codes, including the
     interleaved kernels, against the oracle."""
