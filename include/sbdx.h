@@ -179,6 +179,20 @@ typedef struct {
 int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_from_W, double* W,
                   sbdx_davidson_info* info);
 
+/* Several lowest roots; no counterpart in the reference, whose Davidson is
+ * single-root. W: host buffer of nroots*na*nb doubles (root r at offset
+ * r*na*nb); on input the start vectors if init_from_W != 0, else unit vectors
+ * on the nroots lowest diagonal elements; on output the orthonormal Ritz
+ * vectors. energies and residuals (may be NULL): nroots doubles each, the
+ * Rayleigh quotients and exact residual norms |H W_r - E_r W_r|. 1 <= nroots
+ * <= 4. SBDX_FP64: block Davidson whose subspace holds the nroots Ritz
+ * vectors plus max_nb FP64 corrections; SBDX_FP32: the mixed-precision solver
+ * with one FP64 anchor per root and 2*max_nb FP32 corrections. Both add one
+ * Olsen-corrected preconditioned residual per unconverged root per step.
+ * Converged when every exact residual is below eps. */
+int sbdx_davidson_roots(sbdx_ctx* ctx, const sbdx_davidson_params* params, int nroots, int init_from_W,
+                        double* W, double* energies, double* residuals, sbdx_davidson_info* info);
+
 /* 1-/2-RDM of a vector W (host, na*nb doubles). Replaces Correlation
  * (chemistry/tpb/correlation.h:194-444). one: 2*L*L doubles; two: 4*L^4
  * doubles (may be NULL to skip the 2-RDM). */

@@ -2,6 +2,7 @@
 // here, before any kernel sees it: sizes, orbital range, equal electron counts
 // per spin, finite integrals. No C++ exception crosses the boundary.
 #include "sbdx.h"
+#include <vector>
 #include "sbdx_internal.cuh"
 
 #include <cmath>
@@ -34,6 +35,9 @@ int check_device_error(Ctx* c) {
 void free_connectivity(Ctx* c);
 int build_g_table(Ctx* c);
 int davidson(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info);
+int davidson_roots(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, double* E, double* res,
+                   sbdx_davidson_info& info);
+int lowest_diagonal(Ctx* c, int k, std::vector<size_t>& idx);
 int rdm_device(Ctx* c, const double* dW, double* d_one, double* d_two);
 int occupation_device(Ctx* c, const double* dW, double* d_density);
 int alpha_weights_device(Ctx* c, const double* dW, double* d_w);
@@ -375,6 +379,47 @@ int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_fr
     if ((rc = sbdx::check_device_error(c))) return rc;
     SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * D, cudaMemcpyDeviceToHost, c->stream));
     SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (info) *info = inf;
+    return SBDX_OK;
+  });
+}
+
+int sbdx_davidson_roots(sbdx_ctx* ctx, const sbdx_davidson_params* params, int nroots, int init_from_W,
+                        double* W, double* energies, double* residuals, sbdx_davidson_info* info) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!params || !W || !energies) { c->err = "davidson_roots: null pointer"; return SBDX_ERR_ARG; }
+    if (nroots < 1 || nroots > 4) { c->err = "davidson_roots: nroots must be in [1, 4]"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "davidson_roots");
+    if (rc) return rc;
+    const size_t D = c->na * c->nb;
+    if ((size_t)nroots > D) { c->err = "davidson_roots: more roots than determinants"; return SBDX_ERR_ARG; }
+    if (init_from_W)
+      for (size_t q = 0; q < D * nroots; ++q)
+        if (!std::isfinite(W[q])) { c->err = "davidson_roots: non-finite start vector"; return SBDX_ERR_NUMERIC; }
+    double* dW = nullptr;
+    SBDX_CUDA(c, cudaMalloc(&dW, sizeof(double) * D * nroots));
+    struct Guard { double* p; ~Guard() { cudaFree(p); } } g{dW};
+    if (init_from_W) {
+      SBDX_CUDA(c, cudaMemcpyAsync(dW, W, sizeof(double) * D * nroots, cudaMemcpyHostToDevice, c->stream));
+    } else {  // unit vectors on the nroots lowest diagonal elements
+      std::vector<size_t> idx;
+      if ((rc = sbdx::lowest_diagonal(c, nroots, idx))) return rc;
+      SBDX_CUDA(c, cudaMemsetAsync(dW, 0, sizeof(double) * D * nroots, c->stream));
+      static const double one = 1.0;
+      for (int r = 0; r < nroots; ++r)
+        SBDX_CUDA(c, cudaMemcpyAsync(dW + (size_t)r * D + idx[r], &one, sizeof(double), cudaMemcpyHostToDevice,
+                                     c->stream));
+    }
+    std::vector<double> e(nroots), res(nroots);
+    sbdx_davidson_info inf{};
+    if ((rc = sbdx::davidson_roots(c, *params, nroots, dW, e.data(), res.data(), inf))) return rc;
+    if ((rc = sbdx::check_device_error(c))) return rc;
+    SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * D * nroots, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int r = 0; r < nroots; ++r) {
+      energies[r] = e[r];
+      if (residuals) residuals[r] = res[r];
+    }
     if (info) *info = inf;
     return SBDX_OK;
   });

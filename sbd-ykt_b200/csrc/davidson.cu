@@ -28,6 +28,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <type_traits>
 
 namespace sbdx {
@@ -794,6 +795,462 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
   return 0;
 }
 
+// ---- several roots: FP64 anchors + corrections (FP32 or FP64) ---------------
+//
+// Basis [W_0..W_{k-1}, C_0..C_{nv-1}]: the anchors are the current Ritz vectors
+// of the k lowest roots, kept in FP64 with their products HW_r; the
+// corrections C_j (type TC) carry products HC_j of the same type. Each step
+// adds one Olsen-corrected preconditioned residual per root that is not yet
+// converged, solves the generalised projected problem M x = theta S x (M, S
+// from exact FP64 dots of the stored vectors), and moves the anchors to the
+// new Ritz vectors (W'_r = X^T basis, HW'_r = X^T products, out of place).
+// With FP32 corrections HW'_r carries the FP32 error of the products, so the
+// anchors are refreshed with exact FP64 sigmas when the largest estimated
+// residual has fallen 1e4-fold since the last exact one (or below eps);
+// convergence is decided on exact residuals only. With FP64 corrections the
+// products are exact and no refresh is needed.
+
+// Scalar slots of the block solver in Work::scal.
+enum { kbAB = 0, kbOlap = 2, kbNV = 3, kbTheta = 4, kbNW2 = 8, kbNR2 = 12, kbDots = 16 };
+constexpr int kMaxRoots = 4;
+
+// v -= sum_a o[a] A_a (FP64, na vectors) + sum_k o[na + k] V_k; partial |v|^2.
+template <typename TV>
+__global__ void __launch_bounds__(kRedThreads)
+gs_subtract_block_kernel(double* __restrict__ v, const double* __restrict__ A, int na, const TV* __restrict__ V,
+                         int m, const double* __restrict__ o, size_t D, double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  __shared__ double so[72];
+  for (int k = threadIdx.x; k < na + m; k += blockDim.x) so[k] = o[k];
+  __syncthreads();
+  double nn = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    double x = v[s];
+    for (int a = 0; a < na; ++a) x = fma(-so[a], A[(size_t)a * D + s], x);
+    for (int k = 0; k < m; ++k) x = fma(-so[na + k], (double)V[(size_t)k * D + s], x);
+    v[s] = x;
+    nn = fma(x, x, nn);
+  }
+  const double t = block_sum(nn, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+// For each root r < K: W'_r = sum_a X[a][r] W_a + sum_j X[K+j][r] C_j, the same
+// for HW', and R_r = theta_r W'_r - HW'_r (all FP64, out of place). Partials
+// |W'_r|^2 (slot r) and |R_r|^2 (slot K + r). X is column-major n x K.
+template <typename TC, int K>
+__global__ void __launch_bounds__(kRedThreads)
+update_anchors_kernel(const double* __restrict__ W, const double* __restrict__ HW, const TC* __restrict__ C,
+                      const TC* __restrict__ HC, int m, const double* __restrict__ X, const double* __restrict__ theta,
+                      size_t D, double* __restrict__ Wn, double* __restrict__ HWn, double* __restrict__ R,
+                      double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  __shared__ double sx[(kMaxRoots + 64) * kMaxRoots];
+  const int n = K + m;
+  for (int t = threadIdx.x; t < n * K; t += blockDim.x) sx[t] = X[t];
+  __syncthreads();
+  double th[K];
+#pragma unroll
+  for (int r = 0; r < K; ++r) th[r] = theta[r];
+  double nw[K], nr[K];
+#pragma unroll
+  for (int r = 0; r < K; ++r) nw[r] = nr[r] = 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    double w[K], hw[K];
+#pragma unroll
+    for (int r = 0; r < K; ++r) w[r] = hw[r] = 0.0;
+#pragma unroll
+    for (int a = 0; a < K; ++a) {
+      const double wa = W[(size_t)a * D + s], ha = HW[(size_t)a * D + s];
+#pragma unroll
+      for (int r = 0; r < K; ++r) {
+        w[r] = fma(sx[a + n * r], wa, w[r]);
+        hw[r] = fma(sx[a + n * r], ha, hw[r]);
+      }
+    }
+    for (int j = 0; j < m; ++j) {
+      const double cj = (double)C[(size_t)j * D + s], hj = (double)HC[(size_t)j * D + s];
+#pragma unroll
+      for (int r = 0; r < K; ++r) {
+        w[r] = fma(sx[K + j + n * r], cj, w[r]);
+        hw[r] = fma(sx[K + j + n * r], hj, hw[r]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < K; ++r) {
+      const double rr = th[r] * w[r] - hw[r];
+      Wn[(size_t)r * D + s] = w[r];
+      HWn[(size_t)r * D + s] = hw[r];
+      R[(size_t)r * D + s] = rr;
+      nw[r] = fma(w[r], w[r], nw[r]);
+      nr[r] = fma(rr, rr, nr[r]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    double t = block_sum(nw[r], sh);
+    if (threadIdx.x == 0) partial[(size_t)r * gridDim.x + blockIdx.x] = t;
+    t = block_sum(nr[r], sh);
+    if (threadIdx.x == 0) partial[(size_t)(K + r) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// R_r = E_r W_r - HW_r for r < k (E in device memory), partial |R_r|^2.
+__global__ void __launch_bounds__(kRedThreads)
+residual_block_kernel(const double* __restrict__ W, const double* __restrict__ HW, const double* __restrict__ E,
+                      int k, size_t D, double* __restrict__ R, double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  for (int r = 0; r < k; ++r) {
+    const double e = E[r];
+    double acc = 0.0;
+    for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+      const double x = e * W[(size_t)r * D + s] - HW[(size_t)r * D + s];
+      R[(size_t)r * D + s] = x;
+      acc = fma(x, x, acc);
+    }
+    const double t = block_sum(acc, sh);
+    if (threadIdx.x == 0) partial[(size_t)r * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// Lowest k eigenpairs of M x = theta S x (n x n, upper triangles of the ld-
+// strided arrays; S positive definite): theta[0..k), X column-major n x k.
+bool gen_eigen_k(int n, int k, const std::vector<double>& M, const std::vector<double>& S, int ld,
+                 std::vector<double>& theta, std::vector<double>& X) {
+  std::vector<double> Lc((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    double d = S[j + (size_t)ld * j];
+    for (int q = 0; q < j; ++q) d -= Lc[j + (size_t)n * q] * Lc[j + (size_t)n * q];
+    if (!(d > 0.0)) return false;
+    d = std::sqrt(d);
+    Lc[j + (size_t)n * j] = d;
+    for (int i = j + 1; i < n; ++i) {
+      double v = S[std::min(i, j) + (size_t)ld * std::max(i, j)];
+      for (int q = 0; q < j; ++q) v -= Lc[i + (size_t)n * q] * Lc[j + (size_t)n * q];
+      Lc[i + (size_t)n * j] = v / d;
+    }
+  }
+  std::vector<double> T((size_t)n * n), A((size_t)n * n);
+  for (int col = 0; col < n; ++col)
+    for (int i = 0; i < n; ++i) {
+      double v = M[std::min(i, col) + (size_t)ld * std::max(i, col)];
+      for (int q = 0; q < i; ++q) v -= Lc[i + (size_t)n * q] * T[q + (size_t)n * col];
+      T[i + (size_t)n * col] = v / Lc[i + (size_t)n * i];
+    }
+  for (int row = 0; row < n; ++row)
+    for (int i = 0; i < n; ++i) {
+      double v = T[row + (size_t)n * i];
+      for (int q = 0; q < i; ++q) v -= Lc[i + (size_t)n * q] * A[row + (size_t)n * q];
+      A[row + (size_t)n * i] = v / Lc[i + (size_t)n * i];
+    }
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < j; ++i) A[i + (size_t)n * j] = A[j + (size_t)n * i] = 0.5 * (A[i + (size_t)n * j] + A[j + (size_t)n * i]);
+  std::vector<double> w(n);
+  jacobi_eigen(n, A.data(), n, w.data());
+  theta.assign(w.begin(), w.begin() + k);
+  X.assign((size_t)n * k, 0.0);
+  for (int r = 0; r < k; ++r)
+    for (int i = n - 1; i >= 0; --i) {  // x = L^-T y
+      double v = A[i + (size_t)n * r];
+      for (int q = i + 1; q < n; ++q) v -= Lc[q + (size_t)n * i] * X[q + (size_t)n * r];
+      X[i + (size_t)n * r] = v / Lc[i + (size_t)n * i];
+    }
+  return true;
+}
+
+// Olsen-corrected preconditioned residual of root r, Gram-Schmidt against the
+// k anchors and the nv corrections (classical, repeated once when the first
+// pass removed more than three quarters of the norm), normalised into dst.
+// Returns 0, or -1 when nothing of the direction is left.
+template <typename TC>
+int expand_block(Ctx* c, Work& wk, const double* Rr, const double* Wr, const double* A, int k, const TC* V, int nv,
+                 size_t D, double* v, double* o, const double* thetap, const double* nr2p, TC* dst) {
+  double* s = wk.scal;
+  olsen_precond_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(Rr, Wr, c->d_hii, thetap, nr2p, D, v, wk.partial);
+  SBDX_LAUNCHED(c);
+  int rc = finalize(c, wk, 2, s + kbAB);
+  if (rc) return rc;
+  olsen_apply_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(v, Wr, c->d_hii, thetap, s + kbAB, D, wk.partial);
+  SBDX_LAUNCHED(c);
+  if ((rc = finalize(c, wk, 2, s + kbOlap))) return rc;  // kbOlap, kbNV
+  double before = 0.0;
+  SBDX_CUDA(c, cudaMemcpyAsync(&before, s + kbNV, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  for (int pass = 0; pass < 2; ++pass) {
+    if ((rc = multidot<double, double>(c, wk, A, D, k, v, D, o))) return rc;
+    if (nv > 0 && (rc = multidot<TC, double>(c, wk, V, D, nv, v, D, o + k))) return rc;
+    gs_subtract_block_kernel<TC><<<kRedBlocks, kRedThreads, 0, c->stream>>>(v, A, k, V, nv, o, D, wk.partial);
+    SBDX_LAUNCHED(c);
+    if ((rc = finalize(c, wk, 1, s + kbNV))) return rc;
+    double after = 0.0;
+    SBDX_CUDA(c, cudaMemcpyAsync(&after, s + kbNV, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (!(after > 1e-24 * before)) return -1;
+    if (after > 0.0625 * before) break;
+    before = after;
+  }
+  scale_store_kernel<TC, double><<<kRedBlocks, kRedThreads, 0, c->stream>>>(v, s + kbNV, D, dst);
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+template <typename TC>
+int launch_update_anchors(Ctx* c, Work& wk, int k, const double* W, const double* HW, const TC* C, const TC* HC,
+                          int m, const double* X, const double* theta, size_t D, double* Wn, double* HWn, double* R) {
+  switch (k) {
+    case 1: update_anchors_kernel<TC, 1><<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, C, HC, m, X, theta, D, Wn, HWn, R, wk.partial); break;
+    case 2: update_anchors_kernel<TC, 2><<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, C, HC, m, X, theta, D, Wn, HWn, R, wk.partial); break;
+    case 3: update_anchors_kernel<TC, 3><<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, C, HC, m, X, theta, D, Wn, HWn, R, wk.partial); break;
+    default: update_anchors_kernel<TC, 4><<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, C, HC, m, X, theta, D, Wn, HWn, R, wk.partial); break;
+  }
+  SBDX_LAUNCHED(c);
+  return 0;
+}
+
+// dW: k device vectors of D (start vectors in, Ritz vectors out); E, res: k.
+template <typename TC>
+int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, double* E, double* res,
+                   sbdx_davidson_info& info) {
+  constexpr bool kMixed = std::is_same<TC, float>::value;
+  const size_t D = c->na * c->nb;
+  const int nc = std::max(std::min(kMixed ? 2 * p.max_nb : p.max_nb, 64 - k), 2 * k);
+  const int keep = std::max(k, nc / 3);
+  const int period = p.defect_every > 0 ? p.defect_every : 0;
+  Work wk;
+  SBDX_CUDA(c, cudaMalloc(&wk.partial, sizeof(double) * kRedBlocks * (2 * nc + 2 * kMaxRoots + 4)));
+  SBDX_CUDA(c, cudaMalloc(&wk.scal, sizeof(double) * (kbDots + (size_t)(k + 2) * nc + 64)));
+  SBDX_CUDA(c, cudaMalloc(&wk.u, sizeof(double) * ((size_t)(k + nc) * k + k + nc + 8)));
+  TC *C = nullptr, *HC = nullptr;
+  double *A = nullptr, *R = nullptr, *V = nullptr;
+  SBDX_CUDA(c, cudaMalloc(&C, sizeof(TC) * D * nc));
+  SBDX_CUDA(c, cudaMalloc(&HC, sizeof(TC) * D * nc));
+  SBDX_CUDA(c, cudaMalloc(&A, sizeof(double) * D * 4 * k));  // W | HW | W' | HW'
+  SBDX_CUDA(c, cudaMalloc(&R, sizeof(double) * D * k));
+  SBDX_CUDA(c, cudaMalloc(&V, sizeof(double) * D));
+  struct Guard {
+    void *a, *b, *c, *d, *e;
+    ~Guard() { cudaFree(a); cudaFree(b); cudaFree(c); cudaFree(d); cudaFree(e); }
+  } g{C, HC, A, R, V};
+  double* W = A;
+  double* HW = A + D * k;
+  double* Wn = A + 2 * D * k;
+  double* HWn = A + 3 * D * k;
+  double* s = wk.scal;
+  double* gso = wk.u;                       // Gram-Schmidt coefficients (k + nc)
+  double* Xd = wk.u + k + nc + 8;           // Ritz coefficients (k + nc) x k
+  const auto t0 = std::chrono::steady_clock::now();
+  int rc = 0;
+  // start vectors: MGS-orthonormalised in FP64
+  SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * D * k, cudaMemcpyDeviceToDevice, c->stream));
+  for (int r = 0; r < k; ++r) {
+    double* wr = W + (size_t)r * D;
+    for (int pass = 0; pass < 2 && r > 0; ++pass) {
+      if ((rc = multidot<double, double>(c, wk, W, D, r, wr, D, gso))) return rc;
+      gs_subtract_block_kernel<double><<<kRedBlocks, kRedThreads, 0, c->stream>>>(wr, W, r, (const double*)nullptr, 0,
+                                                                                gso, D, wk.partial);
+      SBDX_LAUNCHED(c);
+    }
+    if ((rc = multidot<double, double>(c, wk, wr, D, 1, wr, D, s + kbNV))) return rc;
+    scale_store_kernel<double, double><<<kRedBlocks, kRedThreads, 0, c->stream>>>(wr, s + kbNV, D, wr);
+    SBDX_LAUNCHED(c);
+  }
+  const int ld = k + nc;
+  std::vector<double> M((size_t)ld * ld, 0.0), S((size_t)ld * ld, 0.0), col((size_t)(k + 2) * nc + 64), theta, X,
+      rowM((size_t)k * ld), rowS((size_t)k * ld), h(4 * kMaxRoots + 8);
+  std::vector<double> r_est(k, 1e300), r_exact(k, 1e300);
+  int nv = 0;
+  auto set_pair = [&](std::vector<double>& Q, int i, int j, double v) {
+    Q[i + (size_t)ld * j] = v;
+    Q[j + (size_t)ld * i] = v;
+  };
+  // exact products of the anchors; anchor block of M and S; exact residuals
+  auto refresh = [&]() -> int {
+    for (int r = 0; r < k; ++r) {
+      int r2 = sigma_typed<double>(c, W + (size_t)r * D, HW + (size_t)r * D);
+      if (r2) return r2;
+      info.n_sigma64++;
+    }
+    int r2;
+    for (int r = 0; r < k; ++r) {
+      if ((r2 = multidot<double, double>(c, wk, W, D, k, HW + (size_t)r * D, D, s + kbDots + 2 * k * r))) return r2;
+      if ((r2 = multidot<double, double>(c, wk, W, D, k, W + (size_t)r * D, D, s + kbDots + 2 * k * r + k))) return r2;
+    }
+    SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kbDots, sizeof(double) * 2 * k * k, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int r = 0; r < k; ++r)
+      for (int q = 0; q <= r; ++q) {
+        set_pair(M, q, r, col[2 * k * r + q]);
+        set_pair(S, q, r, col[2 * k * r + k + q]);
+      }
+    for (int r = 0; r < k; ++r) h[r] = M[r + (size_t)ld * r] / S[r + (size_t)ld * r];
+    SBDX_CUDA(c, cudaMemcpyAsync(s + kbTheta, h.data(), sizeof(double) * k, cudaMemcpyHostToDevice, c->stream));
+    residual_block_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, s + kbTheta, k, D, R, wk.partial);
+    SBDX_LAUNCHED(c);
+    if ((r2 = finalize(c, wk, k, s + kbNR2))) return r2;
+    SBDX_CUDA(c, cudaMemcpyAsync(h.data() + kMaxRoots, s + kbNR2, sizeof(double) * k, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int r = 0; r < k; ++r) {
+      E[r] = h[r];
+      r_exact[r] = r_est[r] = std::sqrt(h[kMaxRoots + r]);
+    }
+    if (nv > 0) {  // <HW_r|C_j> with the exact products (<W_r|C_j> is unchanged)
+      for (int r = 0; r < k; ++r)
+        if ((r2 = multidot<TC, double>(c, wk, C, D, nv, HW + (size_t)r * D, D, s + kbDots + (size_t)r * nv))) return r2;
+      SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kbDots, sizeof(double) * k * nv, cudaMemcpyDeviceToHost, c->stream));
+      SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+      for (int r = 0; r < k; ++r)
+        for (int j = 0; j < nv; ++j) set_pair(M, r, k + j, col[(size_t)r * nv + j]);
+    }
+    return 0;
+  };
+  if ((rc = refresh())) return rc;
+  double r_ref = *std::max_element(r_exact.begin(), r_exact.end());
+  int steps = 0, since = 0;
+  const int max_steps = p.max_it * p.max_nb;
+  bool stalled = false;
+  auto all_below = [&](const std::vector<double>& x) {
+    for (double v : x) if (!(v < p.eps)) return false;
+    return true;
+  };
+  while (true) {
+    if (p.verbose) {
+      std::printf(" Davidson block step %d: E0=%.12f max exact residual %.6e\n", steps, E[0],
+                  *std::max_element(r_exact.begin(), r_exact.end()));
+      std::fflush(stdout);
+    }
+    if (all_below(r_exact)) { info.converged = 1; break; }
+    if (steps >= max_steps || seconds_since(t0) > p.max_time || stalled) break;
+    bool exact = false;
+    while (!exact) {
+      // expansions, one per root whose residual is not below eps
+      int added = 0;
+      for (int r = 0; r < k; ++r) {
+        if (r_est[r] < p.eps) continue;
+        if (nv == nc) {  // thick restart: keep the newest corrections beside the anchors
+          const int drop = nc - keep;
+          SBDX_CUDA(c, cudaMemcpyAsync(C, C + (size_t)drop * D, sizeof(TC) * D * keep, cudaMemcpyDeviceToDevice, c->stream));
+          SBDX_CUDA(c, cudaMemcpyAsync(HC, HC + (size_t)drop * D, sizeof(TC) * D * keep, cudaMemcpyDeviceToDevice, c->stream));
+          for (int i = 0; i < k + keep; ++i)
+            for (int j = 0; j < k + keep; ++j) {
+              const int si = i < k ? i : i + drop, sj = j < k ? j : j + drop;
+              M[i + (size_t)ld * j] = M[si + (size_t)ld * sj];
+              S[i + (size_t)ld * j] = S[si + (size_t)ld * sj];
+            }
+          nv = keep;
+        }
+        rc = expand_block<TC>(c, wk, R + (size_t)r * D, W + (size_t)r * D, W, k, C, nv, D, V, gso, s + kbTheta + r,
+                              s + kbNR2 + r, C + (size_t)nv * D);
+        if (rc > 0) return rc;
+        if (rc < 0) { rc = 0; continue; }
+        const int j = nv++;
+        TC* Cb = C + (size_t)j * D;
+        TC* HCb = HC + (size_t)j * D;
+        if ((rc = sigma_typed<TC>(c, Cb, HCb))) return rc;
+        if (kMixed) info.n_sigma++; else info.n_sigma64++;
+        ++added;
+        // (<C_i|HC_j>, <C_i|C_j>) for i <= j; <W_r|C_j>, <HW_r|C_j>
+        {
+          dim3 grid(kRedBlocks, (unsigned)((nv + kDotChunk - 1) / kDotChunk));
+          multidot2_kernel<TC, TC><<<grid, kRedThreads, 0, c->stream>>>(C, D, nv, HCb, Cb, D, wk.partial);
+          SBDX_LAUNCHED(c);
+          if ((rc = finalize(c, wk, 2 * nv, s + kbDots))) return rc;
+        }
+        // W and HW are contiguous (HW = W + k*D) in either half of A
+        if ((rc = multidot<double, TC>(c, wk, W, D, 2 * k, Cb, D, s + kbDots + 2 * nv))) return rc;
+        SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kbDots, sizeof(double) * (2 * nv + 2 * k), cudaMemcpyDeviceToHost,
+                                     c->stream));
+        SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+        for (int i = 0; i < nv; ++i) {
+          set_pair(M, k + i, k + j, col[2 * i]);
+          set_pair(S, k + i, k + j, col[2 * i + 1]);
+        }
+        for (int q = 0; q < k; ++q) {
+          set_pair(S, q, k + j, col[2 * nv + q]);
+          set_pair(M, q, k + j, col[2 * nv + k + q]);
+        }
+      }
+      if (added == 0) {  // nothing new: refresh, or stop if a refresh changes nothing
+        if (since == 0) stalled = true;
+        break;
+      }
+      steps += added;
+      since += added;
+      const int n = k + nv;
+      if (!gen_eigen_k(n, k, M, S, ld, theta, X)) {
+        c->err = "davidson: projected overlap matrix is not positive definite";
+        return 5;
+      }
+      SBDX_CUDA(c, cudaMemcpyAsync(Xd, X.data(), sizeof(double) * n * k, cudaMemcpyHostToDevice, c->stream));
+      SBDX_CUDA(c, cudaMemcpyAsync(s + kbTheta, theta.data(), sizeof(double) * k, cudaMemcpyHostToDevice, c->stream));
+      if ((rc = launch_update_anchors<TC>(c, wk, k, W, HW, C, HC, nv, Xd, s + kbTheta, D, Wn, HWn, R))) return rc;
+      // |W'_r|^2 -> kbNW2 + r, |R_r|^2 -> kbNR2 + r
+      finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, kRedBlocks, k, s + kbNW2);
+      SBDX_LAUNCHED(c);
+      finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial + (size_t)k * kRedBlocks, kRedBlocks, k, s + kbNR2);
+      SBDX_LAUNCHED(c);
+      // A holds [W | HW | W' | HW']; the swaps exchange the halves, HW = W + k*D
+      std::swap(W, Wn);
+      std::swap(HW, HWn);
+      SBDX_CUDA(c, cudaMemcpyAsync(h.data(), s + kbNW2, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->stream));
+      SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+      for (int r = 0; r < k; ++r) {
+        if (std::fabs(h[r] - 1.0) > 1e-6) {
+          c->err = "davidson: Ritz vector lost its normalisation";
+          return 5;
+        }
+        r_est[r] = std::sqrt(h[4 + r]);
+        E[r] = theta[r];
+      }
+      // projected rows of the new anchors: X^T M, X^T S (anchor block: diag(theta), I)
+      for (int r = 0; r < k; ++r)
+        for (int q = 0; q < n; ++q) {
+          double sm = 0.0, ss = 0.0;
+          for (int i = 0; i < n; ++i) {
+            sm += X[i + (size_t)n * r] * M[std::min(i, q) + (size_t)ld * std::max(i, q)];
+            ss += X[i + (size_t)n * r] * S[std::min(i, q) + (size_t)ld * std::max(i, q)];
+          }
+          rowM[(size_t)r * ld + q] = sm;
+          rowS[(size_t)r * ld + q] = ss;
+        }
+      for (int r = 0; r < k; ++r) {
+        for (int j = 0; j < nv; ++j) {
+          set_pair(M, r, k + j, rowM[(size_t)r * ld + k + j]);
+          set_pair(S, r, k + j, rowS[(size_t)r * ld + k + j]);
+        }
+        for (int q = 0; q < k; ++q) {
+          set_pair(M, r, q, r == q ? theta[r] : 0.0);
+          set_pair(S, r, q, r == q ? 1.0 : 0.0);
+        }
+      }
+      if (p.verbose) {
+        std::printf("   step %d: theta0=%.12f est.res0=%.3e\n", steps, theta[0], r_est[0]);
+        std::fflush(stdout);
+      }
+      const double worst = *std::max_element(r_est.begin(), r_est.end());
+      if (!kMixed) {  // exact products: the estimated residuals are exact
+        r_exact = r_est;
+        if (all_below(r_exact) || steps >= max_steps || seconds_since(t0) > p.max_time) break;
+        continue;
+      }
+      const bool due = period > 0 ? since >= period : (worst < kRefreshDrop * r_ref || all_below(r_est));
+      if (due || steps >= max_steps || seconds_since(t0) > p.max_time) exact = true;
+    }
+    if (stalled) break;
+    if (kMixed) {
+      if ((rc = refresh())) return rc;
+      r_ref = *std::max_element(r_exact.begin(), r_exact.end());
+    }
+    since = 0;
+  }
+  // anchors back to the caller's buffer, in the first half of A or not
+  SBDX_CUDA(c, cudaMemcpyAsync(dW, W, sizeof(double) * D * k, cudaMemcpyDeviceToDevice, c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int r = 0; r < k; ++r) res[r] = r_exact[r];
+  info.energy = E[0];
+  info.residual = *std::max_element(r_exact.begin(), r_exact.end());
+  info.seconds = seconds_since(t0);
+  return 0;
+}
+
 }  // namespace
 
 int davidson(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info) {
@@ -806,6 +1263,90 @@ int davidson(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_in
   if (p.precision == 0) return davidson_fp64(c, p, dW, info);
   if (p.precision == 1) return davidson_mixed(c, p, dW, info);
   c->err = "davidson: precision must be SBDX_FP64 or SBDX_FP32";
+  return 1;
+}
+
+namespace {
+
+// Per-block minimum of hii over the indices not in `skip` (at most 4): value
+// and index pairs, reduced on the host.
+__global__ void __launch_bounds__(kRedThreads)
+argmin_kernel(const double* __restrict__ d, size_t D, const unsigned long long* __restrict__ skip, int nskip,
+              double* __restrict__ best_v, unsigned long long* __restrict__ best_i) {
+  __shared__ double sv[kRedThreads];
+  __shared__ unsigned long long si[kRedThreads];
+  double v = 1e300;
+  unsigned long long bi = ~0ull;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+    bool skipped = false;
+    for (int q = 0; q < nskip; ++q) skipped |= (skip[q] == s);
+    if (!skipped && d[s] < v) { v = d[s]; bi = s; }
+  }
+  sv[threadIdx.x] = v;
+  si[threadIdx.x] = bi;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      const double v2 = sv[threadIdx.x + o];
+      const unsigned long long i2 = si[threadIdx.x + o];
+      if (v2 < sv[threadIdx.x] || (v2 == sv[threadIdx.x] && i2 < si[threadIdx.x])) {
+        sv[threadIdx.x] = v2;
+        si[threadIdx.x] = i2;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    best_v[blockIdx.x] = sv[0];
+    best_i[blockIdx.x] = si[0];
+  }
+}
+
+}  // namespace
+
+// Indices of the k lowest diagonal elements (ascending, ties by index).
+int lowest_diagonal(Ctx* c, int k, std::vector<size_t>& idx) {
+  if (!c->have_conn) { int rc = build_connectivity(c); if (rc) return rc; }
+  if (!c->have_hii) { int rc = diag_terms(c); if (rc) return rc; }
+  const size_t D = c->na * c->nb;
+  double* bv = nullptr;
+  unsigned long long *bi = nullptr, *sk = nullptr;
+  SBDX_CUDA(c, cudaMalloc(&bv, sizeof(double) * kRedBlocks));
+  SBDX_CUDA(c, cudaMalloc(&bi, sizeof(unsigned long long) * kRedBlocks));
+  SBDX_CUDA(c, cudaMalloc(&sk, sizeof(unsigned long long) * kMaxRoots));
+  struct Guard { void *a, *b, *c; ~Guard() { cudaFree(a); cudaFree(b); cudaFree(c); } } g{bv, bi, sk};
+  std::vector<double> hv(kRedBlocks);
+  std::vector<unsigned long long> hi(kRedBlocks), chosen;
+  idx.clear();
+  for (int r = 0; r < k && (size_t)r < D; ++r) {
+    if (r > 0)
+      SBDX_CUDA(c, cudaMemcpyAsync(sk, chosen.data(), sizeof(unsigned long long) * r, cudaMemcpyHostToDevice, c->stream));
+    argmin_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->d_hii, D, sk, r, bv, bi);
+    SBDX_LAUNCHED(c);
+    SBDX_CUDA(c, cudaMemcpyAsync(hv.data(), bv, sizeof(double) * kRedBlocks, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaMemcpyAsync(hi.data(), bi, sizeof(unsigned long long) * kRedBlocks, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    double v = 1e300;
+    unsigned long long b = ~0ull;
+    for (int q = 0; q < kRedBlocks; ++q)
+      if (hv[q] < v || (hv[q] == v && hi[q] < b)) { v = hv[q]; b = hi[q]; }
+    chosen.push_back(b);
+    idx.push_back((size_t)b);
+  }
+  return 0;
+}
+
+int davidson_roots(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, double* E, double* res,
+                   sbdx_davidson_info& info) {
+  if (p.max_nb < 1 || p.max_nb > 60 || p.max_it < 1 || k < 1 || k > kMaxRoots) {
+    c->err = "davidson_roots: need 1 <= nroots <= 4, max_nb in [1, 60], max_it >= 1";
+    return 1;
+  }
+  if (!c->have_conn) { int rc = build_connectivity(c); if (rc) return rc; }
+  if (!c->have_hii) { int rc = diag_terms(c); if (rc) return rc; }
+  if (p.precision == 0) return davidson_block<double>(c, p, k, dW, E, res, info);
+  if (p.precision == 1) return davidson_block<float>(c, p, k, dW, E, res, info);
+  c->err = "davidson_roots: precision must be SBDX_FP64 or SBDX_FP32";
   return 1;
 }
 

@@ -31,7 +31,7 @@ EXPORTS = [
     "sbdx_set_integrals", "sbdx_set_strings", "sbdx_build_connectivity", "sbdx_connectivity_size",
     "sbdx_get_connectivity", "sbdx_diag_terms", "sbdx_sigma", "sbdx_sigma_device", "sbdx_davidson",
     "sbdx_rdm", "sbdx_occupation", "sbdx_alpha_weights", "sbdx_energy_backward", "sbdx_set_profiling",
-    "sbdx_phase_times", "sbdx_set_tuning", "sbdx_autotune",
+    "sbdx_phase_times", "sbdx_set_tuning", "sbdx_autotune", "sbdx_davidson_roots",
 ]
 PHASES = ["alpha_same_spin", "transpose", "beta_same_spin", "alpha_beta", "combine"]
 
@@ -201,6 +201,21 @@ class Context:
         info = DavidsonInfo()
         self._check(self.lib.sbdx_davidson(self.h, ctypes.byref(p), ctypes.c_int(init), _d(W), ctypes.byref(info)))
         return info, W
+
+    def davidson_roots(self, nroots, max_it=1, max_nb=10, eps=1e-4, max_time=86400.0, precision=SBDX_FP64,
+                       defect_every=0, verbose=0, W=None):
+        """sbdx_davidson_roots: the nroots lowest eigenpairs. Returns
+        (info, energies[nroots], residuals[nroots], W[nroots, D])."""
+        p = DavidsonParams(max_it, max_nb, eps, max_time, precision, defect_every, verbose)
+        D = self.na * self.nb
+        init = 1 if W is not None else 0
+        Wb = np.zeros((nroots, D)) if W is None else np.ascontiguousarray(W, dtype=np.float64).reshape(nroots, D).copy()
+        E = np.zeros(nroots)
+        res = np.zeros(nroots)
+        info = DavidsonInfo()
+        self._check(self.lib.sbdx_davidson_roots(self.h, ctypes.byref(p), ctypes.c_int(nroots), ctypes.c_int(init),
+                                                 _d(Wb), _d(E), _d(res), ctypes.byref(info)))
+        return info, E, res, Wb
 
     def rdm(self, W, two=True):
         L = self.L
