@@ -184,8 +184,12 @@ void free_conn(Conn& c) {
   cudaFree(c.val); cudaFree(c.val32); cudaFree(c.omask); cudaFree(c.info);
   cudaFree(c.srec); cudaFree(c.order); cudaFree(c.spos);
   cudaFree(c.sell); cudaFree(c.soff); cudaFree(c.slen);
-  cudaFree(c.bsell); cudaFree(c.bsoff); cudaFree(c.bslen); cudaFree(c.vrow);
-  cudaFree(c.split_row); cudaFree(c.split_slot);
+  auto free_panel = [](SellPanel& p) {
+    cudaFree(p.sell); cudaFree(p.soff); cudaFree(p.slen); cudaFree(p.vrow);
+    cudaFree(p.split_row); cudaFree(p.split_slot);
+  };
+  free_panel(c.bal);
+  for (auto& p : c.panels) free_panel(p);
   c = Conn{};
 }
 
@@ -194,9 +198,26 @@ void free_conn(Conn& c) {
 // list much longer than the others, and doubles until the partial-sum slots
 // fit the kernel's shared-memory budget. The slices per warp are the smallest
 // of 8, 12, 16 that cover the virtual rows in the fewest CTAs.
-int build_balanced_sell(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const std::vector<uint64_t>& off,
-                        const std::vector<uint32_t>& order, const std::vector<uint64_t>& rec) {
-  const size_t n = cn.n;
+int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32_t>& hs_all,
+                        const std::vector<uint64_t>& off_all, const std::vector<uint64_t>& rec, uint32_t jb0,
+                        uint32_t jb1) {
+  // the singles of row r are rec[off_all[r] .. off_all[r] + hs_all[r]), ascending
+  // ket index: the ones in [jb0, jb1) are a contiguous sub-range
+  std::vector<uint32_t> hs(n);
+  std::vector<uint64_t> off(n);
+  for (size_t r = 0; r < n; ++r) {
+    const uint64_t* b = rec.data() + off_all[r];
+    const uint64_t* e = b + hs_all[r];
+    const uint64_t* lo = std::lower_bound(b, e, jb0, [](uint64_t x, uint32_t v) { return (x & 0xffffu) < v; });
+    const uint64_t* hi = std::lower_bound(lo, e, jb1, [](uint64_t x, uint32_t v) { return (x & 0xffffu) < v; });
+    off[r] = (uint64_t)(lo - rec.data());
+    hs[r] = (uint32_t)(hi - lo);
+  }
+  std::vector<uint32_t> order(n);
+  for (size_t r = 0; r < n; ++r) order[r] = (uint32_t)r;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return hs[x] > hs[y]; });
+  P.jb0 = jb0;
+  P.jb1 = jb1;
   uint64_t total = 0;
   uint32_t mx = 0;
   for (size_t r = 0; r < n; ++r) { total += hs[r]; mx = std::max(mx, hs[r]); }
@@ -252,7 +273,9 @@ int build_balanced_sell(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const
     slen[sl] = m;
     soff[sl + 1] = soff[sl] + 32ull * m;
   }
-  const uint64_t kPad = 1ull << 41;
+  // padding records contribute nothing (bit 41) and point at the panel's first
+  // ket index, so the kernels' shared-memory index stays in range
+  const uint64_t kPad = (1ull << 41) | (uint64_t)jb0;
   std::vector<uint64_t> sell(soff[ns] ? soff[ns] : 1, kPad);
   std::vector<uint32_t> vrow(nv ? nv : 1, 0);
   // Record order inside each virtual row is free (it only changes the order of
@@ -293,26 +316,26 @@ int build_balanced_sell(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const
         }
       }
   }
-  cn.bnslice = ns;
-  cn.nv = nv;
-  cn.nsplit = (int)split_row.size();
-  cn.nslot = (int)split_slot.back();
-  cn.cap = (int)cap;
-  cn.slices_per_warp = ks;
+  P.nslice = ns;
+  P.nv = nv;
+  P.nsplit = (int)split_row.size();
+  P.nslot = (int)split_slot.back();
+  P.cap = (int)cap;
+  P.slices_per_warp = ks;
   if (split_row.empty()) split_row.push_back(0);
-  SBDX_CUDA(c, cudaMalloc(&cn.bsell, sizeof(uint64_t) * sell.size()));
-  SBDX_CUDA(c, cudaMalloc(&cn.bsoff, sizeof(uint64_t) * (ns + 1)));
-  SBDX_CUDA(c, cudaMalloc(&cn.bslen, sizeof(uint32_t) * slen.size()));
-  SBDX_CUDA(c, cudaMalloc(&cn.vrow, sizeof(uint32_t) * vrow.size()));
-  SBDX_CUDA(c, cudaMalloc(&cn.split_row, sizeof(uint32_t) * split_row.size()));
-  SBDX_CUDA(c, cudaMalloc(&cn.split_slot, sizeof(uint32_t) * split_slot.size()));
-  SBDX_CUDA(c, cudaMemcpyAsync(cn.bsell, sell.data(), sizeof(uint64_t) * sell.size(), cudaMemcpyHostToDevice, c->stream));
-  SBDX_CUDA(c, cudaMemcpyAsync(cn.bsoff, soff.data(), sizeof(uint64_t) * (ns + 1), cudaMemcpyHostToDevice, c->stream));
-  SBDX_CUDA(c, cudaMemcpyAsync(cn.bslen, slen.data(), sizeof(uint32_t) * slen.size(), cudaMemcpyHostToDevice, c->stream));
-  SBDX_CUDA(c, cudaMemcpyAsync(cn.vrow, vrow.data(), sizeof(uint32_t) * vrow.size(), cudaMemcpyHostToDevice, c->stream));
-  SBDX_CUDA(c, cudaMemcpyAsync(cn.split_row, split_row.data(), sizeof(uint32_t) * split_row.size(),
+  SBDX_CUDA(c, cudaMalloc(&P.sell, sizeof(uint64_t) * sell.size()));
+  SBDX_CUDA(c, cudaMalloc(&P.soff, sizeof(uint64_t) * (ns + 1)));
+  SBDX_CUDA(c, cudaMalloc(&P.slen, sizeof(uint32_t) * slen.size()));
+  SBDX_CUDA(c, cudaMalloc(&P.vrow, sizeof(uint32_t) * vrow.size()));
+  SBDX_CUDA(c, cudaMalloc(&P.split_row, sizeof(uint32_t) * split_row.size()));
+  SBDX_CUDA(c, cudaMalloc(&P.split_slot, sizeof(uint32_t) * split_slot.size()));
+  SBDX_CUDA(c, cudaMemcpyAsync(P.sell, sell.data(), sizeof(uint64_t) * sell.size(), cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(P.soff, soff.data(), sizeof(uint64_t) * (ns + 1), cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(P.slen, slen.data(), sizeof(uint32_t) * slen.size(), cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(P.vrow, vrow.data(), sizeof(uint32_t) * vrow.size(), cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(P.split_row, split_row.data(), sizeof(uint32_t) * split_row.size(),
                                cudaMemcpyHostToDevice, c->stream));
-  SBDX_CUDA(c, cudaMemcpyAsync(cn.split_slot, split_slot.data(), sizeof(uint32_t) * split_slot.size(),
+  SBDX_CUDA(c, cudaMemcpyAsync(P.split_slot, split_slot.data(), sizeof(uint32_t) * split_slot.size(),
                                cudaMemcpyHostToDevice, c->stream));
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // host vectors die at return
   return 0;
@@ -387,8 +410,21 @@ int build_one(Ctx* c, int spin) {
     if (ns) SBDX_CUDA(c, cudaMemcpyAsync(cn.slen, slen.data(), sizeof(uint32_t) * ns, cudaMemcpyHostToDevice, c->stream));
     SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
     if (spin == 1) {
-      const int rc = build_balanced_sell(c, cn, hs, off, order, rec);
+      int rc = build_balanced_sell(c, cn.bal, n, hs, off, rec, 0, (uint32_t)n);
       if (rc) return rc;
+      // ket-range panels when the packed alpha-beta kernel (16 bytes per ket
+      // and per pair index, 8 per split slot) cannot stage a whole ket row
+      const size_t fixed = 16 * c->npair + sizeof(double) * kMaxSplitSlots;
+      if (16 * (n + c->npair) + sizeof(double) * (size_t)cn.bal.nslot > kAbSmemBudget && fixed < kAbSmemBudget) {
+        const size_t width = ((kAbSmemBudget - fixed) / 16) & ~(size_t)1;
+        const size_t np = (n + width - 1) / width;
+        const size_t w = (n + np - 1) / np;
+        cn.panels.resize(np);
+        for (size_t q = 0; q < np; ++q) {
+          const uint32_t lo = (uint32_t)(q * w), hi = (uint32_t)std::min(n, (q + 1) * w);
+          if ((rc = build_balanced_sell(c, cn.panels[q], n, hs, off, rec, lo, hi))) return rc;
+        }
+      }
     }
   }
   // the host copy of `off` must stay alive until the async copy ran

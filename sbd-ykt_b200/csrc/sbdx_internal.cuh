@@ -32,6 +32,28 @@ namespace sbdx {
 constexpr uint32_t kInfoNeg = 1u << 31;
 constexpr uint32_t kInfoSingle = 1u << 30;
 
+// Balanced SELL-32 of the single-excitation records whose ket index lies in
+// [jb0, jb1). A bra string with more than `cap` such singles is split into
+// equal parts ("virtual rows") of at most `cap` records; the split parts come
+// first, then the unsplit rows longest first. vrow[v]: bits 0-15 bra string,
+// bits 16-31 = 1 + partial-sum slot of a split part (0 for an unsplit row).
+// The parts of split string s occupy slots split_slot[s] .. split_slot[s+1]-1
+// and are summed in that order. Record m of lane l of slice s sits at
+// sell[soff[s] + 32m + l]; shorter lists are padded with records that have
+// bit 41 set.
+struct SellPanel {
+  uint64_t* sell = nullptr;        // [soff[nslice]]
+  uint64_t* soff = nullptr;        // [nslice + 1]
+  uint32_t* slen = nullptr;        // [nslice]
+  uint32_t* vrow = nullptr;        // [nv]
+  uint32_t* split_row = nullptr;   // [nsplit]
+  uint32_t* split_slot = nullptr;  // [nsplit + 1]
+  size_t nslice = 0, nv = 0;
+  int nsplit = 0, nslot = 0, cap = 0;
+  int slices_per_warp = 8;         // 8, 12 or 16: virtual rows per CTA = 1024 * this
+  uint32_t jb0 = 0, jb1 = 0;
+};
+
 struct Conn {
   size_t n = 0;          // number of bra strings
   size_t total = 0;      // number of entries
@@ -60,27 +82,19 @@ struct Conn {
   uint64_t* soff = nullptr;   // [nslice + 1]
   uint32_t* slen = nullptr;   // [nslice] records per lane of each slice
   size_t nslice = 0;
-  // balanced SELL-32 of the single-excitation records (beta spin only), read
-  // by the alpha-first alpha-beta kernel. A bra string with more than `cap`
-  // singles is split into equal parts ("virtual rows") of at most `cap`
-  // records; the split parts come first, then the unsplit rows longest first.
-  // vrow[v]: bits 0-15 bra string, bits 16-31 = 1 + partial-sum slot of a
-  // split part (0 for an unsplit row). The parts of split string s occupy
-  // slots split_slot[s] .. split_slot[s+1]-1 and are summed in that order.
-  uint64_t* bsell = nullptr;      // [bsoff[bnslice]]
-  uint64_t* bsoff = nullptr;      // [bnslice + 1]
-  uint32_t* bslen = nullptr;      // [bnslice]
-  uint32_t* vrow = nullptr;       // [nv]
-  uint32_t* split_row = nullptr;  // [nsplit]
-  uint32_t* split_slot = nullptr; // [nsplit + 1]
-  size_t bnslice = 0, nv = 0;
-  int nsplit = 0, nslot = 0, cap = 0;
-  int slices_per_warp = 8;        // 8, 12 or 16: virtual rows per CTA = 1024 * this
+  // balanced SELL-32 panels of the single-excitation records (beta spin only),
+  // read by the alpha-first alpha-beta kernels: `bal` covers all ket indices;
+  // `panels` (empty unless the packed kernel cannot stage a whole ket row in
+  // shared memory) split the ket range into slices that it can.
+  SellPanel bal;
+  std::vector<SellPanel> panels;
 };
 
 // Largest number of partial-sum slots of split rows (shared memory of the
 // alpha-first alpha-beta kernel: 8 bytes each).
 constexpr int kMaxSplitSlots = 2048;
+// Dynamic shared memory the alpha-beta kernels may use per CTA.
+constexpr size_t kAbSmemBudget = 227 * 1024 - 1024;
 
 // Launch shape of the sigma kernels. Codes (also the C-ABI encoding):
 //   same-spin: 1/2/4/8 = columns per thread of the prefix-parity-table kernel,

@@ -1297,14 +1297,14 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
                    const uint64_t* __restrict__ soff, const uint32_t* __restrict__ slen, size_t nslice,
                    const uint32_t* __restrict__ vrow, size_t nv, const uint32_t* __restrict__ split_row,
                    const uint32_t* __restrict__ split_slot, int nsplit, const T* __restrict__ Vt, size_t vstride,
-                   int npair, double* __restrict__ Y) {
+                   int npair, uint32_t jb0, size_t nbp, double* __restrict__ Y) {
   using RP = RowPack<T>;
   using P = typename RP::P;
   constexpr int VR = RP::kRows;
   constexpr int kWarps = kAb6Threads / 32;
   extern __shared__ __align__(16) unsigned char smem[];
-  P* xs = reinterpret_cast<P*>(smem);   // [nb]
-  P* er = xs + nb;                      // [npair]
+  P* xs = reinterpret_cast<P*>(smem);   // [nbp]: ket indices jb0 .. jb0 + nbp - 1
+  P* er = xs + nbp;                     // [npair]
   double* part = reinterpret_cast<double*>(er + npair);
   const size_t ia = blockIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1326,12 +1326,12 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
     for (int e = 0; e < VR; ++e) {
       const uint64_t ent = e0 + k0 + (e < nr ? e : 0);
       const uint32_t inf = a_info[ent];
-      xrow[e] = Xp + (size_t)a_ket[ent] * nb;
+      xrow[e] = Xp + (size_t)a_ket[ent] * nb + jb0;
       vrow_p[e] = Vt + (size_t)((inf >> 12) & 0xfffu) * vstride;
       neg[e] = (inf >> 31) != 0;
     }
     __syncthreads();
-    for (size_t t = threadIdx.x; t < nb; t += kAb6Threads) {
+    for (size_t t = threadIdx.x; t < nbp; t += kAb6Threads) {
       P p;
 #pragma unroll
       for (int e = 0; e < VR; ++e) RP::set(p, e, e < nr ? __ldg(xrow[e] + t) : (T)0);
@@ -1358,7 +1358,7 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
       for (uint32_t m = 0; m < len; ++m) {
         const uint64_t rec = next;
         if (m + 1 < len) next = __ldg(rp + 32ull * (m + 1));
-        const P x = xs[rec & 0xffffu];
+        const P x = xs[(uint32_t)(rec & 0xffffu) - jb0];  // pad records: jb = jb0
         const P ev = er[(rec >> 16) & 0xfffu];
         double d = RP::dot(ev, x);
         d = ((rec >> 41) & 1ull) ? 0.0 : d;
@@ -1388,29 +1388,56 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
   }
 }
 
-// Shared memory of v7: nb + npair 16-byte packs plus the split slots.
-size_t ab7_smem_bytes(const Ctx* c) {
-  return 16 * (c->nb + c->npair) + sizeof(double) * (size_t)c->conn[1].nslot;
+// Shared memory of v7 on one panel: its ket range and npair 16-byte packs
+// plus its split slots.
+size_t ab7_smem_bytes(const Ctx* c, const SellPanel& p) {
+  return 16 * ((size_t)(p.jb1 - p.jb0) + c->npair) + sizeof(double) * (size_t)p.nslot;
 }
-constexpr size_t kAbSmemBudget = 227 * 1024 - 1024;
+
+// The panels v7 runs on: the whole ket range, or the ket-range slices.
+const std::vector<SellPanel>* ab7_panels(const Ctx* c, std::vector<SellPanel>& one) {
+  const Conn& cb = c->conn[1];
+  if (!cb.panels.empty()) return &cb.panels;
+  one.assign(1, cb.bal);
+  return &one;
+}
+
+bool ab7_fits(const Ctx* c) {
+  std::vector<SellPanel> one;
+  for (const SellPanel& p : *ab7_panels(c, one))
+    if (ab7_smem_bytes(c, p) > kAbSmemBudget) return false;
+  return true;
+}
 
 template <typename T, int KS>
-int launch_ab_v7(Ctx* c, const T* Xp) {
+int launch_ab_v7(Ctx* c, const T* Xp, const SellPanel& bp) {
   const Conn& ca = c->conn[0];
-  const Conn& cb = c->conn[1];
   const bool f64 = std::is_same<T, double>::value;
   const T* Vt = f64 ? (const T*)c->d_V : (const T*)c->d_V32;
   const size_t vs = f64 ? c->vstride : c->vstride32;
-  const size_t smem = ab7_smem_bytes(c);
+  const size_t smem = ab7_smem_bytes(c, bp);
   SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v7_kernel<T, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
   const size_t per_cta = (size_t)(kAb6Threads / 32) * KS;
-  dim3 grid((unsigned)c->na, (unsigned)((cb.bnslice + per_cta - 1) / per_cta));
+  dim3 grid((unsigned)c->na, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
   if (grid.y == 0) grid.y = 1;
   sigma_ab_v7_kernel<T, KS><<<grid, kAb6Threads, smem, c->stream>>>(
-      Xp, c->nb, ca.off, ca.nsing, ca.ket, ca.info, cb.bsell, cb.bsoff, cb.bslen, cb.bnslice, cb.vrow, cb.nv,
-      cb.split_row, cb.split_slot, cb.nsplit, Vt, vs, (int)c->npair, c->d_y);
+      Xp, c->nb, ca.off, ca.nsing, ca.ket, ca.info, bp.sell, bp.soff, bp.slen, bp.nslice, bp.vrow, bp.nv,
+      bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, (int)c->npair, bp.jb0, (size_t)(bp.jb1 - bp.jb0), c->d_y);
   SBDX_LAUNCHED(c);
+  return 0;
+}
+
+template <typename T>
+int run_ab_v7(Ctx* c, const T* Xp) {
+  std::vector<SellPanel> one;
+  for (const SellPanel& bp : *ab7_panels(c, one)) {
+    int rc;
+    if (bp.slices_per_warp >= 16) rc = launch_ab_v7<T, 16>(c, Xp, bp);
+    else if (bp.slices_per_warp >= 12) rc = launch_ab_v7<T, 12>(c, Xp, bp);
+    else rc = launch_ab_v7<T, 8>(c, Xp, bp);
+    if (rc) return rc;
+  }
   return 0;
 }
 
@@ -1450,18 +1477,19 @@ int launch_ab_v6(Ctx* c, const T* Xp, size_t smem, size_t xstride) {
   SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v6_kernel<T, R, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
   const size_t per_cta = (size_t)(kAb6Threads / 32) * KS;  // slices
-  dim3 grid((unsigned)c->na, (unsigned)((cb.bnslice + per_cta - 1) / per_cta));
+  const SellPanel& bp = cb.bal;
+  dim3 grid((unsigned)c->na, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
   if (grid.y == 0) grid.y = 1;
   sigma_ab_v6_kernel<T, R, KS><<<grid, kAb6Threads, smem, c->stream>>>(
-      Xp, c->nb, ca.off, ca.nsing, ca.ket, ca.info, cb.bsell, cb.bsoff, cb.bslen, cb.bnslice, cb.vrow, cb.nv,
-      cb.split_row, cb.split_slot, cb.nsplit, Vt, vs, xstride, c->d_y);
+      Xp, c->nb, ca.off, ca.nsing, ca.ket, ca.info, bp.sell, bp.soff, bp.slen, bp.nslice, bp.vrow, bp.nv,
+      bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, xstride, c->d_y);
   SBDX_LAUNCHED(c);
   return 0;
 }
 
 template <typename T, int R>
 int launch_ab_v6_ks(Ctx* c, const T* Xp, size_t smem, size_t xstride) {
-  const int ks = c->conn[1].slices_per_warp;
+  const int ks = c->conn[1].bal.slices_per_warp;
   if (ks >= 16) return launch_ab_v6<T, R, 16>(c, Xp, smem, xstride);
   if (ks >= 12) return launch_ab_v6<T, R, 12>(c, Xp, smem, xstride);
   return launch_ab_v6<T, R, 8>(c, Xp, smem, xstride);
@@ -1472,21 +1500,16 @@ int launch_ab_v6_ks(Ctx* c, const T* Xp, size_t smem, size_t xstride) {
 template <typename T>
 int run_ab_v6(Ctx* c, int code, const T* Xp) {
   using V = typename Prec<T>::V;
-  if (code / 10 == 7) {  // 71: packed rows, when nb + npair packs fit in shared memory
-    if (ab7_smem_bytes(c) <= kAbSmemBudget) {
-      const int ks = c->conn[1].slices_per_warp;
-      if (ks >= 16) return launch_ab_v7<T, 16>(c, Xp);
-      if (ks >= 12) return launch_ab_v7<T, 12>(c, Xp);
-      return launch_ab_v7<T, 8>(c, Xp);
-    }
+  if (code / 10 == 7) {  // 71: packed rows, on ket-range panels when a whole row does not fit
+    if (ab7_fits(c)) return run_ab_v7<T>(c, Xp);
     code = std::is_same<T, double>::value ? 62 : 64;
   }
   const bool f64 = std::is_same<T, double>::value;
   const size_t vs = f64 ? c->vstride : c->vstride32;
   const size_t per = 16 / sizeof(T);
   const size_t xstride = (c->nb + per - 1) / per * per;
-  const size_t budget = 227 * 1024 - 1024;  // dynamic part; the static part is a few bytes
-  const size_t extra = sizeof(double) * (size_t)c->conn[1].nslot;
+  const size_t budget = kAbSmemBudget;  // dynamic part; the static part is a few bytes
+  const size_t extra = sizeof(double) * (size_t)c->conn[1].bal.nslot;
   int R = code % 10 > 0 ? code % 10 : 2;
   size_t smem = 0;
   for (; R >= 1; --R) {
