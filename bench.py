@@ -59,6 +59,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU-baseline sample duration")
     ap.add_argument("--davidson-tol", type=float, default=1e-8)
+    ap.add_argument("--roots", type=int, default=2, help="roots of the multi-root Davidson runs (0 = skip them)")
     ap.add_argument("--tune", default=None, metavar="SAME,AB",
                     help="fixed sigma launch codes for both precisions instead of the autotuner (profiling runs)")
     return ap.parse_args()
@@ -367,6 +368,25 @@ def run_ours(args, rank, world, local):
                          "energy": i32.energy, "residual": i32.residual, "converged": bool(i32.converged),
                          "dE_vs_fp64": i32.energy - i64.energy},
                "speedup_mixed_vs_fp64": i64.seconds / i32.seconds if i32.seconds > 0 else None}
+        # the mixed solver's algorithm (Olsen-Davidson, FP64 anchor, thick restart)
+        # with FP64 corrections: separates the algorithmic gain from the precision gain
+        ib, Eb, rb, _ = ctx.davidson_roots(1, max_it=100, max_nb=12, eps=args.davidson_tol)
+        dav["fp64_same_algorithm"] = {"seconds": ib.seconds, "sigmas": ib.n_sigma64, "energy": float(Eb[0]),
+                                      "residual": float(rb[0]), "converged": bool(ib.converged),
+                                      "speedup_mixed_vs_this": ib.seconds / i32.seconds if i32.seconds > 0 else None}
+        if args.roots > 1:
+            k = args.roots
+            f64, E64, r64, _ = ctx.davidson_roots(k, max_it=100, max_nb=12, eps=args.davidson_tol)
+            f32, E32, r32, _ = ctx.davidson_roots(k, max_it=100, max_nb=12, eps=args.davidson_tol,
+                                                  precision=sbdx.SBDX_FP32)
+            dav["roots"] = {"nroots": k,
+                            "fp64": {"seconds": f64.seconds, "sigmas": f64.n_sigma64, "energies": E64.tolist(),
+                                     "residuals": r64.tolist(), "converged": bool(f64.converged)},
+                            "mixed": {"seconds": f32.seconds, "sigmas_fp32": f32.n_sigma, "sigmas_fp64": f32.n_sigma64,
+                                      "energies": E32.tolist(), "residuals": r32.tolist(),
+                                      "converged": bool(f32.converged),
+                                      "dE_vs_fp64": (E32 - E64).tolist()},
+                            "speedup_mixed_vs_fp64": f64.seconds / f32.seconds if f32.seconds > 0 else None}
 
     # ---- CPU baseline (reference OpenMP mult, bounded sample, rank 0, N=1) -------------
     cpu = None
