@@ -215,6 +215,38 @@ int sbdx_alpha_weights(sbdx_ctx* ctx, const double* W, double* weights);
  * them (samples/selected_basis_diagonalization/main.cc:166-216). */
 int sbdx_energy_backward(sbdx_ctx* ctx, const double* W, double* dE_dh, double* dE_deri);
 
+/* ---- batches of subspaces -------------------------------------------------
+ * No counterpart in the reference, which solves one basis per tpb::diag call
+ * (sbdiag.h:113-124). A batch holds many independent alpha x beta string sets
+ * that share one Hamiltonian and solves them concurrently on one GPU: each
+ * subspace has its own context on its own stream, its sigmas are replayed
+ * from captured CUDA graphs, and a pool of host threads drives the Davidson
+ * solves (sbdx_davidson_roots for every subspace), largest first. */
+typedef struct sbdx_batch sbdx_batch;
+/* Integrals as in sbdx_set_integrals (exact doubles, copied). */
+int sbdx_batch_create(sbdx_batch** batch, int device, int norb, double I0, const double* h, const double* eri,
+                      size_t eri_len);
+int sbdx_batch_destroy(sbdx_batch* batch);
+const char* sbdx_batch_last_error(const sbdx_batch* batch);
+/* Adds one subspace (strings as in sbdx_set_strings); builds its
+ * connectivity and diagonal. *index receives its position. */
+int sbdx_batch_add(sbdx_batch* batch, const uint64_t* alpha, size_t na, const uint64_t* beta, size_t nb,
+                   int* index);
+int sbdx_batch_size(const sbdx_batch* batch);
+int sbdx_batch_dims(const sbdx_batch* batch, int index, size_t* na, size_t* nb);
+/* Tunes the sigma launch shapes on the largest subspace (sbdx_autotune) and
+ * applies them to all subspaces. */
+int sbdx_batch_tune(sbdx_batch* batch, int* same_code, int* ab_code);
+/* Lowest nroots (1-4) of every subspace, start vectors on the lowest diagonal
+ * elements, nthreads host threads (0 = 8). energies, residuals: size*nroots
+ * doubles (subspace-major; residuals may be NULL); infos: size entries (may be
+ * NULL), each with that subspace's own solve time; *seconds (may be NULL):
+ * wall time of the whole batch. */
+int sbdx_batch_solve(sbdx_batch* batch, const sbdx_davidson_params* params, int nroots, int nthreads,
+                     double* energies, double* residuals, sbdx_davidson_info* infos, double* seconds);
+/* Ritz vector `root` of subspace `index` of the last solve (host, na*nb). */
+int sbdx_batch_vector(sbdx_batch* batch, int index, int root, double* W);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2,17 +2,13 @@
 // here, before any kernel sees it: sizes, orbital range, equal electron counts
 // per spin, finite integrals. No C++ exception crosses the boundary.
 #include "sbdx.h"
-#include <vector>
 #include "sbdx_internal.cuh"
 
 #include <cmath>
 #include <cstring>
 #include <exception>
 #include <new>
-
-struct sbdx_ctx {
-  sbdx::Ctx c;
-};
+#include <vector>
 
 namespace sbdx {
 
@@ -35,9 +31,6 @@ int check_device_error(Ctx* c) {
 void free_connectivity(Ctx* c);
 int build_g_table(Ctx* c);
 int davidson(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info);
-int davidson_roots(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, double* E, double* res,
-                   sbdx_davidson_info& info);
-int lowest_diagonal(Ctx* c, int k, std::vector<size_t>& idx);
 int rdm_device(Ctx* c, const double* dW, double* d_one, double* d_two);
 int occupation_device(Ctx* c, const double* dW, double* d_density);
 int alpha_weights_device(Ctx* c, const double* dW, double* d_w);
@@ -47,6 +40,7 @@ int autotune(Ctx* c);
 namespace {
 
 void free_vector_state(Ctx* c) {
+  sbdx::clear_sigma_graphs(c);
   cudaFree(c->d_hii); c->d_hii = nullptr; c->have_hii = false;
   cudaFree(c->d_xt); c->d_xt = nullptr;
   cudaFree(c->d_xp); c->d_xp = nullptr;
@@ -134,6 +128,7 @@ int sbdx_ctx_destroy(sbdx_ctx* ctx) {
   cudaFree(c->d_a); cudaFree(c->d_b); cudaFree(c->d_red);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete ctx;
   return SBDX_OK;
 }
@@ -182,6 +177,7 @@ int sbdx_set_tuning(sbdx_ctx* ctx, int same_code, int ab_code) {
       t.same_code = same_code;
       t.ab_code = ab_code;
     }
+    sbdx::clear_sigma_graphs(c);
     return SBDX_OK;
   });
 }
@@ -200,6 +196,9 @@ int sbdx_autotune(sbdx_ctx* ctx, int* same_vec, int* ab_rows) {
 
 int sbdx_set_stream(sbdx_ctx* ctx, void* stream) {
   return sbdx::guarded(ctx, [&](Ctx* c) {
+    sbdx::clear_sigma_graphs(c);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    c->own_stream = false;
     c->stream = (cudaStream_t)stream;
     return SBDX_OK;
   });
@@ -397,8 +396,8 @@ int sbdx_davidson_roots(sbdx_ctx* ctx, const sbdx_davidson_params* params, int n
       for (size_t q = 0; q < D * nroots; ++q)
         if (!std::isfinite(W[q])) { c->err = "davidson_roots: non-finite start vector"; return SBDX_ERR_NUMERIC; }
     double* dW = nullptr;
-    SBDX_CUDA(c, cudaMalloc(&dW, sizeof(double) * D * nroots));
-    struct Guard { double* p; ~Guard() { cudaFree(p); } } g{dW};
+    SBDX_CUDA(c, cudaMallocAsync(&dW, sizeof(double) * D * nroots, c->stream));
+    struct Guard { double* p; cudaStream_t st; ~Guard() { cudaFreeAsync(p, st); } } g{dW, c->stream};
     if (init_from_W) {
       SBDX_CUDA(c, cudaMemcpyAsync(dW, W, sizeof(double) * D * nroots, cudaMemcpyHostToDevice, c->stream));
     } else {  // unit vectors on the nroots lowest diagonal elements

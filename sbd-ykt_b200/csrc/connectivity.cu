@@ -435,6 +435,7 @@ int build_one(Ctx* c, int spin) {
 }  // namespace
 
 void free_connectivity(Ctx* c) {
+  clear_sigma_graphs(c);
   free_conn(c->conn[0]);
   free_conn(c->conn[1]);
   cudaFree(c->d_Da); cudaFree(c->d_Db); cudaFree(c->d_Da32); cudaFree(c->d_Db32);

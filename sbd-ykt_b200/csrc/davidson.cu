@@ -1015,21 +1015,37 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
   const int nc = std::max(std::min(kMixed ? 2 * p.max_nb : p.max_nb, 64 - k), 2 * k);
   const int keep = std::max(k, nc / 3);
   const int period = p.defect_every > 0 ? p.defect_every : 0;
-  Work wk;
-  SBDX_CUDA(c, cudaMalloc(&wk.partial, sizeof(double) * kRedBlocks * (2 * nc + 2 * kMaxRoots + 4)));
-  SBDX_CUDA(c, cudaMalloc(&wk.scal, sizeof(double) * (kbDots + (size_t)(k + 2) * nc + 64)));
-  SBDX_CUDA(c, cudaMalloc(&wk.u, sizeof(double) * ((size_t)(k + nc) * k + k + nc + 8)));
+  // stream-ordered allocations: several solves can run concurrently on their
+  // own streams without a device-wide synchronisation at allocation or release
+  struct AsyncGuard {
+    cudaStream_t st;
+    std::vector<void*> p;
+    ~AsyncGuard() { for (void* q : p) cudaFreeAsync(q, st); }
+  } g{c->stream, {}};
+  auto alloc = [&](void** ptr, size_t bytes) -> cudaError_t {
+    const cudaError_t e = cudaMallocAsync(ptr, bytes, c->stream);
+    if (e == cudaSuccess) g.p.push_back(*ptr);
+    return e;
+  };
+  Work wk;  // its pointers stay owned by g (Work's destructor frees null pointers)
+  double *wpartial = nullptr, *wscal = nullptr, *wu = nullptr;
+  SBDX_CUDA(c, alloc((void**)&wpartial, sizeof(double) * kRedBlocks * (2 * nc + 2 * kMaxRoots + 4)));
+  SBDX_CUDA(c, alloc((void**)&wscal, sizeof(double) * (kbDots + (size_t)(k + 2) * nc + 64)));
+  SBDX_CUDA(c, alloc((void**)&wu, sizeof(double) * ((size_t)(k + nc) * k + k + nc + 8)));
   TC *C = nullptr, *HC = nullptr;
   double *A = nullptr, *R = nullptr, *V = nullptr;
-  SBDX_CUDA(c, cudaMalloc(&C, sizeof(TC) * D * nc));
-  SBDX_CUDA(c, cudaMalloc(&HC, sizeof(TC) * D * nc));
-  SBDX_CUDA(c, cudaMalloc(&A, sizeof(double) * D * 4 * k));  // W | HW | W' | HW'
-  SBDX_CUDA(c, cudaMalloc(&R, sizeof(double) * D * k));
-  SBDX_CUDA(c, cudaMalloc(&V, sizeof(double) * D));
-  struct Guard {
-    void *a, *b, *c, *d, *e;
-    ~Guard() { cudaFree(a); cudaFree(b); cudaFree(c); cudaFree(d); cudaFree(e); }
-  } g{C, HC, A, R, V};
+  SBDX_CUDA(c, alloc((void**)&C, sizeof(TC) * D * nc));
+  SBDX_CUDA(c, alloc((void**)&HC, sizeof(TC) * D * nc));
+  SBDX_CUDA(c, alloc((void**)&A, sizeof(double) * D * 4 * k));  // W | HW | W' | HW'
+  SBDX_CUDA(c, alloc((void**)&R, sizeof(double) * D * k));
+  SBDX_CUDA(c, alloc((void**)&V, sizeof(double) * D));
+  struct Borrow {
+    Work& w;
+    ~Borrow() { w.partial = w.scal = w.u = nullptr; }
+  } borrow{wk};
+  wk.partial = wpartial;
+  wk.scal = wscal;
+  wk.u = wu;
   double* W = A;
   double* HW = A + D * k;
   double* Wn = A + 2 * D * k;
@@ -1311,10 +1327,14 @@ int lowest_diagonal(Ctx* c, int k, std::vector<size_t>& idx) {
   const size_t D = c->na * c->nb;
   double* bv = nullptr;
   unsigned long long *bi = nullptr, *sk = nullptr;
-  SBDX_CUDA(c, cudaMalloc(&bv, sizeof(double) * kRedBlocks));
-  SBDX_CUDA(c, cudaMalloc(&bi, sizeof(unsigned long long) * kRedBlocks));
-  SBDX_CUDA(c, cudaMalloc(&sk, sizeof(unsigned long long) * kMaxRoots));
-  struct Guard { void *a, *b, *c; ~Guard() { cudaFree(a); cudaFree(b); cudaFree(c); } } g{bv, bi, sk};
+  SBDX_CUDA(c, cudaMallocAsync(&bv, sizeof(double) * kRedBlocks, c->stream));
+  SBDX_CUDA(c, cudaMallocAsync(&bi, sizeof(unsigned long long) * kRedBlocks, c->stream));
+  SBDX_CUDA(c, cudaMallocAsync(&sk, sizeof(unsigned long long) * kMaxRoots, c->stream));
+  struct Guard {
+    cudaStream_t st;
+    void *a, *b, *c;
+    ~Guard() { cudaFreeAsync(a, st); cudaFreeAsync(b, st); cudaFreeAsync(c, st); }
+  } g{c->stream, bv, bi, sk};
   std::vector<double> hv(kRedBlocks);
   std::vector<unsigned long long> hi(kRedBlocks), chosen;
   idx.clear();

@@ -398,7 +398,7 @@ int rdm_device(Ctx* c, const double* dW, double* d_one, double* d_two) {
   {
     const size_t smem = sizeof(double) * (L2 + nb);
     if (smem > 220 * 1024) { c->err = "rdm: beta dimension too large for the shared-memory row"; return 1; }
-    SBDX_CUDA(c, cudaFuncSetAttribute(rdm_ab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SBDX_CUDA(c, cudaFuncSetAttribute(rdm_ab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAbSmemBudget));
     const Conn& ca = c->conn[0];
     const Conn& cb = c->conn[1];
     rdm_ab_kernel<<<(unsigned)na, 512, smem, c->stream>>>(dW, nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket, ca.info,

@@ -15,6 +15,8 @@
 //                and a packed info word (see below).
 #pragma once
 #include <cuda_runtime.h>
+
+#include "sbdx.h"
 #include <cstdint>
 #include <cstddef>
 #include <string>
@@ -159,12 +161,34 @@ struct Ctx {
   unsigned long long launches = 0;
   // launch shapes of the sigma kernels per precision (index 0 = FP64, 1 = FP32)
   Tune tune[2];
+  // CUDA graphs of whole sigmas, one per (precision, input, output) buffers,
+  // captured on first use and replayed when use_graphs is set (needs a
+  // non-default stream); cleared whenever the data they read changes
+  struct SigmaGraph {
+    int precision;
+    const void* X;
+    void* S;
+    cudaGraphExec_t exec;
+    unsigned long long kernels;
+  };
+  bool use_graphs = false;
+  bool own_stream = false;  // stream created by the library (destroyed with the context)
+  std::vector<SigmaGraph> graphs;
   // optional per-phase timing of the sigma (CUDA events on the context stream)
   bool profiling = false;
   cudaEvent_t ev[8] = {};
   double phase_ms[8] = {};
   unsigned long long phase_calls = 0;
 };
+
+}  // namespace sbdx
+
+// The opaque handle of the C-ABI.
+struct sbdx_ctx {
+  sbdx::Ctx c;
+};
+
+namespace sbdx {
 
 constexpr int kSigmaPhases = 5;  // alpha same-spin, transpose, beta same-spin, alpha-beta, combine
 
@@ -252,11 +276,16 @@ int diag_terms(Ctx* c);
 // sigma: X (na x nb, type by precision: 0 = FP64, 1 = FP32) -> S (same type)
 int sigma_device(Ctx* c, int precision, const void* X, void* S);
 int ensure_sigma_scratch(Ctx* c);
+void clear_sigma_graphs(Ctx* c);
 int ensure_reduction(Ctx* c, size_t n);
 int autotune(Ctx* c);
 // Returns 0, or sets c->err and returns SBDX_ERR_CUDA when a kernel recorded a
 // watchdog timeout in the device error word (which is then cleared).
 int check_device_error(Ctx* c);
+// Several lowest roots on device vectors (dW: k vectors of na*nb), see davidson.cu.
+int davidson_roots(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, double* E, double* res,
+                   sbdx_davidson_info& info);
+int lowest_diagonal(Ctx* c, int k, std::vector<size_t>& idx);
 
 // Device error codes written to Ctx::d_err.
 constexpr int kErrWatchdogAb = 1;  // alpha-beta kernel: TMA completion wait timed out

@@ -862,7 +862,7 @@ int launch_ab2(Ctx* c, const T* X, size_t smem, size_t xstride, int threads) {
   dim3 grid((unsigned)c->na, (unsigned)((c->nb + per_cta - 1) / per_cta));
   if (threads == 512) {
     SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v2_kernel<T, R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
+                                      (int)kAbSmemBudget));
     sigma_ab_v2_kernel<T, R, 512><<<grid, 512, smem, c->stream>>>(
         X, c->nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket, ca.info, ca.omask, cb.off, cb.nsing, cb.srec, cb.order,
         eri, (int)c->npair, xstride, c->d_y);
@@ -870,7 +870,7 @@ int launch_ab2(Ctx* c, const T* X, size_t smem, size_t xstride, int threads) {
     return 0;
   }
   SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v2_kernel<T, R, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+                                    (int)kAbSmemBudget));
   sigma_ab_v2_kernel<T, R, 1024><<<grid, 1024, smem, c->stream>>>(
       X, c->nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket, ca.info, ca.omask, cb.off, cb.nsing, cb.srec, cb.order, eri,
       (int)c->npair, xstride, c->d_y);
@@ -901,7 +901,7 @@ int launch_ab4(Ctx* c, const T* X, size_t smem) {
   const Conn& cb = c->conn[1];
   const V* Vt = std::is_same<T, double>::value ? (const V*)c->d_V : (const V*)c->d_V32;
   const size_t vs = std::is_same<T, double>::value ? c->vstride : c->vstride32;
-  SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v4_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v4_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAbSmemBudget));
   const size_t per_cta = (size_t)kAb2Threads * kAb2Slots;
   dim3 grid((unsigned)c->na, (unsigned)((c->nb + per_cta - 1) / per_cta));
   sigma_ab_v4_kernel<T, R><<<grid, kAb2Threads, smem, c->stream>>>(
@@ -942,7 +942,7 @@ int launch_ab5(Ctx* c, const T* X, size_t smem, size_t xstride) {
   const V* eri = std::is_same<T, double>::value ? (const V*)c->d_eri : (const V*)c->d_eri32;
   constexpr int NT = 1024;
   SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v5_kernel<T, R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+                                    (int)kAbSmemBudget));
   const size_t slices_per_cta = 8192 / 32;
   dim3 grid((unsigned)c->na, (unsigned)((cb.nslice + slices_per_cta - 1) / slices_per_cta));
   sigma_ab_v5_kernel<T, R, NT><<<grid, NT, smem, c->stream>>>(
@@ -1389,7 +1389,9 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
 }
 
 // Shared memory of v7 on one panel: its ket range and npair 16-byte packs
-// plus its split slots.
+// plus its split slots. (The kernels' dynamic shared-memory limit is always set
+// to the full budget: the attribute is global per kernel, and contexts on
+// other host threads launch the same kernel with other sizes.)
 size_t ab7_smem_bytes(const Ctx* c, const SellPanel& p) {
   return 16 * ((size_t)(p.jb1 - p.jb0) + c->npair) + sizeof(double) * (size_t)p.nslot;
 }
@@ -1417,7 +1419,7 @@ int launch_ab_v7(Ctx* c, const T* Xp, const SellPanel& bp) {
   const size_t vs = f64 ? c->vstride : c->vstride32;
   const size_t smem = ab7_smem_bytes(c, bp);
   SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v7_kernel<T, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+                                    (int)kAbSmemBudget));
   const size_t per_cta = (size_t)(kAb6Threads / 32) * KS;
   dim3 grid((unsigned)c->na, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
   if (grid.y == 0) grid.y = 1;
@@ -1475,7 +1477,7 @@ int launch_ab_v6(Ctx* c, const T* Xp, size_t smem, size_t xstride) {
   const V* Vt = f64 ? (const V*)c->d_V : (const V*)c->d_V32;
   const size_t vs = f64 ? c->vstride : c->vstride32;
   SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v6_kernel<T, R, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+                                    (int)kAbSmemBudget));
   const size_t per_cta = (size_t)(kAb6Threads / 32) * KS;  // slices
   const SellPanel& bp = cb.bal;
   dim3 grid((unsigned)c->na, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
@@ -1721,6 +1723,7 @@ int ensure_sigma_scratch(Ctx* c) {
 // same-spin and alpha-beta choice separately.
 int autotune(Ctx* c) {
   int rc = 0;
+  clear_sigma_graphs(c);
   if (!c->have_conn && (rc = build_connectivity(c))) return rc;
   if (!c->have_hii && (rc = diag_terms(c))) return rc;
   if ((rc = ensure_sigma_scratch(c))) return rc;
@@ -1779,6 +1782,59 @@ int autotune(Ctx* c) {
   return 0;
 }
 
+void clear_sigma_graphs(Ctx* c) {
+  for (auto& g : c->graphs) cudaGraphExecDestroy(g.exec);
+  c->graphs.clear();
+}
+
+namespace {
+
+int run_sigma_any(Ctx* c, int precision, const void* X, void* S) {
+  if (precision == 0) return run_sigma<double>(c, (const double*)X, (double*)S);
+  return run_sigma<float>(c, (const float*)X, (float*)S);
+}
+
+// Replays the captured graph of this (precision, X, S), capturing it first.
+// Returns -1 (nothing launched) when capture is not possible here, so that
+// the caller runs the sigma directly.
+int sigma_graph(Ctx* c, int precision, const void* X, void* S) {
+  for (const auto& g : c->graphs)
+    if (g.precision == precision && g.X == X && g.S == S) {
+      SBDX_CUDA(c, cudaGraphLaunch(g.exec, c->stream));
+      c->launches += g.kernels;
+      return 0;
+    }
+  if (c->graphs.size() >= 96) clear_sigma_graphs(c);
+  const unsigned long long before = c->launches;
+  if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  const int rc = run_sigma_any(c, precision, X, S);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+  const unsigned long long kernels = c->launches - before;
+  c->launches = before;
+  if (rc != 0 || e != cudaSuccess || graph == nullptr) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return rc != 0 ? rc : -1;
+  }
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  c->graphs.push_back({precision, X, S, exec, kernels});
+  SBDX_CUDA(c, cudaGraphLaunch(exec, c->stream));
+  c->launches += kernels;
+  return 0;
+}
+
+}  // namespace
+
 int sigma_device(Ctx* c, int precision, const void* X, void* S) {
   if (!c->have_conn) {
     int rc = build_connectivity(c);
@@ -1790,10 +1846,16 @@ int sigma_device(Ctx* c, int precision, const void* X, void* S) {
   }
   int rc = ensure_sigma_scratch(c);
   if (rc) return rc;
-  if (precision == 0) return run_sigma<double>(c, (const double*)X, (double*)S);
-  if (precision == 1) return run_sigma<float>(c, (const float*)X, (float*)S);
-  c->err = "sigma: precision must be SBDX_FP64 or SBDX_FP32";
-  return 1;
+  if (precision != 0 && precision != 1) {
+    c->err = "sigma: precision must be SBDX_FP64 or SBDX_FP32";
+    return 1;
+  }
+  if (c->use_graphs && !c->profiling && c->stream != nullptr) {
+    rc = sigma_graph(c, precision, X, S);
+    if (rc >= 0) return rc;
+    c->use_graphs = false;  // capture unavailable: plain launches from now on
+  }
+  return run_sigma_any(c, precision, X, S);
 }
 
 }  // namespace sbdx

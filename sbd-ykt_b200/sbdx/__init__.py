@@ -259,3 +259,80 @@ def diag_terms_noalloc(norb: int, I0: float, h_ptr: int, eri_ptr: int, alpha_ptr
     rc = fn(norb, I0, h_ptr, eri_ptr, alpha_ptr, na, beta_ptr, nb, hii_ptr, stream_ptr, buf, len(buf))
     if rc != SBDX_OK:
         raise SbdxError(rc, buf.value.decode())
+
+
+class Batch:
+    """sbdx_batch: many alpha x beta subspaces sharing one Hamiltonian, solved
+    concurrently on one GPU (per-subspace streams, graph-replayed sigmas)."""
+
+    def __init__(self, L, I0, h, eri, device: int = 0):
+        self.lib = load_library()
+        lib = self.lib
+        lib.sbdx_batch_last_error.restype = ctypes.c_char_p
+        lib.sbdx_batch_last_error.argtypes = [ctypes.c_void_p]
+        for name in ("sbdx_batch_create", "sbdx_batch_destroy", "sbdx_batch_add", "sbdx_batch_size",
+                     "sbdx_batch_dims", "sbdx_batch_tune", "sbdx_batch_solve", "sbdx_batch_vector"):
+            getattr(lib, name).restype = ctypes.c_int
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        eri = np.ascontiguousarray(eri, dtype=np.float64)
+        b = ctypes.c_void_p()
+        rc = lib.sbdx_batch_create(ctypes.byref(b), ctypes.c_int(device), ctypes.c_int(L), ctypes.c_double(I0), _d(h),
+                                   _d(eri), ctypes.c_size_t(len(eri)))
+        if rc != SBDX_OK:
+            raise SbdxError(rc, "batch creation failed")
+        self.b = b
+        self.dims = []
+
+    def _check(self, rc):
+        if rc != SBDX_OK:
+            raise SbdxError(rc, self.lib.sbdx_batch_last_error(self.b).decode())
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.lib.sbdx_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add(self, alpha, beta) -> int:
+        a = np.ascontiguousarray(alpha, dtype=np.uint64)
+        b = np.ascontiguousarray(beta, dtype=np.uint64)
+        idx = ctypes.c_int(-1)
+        self._check(self.lib.sbdx_batch_add(self.b, _u(a), ctypes.c_size_t(len(a)), _u(b), ctypes.c_size_t(len(b)),
+                                            ctypes.byref(idx)))
+        self.dims.append((len(a), len(b)))
+        return idx.value
+
+    def tune(self):
+        s, a = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(self.lib.sbdx_batch_tune(self.b, ctypes.byref(s), ctypes.byref(a)))
+        return s.value, a.value
+
+    def solve(self, nroots=1, max_it=100, max_nb=12, eps=1e-8, precision=SBDX_FP64, nthreads=0, max_time=86400.0,
+              defect_every=0):
+        """Returns (energies[K, nroots], residuals[K, nroots], infos[K], seconds)."""
+        K = len(self.dims)
+        p = DavidsonParams(max_it, max_nb, eps, max_time, precision, defect_every, 0)
+        E = np.zeros((K, nroots))
+        R = np.zeros((K, nroots))
+        infos = (DavidsonInfo * K)()
+        sec = ctypes.c_double(0.0)
+        self._check(self.lib.sbdx_batch_solve(self.b, ctypes.byref(p), ctypes.c_int(nroots), ctypes.c_int(nthreads),
+                                              _d(E), _d(R), infos, ctypes.byref(sec)))
+        return E, R, list(infos), sec.value
+
+    def vector(self, index, root=0):
+        na, nb = self.dims[index]
+        W = np.zeros(na * nb)
+        self._check(self.lib.sbdx_batch_vector(self.b, ctypes.c_int(index), ctypes.c_int(root), _d(W)))
+        return W
