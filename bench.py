@@ -36,6 +36,8 @@ import tempfile
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 for _p in (os.path.join(ROOT, "sbd-ykt_b200"), os.path.join(ROOT, "oracle")):
     if _p not in sys.path:
@@ -60,6 +62,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU-baseline sample duration")
     ap.add_argument("--davidson-tol", type=float, default=1e-8)
     ap.add_argument("--roots", type=int, default=2, help="roots of the multi-root Davidson runs (0 = skip them)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-subspace runs")
+    ap.add_argument("--batch-threads", type=int, default=16)
     ap.add_argument("--tune", default=None, metavar="SAME,AB",
                     help="fixed sigma launch codes for both precisions instead of the autotuner (profiling runs)")
     return ap.parse_args()
@@ -216,6 +220,54 @@ def load_workload(name: str):
         base, scale = name.split("@", 1)
         return synth.config(base, float(scale))
     return synth.config(name)
+
+
+def run_batched(args) -> dict:
+    """64 subspaces sharing one Hamiltonian (L=40, 8+8 electrons, Na and Nb
+    log-uniform in [200, 4000]), 2 roots each to the Davidson tolerance:
+    batched mixed precision (concurrent solves) against the same subspaces
+    solved one after another (FP64 and mixed)."""
+    import sbdx
+    from sbdx import synth
+
+    subs = synth.batched_config()
+    p0 = subs[0]
+    pairs = []
+    for p in subs:  # det-pairs of one sigma of each subspace, from its connectivity lengths
+        with sbdx.Context(0) as ctx:
+            ctx.load(p)
+            ctx.build_connectivity()
+            sa, da, _ = ctx.connectivity(0)
+            sb, db, _ = ctx.connectivity(1)
+            pairs.append(synth.det_pairs(sa, da, sb, db)["total"])
+    out = {"workload": "64 subspaces, L=40, 8a+8b electrons, Na, Nb log-uniform in [200, 4000], K=96 integrals",
+           "subspaces": len(subs), "dets": int(sum(p.D for p in subs)),
+           "dets_min": int(min(p.D for p in subs)), "dets_max": int(max(p.D for p in subs)),
+           "nroots": 2, "tol": args.davidson_tol}
+    with sbdx.Batch(p0.L, p0.I0, p0.h, p0.eri) as batch:
+        for p in subs:
+            batch.add(p.alpha, p.beta)
+        out["tuning"] = batch.tune()
+        runs = {}
+        ref_E = None
+        for label, prec, threads in (("sequential_fp64", sbdx.SBDX_FP64, 1), ("sequential_mixed", sbdx.SBDX_FP32, 1),
+                                     ("batched_fp64", sbdx.SBDX_FP64, args.batch_threads),
+                                     ("batched_mixed", sbdx.SBDX_FP32, args.batch_threads)):
+            E, R, infos, sec = batch.solve(nroots=2, max_it=100, max_nb=12, eps=args.davidson_tol, precision=prec,
+                                           nthreads=threads)
+            if ref_E is None:
+                ref_E = E
+            nsig = [i.n_sigma + i.n_sigma64 for i in infos]
+            t_sub = [i.seconds for i in infos]
+            runs[label] = {"seconds": sec, "threads": threads, "converged": int(sum(i.converged for i in infos)),
+                           "sigmas": int(sum(nsig)), "max_abs_dE_vs_sequential_fp64": float(np.abs(E - ref_E).max()),
+                           "max_residual": float(R.max()),
+                           "sigma_det_pairs_per_s": float(sum(n * q for n, q in zip(nsig, pairs)) / sec),
+                           "subspace_seconds_median": float(np.median(t_sub)),
+                           "subspace_seconds_max": float(np.max(t_sub))}
+        out["runs"] = runs
+        out["speedup_batched_mixed_vs_sequential_fp64"] = runs["sequential_fp64"]["seconds"] / runs["batched_mixed"]["seconds"]
+    return out
 
 
 def run_reference_arm(args, rank, world):
@@ -388,6 +440,11 @@ def run_ours(args, rank, world, local):
                                       "dE_vs_fp64": (E32 - E64).tolist()},
                             "speedup_mixed_vs_fp64": f64.seconds / f32.seconds if f32.seconds > 0 else None}
 
+    # ---- batched subspaces (64 independent solves sharing one Hamiltonian) ---------
+    batched = None
+    if not args.no_davidson and not args.no_batched and world == 1:
+        batched = run_batched(args)
+
     # ---- CPU baseline (reference OpenMP mult, bounded sample, rank 0, N=1) -------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -434,6 +491,7 @@ def run_ours(args, rank, world, local):
                        "phases": {k: {"ms": phases32[k], "gbs": pb32[k] / (phases32[k] * 1e-3) / 1e9}
                                   for k in phases32}},
         "davidson": dav,
+        "batched": batched,
         "cpu_baseline": cpu,
     }
     if rank == 0:
