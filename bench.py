@@ -463,6 +463,8 @@ def run_ours(args, rank, world, local):
     pb = phase_bytes(prob, dp, 8)
     pb32 = phase_bytes(prob, dp, 4)
     kern = PHASE_KERNELS[dominant]
+    if dominant == "alpha_beta" and tune[1] // 10 == 7:
+        kern = "sigma_ab_v7"  # code 71: packed staged rows
     achieved = pb[dominant] / (phases[dominant] * 1e-3) / 1e9
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
