@@ -185,7 +185,7 @@ void free_conn(Conn& c) {
   cudaFree(c.srec); cudaFree(c.order); cudaFree(c.spos);
   cudaFree(c.sell); cudaFree(c.soff); cudaFree(c.slen);
   auto free_panel = [](SellPanel& p) {
-    cudaFree(p.sell); cudaFree(p.soff); cudaFree(p.slen); cudaFree(p.vrow);
+    cudaFree(p.sell); cudaFree(p.sell32); cudaFree(p.soff); cudaFree(p.slen); cudaFree(p.vrow);
     cudaFree(p.split_row); cudaFree(p.split_slot);
   };
   free_panel(c.bal);
@@ -323,6 +323,15 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
   P.cap = (int)cap;
   P.slices_per_warp = ks;
   if (split_row.empty()) split_row.push_back(0);
+  std::vector<uint32_t> sell32(sell.size());
+  for (size_t q = 0; q < sell.size(); ++q) {
+    const uint64_t r = sell[q];
+    sell32[q] = (uint32_t)(r & 0xffffu) | (uint32_t)(((r >> 16) & 0xfffu) << 16) |
+                (uint32_t)(((r >> 40) & 1u) << 28) | (uint32_t)(((r >> 41) & 1u) << 29);
+  }
+  SBDX_CUDA(c, cudaMalloc(&P.sell32, sizeof(uint32_t) * sell32.size()));
+  SBDX_CUDA(c, cudaMemcpyAsync(P.sell32, sell32.data(), sizeof(uint32_t) * sell32.size(), cudaMemcpyHostToDevice,
+                               c->stream));
   SBDX_CUDA(c, cudaMalloc(&P.sell, sizeof(uint64_t) * sell.size()));
   SBDX_CUDA(c, cudaMalloc(&P.soff, sizeof(uint64_t) * (ns + 1)));
   SBDX_CUDA(c, cudaMalloc(&P.slen, sizeof(uint32_t) * slen.size()));

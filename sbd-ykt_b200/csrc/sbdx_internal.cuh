@@ -45,6 +45,9 @@ constexpr uint32_t kInfoSingle = 1u << 30;
 // bit 41 set.
 struct SellPanel {
   uint64_t* sell = nullptr;        // [soff[nslice]]
+  // the same records in 32 bits (bits 0-15 ket, 16-27 pair index, 28 sign,
+  // 29 padding), read by the packed alpha-beta kernel
+  uint32_t* sell32 = nullptr;      // [soff[nslice]]
   uint64_t* soff = nullptr;        // [nslice + 1]
   uint32_t* slen = nullptr;        // [nslice]
   uint32_t* vrow = nullptr;        // [nv]
