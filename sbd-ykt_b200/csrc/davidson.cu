@@ -51,6 +51,31 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return t;  // valid in thread 0
 }
 
+// Four consecutive elements as doubles. The vector kernels below take this
+// path for element quads when D % 4 == 0: every vector of the solvers starts
+// at a cudaMalloc base plus a multiple of D elements, so quads are 16-byte
+// aligned; the remaining elements (or all, when D % 4 != 0) go one by one.
+__device__ __forceinline__ void ld4(const float* p, double (&o)[4]) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&o)[4]) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+// coherent load (the kernel also writes this vector)
+__device__ __forceinline__ void ld4_rw(const double* p, double (&o)[4]) {
+  const double2 a = reinterpret_cast<const double2*>(p)[0];
+  const double2 b = reinterpret_cast<const double2*>(p)[1];
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ size_t quads(size_t D) { return D % 4 == 0 ? D / 4 : 0; }
+
 // partial[k * gridDim.x + blk] = partial sums of <V_k, x>, k in [k0, k0+mc)
 template <typename TV, typename TX>
 __global__ void __launch_bounds__(kRedThreads)
@@ -62,7 +87,20 @@ multidot_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restric
   double acc[kDotChunk];
 #pragma unroll
   for (int k = 0; k < kDotChunk; ++k) acc[k] = 0.0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nq = quads(D);
+  for (size_t q = t0; q < nq; q += st) {
+    double xv[4];
+    ld4(x + 4 * q, xv);
+#pragma unroll
+    for (int k = 0; k < kDotChunk; ++k)
+      if (k < mc) {
+        double vv[4];
+        ld4(V + (size_t)(k0 + k) * ldv + 4 * q, vv);
+        acc[k] = fma(vv[0], xv[0], fma(vv[1], xv[1], fma(vv[2], xv[2], fma(vv[3], xv[3], acc[k]))));
+      }
+  }
+  for (size_t s = 4 * nq + t0; s < D; s += st) {
     const double xv = (double)x[s];
 #pragma unroll
     for (int k = 0; k < kDotChunk; ++k)
@@ -396,7 +434,36 @@ update_anchor_kernel(const TV* __restrict__ C, const TV* __restrict__ HC, size_t
   __syncthreads();
   const double th = *thetap;
   double nw = 0.0, nr = 0.0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nq = quads(D);
+  for (size_t q = t0; q < nq; q += st) {
+    double w[4], hw[4];
+    ld4_rw(W + 4 * q, w);
+    ld4_rw(HW + 4 * q, hw);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) { w[e] *= u0; hw[e] *= u0; }
+    for (int k = 0; k < m; ++k) {
+      double cv[4], hv[4];
+      ld4(C + (size_t)k * ldv + 4 * q, cv);
+      ld4(HC + (size_t)k * ldv + 4 * q, hv);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        w[e] = fma(cv[e], su[k], w[e]);
+        hw[e] = fma(hv[e], su[k], hw[e]);
+      }
+    }
+    double r[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      r[e] = th * w[e] - hw[e];
+      nw = fma(w[e], w[e], nw);
+      nr = fma(r[e], r[e], nr);
+    }
+    st4(W + 4 * q, w);
+    st4(HW + 4 * q, hw);
+    st4(R + 4 * q, r);
+  }
+  for (size_t s = 4 * nq + t0; s < D; s += st) {
     double w = u0 * W[s], hw = u0 * HW[s];
     for (int k = 0; k < m; ++k) {
       w = fma((double)C[(size_t)k * ldv + s], su[k], w);
@@ -479,7 +546,22 @@ multidot2_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restri
   double a0[kDotChunk], a1[kDotChunk];
 #pragma unroll
   for (int k = 0; k < kDotChunk; ++k) a0[k] = a1[k] = 0.0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nq = quads(D);
+  for (size_t q = t0; q < nq; q += st) {
+    double y0[4], y1[4];
+    ld4(x0 + 4 * q, y0);
+    ld4(x1 + 4 * q, y1);
+#pragma unroll
+    for (int k = 0; k < kDotChunk; ++k)
+      if (k < mc) {
+        double v[4];
+        ld4(V + (size_t)(k0 + k) * ldv + 4 * q, v);
+        a0[k] = fma(v[0], y0[0], fma(v[1], y0[1], fma(v[2], y0[2], fma(v[3], y0[3], a0[k]))));
+        a1[k] = fma(v[0], y1[0], fma(v[1], y1[1], fma(v[2], y1[2], fma(v[3], y1[3], a1[k]))));
+      }
+  }
+  for (size_t s = 4 * nq + t0; s < D; s += st) {
     const double y0 = (double)x0[s], y1 = (double)x1[s];
 #pragma unroll
     for (int k = 0; k < kDotChunk; ++k)
@@ -507,7 +589,25 @@ gs_subtract_kernel(double* __restrict__ v, const double* __restrict__ W, const T
   for (int k = threadIdx.x; k <= m; k += blockDim.x) so[k] = o[k];
   __syncthreads();
   double nn = 0.0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nq = quads(D);
+  for (size_t q = t0; q < nq; q += st) {
+    double x[4], w[4];
+    ld4_rw(v + 4 * q, x);
+    ld4(W + 4 * q, w);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) x[e] = fma(-so[0], w[e], x[e]);
+    for (int k = 0; k < m; ++k) {
+      double vk[4];
+      ld4(V + (size_t)k * ldv + 4 * q, vk);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) x[e] = fma(-so[k + 1], vk[e], x[e]);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) nn = fma(x[e], x[e], nn);
+    st4(v + 4 * q, x);
+  }
+  for (size_t s = 4 * nq + t0; s < D; s += st) {
     double x = fma(-so[0], W[s], v[s]);
     for (int k = 0; k < m; ++k) x = fma(-so[k + 1], (double)V[(size_t)k * ldv + s], x);
     v[s] = x;
@@ -824,7 +924,28 @@ gs_subtract_block_kernel(double* __restrict__ v, const double* __restrict__ A, i
   for (int k = threadIdx.x; k < na + m; k += blockDim.x) so[k] = o[k];
   __syncthreads();
   double nn = 0.0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nq = quads(D);
+  for (size_t q = t0; q < nq; q += st) {
+    double x[4];
+    ld4_rw(v + 4 * q, x);
+    for (int a = 0; a < na; ++a) {
+      double w[4];
+      ld4(A + (size_t)a * D + 4 * q, w);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) x[e] = fma(-so[a], w[e], x[e]);
+    }
+    for (int k = 0; k < m; ++k) {
+      double vk[4];
+      ld4(V + (size_t)k * D + 4 * q, vk);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) x[e] = fma(-so[na + k], vk[e], x[e]);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) nn = fma(x[e], x[e], nn);
+    st4(v + 4 * q, x);
+  }
+  for (size_t s = 4 * nq + t0; s < D; s += st) {
     double x = v[s];
     for (int a = 0; a < na; ++a) x = fma(-so[a], A[(size_t)a * D + s], x);
     for (int k = 0; k < m; ++k) x = fma(-so[na + k], (double)V[(size_t)k * D + s], x);
