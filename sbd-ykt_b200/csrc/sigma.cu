@@ -1148,6 +1148,111 @@ sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __res
   }
 }
 
+// FP32-storage variant of sigma_same_v6_kernel: products and short runs of up
+// to kRun entries are summed in FP32, and each run's sum is added to the FP64
+// row accumulator (one conversion per run and column instead of one per pair).
+constexpr int kRun = 8;
+
+template <int VEC> struct VecF;
+template <> struct VecF<1> {
+  static __device__ __forceinline__ void load(const float* p, float* o) { o[0] = __ldg(p); }
+};
+template <> struct VecF<2> {
+  static __device__ __forceinline__ void load(const float* p, float* o) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    o[0] = v.x; o[1] = v.y;
+  }
+};
+template <> struct VecF<4> {
+  static __device__ __forceinline__ void load(const float* p, float* o) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+  }
+};
+template <> struct VecF<8> {
+  static __device__ __forceinline__ void load(const float* p, float* o) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    const float4 w = __ldg(reinterpret_cast<const float4*>(p) + 1);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; o[4] = w.x; o[5] = w.y; o[6] = w.z; o[7] = w.w;
+  }
+};
+
+template <int VEC>
+__global__ void __launch_bounds__(kSameThreads)
+sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, const uint64_t* __restrict__ off,
+                      const uint32_t* __restrict__ nsing, const uint32_t* __restrict__ ket,
+                      const float* __restrict__ val, const uint32_t* __restrict__ info, const float* __restrict__ Dt,
+                      size_t dstride, const double* __restrict__ hii, double* __restrict__ Y) {
+  __shared__ uint32_t s_ket[kSameThreads], s_pq[kSameThreads];
+  __shared__ float s_val[kSameThreads];
+  const size_t r = blockIdx.x;
+  const size_t c0 = ((size_t)blockIdx.y * kSameThreads + threadIdx.x) * VEC;
+  const bool active = c0 < ncol;
+  double acc[VEC];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) acc[v] = 0.0;
+  if (hii != nullptr && active) {
+    float x[VEC];
+    VecF<VEC>::load(X + r * ncol + c0, x);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = hii[r * ncol + c0 + v] * (double)x[v];
+  }
+  const uint64_t beg = off[r], end = off[r + 1], send = beg + nsing[r];
+  const unsigned t = threadIdx.x;
+  for (uint64_t base = beg; base < end; base += kSameThreads) {
+    const int cnt = (int)min((uint64_t)kSameThreads, end - base);
+    const int nsb = send > base ? (int)min((uint64_t)cnt, send - base) : 0;
+    __syncthreads();
+    if ((int)t < cnt) {
+      const uint64_t e = base + t;
+      const uint32_t inf = info[e];
+      const float v = val[e];
+      s_ket[t] = ket[e];
+      s_val[t] = (inf >> 31) ? -v : v;
+      s_pq[t] = ((inf >> 12) & 0xfffu) | (inf & kInfoNeg);
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (int e0 = 0; e0 < nsb; e0 += kRun) {  // singles: value + signed Coulomb-table element
+      const int e1 = min(e0 + kRun, nsb);
+      float pf[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) pf[v] = 0.f;
+      for (int e = e0; e < e1; ++e) {
+        const uint32_t pqs = s_pq[e];
+        const float hv = s_val[e];
+        float x[VEC], d[VEC];
+        VecF<VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+        VecF<VEC>::load(Dt + (size_t)(pqs & 0xfffu) * dstride + c0, d);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) pf[v] = fmaf(hv + ((pqs >> 31) ? -d[v] : d[v]), x[v], pf[v]);
+      }
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) acc[v] += (double)pf[v];
+    }
+    for (int e0 = nsb; e0 < cnt; e0 += kRun) {  // doubles
+      const int e1 = min(e0 + kRun, cnt);
+      float pf[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) pf[v] = 0.f;
+#pragma unroll 4
+      for (int e = e0; e < e1; ++e) {
+        const float hv = s_val[e];
+        float x[VEC];
+        VecF<VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) pf[v] = fmaf(hv, x[v], pf[v]);
+      }
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) acc[v] += (double)pf[v];
+    }
+  }
+  if (active) {
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) Y[r * ncol + c0 + v] = acc[v];
+  }
+}
+
 constexpr int kAb6Threads = 1024;
 
 // Alpha single x beta single in the alpha-first basis, balanced. One CTA per
@@ -1277,9 +1382,9 @@ template <> struct RowPack<float> {
   static __device__ __forceinline__ void set(P& p, int e, float v) {
     if (e == 0) p.x = v; else if (e == 1) p.y = v; else if (e == 2) p.z = v; else p.w = v;
   }
+  // the 4-term dot of one record in FP32, added to the FP64 row sum by the caller
   static __device__ __forceinline__ double dot(const P& a, const P& b) {
-    return fma((double)a.x, (double)b.x,
-               fma((double)a.y, (double)b.y, fma((double)a.z, (double)b.z, (double)a.w * (double)b.w)));
+    return (double)fmaf(a.x, b.x, fmaf(a.y, b.y, fmaf(a.z, b.z, a.w * b.w)));
   }
 };
 
@@ -1450,8 +1555,13 @@ template <typename T, int VEC>
 int launch_same_v6(Ctx* c, const T* X, size_t nrow, size_t ncol, const Conn& cn, const typename Prec<T>::V* val,
                    const typename Prec<T>::V* Dt, size_t dstride, const double* hii, double* Y) {
   dim3 grid((unsigned)nrow, (unsigned)((ncol + (size_t)kSameThreads * VEC - 1) / ((size_t)kSameThreads * VEC)));
-  sigma_same_v6_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, cn.off, cn.nsing, cn.ket, val, cn.info,
-                                                                     Dt, dstride, hii, Y);
+  if constexpr (std::is_same<T, float>::value) {
+    sigma_same_v6f_kernel<VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, cn.off, cn.nsing, cn.ket, val, cn.info,
+                                                                      Dt, dstride, hii, Y);
+  } else {
+    sigma_same_v6_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, cn.off, cn.nsing, cn.ket, val, cn.info,
+                                                                       Dt, dstride, hii, Y);
+  }
   SBDX_LAUNCHED(c);
   return 0;
 }
