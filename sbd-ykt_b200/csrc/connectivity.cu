@@ -282,8 +282,10 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
   // the sum). Per slice, step m and quarter-warp (8 lanes, one 128-byte
   // shared-memory wavefront of 16-byte loads), pick for every lane the record
   // whose ket index and pair index fall in the least used of the 8 bank slots
-  // (index mod 8), most constrained lane first: fewer bank conflicts on the
-  // two shared-memory loads of each record.
+  // (index mod 8), most constrained lane first, then improve the picks by
+  // local search on the quarter's wavefront count (distinct indices per slot;
+  // equal indices are broadcast): fewer bank conflicts on the two
+  // shared-memory loads of each record.
   std::vector<std::vector<uint64_t>> left(32);
   for (size_t sl = 0; sl < ns; ++sl) {
     const size_t l_end = std::min<size_t>(32, nv - sl * 32);
@@ -294,25 +296,68 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
     }
     for (uint32_t m = 0; m < slen[sl]; ++m)
       for (size_t q = 0; q * 8 < l_end; ++q) {
-        int cj[8] = {0}, cp[8] = {0};
         size_t lanes[8];
         size_t nl = 0;
         for (size_t l = q * 8; l < std::min(l_end, q * 8 + 8); ++l)
           if (!left[l].empty()) lanes[nl++] = l;
         std::sort(lanes, lanes + nl, [&](size_t x, size_t y) { return left[x].size() < left[y].size(); });
+        // greedy start: least used slots first, most constrained lane first
+        size_t pick[8];
+        {
+          int cj[8] = {0}, cp[8] = {0};
+          for (size_t i = 0; i < nl; ++i) {
+            const std::vector<uint64_t>& lst = left[lanes[i]];
+            size_t best = 0;
+            int bc = 1 << 30;
+            for (size_t t = 0; t < lst.size(); ++t) {
+              const int c = cj[lst[t] & 7u] + cp[(lst[t] >> 16) & 7u];
+              if (c < bc) { bc = c; best = t; }
+            }
+            pick[i] = best;
+            ++cj[lst[best] & 7u];
+            ++cp[(lst[best] >> 16) & 7u];
+          }
+        }
+        // local search on the wavefront count of the quarter: per slot, the
+        // number of distinct ket (and pair) indices, maximum over slots
+        auto wavefronts = [&]() {
+          int w = 0;
+          for (int field = 0; field < 2; ++field) {
+            int worst = 0;
+            for (int slot = 0; slot < 8; ++slot) {
+              uint32_t seen[8];
+              int nd = 0;
+              for (size_t i = 0; i < nl; ++i) {
+                const uint64_t r = left[lanes[i]][pick[i]];
+                const uint32_t idx = field == 0 ? (uint32_t)(r & 0xffffu) : (uint32_t)((r >> 16) & 0xfffu);
+                if ((idx & 7u) != (uint32_t)slot) continue;
+                bool dup = false;
+                for (int d = 0; d < nd; ++d) dup |= seen[d] == idx;
+                if (!dup) seen[nd++] = idx;
+              }
+              worst = std::max(worst, nd);
+            }
+            w += worst;
+          }
+          return w;
+        };
+        int cur = wavefronts();
+        for (int pass = 0; pass < 3; ++pass) {
+          bool better = false;
+          for (size_t i = 0; i < nl; ++i)
+            for (size_t t = 0; t < left[lanes[i]].size(); ++t) {
+              if (t == pick[i]) continue;
+              const size_t old = pick[i];
+              pick[i] = t;
+              const int w = wavefronts();
+              if (w < cur) { cur = w; better = true; } else { pick[i] = old; }
+            }
+          if (!better) break;
+        }
         for (size_t i = 0; i < nl; ++i) {
           std::vector<uint64_t>& lst = left[lanes[i]];
-          size_t best = 0;
-          int bc = 1 << 30;
-          for (size_t t = 0; t < lst.size(); ++t) {
-            const int c = cj[lst[t] & 7u] + cp[(lst[t] >> 16) & 7u];
-            if (c < bc) { bc = c; best = t; }
-          }
-          const uint64_t r = lst[best];
-          lst.erase(lst.begin() + (std::ptrdiff_t)best);
-          ++cj[r & 7u];
-          ++cp[(r >> 16) & 7u];
-          sell[soff[sl] + 32ull * m + lanes[i]] = r;
+          sell[soff[sl] + 32ull * m + lanes[i]] = lst[pick[i]];
+          lst.erase(lst.begin() + (std::ptrdiff_t)pick[i]);
         }
       }
   }

@@ -137,7 +137,38 @@ combine_kernel(const TV* __restrict__ C, const TV* __restrict__ HC, size_t ldv, 
   __syncthreads();
   const double E0 = *E0p;
   double nw = 0.0, nr = 0.0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nq = quads(D);
+  for (size_t q = t0; q < nq; q += st) {
+    double w[4] = {0.0, 0.0, 0.0, 0.0}, hw[4] = {0.0, 0.0, 0.0, 0.0};
+    if (W0 != nullptr) {
+      double a[4], b[4];
+      ld4(W0 + 4 * q, a);
+      ld4(HW0 + 4 * q, b);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) { w[e] = u0 * a[e]; hw[e] = u0 * b[e]; }
+    }
+    for (int k = 0; k < m; ++k) {
+      double cv[4], hv[4];
+      ld4(C + (size_t)k * ldv + 4 * q, cv);
+      ld4(HC + (size_t)k * ldv + 4 * q, hv);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        w[e] = fma(cv[e], su[k], w[e]);
+        hw[e] = fma(hv[e], su[k], hw[e]);
+      }
+    }
+    double r[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      r[e] = E0 * w[e] - hw[e];
+      nw = fma(w[e], w[e], nw);
+      nr = fma(r[e], r[e], nr);
+    }
+    st4(W + 4 * q, w);
+    st4(R + 4 * q, r);
+  }
+  for (size_t s = 4 * nq + t0; s < D; s += st) {
     double w = 0.0, hw = 0.0;
     if (W0 != nullptr) { w = u0 * W0[s]; hw = u0 * HW0[s]; }
     for (int k = 0; k < m; ++k) {
@@ -188,7 +219,25 @@ axpy_dot_kernel(double* __restrict__ v, const TV* __restrict__ Vk, const double*
   __shared__ double sh[kRedThreads / 32];
   const double olap = -(*olap_p);
   double acc = 0.0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nq = quads(D);
+  for (size_t q = t0; q < nq; q += st) {
+    double bq[4], x[4], y[4];
+    if (Vkd != nullptr) ld4(Vkd + 4 * q, bq); else ld4(Vk + 4 * q, bq);
+    ld4_rw(v + 4 * q, x);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) x[e] = fma(bq[e], olap, x[e]);
+    st4(v + 4 * q, x);
+    if (Vn != nullptr) {
+      ld4(Vn + 4 * q, y);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc = fma(y[e], x[e], acc);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc = fma(x[e], x[e], acc);
+    }
+  }
+  for (size_t s = 4 * nq + t0; s < D; s += st) {
     const double b = Vkd != nullptr ? Vkd[s] : (double)Vk[s];
     const double x = fma(b, olap, v[s]);
     v[s] = x;
@@ -655,6 +704,19 @@ int expand_olsen(Ctx* c, Work& wk, const double* R, const double* W, const float
   return 0;
 }
 
+// W_r, HW_r, R_r *= f[r] for r < k (f in device memory).
+__global__ void scale_anchors_kernel(double* W, double* HW, double* R, const double* __restrict__ f, int k, size_t D) {
+  for (int r = 0; r < k; ++r) {
+    const double g = f[r];
+    if (g == 1.0) continue;
+    for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+      W[(size_t)r * D + s] *= g;
+      HW[(size_t)r * D + s] *= g;
+      R[(size_t)r * D + s] *= g;
+    }
+  }
+}
+
 // ---- FP32 storage with FP64 defect correction --------------------------------
 // Generalised Rayleigh-Ritz M x = theta S x over the basis [W, C_0..C_{nv-1}]:
 // the C_j are orthonormal among themselves (MGS), the anchor W is not
@@ -715,6 +777,10 @@ bool gen_eigen(int n, const std::vector<double>& M, const std::vector<double>& S
 // convergence is decided on the exact FP64 residual only. On a full subspace
 // the newest third of the corrections is kept (thick restart).
 constexpr double kRefreshDrop = 1e-4;
+// Exact refresh also when the largest estimated residual has not fallen below
+// kStallGain times its best value for kStallSteps consecutive steps.
+constexpr double kStallGain = 0.7;
+constexpr int kStallSteps = 6;
 
 int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info) {
   const size_t D = c->na * c->nb;
@@ -777,8 +843,8 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
     return 0;
   };
   if ((rc = refresh())) return rc;
-  double r_ref = normR;
-  int steps = 0, since = 0;
+  double r_ref = normR, best = 1e300;
+  int steps = 0, since = 0, stale = 0;
   bool stalled = false;
   const int max_steps = p.max_it * p.max_nb;
   while (true) {
@@ -856,10 +922,20 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
       double nrm[2];
       SBDX_CUDA(c, cudaMemcpyAsync(nrm, s + kNW, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
       SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
-      const double r_est = std::sqrt(nrm[1]);
-      if (std::fabs(nrm[0] - 1.0) > 1e-6) {
+      if (!(nrm[0] > 0.5 && nrm[0] < 2.0)) {
         c->err = "davidson (FP32): Ritz vector lost its normalisation";
         return 5;
+      }
+      // renormalise (the rounding of x^T S x = 1 would accumulate otherwise)
+      const double fs = std::fabs(nrm[0] - 1.0) > 1e-13 ? 1.0 / std::sqrt(nrm[0]) : 1.0;
+      const double r_est = std::sqrt(nrm[1]) * fs;
+      if (fs != 1.0) {
+        SBDX_CUDA(c, cudaMemcpyAsync(s + kNW, &fs, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        scale_anchors_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, R, s + kNW, 1, D);
+        SBDX_LAUNCHED(c);
+        const double nr2 = r_est * r_est;
+        SBDX_CUDA(c, cudaMemcpyAsync(s + kNR, &nr2, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // fs, nr2 are host locals
       }
       // projected row of the new anchor: x^T M, x^T S
       for (int k = 0; k < n; ++k) {
@@ -868,8 +944,8 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
           sm += x[i] * M[std::min(i, k) + (size_t)ld * std::max(i, k)];
           ss += x[i] * S[std::min(i, k) + (size_t)ld * std::max(i, k)];
         }
-        row[k] = sm;
-        row[ld + k] = ss;
+        row[k] = sm * fs;
+        row[ld + k] = ss * fs;
       }
       for (int k = 1; k < n; ++k) { set_pair(M, 0, k, row[k]); set_pair(S, 0, k, row[ld + k]); }
       set_pair(M, 0, 0, theta);
@@ -879,13 +955,19 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
         std::printf("   step %d: theta=%.12f est.res=%.3e\n", steps, theta, r_est);
         std::fflush(stdout);
       }
-      const bool due = period > 0 ? since >= period : (r_est < kRefreshDrop * r_ref || r_est < p.eps);
+      // stagnation: the FP32 error carried by HW bounds the estimated residual
+      // from below; an exact refresh clears it
+      if (r_est < kStallGain * best) { best = r_est; stale = 0; } else { ++stale; }
+      const bool due = period > 0 ? since >= period
+                                  : (r_est < kRefreshDrop * r_ref || r_est < p.eps || stale >= kStallSteps);
       if (due || steps >= max_steps || seconds_since(t0) > p.max_time) exact = true;
     }
     if (stalled) break;
     if ((rc = refresh())) return rc;
     r_ref = normR;
     since = 0;
+    best = 1e300;
+    stale = 0;
   }
   SBDX_CUDA(c, cudaMemcpyAsync(dW, W, sizeof(double) * D, cudaMemcpyDeviceToDevice, c->stream));
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1241,7 +1323,8 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
   };
   if ((rc = refresh())) return rc;
   double r_ref = *std::max_element(r_exact.begin(), r_exact.end());
-  int steps = 0, since = 0;
+  int steps = 0, since = 0, stale = 0;
+  double best = 1e300;
   const int max_steps = p.max_it * p.max_nb;
   bool stalled = false;
   auto all_below = [&](const std::vector<double>& x) {
@@ -1329,13 +1412,32 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
       std::swap(HW, HWn);
       SBDX_CUDA(c, cudaMemcpyAsync(h.data(), s + kbNW2, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->stream));
       SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+      if (p.verbose) {
+        std::printf("   step %d: |W'|^2 - 1 =", steps);
+        for (int r = 0; r < k; ++r) std::printf(" %.3e", h[r] - 1.0);
+        std::printf(", n = %d\n", k + nv);
+        std::fflush(stdout);
+      }
+      // renormalise: x^T S x = 1 up to rounding, which would otherwise
+      // accumulate over the steps between refreshes
+      double fscale[kMaxRoots];
+      bool rescale = false;
       for (int r = 0; r < k; ++r) {
-        if (std::fabs(h[r] - 1.0) > 1e-6) {
+        if (!(h[r] > 0.5 && h[r] < 2.0)) {
           c->err = "davidson: Ritz vector lost its normalisation";
           return 5;
         }
-        r_est[r] = std::sqrt(h[4 + r]);
+        fscale[r] = std::fabs(h[r] - 1.0) > 1e-13 ? 1.0 / std::sqrt(h[r]) : 1.0;
+        rescale |= fscale[r] != 1.0;
+        r_est[r] = std::sqrt(h[4 + r]) * fscale[r];
         E[r] = theta[r];
+      }
+      if (rescale) {
+        SBDX_CUDA(c, cudaMemcpyAsync(s + kbNW2, fscale, sizeof(double) * k, cudaMemcpyHostToDevice, c->stream));
+        scale_anchors_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, R, s + kbNW2, k, D);
+        SBDX_LAUNCHED(c);
+        for (int r = 0; r < k; ++r) h[4 + r] = r_est[r] * r_est[r];
+        SBDX_CUDA(c, cudaMemcpyAsync(s + kbNR2, h.data() + 4, sizeof(double) * k, cudaMemcpyHostToDevice, c->stream));
       }
       // projected rows of the new anchors: X^T M, X^T S (anchor block: diag(theta), I)
       for (int r = 0; r < k; ++r)
@@ -1345,8 +1447,8 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
             sm += X[i + (size_t)n * r] * M[std::min(i, q) + (size_t)ld * std::max(i, q)];
             ss += X[i + (size_t)n * r] * S[std::min(i, q) + (size_t)ld * std::max(i, q)];
           }
-          rowM[(size_t)r * ld + q] = sm;
-          rowS[(size_t)r * ld + q] = ss;
+          rowM[(size_t)r * ld + q] = sm * fscale[r];
+          rowS[(size_t)r * ld + q] = ss * fscale[r];
         }
       for (int r = 0; r < k; ++r) {
         for (int j = 0; j < nv; ++j) {
@@ -1368,9 +1470,15 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
         if (all_below(r_exact) || steps >= max_steps || seconds_since(t0) > p.max_time) break;
         continue;
       }
-      const bool due = period > 0 ? since >= period : (worst < kRefreshDrop * r_ref || all_below(r_est));
+      // stagnation: the FP32 error carried by HW bounds the estimated
+      // residual from below; an exact refresh clears it
+      if (worst < kStallGain * best) { best = worst; stale = 0; } else { ++stale; }
+      const bool due = period > 0 ? since >= period
+                                  : (worst < kRefreshDrop * r_ref || all_below(r_est) || stale >= kStallSteps);
       if (due || steps >= max_steps || seconds_since(t0) > p.max_time) exact = true;
     }
+    best = 1e300;
+    stale = 0;
     if (stalled) break;
     if (kMixed) {
       if ((rc = refresh())) return rc;
