@@ -1,12 +1,12 @@
 /*
  * Command-line front end of the reference build (test infrastructure only).
  *
- *   sbd_ref_cli sigma-sample <input.bin> <rows> <reps> <threads>
+ *   sbd_ref_cli sigma-sample <input.bin> <rows> <reps> <threads> [<row0>]
  *
  * Reads a problem written by sbdx.synth.write_problem_bin (header: L, nelec,
  * na, nb as int64; I0; h[L*L]; eri[packed]; alpha strings; beta strings), runs
  * the reference's own sigma (mult.h:376-632) restricted to bra alpha rows
- * [0, rows) `reps` times (helpers built once), and prints one JSON line per
+ * [row0, row0 + rows) (row0 = 0 by default) `reps` times (helpers built once), and prints one JSON line per
  * run with the seconds and the number of off-diagonal det-pairs evaluated.
  */
 #include <cstdio>
@@ -17,15 +17,15 @@
 #include <string>
 #include <omp.h>
 
-extern "C" double ref_sigma_sample_multi(int L, int nelec, double I0, const double* h,
+extern "C" double ref_sigma_sample_range(int L, int nelec, double I0, const double* h,
                                          const double* eri, int bit_length, const uint64_t* astr,
                                          size_t na, const uint64_t* bstr, size_t nb, const double* C,
-                                         double* S, size_t rows, int threads, int reps,
+                                         double* S, size_t row0, size_t rows, int threads, int reps,
                                          double* seconds, double* pairs);
 
 int main(int argc, char** argv) {
   if (argc < 6 || std::string(argv[1]) != "sigma-sample") {
-    std::fprintf(stderr, "usage: %s sigma-sample <input.bin> <rows> <reps> <threads>\n", argv[0]);
+    std::fprintf(stderr, "usage: %s sigma-sample <input.bin> <rows> <reps> <threads> [<row0>]\n", argv[0]);
     return 2;
   }
   FILE* f = std::fopen(argv[2], "rb");
@@ -47,6 +47,7 @@ int main(int argc, char** argv) {
   size_t rows = (size_t)std::atoll(argv[3]);
   int reps = std::atoi(argv[4]);
   int threads = std::atoi(argv[5]);
+  const size_t row0 = argc > 6 ? (size_t)std::atoll(argv[6]) : 0;
   if (threads <= 0) threads = omp_get_max_threads();
   std::vector<double> C(na * nb);
   uint64_t s = 0x9E3779B97F4A7C15ull;
@@ -56,11 +57,11 @@ int main(int argc, char** argv) {
   }
   std::vector<double> secs(reps > 0 ? reps : 1);
   double pairs = 0;
-  ref_sigma_sample_multi(L, nelec, I0, h.data(), eri.data(), 20, a.data(), na, b.data(), nb, C.data(),
-                         nullptr, rows, threads, reps, secs.data(), &pairs);
+  ref_sigma_sample_range(L, nelec, I0, h.data(), eri.data(), 20, a.data(), na, b.data(), nb, C.data(),
+                         nullptr, row0, rows, threads, reps, secs.data(), &pairs);
   for (int r = 0; r < reps; ++r)
-    std::printf("{\"seconds\": %.6f, \"pairs\": %.0f, \"rows\": %zu, \"threads\": %d}\n", secs[r],
-                pairs, rows, threads);
+    std::printf("{\"seconds\": %.6f, \"pairs\": %.0f, \"rows\": %zu, \"row0\": %zu, \"threads\": %d}\n",
+                secs[r], pairs, rows, row0, threads);
   std::fflush(stdout);
   return 0;
 }

@@ -178,25 +178,27 @@ void ref_sigma(int L, int nelec, double I0, const double* h, const double* eri, 
 
 /* A bounded sample of the reference sigma for CPU-baseline timing: the
  * reference mult over helpers whose bra alpha range is restricted to
- * [0, rows) (ket ranges stay full), exactly the per-task loops of
- * mult.h:453-610. The helpers are built once; mult runs `reps` times and
- * seconds[r] receives the duration of run r. *pairs receives the number of
- * off-diagonal det-pairs one run evaluates. Returns the mean seconds. */
-double ref_sigma_sample_multi(int L, int nelec, double I0, const double* h, const double* eri,
+ * [row0, row0 + rows) (ket ranges stay full), exactly the per-task loops of
+ * mult.h:453-610, which index the bra block relative to its start as an MPI
+ * rank's block would be. The helpers are built once; mult runs `reps` times
+ * and seconds[r] receives the duration of run r. *pairs receives the number
+ * of off-diagonal det-pairs one run evaluates. Returns the mean seconds. */
+double ref_sigma_sample_range(int L, int nelec, double I0, const double* h, const double* eri,
                               int bit_length, const uint64_t* astr, size_t na, const uint64_t* bstr,
-                              size_t nb, const double* C, double* S, size_t rows, int threads,
+                              size_t nb, const double* C, double* S, size_t row0, size_t rows, int threads,
                               int reps, double* seconds, double* pairs) {
   if (threads > 0) omp_set_num_threads(threads);
   Ham H = setup(L, nelec, I0, h, eri);
   size_t bl = (size_t)bit_length;
   Dets a = to_words(astr, na, L, bl), b = to_words(bstr, nb, L, bl);
-  if (rows > na) rows = na;
+  if (row0 >= na) row0 = na - 1;
+  if (rows > na - row0) rows = na - row0;
   std::vector<sbd::TaskHelpers> helper(3);
   const size_t types[3] = {2, 1, 0};
   std::vector<std::vector<size_t>> shm(3);
   for (int t = 0; t < 3; ++t) {
     sbd::TaskHelpers& hp = helper[t];
-    hp.braAlphaStart = 0; hp.braAlphaEnd = rows; hp.ketAlphaStart = 0; hp.ketAlphaEnd = na;
+    hp.braAlphaStart = row0; hp.braAlphaEnd = row0 + rows; hp.ketAlphaStart = 0; hp.ketAlphaEnd = na;
     hp.braBetaStart = 0; hp.braBetaEnd = nb; hp.ketBetaStart = 0; hp.ketBetaEnd = nb;
     hp.taskType = types[t]; hp.adetShift = 0; hp.bdetShift = 0;
     sbd::GenerateExcitation(a, b, bl, (size_t)L, hp);
@@ -227,6 +229,14 @@ double ref_sigma_sample_multi(int L, int nelec, double I0, const double* h, cons
   if (S) std::memcpy(S, Wb.data(), sizeof(double) * rows * nb);
   sbd::FreeHelpers(helper);
   return reps > 0 ? total / reps : 0.0;
+}
+
+double ref_sigma_sample_multi(int L, int nelec, double I0, const double* h, const double* eri,
+                              int bit_length, const uint64_t* astr, size_t na, const uint64_t* bstr,
+                              size_t nb, const double* C, double* S, size_t rows, int threads,
+                              int reps, double* seconds, double* pairs) {
+  return ref_sigma_sample_range(L, nelec, I0, h, eri, bit_length, astr, na, bstr, nb, C, S, 0, rows, threads,
+                                reps, seconds, pairs);
 }
 
 double ref_sigma_sample(int L, int nelec, double I0, const double* h, const double* eri,
