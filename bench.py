@@ -220,6 +220,24 @@ def traffic_per_launch(kernel: str, workload: str):
     return None
 
 
+def max_over_ranks(x: float, pg=None, device: str = "cuda") -> float:
+    """Maximum of x over all ranks of the process group (x itself at N=1)."""
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(pairs_per_step: float, ms_local: float, world: int, pg=None, device: str = "cuda"):
+    """Whole-job det-pairs/s of N independent replicas: every rank evaluates
+    pairs_per_step per step; the job's step time is the slowest rank's."""
+    ms = max_over_ranks(ms_local, pg, device)
+    return ms, world * pairs_per_step / (ms * 1e-3)
+
+
 def workload_desc(name: str) -> str:
     from sbdx import synth
 
@@ -359,12 +377,8 @@ def run_ours(args, rank, world, local):
             pg.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x: float) -> float:
-        if pg is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    def max_over_ranks_(x: float) -> float:
+        return max_over_ranks(x, pg)
 
     # ---- device-resident FP64 sigma (value) --------------------------------------
     for _ in range(args.warmup):
@@ -381,8 +395,7 @@ def run_ours(args, rank, world, local):
     barrier()
     clocks = sampler.stop()
     launches = ctx.launches - launches0
-    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-    value = world * dp["total"] / (ms * 1e-3)
+    ms, value = replica_throughput(dp["total"], e0.elapsed_time(e1) / args.steps, world, pg)
 
     # ---- per-phase durations (events between the sigma's kernels) ---------------
     ctx.set_profiling(True)
@@ -404,7 +417,7 @@ def run_ours(args, rank, world, local):
         ctx.sigma_device(sbdx.SBDX_FP32, C32.data_ptr(), S32.data_ptr())
     e1.record(stream)
     barrier()
-    ms32 = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    ms32 = max_over_ranks_(e0.elapsed_time(e1) / args.steps)
     ctx.set_profiling(True)
     for _ in range(nprof):
         ctx.sigma_device(sbdx.SBDX_FP32, C32.data_ptr(), S32.data_ptr())
@@ -426,7 +439,7 @@ def run_ours(args, rank, world, local):
     e1.record(stream)
     barrier()
     wall_e2e = (time.perf_counter() - t0) / n_e2e
-    ms_e2e = max_over_ranks(max(e0.elapsed_time(e1) / n_e2e, 1e3 * wall_e2e))
+    ms_e2e = max_over_ranks_(max(e0.elapsed_time(e1) / n_e2e, 1e3 * wall_e2e))
     e2e_value = world * dp["total"] / (ms_e2e * 1e-3)
     del hC, hS
 
