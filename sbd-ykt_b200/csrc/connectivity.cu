@@ -185,7 +185,8 @@ void free_conn(Conn& c) {
   cudaFree(c.srec); cudaFree(c.order); cudaFree(c.spos);
   cudaFree(c.sell); cudaFree(c.soff); cudaFree(c.slen);
   auto free_panel = [](SellPanel& p) {
-    cudaFree(p.sell); cudaFree(p.sell32); cudaFree(p.soff); cudaFree(p.slen); cudaFree(p.vrow);
+    cudaFree(p.sell); cudaFree(p.sell32); cudaFree(p.soff4); cudaFree(p.slen4);
+    cudaFree(p.soff); cudaFree(p.slen); cudaFree(p.vrow);
     cudaFree(p.split_row); cudaFree(p.split_slot);
   };
   free_panel(c.bal);
@@ -368,14 +369,31 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
   P.cap = (int)cap;
   P.slices_per_warp = ks;
   if (split_row.empty()) split_row.push_back(0);
-  std::vector<uint32_t> sell32(sell.size());
-  for (size_t q = 0; q < sell.size(); ++q) {
-    const uint64_t r = sell[q];
-    sell32[q] = (uint32_t)(r & 0xffffu) | (uint32_t)(((r >> 16) & 0xfffu) << 16) |
-                (uint32_t)(((r >> 40) & 1u) << 28) | (uint32_t)(((r >> 41) & 1u) << 29);
+  // 32-bit records in blocks of 4 per lane (see SellPanel::sell32)
+  std::vector<uint64_t> soff4(ns + 1, 0);
+  std::vector<uint32_t> slen4(ns ? ns : 1, 0);
+  for (size_t sl = 0; sl < ns; ++sl) {
+    slen4[sl] = (slen[sl] + 3u) & ~3u;
+    soff4[sl + 1] = soff4[sl] + 32ull * slen4[sl];
   }
+  const uint32_t kPad32 = (1u << 29) | jb0;
+  std::vector<uint32_t> sell32(soff4[ns] ? soff4[ns] : 4, kPad32);
+  for (size_t sl = 0; sl < ns; ++sl)
+    for (uint32_t m = 0; m < slen[sl]; ++m)
+      for (size_t l = 0; l < 32; ++l) {
+        const uint64_t r = sell[soff[sl] + 32ull * m + l];
+        sell32[soff4[sl] + 128ull * (m >> 2) + 4 * l + (m & 3u)] =
+            (uint32_t)(r & 0xffffu) | (uint32_t)(((r >> 16) & 0xfffu) << 16) | (uint32_t)(((r >> 40) & 1u) << 28) |
+            (uint32_t)(((r >> 41) & 1u) << 29);
+      }
   SBDX_CUDA(c, cudaMalloc(&P.sell32, sizeof(uint32_t) * sell32.size()));
+  SBDX_CUDA(c, cudaMalloc(&P.soff4, sizeof(uint64_t) * (ns + 1)));
+  SBDX_CUDA(c, cudaMalloc(&P.slen4, sizeof(uint32_t) * slen4.size()));
   SBDX_CUDA(c, cudaMemcpyAsync(P.sell32, sell32.data(), sizeof(uint32_t) * sell32.size(), cudaMemcpyHostToDevice,
+                               c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(P.soff4, soff4.data(), sizeof(uint64_t) * (ns + 1), cudaMemcpyHostToDevice,
+                               c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(P.slen4, slen4.data(), sizeof(uint32_t) * slen4.size(), cudaMemcpyHostToDevice,
                                c->stream));
   SBDX_CUDA(c, cudaMalloc(&P.sell, sizeof(uint64_t) * sell.size()));
   SBDX_CUDA(c, cudaMalloc(&P.soff, sizeof(uint64_t) * (ns + 1)));

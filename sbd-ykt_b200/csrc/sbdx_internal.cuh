@@ -46,8 +46,12 @@ constexpr uint32_t kInfoSingle = 1u << 30;
 struct SellPanel {
   uint64_t* sell = nullptr;        // [soff[nslice]]
   // the same records in 32 bits (bits 0-15 ket, 16-27 pair index, 28 sign,
-  // 29 padding), read by the packed alpha-beta kernel
-  uint32_t* sell32 = nullptr;      // [soff[nslice]]
+  // 29 padding), read by the packed alpha-beta kernel in blocks of 4 per lane:
+  // record m of lane l of slice s at sell32[soff4[s] + 128*(m/4) + 4*l + m%4],
+  // slen4[s] = slen[s] rounded up to a multiple of 4 (padding records)
+  uint32_t* sell32 = nullptr;      // [soff4[nslice]]
+  uint64_t* soff4 = nullptr;       // [nslice + 1]
+  uint32_t* slen4 = nullptr;       // [nslice]
   uint64_t* soff = nullptr;        // [nslice + 1]
   uint32_t* slen = nullptr;        // [nslice]
   uint32_t* vrow = nullptr;        // [nv]

@@ -1399,7 +1399,7 @@ __global__ void __launch_bounds__(kAb6Threads, 1)
 sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restrict__ a_off,
                    const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
                    const uint32_t* __restrict__ a_info, const uint32_t* __restrict__ sell,
-                   const uint64_t* __restrict__ soff, const uint32_t* __restrict__ slen, size_t nslice,
+                   const uint64_t* __restrict__ soff4, const uint32_t* __restrict__ slen4, size_t nslice,
                    const uint32_t* __restrict__ vrow, size_t nv, const uint32_t* __restrict__ split_row,
                    const uint32_t* __restrict__ split_slot, int nsplit, const T* __restrict__ Vt, size_t vstride,
                    int npair, uint32_t jb0, size_t nbp, double* __restrict__ Y) {
@@ -1456,21 +1456,25 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
     for (int k = 0; k < KS; ++k) {
       const size_t sl = slice_of(k);
       if (sl >= nslice) continue;
-      const uint32_t len = slen[sl];
-      const uint32_t* rp = sell + soff[sl] + lane;
+      // 32-bit records (bits 0-15 ket, 16-27 pair, 28 sign, 29 pad), four per
+      // lane per 16-byte load, the next block in flight
+      const uint32_t nblk = slen4[sl] >> 2;
+      const uint4* rp = reinterpret_cast<const uint4*>(sell + soff4[sl]) + lane;
       double s = acc[k];
-      // records two ahead in flight (32-bit: bits 0-15 ket, 16-27 pair, 28 sign, 29 pad)
-      uint32_t r0 = len > 0 ? __ldg(rp) : 0u;
-      uint32_t r1 = len > 1 ? __ldg(rp + 32) : 0u;
-      for (uint32_t m = 0; m < len; ++m) {
-        const uint32_t rec = r0;
-        r0 = r1;
-        if (m + 2 < len) r1 = __ldg(rp + 32ull * (m + 2));
-        const P x = xs[(rec & 0xffffu) - jb0];  // pad records: ket = jb0
-        const P ev = er[(rec >> 16) & 0xfffu];
-        double d = RP::dot(ev, x);
-        d = ((rec >> 29) & 1u) ? 0.0 : d;
-        s += flip_sign(d, (rec >> 28) & 1u);
+      uint4 cur = nblk ? __ldg(rp) : make_uint4(0u, 0u, 0u, 0u);
+      for (uint32_t bk = 0; bk < nblk; ++bk) {
+        const uint4 nxt = bk + 1 < nblk ? __ldg(rp + 32ull * (bk + 1)) : cur;
+        const uint32_t recs[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint32_t rec = recs[q];
+          const P x = xs[(rec & 0xffffu) - jb0];  // pad records: ket = jb0
+          const P ev = er[(rec >> 16) & 0xfffu];
+          double d = RP::dot(ev, x);
+          d = ((rec >> 29) & 1u) ? 0.0 : d;
+          s += flip_sign(d, (rec >> 28) & 1u);
+        }
+        cur = nxt;
       }
       acc[k] = s;
     }
@@ -1532,7 +1536,7 @@ int launch_ab_v7(Ctx* c, const T* Xp, const SellPanel& bp) {
   dim3 grid((unsigned)c->na, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
   if (grid.y == 0) grid.y = 1;
   sigma_ab_v7_kernel<T, KS><<<grid, kAb6Threads, smem, c->stream>>>(
-      Xp, c->nb, ca.off, ca.nsing, ca.ket, ca.info, bp.sell32, bp.soff, bp.slen, bp.nslice, bp.vrow, bp.nv,
+      Xp, c->nb, ca.off, ca.nsing, ca.ket, ca.info, bp.sell32, bp.soff4, bp.slen4, bp.nslice, bp.vrow, bp.nv,
       bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, (int)c->npair, bp.jb0, (size_t)(bp.jb1 - bp.jb0), c->d_y);
   SBDX_LAUNCHED(c);
   return 0;
