@@ -191,7 +191,55 @@ void free_conn(Conn& c) {
   };
   free_panel(c.bal);
   for (auto& p : c.panels) free_panel(p);
+  cudaFree(c.ab_item); cudaFree(c.ab_split); cudaFree(c.ypart);
   c = Conn{};
+}
+
+// Work items of the packed alpha-beta kernel (see Conn::ab_item). A CTA
+// handles one item and the kernel lasts about as long as the busiest SM, so
+// a few strings with many singles (near-Aufbau strings of a small sample
+// connect to ten times the mean) would set its duration: strings are split
+// into items of at most cap singles, cap = a quarter of the mean work per SM
+// (rounded up to a multiple of 4, at least 8), and items run longest first.
+// Large samples have many strings per SM and split nothing.
+int build_ab_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, size_t nb) {
+  const size_t n = hs.size();
+  int nsm = 148;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || nsm < 1) nsm = 148;
+  uint64_t total = 0;
+  for (uint32_t h : hs) total += h;
+  const uint64_t quarter = (total + 4ull * nsm - 1) / (4ull * nsm);
+  const uint32_t cap = (uint32_t)std::max<uint64_t>(8, (quarter + 3) & ~3ull);
+  std::vector<uint4> items, split;
+  int slot = 0;
+  for (size_t r = 0; r < n; ++r) {
+    if (hs[r] <= cap) {
+      if (hs[r]) items.push_back(make_uint4((uint32_t)r, 0u, hs[r], 0u));
+      continue;
+    }
+    const uint32_t parts = (hs[r] + cap - 1) / cap;
+    split.push_back(make_uint4((uint32_t)r, (uint32_t)slot, parts, 0u));
+    for (uint32_t q = 0; q < parts; ++q)
+      items.push_back(make_uint4((uint32_t)r, q * cap, std::min(hs[r], (q + 1) * cap), (uint32_t)(slot + q + 1)));
+    slot += (int)parts;
+  }
+  std::stable_sort(items.begin(), items.end(), [](const uint4& x, const uint4& y) { return x.z - x.y > y.z - y.y; });
+  cn.item_cap = (int)cap;
+  cn.n_item = items.size();
+  cn.n_split = (int)split.size();
+  cn.n_part = slot;
+  SBDX_CUDA(c, cudaMalloc(&cn.ab_item, sizeof(uint4) * std::max<size_t>(1, items.size())));
+  SBDX_CUDA(c, cudaMalloc(&cn.ab_split, sizeof(uint4) * std::max<size_t>(1, split.size())));
+  if (!items.empty())
+    SBDX_CUDA(c, cudaMemcpyAsync(cn.ab_item, items.data(), sizeof(uint4) * items.size(), cudaMemcpyHostToDevice,
+                                 c->stream));
+  if (!split.empty()) {
+    SBDX_CUDA(c, cudaMemcpyAsync(cn.ab_split, split.data(), sizeof(uint4) * split.size(), cudaMemcpyHostToDevice,
+                                 c->stream));
+    SBDX_CUDA(c, cudaMalloc(&cn.ypart, sizeof(double) * (size_t)slot * std::max<size_t>(1, nb)));
+  }
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // host vectors die at return
+  return 0;
 }
 
 // Balanced SELL-32 of the single records (see Conn::bsell). The cap starts at
@@ -451,6 +499,10 @@ int build_one(Ctx* c, int spin) {
   for (size_t r = 0; r < n; ++r) order[r] = (uint32_t)r;
   std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return hs[x] > hs[y]; });
   SBDX_CUDA(c, cudaMemcpyAsync(cn.order, order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream));
+  if (spin == 0) {
+    int rc = build_ab_items(c, cn, hs, c->nb);
+    if (rc) return rc;
+  }
   // SELL-32 copy of the single-excitation records in list-length order
   {
     std::vector<uint64_t> rec(cn.total ? cn.total : 1);

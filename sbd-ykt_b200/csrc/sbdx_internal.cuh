@@ -97,6 +97,17 @@ struct Conn {
   // shared memory) split the ket range into slices that it can.
   SellPanel bal;
   std::vector<SellPanel> panels;
+  // work items of the packed alpha-beta kernel (alpha spin only), one CTA
+  // each, longest first: {bra alpha string, first single, one past the last
+  // single, 1 + partial-row slot or 0}. A string with more singles than the
+  // cap is split into items of at most `item_cap` singles (a multiple of 4)
+  // whose partial rows (ypart[slot * nb ..], FP64) are added to the output in
+  // slot order by a fix-up kernel; the others write the output directly.
+  uint4* ab_item = nullptr;    // [n_item]
+  size_t n_item = 0;
+  uint4* ab_split = nullptr;   // [n_split]: {string, first slot, parts, 0}
+  int n_split = 0, n_part = 0, item_cap = 0;
+  double* ypart = nullptr;     // [n_part * nb]
 };
 
 // Largest number of partial-sum slots of split rows (shared memory of the

@@ -1389,20 +1389,23 @@ template <> struct RowPack<float> {
 };
 
 // Alpha single x beta single, v7: as v6 (balanced SELL-32, alpha-first signs,
-// split rows, one CTA per (bra alpha row, chunk)), with the staged rows
-// interleaved into 16-byte packs (2 FP64 or 4 FP32 rows per group): a record
-// costs two 128-bit shared loads (ket pack, integral pack) for all rows of
-// the group, and the alpha sign is applied to the integrals when they are
-// staged, so the per-record sign is the beta one only.
+// split beta rows), with the staged rows interleaved into 16-byte packs (2
+// FP64 or 4 FP32 rows per group): a record costs two 128-bit shared loads (ket
+// pack, integral pack) for all rows of the group, and the alpha sign is
+// applied to the integrals when they are staged, so the per-record sign is
+// the beta one only. One CTA per (alpha work item, chunk of beta slices): an
+// item is a bra alpha string or, for strings with many singles, a range of
+// them whose partial row goes to its own slot (Conn::ab_item).
 template <typename T, int KS>
 __global__ void __launch_bounds__(kAb6Threads, 1)
 sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restrict__ a_off,
-                   const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
+                   const uint32_t* __restrict__ a_ket,
                    const uint32_t* __restrict__ a_info, const uint32_t* __restrict__ sell,
                    const uint64_t* __restrict__ soff4, const uint32_t* __restrict__ slen4, size_t nslice,
                    const uint32_t* __restrict__ vrow, size_t nv, const uint32_t* __restrict__ split_row,
                    const uint32_t* __restrict__ split_slot, int nsplit, const T* __restrict__ Vt, size_t vstride,
-                   int npair, uint32_t jb0, size_t nbp, double* __restrict__ Y) {
+                   int npair, uint32_t jb0, size_t nbp, const uint4* __restrict__ items,
+                   double* __restrict__ ypart, double* __restrict__ Y) {
   using RP = RowPack<T>;
   using P = typename RP::P;
   constexpr int VR = RP::kRows;
@@ -1411,7 +1414,11 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
   P* xs = reinterpret_cast<P*>(smem);   // [nbp]: ket indices jb0 .. jb0 + nbp - 1
   P* er = xs + nbp;                     // [npair]
   double* part = reinterpret_cast<double*>(er + npair);
-  const size_t ia = blockIdx.x;
+  // work item: bra alpha string, range of its singles, output row
+  const uint4 item = items[blockIdx.x];
+  const size_t ia = item.x;
+  const int kend = (int)item.z;
+  double* __restrict__ Yrow = item.w ? ypart + (size_t)(item.w - 1) * nb : Y + ia * nb;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t slice0 = (size_t)blockIdx.y * kWarps * KS;
   auto slice_of = [&](int k) -> size_t {
@@ -1421,9 +1428,8 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
 #pragma unroll
   for (int k = 0; k < KS; ++k) acc[k] = 0.0;
   const uint64_t e0 = a_off[ia];
-  const int ns = (int)a_nsing[ia];
-  for (int k0 = 0; k0 < ns; k0 += VR) {
-    const int nr = min(VR, ns - k0);
+  for (int k0 = (int)item.y; k0 < kend; k0 += VR) {
+    const int nr = min(VR, kend - k0);
     const T* xrow[VR];
     const T* vrow_p[VR];
     bool neg[VR];
@@ -1486,7 +1492,7 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
     if (sl < nslice && pos < nv) {
       const uint32_t w = vrow[pos];
       const uint32_t slot1 = w >> 16;
-      if (slot1 == 0) Y[ia * nb + (w & 0xffffu)] += acc[k];
+      if (slot1 == 0) Yrow[w & 0xffffu] += acc[k];
       else part[slot1 - 1] = acc[k];
     }
   }
@@ -1495,7 +1501,7 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
     for (int s = threadIdx.x; s < nsplit; s += kAb6Threads) {
       double t = 0.0;
       for (uint32_t j = split_slot[s]; j < split_slot[s + 1]; ++j) t += part[j];
-      Y[ia * nb + split_row[s]] += t;
+      Yrow[split_row[s]] += t;
     }
   }
 }
@@ -1533,17 +1539,35 @@ int launch_ab_v7(Ctx* c, const T* Xp, const SellPanel& bp) {
   SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v7_kernel<T, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kAbSmemBudget));
   const size_t per_cta = (size_t)(kAb6Threads / 32) * KS;
-  dim3 grid((unsigned)c->na, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
+  dim3 grid((unsigned)ca.n_item, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
   if (grid.y == 0) grid.y = 1;
   sigma_ab_v7_kernel<T, KS><<<grid, kAb6Threads, smem, c->stream>>>(
-      Xp, c->nb, ca.off, ca.nsing, ca.ket, ca.info, bp.sell32, bp.soff4, bp.slen4, bp.nslice, bp.vrow, bp.nv,
-      bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, (int)c->npair, bp.jb0, (size_t)(bp.jb1 - bp.jb0), c->d_y);
+      Xp, c->nb, ca.off, ca.ket, ca.info, bp.sell32, bp.soff4, bp.slen4, bp.nslice, bp.vrow, bp.nv,
+      bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, (int)c->npair, bp.jb0, (size_t)(bp.jb1 - bp.jb0),
+      ca.ab_item, ca.ypart, c->d_y);
   SBDX_LAUNCHED(c);
   return 0;
 }
 
+// Adds the partial rows of the alpha strings split over several work items to
+// the output, parts in slot order (one fixed summation order).
+__global__ void ab_split_fixup_kernel(const uint4* __restrict__ split, const double* __restrict__ ypart, size_t nb,
+                                      double* __restrict__ Y) {
+  const uint4 sp = split[blockIdx.y];
+  const double* part = ypart + (size_t)sp.y * nb;
+  for (size_t ib = (size_t)blockIdx.x * blockDim.x + threadIdx.x; ib < nb; ib += (size_t)gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (uint32_t q = 0; q < sp.z; ++q) t += part[(size_t)q * nb + ib];
+    Y[(size_t)sp.x * nb + ib] += t;
+  }
+}
+
 template <typename T>
 int run_ab_v7(Ctx* c, const T* Xp) {
+  const Conn& ca = c->conn[0];
+  if (ca.n_item == 0) return 0;  // no alpha string has a single excitation
+  if (ca.n_part > 0)
+    SBDX_CUDA(c, cudaMemsetAsync(ca.ypart, 0, sizeof(double) * (size_t)ca.n_part * c->nb, c->stream));
   std::vector<SellPanel> one;
   for (const SellPanel& bp : *ab7_panels(c, one)) {
     int rc;
@@ -1551,6 +1575,12 @@ int run_ab_v7(Ctx* c, const T* Xp) {
     else if (bp.slices_per_warp >= 12) rc = launch_ab_v7<T, 12>(c, Xp, bp);
     else rc = launch_ab_v7<T, 8>(c, Xp, bp);
     if (rc) return rc;
+  }
+  if (ca.n_split > 0) {
+    const unsigned bx = (unsigned)std::min<size_t>((c->nb + 255) / 256, 64);
+    ab_split_fixup_kernel<<<dim3(bx, (unsigned)ca.n_split), 256, 0, c->stream>>>(ca.ab_split, ca.ypart, c->nb,
+                                                                                  c->d_y);
+    SBDX_LAUNCHED(c);
   }
   return 0;
 }
