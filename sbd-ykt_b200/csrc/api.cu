@@ -17,6 +17,35 @@ bool set_cuda_err(Ctx* c, cudaError_t e, const char* what) {
   return false;
 }
 
+cudaError_t make_pool(int device, cudaMemPool_t* pool) {
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaError_t e = cudaMemPoolCreate(pool, &props);
+  if (e != cudaSuccess) {
+    *pool = nullptr;
+    return e;
+  }
+  uint64_t keep = UINT64_MAX;
+  return cudaMemPoolSetAttribute(*pool, cudaMemPoolAttrReleaseThreshold, &keep);
+}
+
+cudaError_t pool_alloc(Ctx* c, void** p, size_t bytes) {
+  if (!c->pool) {
+    const cudaError_t e = make_pool(c->device, &c->pool);
+    if (e != cudaSuccess) return e;
+    c->own_pool = true;
+  }
+  return cudaMallocFromPoolAsync(p, bytes, c->pool, c->stream);
+}
+
+void pool_trim(Ctx* c) {
+  if (!c->pool || !c->own_pool) return;
+  cudaStreamSynchronize(c->stream);
+  cudaMemPoolTrimTo(c->pool, 0);
+}
+
 int check_device_error(Ctx* c) {
   int h = 0;
   SBDX_CUDA(c, cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -129,6 +158,7 @@ int sbdx_ctx_destroy(sbdx_ctx* ctx) {
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  if (c->own_pool && c->pool) cudaMemPoolDestroy(c->pool);
   delete ctx;
   return SBDX_OK;
 }
@@ -396,8 +426,12 @@ int sbdx_davidson_roots(sbdx_ctx* ctx, const sbdx_davidson_params* params, int n
       for (size_t q = 0; q < D * nroots; ++q)
         if (!std::isfinite(W[q])) { c->err = "davidson_roots: non-finite start vector"; return SBDX_ERR_NUMERIC; }
     double* dW = nullptr;
-    SBDX_CUDA(c, cudaMallocAsync(&dW, sizeof(double) * D * nroots, c->stream));
-    struct Guard { double* p; cudaStream_t st; ~Guard() { cudaFreeAsync(p, st); } } g{dW, c->stream};
+    SBDX_CUDA(c, sbdx::pool_alloc(c, (void**)&dW, sizeof(double) * D * nroots));
+    struct Guard {
+      Ctx* c;
+      double* p;
+      ~Guard() { cudaFreeAsync(p, c->stream); sbdx::pool_trim(c); }
+    } g{c, dW};
     if (init_from_W) {
       SBDX_CUDA(c, cudaMemcpyAsync(dW, W, sizeof(double) * D * nroots, cudaMemcpyHostToDevice, c->stream));
     } else {  // unit vectors on the nroots lowest diagonal elements

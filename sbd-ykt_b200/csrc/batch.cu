@@ -14,8 +14,9 @@
 //     output) buffer pair into a CUDA graph and replayed, so a step of a small
 //     subspace costs one graph launch instead of five kernel launches;
 //   - a pool of host threads drives the Davidson solves, largest subspace
-//     first; the solver allocates stream-ordered (cudaMallocAsync), so no
-//     solve stalls the others with a device-wide synchronisation;
+//     first; the solvers allocate stream-ordered from one memory pool of the
+//     batch that keeps its memory until the batch is done, so no solve stalls
+//     the others with a device-wide synchronisation or a remapping;
 //   - the launch shapes of the sigma kernels are tuned once on the largest
 //     subspace and applied to all.
 #include "sbdx.h"
@@ -32,6 +33,7 @@
 
 struct sbdx_batch {
   int device = 0;
+  cudaMemPool_t pool = nullptr;  // shared by the subspaces' contexts
   std::string err;
   int L = 0;
   double I0 = 0.0;
@@ -52,7 +54,7 @@ int fail(sbdx_batch* b, int code, const std::string& msg) {
 }
 
 void release_vectors(sbdx_batch::Sub& s) {
-  if (s.dW) cudaFree(s.dW);
+  if (s.dW) cudaFreeAsync(s.dW, s.ctx->c.stream);
   s.dW = nullptr;
   s.nroots = 0;
 }
@@ -71,6 +73,11 @@ int sbdx_batch_create(sbdx_batch** out, int device, int norb, double I0, const d
   sbdx_batch* b = new (std::nothrow) sbdx_batch();
   if (!b) return SBDX_ERR_NOMEM;
   b->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || sbdx::make_pool(device, &b->pool) != cudaSuccess) {
+    if (b->pool) cudaMemPoolDestroy(b->pool);
+    delete b;
+    return SBDX_ERR_CUDA;
+  }
   b->L = norb;
   b->I0 = I0;
   b->h.assign(h, h + (size_t)norb * norb);
@@ -86,6 +93,7 @@ int sbdx_batch_destroy(sbdx_batch* b) {
     release_vectors(s);
     sbdx_ctx_destroy(s.ctx);
   }
+  if (b->pool) cudaMemPoolDestroy(b->pool);
   delete b;
   return SBDX_OK;
 }
@@ -105,6 +113,8 @@ int sbdx_batch_add(sbdx_batch* b, const uint64_t* alpha, size_t na, const uint64
       sbdx_ctx_destroy(ctx);
       return code;
     };
+    ctx->c.pool = b->pool;  // not owned: the batch destroys it
+    ctx->c.own_pool = false;
     if ((rc = sbdx_set_integrals(ctx, b->L, b->I0, b->h.data(), b->eri.data(), b->eri.size()))) return drop(rc);
     if ((rc = sbdx_set_strings(ctx, alpha, na, beta, nb))) return drop(rc);
     sbdx::Ctx* c = &ctx->c;
@@ -187,7 +197,7 @@ int sbdx_batch_solve(sbdx_batch* b, const sbdx_davidson_params* params, int nroo
       std::string err;
       try {
         double* dW = nullptr;
-        if (cudaMalloc(&dW, sizeof(double) * D * nroots) != cudaSuccess) {
+        if (sbdx::pool_alloc(c, (void**)&dW, sizeof(double) * D * nroots) != cudaSuccess) {
           rc = SBDX_ERR_NOMEM;
           err = "cudaMalloc(start vectors)";
         } else {
@@ -233,6 +243,7 @@ int sbdx_batch_solve(sbdx_batch* b, const sbdx_davidson_params* params, int nroo
   for (auto& th : pool) th.join();
   cudaDeviceSynchronize();
   if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  cudaMemPoolTrimTo(b->pool, 0);  // keeps only the returned Ritz vectors
   if (first_rc) return fail(b, first_rc, first_err);
   return SBDX_OK;
 }

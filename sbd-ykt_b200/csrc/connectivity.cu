@@ -192,7 +192,74 @@ void free_conn(Conn& c) {
   free_panel(c.bal);
   for (auto& p : c.panels) free_panel(p);
   cudaFree(c.ab_item); cudaFree(c.ab_split); cudaFree(c.ypart);
+  cudaFree(c.same_item); cudaFree(c.same_split); cudaFree(c.same_ypart);
   c = Conn{};
+}
+
+// Splits rows of `len` work units longer than cap into items (see
+// Conn::ab_item): {row, first unit, one past the last, 1 + slot or 0},
+// longest first; split rows as {row, first slot, parts, 0}. Empty rows get an
+// item only with keep_empty (a kernel that assigns its output row).
+void split_rows(const std::vector<uint32_t>& len, uint32_t cap, bool keep_empty, std::vector<uint4>& items,
+                std::vector<uint4>& split, int& nslot) {
+  items.clear();
+  split.clear();
+  nslot = 0;
+  for (size_t r = 0; r < len.size(); ++r) {
+    if (len[r] <= cap) {
+      if (len[r] || keep_empty) items.push_back(make_uint4((uint32_t)r, 0u, len[r], 0u));
+      continue;
+    }
+    const uint32_t parts = (len[r] + cap - 1) / cap;
+    split.push_back(make_uint4((uint32_t)r, (uint32_t)nslot, parts, 0u));
+    for (uint32_t q = 0; q < parts; ++q)
+      items.push_back(make_uint4((uint32_t)r, q * cap, std::min(len[r], (q + 1) * cap), (uint32_t)(nslot + q + 1)));
+    nslot += (int)parts;
+  }
+  std::stable_sort(items.begin(), items.end(), [](const uint4& x, const uint4& y) { return x.z - x.y > y.z - y.y; });
+}
+
+int upload_items(Ctx* c, const std::vector<uint4>& items, const std::vector<uint4>& split, int nslot, size_t ncol,
+                 uint4** d_items, uint4** d_split, double** d_part) {
+  SBDX_CUDA(c, cudaMalloc(d_items, sizeof(uint4) * std::max<size_t>(1, items.size())));
+  SBDX_CUDA(c, cudaMalloc(d_split, sizeof(uint4) * std::max<size_t>(1, split.size())));
+  if (!items.empty())
+    SBDX_CUDA(c, cudaMemcpyAsync(*d_items, items.data(), sizeof(uint4) * items.size(), cudaMemcpyHostToDevice,
+                                 c->stream));
+  if (!split.empty()) {
+    SBDX_CUDA(c, cudaMemcpyAsync(*d_split, split.data(), sizeof(uint4) * split.size(), cudaMemcpyHostToDevice,
+                                 c->stream));
+    SBDX_CUDA(c, cudaMalloc(d_part, sizeof(double) * (size_t)nslot * std::max<size_t>(1, ncol)));
+  }
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // host vectors die at return
+  return 0;
+}
+
+int sm_count(Ctx* c) {
+  int nsm = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || nsm < 1) nsm = 148;
+  return nsm;
+}
+
+// Same-spin work items (see Conn::same_item). A CTA handles one item and one
+// strip of 1024 columns (4 per thread); an item longer than the mean work of
+// a CTA slot (8 resident CTAs per SM) would set the kernel's duration, so
+// rows with more entries are split (at least 64 entries per item).
+int build_same_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const std::vector<uint32_t>& hd, size_t ncol) {
+  std::vector<uint32_t> len(hs.size());
+  uint64_t total = 0;
+  for (size_t r = 0; r < hs.size(); ++r) total += (len[r] = hs[r] + hd[r]);
+  const uint64_t strips = std::max<uint64_t>(1, (ncol + 1023) / 1024);
+  const uint64_t slots = 8ull * sm_count(c);
+  const uint32_t cap = (uint32_t)std::max<uint64_t>(64, (total * strips + slots - 1) / slots);
+  std::vector<uint4> items, split;
+  int nslot = 0;
+  split_rows(len, cap, true, items, split, nslot);  // every row's output is assigned
+  cn.same_cap = (int)cap;
+  cn.n_same_item = items.size();
+  cn.n_same_split = (int)split.size();
+  cn.n_same_part = nslot;
+  return upload_items(c, items, split, nslot, ncol, &cn.same_item, &cn.same_split, &cn.same_ypart);
 }
 
 // Work items of the packed alpha-beta kernel (see Conn::ab_item). A CTA
@@ -203,43 +270,19 @@ void free_conn(Conn& c) {
 // (rounded up to a multiple of 4, at least 8), and items run longest first.
 // Large samples have many strings per SM and split nothing.
 int build_ab_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, size_t nb) {
-  const size_t n = hs.size();
-  int nsm = 148;
-  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || nsm < 1) nsm = 148;
+  const uint64_t nsm = (uint64_t)sm_count(c);
   uint64_t total = 0;
   for (uint32_t h : hs) total += h;
-  const uint64_t quarter = (total + 4ull * nsm - 1) / (4ull * nsm);
+  const uint64_t quarter = (total + 4 * nsm - 1) / (4 * nsm);
   const uint32_t cap = (uint32_t)std::max<uint64_t>(8, (quarter + 3) & ~3ull);
   std::vector<uint4> items, split;
   int slot = 0;
-  for (size_t r = 0; r < n; ++r) {
-    if (hs[r] <= cap) {
-      if (hs[r]) items.push_back(make_uint4((uint32_t)r, 0u, hs[r], 0u));
-      continue;
-    }
-    const uint32_t parts = (hs[r] + cap - 1) / cap;
-    split.push_back(make_uint4((uint32_t)r, (uint32_t)slot, parts, 0u));
-    for (uint32_t q = 0; q < parts; ++q)
-      items.push_back(make_uint4((uint32_t)r, q * cap, std::min(hs[r], (q + 1) * cap), (uint32_t)(slot + q + 1)));
-    slot += (int)parts;
-  }
-  std::stable_sort(items.begin(), items.end(), [](const uint4& x, const uint4& y) { return x.z - x.y > y.z - y.y; });
+  split_rows(hs, cap, false, items, split, slot);  // the kernel adds to its output
   cn.item_cap = (int)cap;
   cn.n_item = items.size();
   cn.n_split = (int)split.size();
   cn.n_part = slot;
-  SBDX_CUDA(c, cudaMalloc(&cn.ab_item, sizeof(uint4) * std::max<size_t>(1, items.size())));
-  SBDX_CUDA(c, cudaMalloc(&cn.ab_split, sizeof(uint4) * std::max<size_t>(1, split.size())));
-  if (!items.empty())
-    SBDX_CUDA(c, cudaMemcpyAsync(cn.ab_item, items.data(), sizeof(uint4) * items.size(), cudaMemcpyHostToDevice,
-                                 c->stream));
-  if (!split.empty()) {
-    SBDX_CUDA(c, cudaMemcpyAsync(cn.ab_split, split.data(), sizeof(uint4) * split.size(), cudaMemcpyHostToDevice,
-                                 c->stream));
-    SBDX_CUDA(c, cudaMalloc(&cn.ypart, sizeof(double) * (size_t)slot * std::max<size_t>(1, nb)));
-  }
-  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // host vectors die at return
-  return 0;
+  return upload_items(c, items, split, slot, nb, &cn.ab_item, &cn.ab_split, &cn.ypart);
 }
 
 // Balanced SELL-32 of the single records (see Conn::bsell). The cap starts at
@@ -499,9 +542,10 @@ int build_one(Ctx* c, int spin) {
   for (size_t r = 0; r < n; ++r) order[r] = (uint32_t)r;
   std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return hs[x] > hs[y]; });
   SBDX_CUDA(c, cudaMemcpyAsync(cn.order, order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream));
-  if (spin == 0) {
-    int rc = build_ab_items(c, cn, hs, c->nb);
+  {
+    int rc = build_same_items(c, cn, hs, hd, spin == 0 ? c->nb : c->na);
     if (rc) return rc;
+    if (spin == 0 && (rc = build_ab_items(c, cn, hs, c->nb))) return rc;
   }
   // SELL-32 copy of the single-excitation records in list-length order
   {

@@ -1221,12 +1221,15 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
   // stream-ordered allocations: several solves can run concurrently on their
   // own streams without a device-wide synchronisation at allocation or release
   struct AsyncGuard {
-    cudaStream_t st;
+    Ctx* c;
     std::vector<void*> p;
-    ~AsyncGuard() { for (void* q : p) cudaFreeAsync(q, st); }
-  } g{c->stream, {}};
+    ~AsyncGuard() {
+      for (void* q : p) cudaFreeAsync(q, c->stream);
+      pool_trim(c);
+    }
+  } g{c, {}};
   auto alloc = [&](void** ptr, size_t bytes) -> cudaError_t {
-    const cudaError_t e = cudaMallocAsync(ptr, bytes, c->stream);
+    const cudaError_t e = pool_alloc(c, ptr, bytes);
     if (e == cudaSuccess) g.p.push_back(*ptr);
     return e;
   };
@@ -1556,9 +1559,9 @@ int lowest_diagonal(Ctx* c, int k, std::vector<size_t>& idx) {
   const size_t D = c->na * c->nb;
   double* bv = nullptr;
   unsigned long long *bi = nullptr, *sk = nullptr;
-  SBDX_CUDA(c, cudaMallocAsync(&bv, sizeof(double) * kRedBlocks, c->stream));
-  SBDX_CUDA(c, cudaMallocAsync(&bi, sizeof(unsigned long long) * kRedBlocks, c->stream));
-  SBDX_CUDA(c, cudaMallocAsync(&sk, sizeof(unsigned long long) * kMaxRoots, c->stream));
+  SBDX_CUDA(c, pool_alloc(c, (void**)&bv, sizeof(double) * kRedBlocks));
+  SBDX_CUDA(c, pool_alloc(c, (void**)&bi, sizeof(unsigned long long) * kRedBlocks));
+  SBDX_CUDA(c, pool_alloc(c, (void**)&sk, sizeof(unsigned long long) * kMaxRoots));
   struct Guard {
     cudaStream_t st;
     void *a, *b, *c;

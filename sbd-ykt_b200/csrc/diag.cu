@@ -84,9 +84,9 @@ int diag_terms(Ctx* c) {
   const size_t na = c->na, nb = c->nb, D = na * nb;
   if (!c->d_hii) SBDX_CUDA(c, cudaMalloc(&c->d_hii, sizeof(double) * D));
   double *Ea = nullptr, *Eb = nullptr, *Jb = nullptr;
-  SBDX_CUDA(c, cudaMallocAsync(&Ea, sizeof(double) * na, c->stream));
-  SBDX_CUDA(c, cudaMallocAsync(&Eb, sizeof(double) * nb, c->stream));
-  SBDX_CUDA(c, cudaMallocAsync(&Jb, sizeof(double) * nb * c->L, c->stream));
+  SBDX_CUDA(c, pool_alloc(c, (void**)&Ea, sizeof(double) * na));
+  SBDX_CUDA(c, pool_alloc(c, (void**)&Eb, sizeof(double) * nb));
+  SBDX_CUDA(c, pool_alloc(c, (void**)&Jb, sizeof(double) * nb * c->L));
   string_energy_kernel<<<(unsigned)((na + 127) / 128), 128, 0, c->stream>>>(c->d_a, na, c->L, c->d_h, c->d_eri, Ea);
   SBDX_LAUNCHED(c);
   string_energy_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, c->stream>>>(c->d_b, nb, c->L, c->d_h, c->d_eri, Eb);
@@ -112,7 +112,7 @@ int diag_terms(Ctx* c) {
 // diag_terms() for callers that must not have a library call cudaMalloc or
 // cudaFree, for instance code whose device memory all comes from its own
 // pre-sized pool. The per-string energies and the beta Coulomb rows that
-// diag_terms() puts in cudaMallocAsync scratch live instead in the file-scope
+// diag_terms() puts in stream-ordered pool scratch live instead in the file-scope
 // array below, which every GPU that loads the library holds until exit.
 
 namespace sbdx {

@@ -108,6 +108,16 @@ struct Conn {
   uint4* ab_split = nullptr;   // [n_split]: {string, first slot, parts, 0}
   int n_split = 0, n_part = 0, item_cap = 0;
   double* ypart = nullptr;     // [n_part * nb]
+  // work items of the alpha-first same-spin kernel (either spin), the same
+  // scheme over the row's entries (singles then doubles): {bra string, first
+  // entry, one past the last entry, 1 + partial-row slot or 0}. Partial rows
+  // are [n_same_part * ncol] (ncol = the other spin's string count); every
+  // part writes all its columns, and the fix-up assigns their sum.
+  uint4* same_item = nullptr;
+  size_t n_same_item = 0;
+  uint4* same_split = nullptr;
+  int n_same_split = 0, n_same_part = 0, same_cap = 0;
+  double* same_ypart = nullptr;
 };
 
 // Largest number of partial-sum slots of split rows (shared memory of the
@@ -191,6 +201,12 @@ struct Ctx {
   };
   bool use_graphs = false;
   bool own_stream = false;  // stream created by the library (destroyed with the context)
+  // pool of the solvers' stream-ordered scratch. It keeps its memory between
+  // allocations (no unmap/map of gigabytes per solve, which stalls the other
+  // streams of a batch); a context that owns it trims it after each solve, a
+  // batch shares one pool among its subspaces and trims it after the batch.
+  cudaMemPool_t pool = nullptr;
+  bool own_pool = false;
   std::vector<SigmaGraph> graphs;
   // optional per-phase timing of the sigma (CUDA events on the context stream)
   bool profiling = false;
@@ -300,6 +316,12 @@ int autotune(Ctx* c);
 // Returns 0, or sets c->err and returns SBDX_ERR_CUDA when a kernel recorded a
 // watchdog timeout in the device error word (which is then cleared).
 int check_device_error(Ctx* c);
+// Stream-ordered allocation from the context's pool (created on first use).
+cudaError_t pool_alloc(Ctx* c, void** p, size_t bytes);
+// Returns the free memory of an owned pool to the device (syncs the stream).
+void pool_trim(Ctx* c);
+// A pool that keeps its memory, on `device`.
+cudaError_t make_pool(int device, cudaMemPool_t* pool);
 // Several lowest roots on device vectors (dW: k vectors of na*nb), see davidson.cu.
 int davidson_roots(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, double* E, double* res,
                    sbdx_davidson_info& info);

@@ -1093,22 +1093,24 @@ sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __res
                      const uint32_t* __restrict__ nsing, const uint32_t* __restrict__ ket,
                      const typename Prec<T>::V* __restrict__ val, const uint32_t* __restrict__ info,
                      const typename Prec<T>::V* __restrict__ Dt, size_t dstride, const double* __restrict__ hii,
-                     double* __restrict__ Y) {
+                     const uint4* __restrict__ items, double* __restrict__ ypart, double* __restrict__ Y) {
   __shared__ uint32_t s_ket[kSameThreads], s_pq[kSameThreads];
   __shared__ double s_val[kSameThreads];
-  const size_t r = blockIdx.x;
+  const uint4 item = items[blockIdx.x];  // bra string, entry range, output row
+  const size_t r = item.x;
+  double* __restrict__ Yrow = item.w ? ypart + (size_t)(item.w - 1) * ncol : Y + r * ncol;
   const size_t c0 = ((size_t)blockIdx.y * kSameThreads + threadIdx.x) * VEC;
   const bool active = c0 < ncol;
   double acc[VEC];
 #pragma unroll
   for (int v = 0; v < VEC; ++v) acc[v] = 0.0;
-  if (hii != nullptr && active) {
+  if (hii != nullptr && item.y == 0 && active) {
     double x[VEC];
     VecIO<T, VEC>::load(X + r * ncol + c0, x);
 #pragma unroll
     for (int v = 0; v < VEC; ++v) acc[v] = hii[r * ncol + c0 + v] * x[v];
   }
-  const uint64_t beg = off[r], end = off[r + 1], send = beg + nsing[r];
+  const uint64_t beg = off[r] + item.y, end = off[r] + item.z, send = off[r] + nsing[r];
   const unsigned t = threadIdx.x;
   for (uint64_t base = beg; base < end; base += kSameThreads) {
     const int cnt = (int)min((uint64_t)kSameThreads, end - base);
@@ -1144,7 +1146,7 @@ sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __res
   }
   if (active) {
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) Y[r * ncol + c0 + v] = acc[v];
+    for (int v = 0; v < VEC; ++v) Yrow[c0 + v] = acc[v];
   }
 }
 
@@ -1182,22 +1184,25 @@ __global__ void __launch_bounds__(kSameThreads)
 sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, const uint64_t* __restrict__ off,
                       const uint32_t* __restrict__ nsing, const uint32_t* __restrict__ ket,
                       const float* __restrict__ val, const uint32_t* __restrict__ info, const float* __restrict__ Dt,
-                      size_t dstride, const double* __restrict__ hii, double* __restrict__ Y) {
+                      size_t dstride, const double* __restrict__ hii, const uint4* __restrict__ items,
+                      double* __restrict__ ypart, double* __restrict__ Y) {
   __shared__ uint32_t s_ket[kSameThreads], s_pq[kSameThreads];
   __shared__ float s_val[kSameThreads];
-  const size_t r = blockIdx.x;
+  const uint4 item = items[blockIdx.x];  // bra string, entry range, output row
+  const size_t r = item.x;
+  double* __restrict__ Yrow = item.w ? ypart + (size_t)(item.w - 1) * ncol : Y + r * ncol;
   const size_t c0 = ((size_t)blockIdx.y * kSameThreads + threadIdx.x) * VEC;
   const bool active = c0 < ncol;
   double acc[VEC];
 #pragma unroll
   for (int v = 0; v < VEC; ++v) acc[v] = 0.0;
-  if (hii != nullptr && active) {
+  if (hii != nullptr && item.y == 0 && active) {
     float x[VEC];
     VecF<VEC>::load(X + r * ncol + c0, x);
 #pragma unroll
     for (int v = 0; v < VEC; ++v) acc[v] = hii[r * ncol + c0 + v] * (double)x[v];
   }
-  const uint64_t beg = off[r], end = off[r + 1], send = beg + nsing[r];
+  const uint64_t beg = off[r] + item.y, end = off[r] + item.z, send = off[r] + nsing[r];
   const unsigned t = threadIdx.x;
   for (uint64_t base = beg; base < end; base += kSameThreads) {
     const int cnt = (int)min((uint64_t)kSameThreads, end - base);
@@ -1249,7 +1254,7 @@ sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, const uint64_t* 
   }
   if (active) {
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) Y[r * ncol + c0 + v] = acc[v];
+    for (int v = 0; v < VEC; ++v) Yrow[c0 + v] = acc[v];
   }
 }
 
@@ -1585,18 +1590,43 @@ int run_ab_v7(Ctx* c, const T* Xp) {
   return 0;
 }
 
+// Assigns the sum of the partial rows of the bra strings split over several
+// same-spin work items, parts in slot order.
+__global__ void same_split_fixup_kernel(const uint4* __restrict__ split, const double* __restrict__ ypart,
+                                        size_t ncol, double* __restrict__ Y) {
+  const uint4 sp = split[blockIdx.y];
+  const double* part = ypart + (size_t)sp.y * ncol;
+  for (size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x; col < ncol; col += (size_t)gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (uint32_t q = 0; q < sp.z; ++q) t += part[(size_t)q * ncol + col];
+    Y[(size_t)sp.x * ncol + col] = t;
+  }
+}
+
 template <typename T, int VEC>
 int launch_same_v6(Ctx* c, const T* X, size_t nrow, size_t ncol, const Conn& cn, const typename Prec<T>::V* val,
                    const typename Prec<T>::V* Dt, size_t dstride, const double* hii, double* Y) {
-  dim3 grid((unsigned)nrow, (unsigned)((ncol + (size_t)kSameThreads * VEC - 1) / ((size_t)kSameThreads * VEC)));
-  if constexpr (std::is_same<T, float>::value) {
-    sigma_same_v6f_kernel<VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, cn.off, cn.nsing, cn.ket, val, cn.info,
-                                                                      Dt, dstride, hii, Y);
-  } else {
-    sigma_same_v6_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, cn.off, cn.nsing, cn.ket, val, cn.info,
-                                                                       Dt, dstride, hii, Y);
+  (void)nrow;
+  if (cn.n_same_item > 0) {
+    dim3 grid((unsigned)cn.n_same_item,
+              (unsigned)((ncol + (size_t)kSameThreads * VEC - 1) / ((size_t)kSameThreads * VEC)));
+    if constexpr (std::is_same<T, float>::value) {
+      sigma_same_v6f_kernel<VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, cn.off, cn.nsing, cn.ket, val,
+                                                                        cn.info, Dt, dstride, hii, cn.same_item,
+                                                                        cn.same_ypart, Y);
+    } else {
+      sigma_same_v6_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, cn.off, cn.nsing, cn.ket, val,
+                                                                         cn.info, Dt, dstride, hii, cn.same_item,
+                                                                         cn.same_ypart, Y);
+    }
+    SBDX_LAUNCHED(c);
   }
-  SBDX_LAUNCHED(c);
+  if (cn.n_same_split > 0) {
+    const unsigned bx = (unsigned)std::min<size_t>((ncol + 255) / 256, 64);
+    same_split_fixup_kernel<<<dim3(bx, (unsigned)cn.n_same_split), 256, 0, c->stream>>>(cn.same_split,
+                                                                                         cn.same_ypart, ncol, Y);
+    SBDX_LAUNCHED(c);
+  }
   return 0;
 }
 
@@ -1876,8 +1906,8 @@ int autotune(Ctx* c) {
   if ((rc = ensure_sigma_scratch(c))) return rc;
   const size_t D = c->na * c->nb;
   void *X = nullptr, *S = nullptr;
-  SBDX_CUDA(c, cudaMallocAsync(&X, sizeof(double) * D, c->stream));
-  SBDX_CUDA(c, cudaMallocAsync(&S, sizeof(double) * D, c->stream));
+  SBDX_CUDA(c, pool_alloc(c, &X, sizeof(double) * D));
+  SBDX_CUDA(c, pool_alloc(c, &S, sizeof(double) * D));
   SBDX_CUDA(c, cudaMemsetAsync(X, 0, sizeof(double) * D, c->stream));
   const bool prof0 = c->profiling;
   if (!c->ev[0])
@@ -1924,6 +1954,7 @@ int autotune(Ctx* c) {
   c->phase_calls = 0;
   cudaFreeAsync(X, c->stream);
   cudaFreeAsync(S, c->stream);
+  pool_trim(c);
   if (rc) return rc;
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
   return 0;
