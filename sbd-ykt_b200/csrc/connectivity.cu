@@ -229,7 +229,7 @@ int upload_items(Ctx* c, const std::vector<uint4>& items, const std::vector<uint
   if (!split.empty()) {
     SBDX_CUDA(c, cudaMemcpyAsync(*d_split, split.data(), sizeof(uint4) * split.size(), cudaMemcpyHostToDevice,
                                  c->stream));
-    SBDX_CUDA(c, cudaMalloc(d_part, sizeof(double) * (size_t)nslot * std::max<size_t>(1, ncol)));
+    SBDX_CUDA(c, cudaMalloc(d_part, sizeof(double) * (size_t)nslot * std::max<size_t>(8, pad8(ncol))));
   }
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // host vectors die at return
   return 0;
@@ -262,7 +262,8 @@ int build_same_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const st
   return upload_items(c, items, split, nslot, ncol, &cn.same_item, &cn.same_split, &cn.same_ypart);
 }
 
-// Work items of the packed alpha-beta kernel (see Conn::ab_item). A CTA
+// Work items of the packed alpha-beta kernel (see Conn::ab_item; partial rows
+// have the padded stride pad8(nb) of the sigma's alpha-major vectors). A CTA
 // handles one item and the kernel lasts about as long as the busiest SM, so
 // a few strings with many singles (near-Aufbau strings of a small sample
 // connect to ten times the mean) would set its duration: strings are split

@@ -107,12 +107,12 @@ struct Conn {
   size_t n_item = 0;
   uint4* ab_split = nullptr;   // [n_split]: {string, first slot, parts, 0}
   int n_split = 0, n_part = 0, item_cap = 0;
-  double* ypart = nullptr;     // [n_part * nb]
+  double* ypart = nullptr;     // [n_part * pad8(nb)]
   // work items of the alpha-first same-spin kernel (either spin), the same
   // scheme over the row's entries (singles then doubles): {bra string, first
   // entry, one past the last entry, 1 + partial-row slot or 0}. Partial rows
-  // are [n_same_part * ncol] (ncol = the other spin's string count); every
-  // part writes all its columns, and the fix-up assigns their sum.
+  // are [n_same_part * pad8(ncol)] (ncol = the other spin's string count);
+  // every part writes all its columns, and the fix-up assigns their sum.
   uint4* same_item = nullptr;
   size_t n_same_item = 0;
   uint4* same_split = nullptr;
@@ -125,6 +125,8 @@ struct Conn {
 constexpr int kMaxSplitSlots = 2048;
 // Dynamic shared memory the alpha-beta kernels may use per CTA.
 constexpr size_t kAbSmemBudget = 227 * 1024 - 1024;
+// n rounded up to a multiple of 8 (row strides of padded vectors and tables).
+constexpr size_t pad8(size_t n) { return (n + 7) / 8 * 8; }
 
 // Launch shape of the sigma kernels. Codes (also the C-ABI encoding):
 //   same-spin: 1/2/4/8 = columns per thread of the prefix-parity-table kernel,
@@ -176,10 +178,15 @@ struct Ctx {
   float *d_Da32 = nullptr, *d_Db32 = nullptr;
   size_t da_stride = 0, db_stride = 0;
   // sigma scratch (sized for D): transposed input, FP64 partial outputs
-  void* d_xt = nullptr;     // D elements of the widest type used (8 B)
-  void* d_xp = nullptr;     // D elements (8 B): phi o C, the input in the alpha-first basis
-  double* d_y = nullptr;    // D FP64: alpha-major partial sigma
-  double* d_yt = nullptr;   // D FP64: beta-major partial sigma
+  // The alpha-first sigma keeps its vectors with row strides padded to 8
+  // elements (xsa >= nb for the alpha-major ones, xsb >= na for the
+  // beta-major ones), so every row starts 32-byte aligned and the same-spin
+  // kernels load whole vectors of columns whatever na and nb are.
+  void* d_xt = nullptr;     // nb x xsb elements of the widest type used (8 B)
+  void* d_xp = nullptr;     // na x xsa elements (8 B): phi o C, the input in the alpha-first basis
+  double* d_y = nullptr;    // na x xsa FP64: alpha-major partial sigma
+  double* d_yt = nullptr;   // nb x xsb FP64: beta-major partial sigma
+  size_t xsa = 0, xsb = 0;
   void* d_io_in = nullptr;  // D FP64 staging for host-buffer entry points
   void* d_io_out = nullptr;
   // reductions

@@ -1010,7 +1010,8 @@ int run_ab(Ctx* c, const T* X) {
 
 template <typename T>
 __global__ void phase_split_kernel(const T* __restrict__ X, size_t na, size_t nb, const uint64_t* __restrict__ astr,
-                                   const uint64_t* __restrict__ bstr, T* __restrict__ Xp, T* __restrict__ Xpt) {
+                                   const uint64_t* __restrict__ bstr, T* __restrict__ Xp, T* __restrict__ Xpt,
+                                   size_t xsa, size_t xsb) {
   __shared__ T tile[32][33];
   __shared__ uint64_t s_pa[32], s_b[32];
   const size_t ib0 = (size_t)blockIdx.x * 32, ia0 = (size_t)blockIdx.y * 32;
@@ -1025,22 +1026,23 @@ __global__ void phase_split_kernel(const T* __restrict__ X, size_t na, size_t nb
     if (ia < na && ib < nb) {
       T v = X[ia * nb + ib];
       if (basis_phase(s_pa[k], s_b[tx])) v = -v;
-      Xp[ia * nb + ib] = v;
+      Xp[ia * xsa + ib] = v;
       tile[k][tx] = v;
     }
   }
   __syncthreads();
   for (int k = threadIdx.y; k < 32; k += blockDim.y) {
     const size_t ib = ib0 + k, ia = ia0 + tx;
-    if (ia < na && ib < nb) Xpt[ib * na + ia] = tile[tx][k];
+    if (ia < na && ib < nb) Xpt[ib * xsb + ia] = tile[tx][k];
   }
 }
 
-// S[ia, ib] = phi(ia, ib) (Y[ia, ib] + Yt[ib, ia]), stored in T.
+// S[ia, ib] = phi(ia, ib) (Y[ia, ib] + Yt[ib, ia]), stored in T; Y and Yt
+// have row strides xsa and xsb.
 template <typename T>
 __global__ void combine_phase_kernel(const double* __restrict__ Y, const double* __restrict__ Yt, size_t na,
                                      size_t nb, const uint64_t* __restrict__ astr, const uint64_t* __restrict__ bstr,
-                                     T* __restrict__ S) {
+                                     T* __restrict__ S, size_t xsa, size_t xsb) {
   __shared__ double tile[32][33];
   __shared__ uint64_t s_pa[32], s_b[32];
   const size_t ib0 = (size_t)blockIdx.x * 32, ia0 = (size_t)blockIdx.y * 32;
@@ -1051,13 +1053,13 @@ __global__ void combine_phase_kernel(const double* __restrict__ Y, const double*
   }
   for (int k = threadIdx.y; k < 32; k += blockDim.y) {
     const size_t ib = ib0 + k, ia = ia0 + tx;
-    if (ib < nb && ia < na) tile[tx][k] = Yt[ib * na + ia];
+    if (ib < nb && ia < na) tile[tx][k] = Yt[ib * xsb + ia];
   }
   __syncthreads();
   for (int k = threadIdx.y; k < 32; k += blockDim.y) {
     const size_t ia = ia0 + k, ib = ib0 + tx;
     if (ia < na && ib < nb) {
-      const double y = Y[ia * nb + ib] + tile[k][tx];
+      const double y = Y[ia * xsa + ib] + tile[k][tx];
       S[ia * nb + ib] = (T)(basis_phase(s_pa[k], s_b[tx]) ? -y : y);
     }
   }
@@ -1086,10 +1088,12 @@ __global__ void coulomb_table_kernel(const double* __restrict__ G, int L, const 
 // of the ket rows, which stays in L2), y = column strip. A CTA stages the
 // entries of its row (ket, signed value, signed pair index) in shared memory;
 // per pair a double costs one FMA and a single one add (the Coulomb table
-// element of its column) and one FMA. Requires ncol % VEC == 0.
+// element of its column) and one FMA. X and Y rows have stride ldx, a multiple
+// of VEC (padding columns up to ldx are computed and never read); hii has
+// stride ncol.
 template <typename T, int VEC>
 __global__ void __launch_bounds__(kSameThreads)
-sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __restrict__ off,
+sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, size_t ldx, const uint64_t* __restrict__ off,
                      const uint32_t* __restrict__ nsing, const uint32_t* __restrict__ ket,
                      const typename Prec<T>::V* __restrict__ val, const uint32_t* __restrict__ info,
                      const typename Prec<T>::V* __restrict__ Dt, size_t dstride, const double* __restrict__ hii,
@@ -1098,7 +1102,7 @@ sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __res
   __shared__ double s_val[kSameThreads];
   const uint4 item = items[blockIdx.x];  // bra string, entry range, output row
   const size_t r = item.x;
-  double* __restrict__ Yrow = item.w ? ypart + (size_t)(item.w - 1) * ncol : Y + r * ncol;
+  double* __restrict__ Yrow = item.w ? ypart + (size_t)(item.w - 1) * ldx : Y + r * ldx;
   const size_t c0 = ((size_t)blockIdx.y * kSameThreads + threadIdx.x) * VEC;
   const bool active = c0 < ncol;
   double acc[VEC];
@@ -1106,9 +1110,9 @@ sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __res
   for (int v = 0; v < VEC; ++v) acc[v] = 0.0;
   if (hii != nullptr && item.y == 0 && active) {
     double x[VEC];
-    VecIO<T, VEC>::load(X + r * ncol + c0, x);
+    VecIO<T, VEC>::load(X + r * ldx + c0, x);
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) acc[v] = hii[r * ncol + c0 + v] * x[v];
+    for (int v = 0; v < VEC; ++v) acc[v] = c0 + v < ncol ? hii[r * ncol + c0 + v] * x[v] : 0.0;
   }
   const uint64_t beg = off[r] + item.y, end = off[r] + item.z, send = off[r] + nsing[r];
   const unsigned t = threadIdx.x;
@@ -1130,7 +1134,7 @@ sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __res
       const uint32_t pqs = s_pq[e];
       const double hv = s_val[e];
       double x[VEC], d[VEC];
-      VecIO<T, VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+      VecIO<T, VEC>::load(X + (size_t)s_ket[e] * ldx + c0, x);
       VecIO<T, VEC>::load(Dt + (size_t)(pqs & 0xfffu) * dstride + c0, d);
 #pragma unroll
       for (int v = 0; v < VEC; ++v) acc[v] = fma(hv + flip_sign(d[v], pqs >> 31), x[v], acc[v]);
@@ -1139,7 +1143,7 @@ sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, const uint64_t* __res
     for (int e = nsb; e < cnt; ++e) {
       const double hv = s_val[e];
       double x[VEC];
-      VecIO<T, VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+      VecIO<T, VEC>::load(X + (size_t)s_ket[e] * ldx + c0, x);
 #pragma unroll
       for (int v = 0; v < VEC; ++v) acc[v] = fma(hv, x[v], acc[v]);
     }
@@ -1181,7 +1185,7 @@ template <> struct VecF<8> {
 
 template <int VEC>
 __global__ void __launch_bounds__(kSameThreads)
-sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, const uint64_t* __restrict__ off,
+sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, size_t ldx, const uint64_t* __restrict__ off,
                       const uint32_t* __restrict__ nsing, const uint32_t* __restrict__ ket,
                       const float* __restrict__ val, const uint32_t* __restrict__ info, const float* __restrict__ Dt,
                       size_t dstride, const double* __restrict__ hii, const uint4* __restrict__ items,
@@ -1190,7 +1194,7 @@ sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, const uint64_t* 
   __shared__ float s_val[kSameThreads];
   const uint4 item = items[blockIdx.x];  // bra string, entry range, output row
   const size_t r = item.x;
-  double* __restrict__ Yrow = item.w ? ypart + (size_t)(item.w - 1) * ncol : Y + r * ncol;
+  double* __restrict__ Yrow = item.w ? ypart + (size_t)(item.w - 1) * ldx : Y + r * ldx;
   const size_t c0 = ((size_t)blockIdx.y * kSameThreads + threadIdx.x) * VEC;
   const bool active = c0 < ncol;
   double acc[VEC];
@@ -1198,9 +1202,9 @@ sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, const uint64_t* 
   for (int v = 0; v < VEC; ++v) acc[v] = 0.0;
   if (hii != nullptr && item.y == 0 && active) {
     float x[VEC];
-    VecF<VEC>::load(X + r * ncol + c0, x);
+    VecF<VEC>::load(X + r * ldx + c0, x);
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) acc[v] = hii[r * ncol + c0 + v] * (double)x[v];
+    for (int v = 0; v < VEC; ++v) acc[v] = c0 + v < ncol ? hii[r * ncol + c0 + v] * (double)x[v] : 0.0;
   }
   const uint64_t beg = off[r] + item.y, end = off[r] + item.z, send = off[r] + nsing[r];
   const unsigned t = threadIdx.x;
@@ -1227,7 +1231,7 @@ sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, const uint64_t* 
         const uint32_t pqs = s_pq[e];
         const float hv = s_val[e];
         float x[VEC], d[VEC];
-        VecF<VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+        VecF<VEC>::load(X + (size_t)s_ket[e] * ldx + c0, x);
         VecF<VEC>::load(Dt + (size_t)(pqs & 0xfffu) * dstride + c0, d);
 #pragma unroll
         for (int v = 0; v < VEC; ++v) pf[v] = fmaf(hv + ((pqs >> 31) ? -d[v] : d[v]), x[v], pf[v]);
@@ -1244,7 +1248,7 @@ sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, const uint64_t* 
       for (int e = e0; e < e1; ++e) {
         const float hv = s_val[e];
         float x[VEC];
-        VecF<VEC>::load(X + (size_t)s_ket[e] * ncol + c0, x);
+        VecF<VEC>::load(X + (size_t)s_ket[e] * ldx + c0, x);
 #pragma unroll
         for (int v = 0; v < VEC; ++v) pf[v] = fmaf(hv, x[v], pf[v]);
       }
@@ -1273,7 +1277,7 @@ constexpr int kAb6Threads = 1024;
 // split parts lie in chunk 0.
 template <typename T, int R, int KS>
 __global__ void __launch_bounds__(kAb6Threads, 1)
-sigma_ab_v6_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restrict__ a_off,
+sigma_ab_v6_kernel(const T* __restrict__ Xp, size_t nb, size_t ldx, const uint64_t* __restrict__ a_off,
                    const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
                    const uint32_t* __restrict__ a_info, const uint64_t* __restrict__ sell,
                    const uint64_t* __restrict__ soff, const uint32_t* __restrict__ slen, size_t nslice,
@@ -1299,7 +1303,7 @@ sigma_ab_v6_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
   for (int k = 0; k < KS; ++k) acc[k] = 0.0;
   const uint64_t e0 = a_off[ia];
   const int ns = (int)a_nsing[ia];
-  const size_t xv = nb * sizeof(T) / 16;        // 16-byte vectors of a ket row (xstride covers the tail)
+  const size_t xv = (nb * sizeof(T) + 15) / 16;  // 16-byte vectors of a ket row (xstride and ldx cover the tail)
   const size_t ev = vstride * sizeof(V) / 16;   // 16-byte vectors of an integral row
   for (int k0 = 0; k0 < ns; k0 += R) {
     const int nr = min(R, ns - k0);
@@ -1307,15 +1311,9 @@ sigma_ab_v6_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
     if ((int)threadIdx.x < nr) s_sa[threadIdx.x] = a_info[e0 + k0 + threadIdx.x] >> 31;
     for (int rr = 0; rr < nr; ++rr) {
       const uint64_t e = e0 + k0 + rr;
-      const T* src = Xp + (size_t)a_ket[e] * nb;
-      T* dst = xs + (size_t)rr * xstride;
-      if ((nb * sizeof(T)) % 16 == 0) {
-        const uint4* s4 = reinterpret_cast<const uint4*>(src);
-        uint4* d4 = reinterpret_cast<uint4*>(dst);
-        for (size_t t = threadIdx.x; t < xv; t += kAb6Threads) d4[t] = __ldg(s4 + t);
-      } else {
-        for (size_t t = threadIdx.x; t < nb; t += kAb6Threads) dst[t] = src[t];
-      }
+      const uint4* s4 = reinterpret_cast<const uint4*>(Xp + (size_t)a_ket[e] * ldx);
+      uint4* d4 = reinterpret_cast<uint4*>(xs + (size_t)rr * xstride);
+      for (size_t t = threadIdx.x; t < xv; t += kAb6Threads) d4[t] = __ldg(s4 + t);
       const uint4* v4 = reinterpret_cast<const uint4*>(Vt + (size_t)((a_info[e] >> 12) & 0xfffu) * vstride);
       uint4* ed = reinterpret_cast<uint4*>(erow + (size_t)rr * vstride);
       for (size_t t = threadIdx.x; t < ev; t += kAb6Threads) ed[t] = __ldg(v4 + t);
@@ -1357,7 +1355,7 @@ sigma_ab_v6_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
     if (sl < nslice && pos < nv) {
       const uint32_t w = vrow[pos];
       const uint32_t slot1 = w >> 16;
-      if (slot1 == 0) Y[ia * nb + (w & 0xffffu)] += acc[k];
+      if (slot1 == 0) Y[ia * ldx + (w & 0xffffu)] += acc[k];
       else part[slot1 - 1] = acc[k];
     }
   }
@@ -1366,7 +1364,7 @@ sigma_ab_v6_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
     for (int s = threadIdx.x; s < nsplit; s += kAb6Threads) {
       double t = 0.0;
       for (uint32_t j = split_slot[s]; j < split_slot[s + 1]; ++j) t += part[j];
-      Y[ia * nb + split_row[s]] += t;
+      Y[ia * ldx + split_row[s]] += t;
     }
   }
 }
@@ -1403,7 +1401,7 @@ template <> struct RowPack<float> {
 // them whose partial row goes to its own slot (Conn::ab_item).
 template <typename T, int KS>
 __global__ void __launch_bounds__(kAb6Threads, 1)
-sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restrict__ a_off,
+sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restrict__ a_off,
                    const uint32_t* __restrict__ a_ket,
                    const uint32_t* __restrict__ a_info, const uint32_t* __restrict__ sell,
                    const uint64_t* __restrict__ soff4, const uint32_t* __restrict__ slen4, size_t nslice,
@@ -1423,7 +1421,7 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
   const uint4 item = items[blockIdx.x];
   const size_t ia = item.x;
   const int kend = (int)item.z;
-  double* __restrict__ Yrow = item.w ? ypart + (size_t)(item.w - 1) * nb : Y + ia * nb;
+  double* __restrict__ Yrow = item.w ? ypart + (size_t)(item.w - 1) * ldx : Y + ia * ldx;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t slice0 = (size_t)blockIdx.y * kWarps * KS;
   auto slice_of = [&](int k) -> size_t {
@@ -1442,7 +1440,7 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t nb, const uint64_t* __restri
     for (int e = 0; e < VR; ++e) {
       const uint64_t ent = e0 + k0 + (e < nr ? e : 0);
       const uint32_t inf = a_info[ent];
-      xrow[e] = Xp + (size_t)a_ket[ent] * nb + jb0;
+      xrow[e] = Xp + (size_t)a_ket[ent] * ldx + jb0;
       vrow_p[e] = Vt + (size_t)((inf >> 12) & 0xfffu) * vstride;
       neg[e] = (inf >> 31) != 0;
     }
@@ -1547,7 +1545,7 @@ int launch_ab_v7(Ctx* c, const T* Xp, const SellPanel& bp) {
   dim3 grid((unsigned)ca.n_item, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
   if (grid.y == 0) grid.y = 1;
   sigma_ab_v7_kernel<T, KS><<<grid, kAb6Threads, smem, c->stream>>>(
-      Xp, c->nb, ca.off, ca.ket, ca.info, bp.sell32, bp.soff4, bp.slen4, bp.nslice, bp.vrow, bp.nv,
+      Xp, c->xsa, ca.off, ca.ket, ca.info, bp.sell32, bp.soff4, bp.slen4, bp.nslice, bp.vrow, bp.nv,
       bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, (int)c->npair, bp.jb0, (size_t)(bp.jb1 - bp.jb0),
       ca.ab_item, ca.ypart, c->d_y);
   SBDX_LAUNCHED(c);
@@ -1557,13 +1555,13 @@ int launch_ab_v7(Ctx* c, const T* Xp, const SellPanel& bp) {
 // Adds the partial rows of the alpha strings split over several work items to
 // the output, parts in slot order (one fixed summation order).
 __global__ void ab_split_fixup_kernel(const uint4* __restrict__ split, const double* __restrict__ ypart, size_t nb,
-                                      double* __restrict__ Y) {
+                                      size_t ldx, double* __restrict__ Y) {
   const uint4 sp = split[blockIdx.y];
-  const double* part = ypart + (size_t)sp.y * nb;
+  const double* part = ypart + (size_t)sp.y * ldx;
   for (size_t ib = (size_t)blockIdx.x * blockDim.x + threadIdx.x; ib < nb; ib += (size_t)gridDim.x * blockDim.x) {
     double t = 0.0;
-    for (uint32_t q = 0; q < sp.z; ++q) t += part[(size_t)q * nb + ib];
-    Y[(size_t)sp.x * nb + ib] += t;
+    for (uint32_t q = 0; q < sp.z; ++q) t += part[(size_t)q * ldx + ib];
+    Y[(size_t)sp.x * ldx + ib] += t;
   }
 }
 
@@ -1572,7 +1570,7 @@ int run_ab_v7(Ctx* c, const T* Xp) {
   const Conn& ca = c->conn[0];
   if (ca.n_item == 0) return 0;  // no alpha string has a single excitation
   if (ca.n_part > 0)
-    SBDX_CUDA(c, cudaMemsetAsync(ca.ypart, 0, sizeof(double) * (size_t)ca.n_part * c->nb, c->stream));
+    SBDX_CUDA(c, cudaMemsetAsync(ca.ypart, 0, sizeof(double) * (size_t)ca.n_part * c->xsa, c->stream));
   std::vector<SellPanel> one;
   for (const SellPanel& bp : *ab7_panels(c, one)) {
     int rc;
@@ -1584,7 +1582,7 @@ int run_ab_v7(Ctx* c, const T* Xp) {
   if (ca.n_split > 0) {
     const unsigned bx = (unsigned)std::min<size_t>((c->nb + 255) / 256, 64);
     ab_split_fixup_kernel<<<dim3(bx, (unsigned)ca.n_split), 256, 0, c->stream>>>(ca.ab_split, ca.ypart, c->nb,
-                                                                                  c->d_y);
+                                                                                  c->xsa, c->d_y);
     SBDX_LAUNCHED(c);
   }
   return 0;
@@ -1593,29 +1591,30 @@ int run_ab_v7(Ctx* c, const T* Xp) {
 // Assigns the sum of the partial rows of the bra strings split over several
 // same-spin work items, parts in slot order.
 __global__ void same_split_fixup_kernel(const uint4* __restrict__ split, const double* __restrict__ ypart,
-                                        size_t ncol, double* __restrict__ Y) {
+                                        size_t ncol, size_t ldx, double* __restrict__ Y) {
   const uint4 sp = split[blockIdx.y];
-  const double* part = ypart + (size_t)sp.y * ncol;
+  const double* part = ypart + (size_t)sp.y * ldx;
   for (size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x; col < ncol; col += (size_t)gridDim.x * blockDim.x) {
     double t = 0.0;
-    for (uint32_t q = 0; q < sp.z; ++q) t += part[(size_t)q * ncol + col];
-    Y[(size_t)sp.x * ncol + col] = t;
+    for (uint32_t q = 0; q < sp.z; ++q) t += part[(size_t)q * ldx + col];
+    Y[(size_t)sp.x * ldx + col] = t;
   }
 }
 
 template <typename T, int VEC>
-int launch_same_v6(Ctx* c, const T* X, size_t nrow, size_t ncol, const Conn& cn, const typename Prec<T>::V* val,
-                   const typename Prec<T>::V* Dt, size_t dstride, const double* hii, double* Y) {
+int launch_same_v6(Ctx* c, const T* X, size_t nrow, size_t ncol, size_t ldx, const Conn& cn,
+                   const typename Prec<T>::V* val, const typename Prec<T>::V* Dt, size_t dstride, const double* hii,
+                   double* Y) {
   (void)nrow;
   if (cn.n_same_item > 0) {
     dim3 grid((unsigned)cn.n_same_item,
               (unsigned)((ncol + (size_t)kSameThreads * VEC - 1) / ((size_t)kSameThreads * VEC)));
     if constexpr (std::is_same<T, float>::value) {
-      sigma_same_v6f_kernel<VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, cn.off, cn.nsing, cn.ket, val,
+      sigma_same_v6f_kernel<VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, ldx, cn.off, cn.nsing, cn.ket, val,
                                                                         cn.info, Dt, dstride, hii, cn.same_item,
                                                                         cn.same_ypart, Y);
     } else {
-      sigma_same_v6_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, cn.off, cn.nsing, cn.ket, val,
+      sigma_same_v6_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, ldx, cn.off, cn.nsing, cn.ket, val,
                                                                          cn.info, Dt, dstride, hii, cn.same_item,
                                                                          cn.same_ypart, Y);
     }
@@ -1624,25 +1623,27 @@ int launch_same_v6(Ctx* c, const T* X, size_t nrow, size_t ncol, const Conn& cn,
   if (cn.n_same_split > 0) {
     const unsigned bx = (unsigned)std::min<size_t>((ncol + 255) / 256, 64);
     same_split_fixup_kernel<<<dim3(bx, (unsigned)cn.n_same_split), 256, 0, c->stream>>>(cn.same_split,
-                                                                                         cn.same_ypart, ncol, Y);
+                                                                                         cn.same_ypart, ncol, ldx, Y);
     SBDX_LAUNCHED(c);
   }
   return 0;
 }
 
 // v6 same-spin codes: 21, 22, 24, 28 = 1, 2, 4, 8 columns per thread, narrowed
-// to the widest vector that divides the row and keeps 16-byte alignment.
+// to the widest vector that divides the row stride and keeps 16-byte
+// alignment (the internal vectors have strides padded to 8 elements, so only
+// a misaligned base narrows).
 template <typename T>
-int run_same_v6(Ctx* c, int code, const T* X, size_t nrow, size_t ncol, const Conn& cn,
+int run_same_v6(Ctx* c, int code, const T* X, size_t nrow, size_t ncol, size_t ldx, const Conn& cn,
                 const typename Prec<T>::V* val, const typename Prec<T>::V* Dt, size_t dstride, const double* hii,
                 double* Y) {
   int vec = code % 10;
   const bool aligned = (reinterpret_cast<uintptr_t>(X) % 16) == 0;
-  while (vec > 1 && (!aligned || ncol % vec != 0)) vec >>= 1;
-  if (vec >= 8) return launch_same_v6<T, 8>(c, X, nrow, ncol, cn, val, Dt, dstride, hii, Y);
-  if (vec >= 4) return launch_same_v6<T, 4>(c, X, nrow, ncol, cn, val, Dt, dstride, hii, Y);
-  if (vec == 2) return launch_same_v6<T, 2>(c, X, nrow, ncol, cn, val, Dt, dstride, hii, Y);
-  return launch_same_v6<T, 1>(c, X, nrow, ncol, cn, val, Dt, dstride, hii, Y);
+  while (vec > 1 && (!aligned || ldx % vec != 0 || dstride % vec != 0)) vec >>= 1;
+  if (vec >= 8) return launch_same_v6<T, 8>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y);
+  if (vec >= 4) return launch_same_v6<T, 4>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y);
+  if (vec == 2) return launch_same_v6<T, 2>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y);
+  return launch_same_v6<T, 1>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y);
 }
 
 template <typename T, int R, int KS>
@@ -1660,7 +1661,7 @@ int launch_ab_v6(Ctx* c, const T* Xp, size_t smem, size_t xstride) {
   dim3 grid((unsigned)c->na, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
   if (grid.y == 0) grid.y = 1;
   sigma_ab_v6_kernel<T, R, KS><<<grid, kAb6Threads, smem, c->stream>>>(
-      Xp, c->nb, ca.off, ca.nsing, ca.ket, ca.info, bp.sell, bp.soff, bp.slen, bp.nslice, bp.vrow, bp.nv,
+      Xp, c->nb, c->xsa, ca.off, ca.nsing, ca.ket, ca.info, bp.sell, bp.soff, bp.slen, bp.nslice, bp.vrow, bp.nv,
       bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, xstride, c->d_y);
   SBDX_LAUNCHED(c);
   return 0;
@@ -1729,19 +1730,22 @@ int run_sigma_v6(Ctx* c, const Tune& tune, const T* X, T* S) {
   mark(0);
   {
     dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((na + 31) / 32));
-    phase_split_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(X, na, nb, c->d_a, c->d_b, xp, xpt);
+    phase_split_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(X, na, nb, c->d_a, c->d_b, xp, xpt, c->xsa, c->xsb);
     SBDX_LAUNCHED(c);
   }
   mark(1);
-  if ((rc = run_same_v6<T>(c, tune.same_code, xp, na, nb, ca, valA, Db, c->db_stride, c->d_hii, c->d_y))) return rc;
+  if ((rc = run_same_v6<T>(c, tune.same_code, xp, na, nb, c->xsa, ca, valA, Db, c->db_stride, c->d_hii, c->d_y)))
+    return rc;
   mark(2);
-  if ((rc = run_same_v6<T>(c, tune.same_code, xpt, nb, na, cb, valB, Da, c->da_stride, nullptr, c->d_yt))) return rc;
+  if ((rc = run_same_v6<T>(c, tune.same_code, xpt, nb, na, c->xsb, cb, valB, Da, c->da_stride, nullptr, c->d_yt)))
+    return rc;
   mark(3);
   if ((rc = run_ab_v6<T>(c, tune.ab_code, xp))) return rc;
   mark(4);
   {
     dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((na + 31) / 32));
-    combine_phase_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(c->d_y, c->d_yt, na, nb, c->d_a, c->d_b, S);
+    combine_phase_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(c->d_y, c->d_yt, na, nb, c->d_a, c->d_b, S, c->xsa,
+                                                                 c->xsb);
     SBDX_LAUNCHED(c);
   }
   mark(5);
@@ -1838,8 +1842,8 @@ int build_coulomb_tables(Ctx* c) {
   cudaFree(c->d_Da); cudaFree(c->d_Db); cudaFree(c->d_Da32); cudaFree(c->d_Db32);
   c->d_Da = c->d_Db = nullptr;
   c->d_Da32 = c->d_Db32 = nullptr;
-  c->da_stride = (c->na + 7) / 8 * 8;
-  c->db_stride = (c->nb + 7) / 8 * 8;
+  c->da_stride = pad8(c->na);
+  c->db_stride = pad8(c->nb);
   const size_t na_el = c->npair * c->da_stride, nb_el = c->npair * c->db_stride;
   SBDX_CUDA(c, cudaMalloc(&c->d_Da, sizeof(double) * na_el));
   SBDX_CUDA(c, cudaMalloc(&c->d_Db, sizeof(double) * nb_el));
@@ -1886,11 +1890,18 @@ int build_g_table(Ctx* c) {
 }
 
 int ensure_sigma_scratch(Ctx* c) {
-  const size_t D = c->na * c->nb;
-  if (!c->d_xt) SBDX_CUDA(c, cudaMalloc(&c->d_xt, sizeof(double) * D));
-  if (!c->d_xp) SBDX_CUDA(c, cudaMalloc(&c->d_xp, sizeof(double) * D));
-  if (!c->d_y) SBDX_CUDA(c, cudaMalloc(&c->d_y, sizeof(double) * D));
-  if (!c->d_yt) SBDX_CUDA(c, cudaMalloc(&c->d_yt, sizeof(double) * D));
+  c->xsa = pad8(c->nb);
+  c->xsb = pad8(c->na);
+  const size_t n = std::max(c->na * c->xsa, c->nb * c->xsb);  // >= D
+  auto get = [&](void** p) -> int {
+    if (*p) return 0;
+    SBDX_CUDA(c, cudaMalloc(p, sizeof(double) * n));
+    SBDX_CUDA(c, cudaMemsetAsync(*p, 0, sizeof(double) * n, c->stream));  // padding columns start at zero
+    return 0;
+  };
+  int rc;
+  if ((rc = get(&c->d_xt)) || (rc = get(&c->d_xp)) || (rc = get((void**)&c->d_y)) || (rc = get((void**)&c->d_yt)))
+    return rc;
   return 0;
 }
 
