@@ -109,6 +109,48 @@ def test_sigma_fp32_storage(port):
     assert np.abs(S - ref).max() <= 2e-6 * np.abs(ref).max()
 
 
+# Degenerate shapes: one string on a side (no same-spin entries there, one
+# output row or column), an empty and a full spin, the 64-orbital limit
+# (pair index 2079, masks up to bit 63); odd sizes exercise the padded row
+# strides of the alpha-first vectors.
+EDGE = [
+    ("1xN", (12, 3, 4, 1, 60, 51)),
+    ("Nx1", (12, 4, 3, 70, 1, 52)),
+    ("1x1", (8, 2, 2, 1, 1, 53)),
+    ("no_alpha_electrons", (10, 0, 3, 1, 50, 54)),
+    ("full_beta", (9, 3, 9, 40, 1, 55)),
+    ("L64", (64, 3, 3, 80, 70, 57)),
+    ("L64_unequal", (64, 6, 5, 121, 93, 58)),
+]
+
+
+@pytest.mark.parametrize("name,spec", EDGE)
+def test_edge_shapes(name, spec, port):
+    torch = pytest.importorskip("torch")
+    prob = _prob(spec)
+    C = np.random.default_rng(5).standard_normal(prob.D)
+    ref = port.sigma(prob, C)
+    ref32 = port.sigma(prob, C.astype(np.float32).astype(np.float64))
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        ctx.build_connectivity()
+        for spin, strings in ((0, prob.alpha), (1, prob.beta)):
+            sl, dl, idx = ctx.connectivity(spin)
+            rsl, rdl, ridx = port.connectivity(strings)
+            assert np.array_equal(sl, rsl) and np.array_equal(dl, rdl) and np.array_equal(idx, ridx)
+        hii = ctx.diag_terms()
+        ref_h = port.diag_terms(prob)
+        assert np.abs(hii - ref_h).max() <= 1e-12 * np.abs(ref_h).max()
+        S = ctx.sigma(C)
+        assert np.abs(S - ref).max() <= 1e-12 * np.abs(ref).max()
+        dC = torch.tensor(C, dtype=torch.float32, device="cuda")
+        dS = torch.empty_like(dC)
+        ctx.sigma_device(sbdx.SBDX_FP32, dC.data_ptr(), dS.data_ptr())
+        torch.cuda.synchronize()
+        S32 = dS.double().cpu().numpy()
+        assert np.abs(S32 - ref32).max() <= 2e-6 * np.abs(ref32).max()
+
+
 @pytest.mark.parametrize("spec", PROBLEMS[1:4])
 def test_davidson_fp64_energy(spec, port):
     prob = _prob(spec)
