@@ -64,6 +64,8 @@ def parse_args():
     ap.add_argument("--roots", type=int, default=2, help="roots of the multi-root Davidson runs (0 = skip them)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-subspace runs")
     ap.add_argument("--batch-threads", type=int, default=16)
+    ap.add_argument("--stored", default="cfg4", metavar="WORKLOAD",
+                    help="workload of the stored-Hamiltonian (method 1) measurement ('' = skip)")
     ap.add_argument("--tune", default=None, metavar="SAME,AB",
                     help="fixed sigma launch codes for both precisions instead of the autotuner (profiling runs)")
     return ap.parse_args()
@@ -310,6 +312,57 @@ def run_batched(args) -> dict:
     return out
 
 
+def run_stored(args, hbm: float) -> dict:
+    """The stored Hamiltonian (method 1, sbdx_build_hamiltonian) on a workload
+    whose matrix fits in HBM: build time, element count, the FP64 product
+    against the on-the-fly sigma of the same context (CUDA events, 10
+    products after 3 warm-up ones; the matrix is far larger than L2). Bytes
+    of a product: 12 per stored element (column + value) plus the row
+    pointers and three D-vectors (input, diagonal, output)."""
+    import torch
+
+    import sbdx
+    from sbdx import synth
+
+    w, _, sc = args.stored.partition("@")
+    prob = synth.config(w, float(sc) if sc else 1.0)
+    with sbdx.Context(torch.cuda.current_device()) as ctx:
+        ctx.load(prob)
+        ctx.build_connectivity()
+        ctx.diag_terms()
+        stream = torch.cuda.current_stream()
+        ctx.set_stream(stream.cuda_stream)
+        C = torch.randn(prob.D, dtype=torch.float64, device="cuda")
+        S = torch.empty_like(C)
+
+        def time_sigma(n=10):
+            for _ in range(3):
+                ctx.sigma_device(sbdx.SBDX_FP64, C.data_ptr(), S.data_ptr())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(n):
+                ctx.sigma_device(sbdx.SBDX_FP64, C.data_ptr(), S.data_ptr())
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / n
+
+        ms_fly = time_sigma()
+        S_fly = S.clone()
+        t0 = time.perf_counter()
+        nnz = ctx.build_hamiltonian()
+        build_s = time.perf_counter() - t0
+        ms_st = time_sigma()
+        rel = float((S - S_fly).abs().max() / S_fly.abs().max())
+        ctx.release_hamiltonian()
+    nbytes = 12 * nnz + 8 * (prob.D + 1) + 24 * prob.D
+    gbs = nbytes / (ms_st * 1e-3) / 1e9
+    return {"workload": args.stored, "desc": workload_desc(args.stored), "dets": int(prob.D), "elements": nnz,
+            "matrix_gb": (12 * nnz + 8 * (prob.D + 1)) / 1e9, "build_seconds": build_s,
+            "ms_stored_product": ms_st, "ms_on_the_fly_sigma": ms_fly, "gbs": gbs, "frac_of_hbm": gbs / hbm,
+            "max_rel_diff_vs_on_the_fly": rel}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -498,6 +551,9 @@ def run_ours(args, rank, world, local):
             cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference", "sample": rows}
 
     hbm, peak_kind = peaks()
+    stored = None
+    if args.stored and world == 1:
+        stored = run_stored(args, hbm)
     B = roofline_bytes(prob, dp, 8)
     pb = phase_bytes(prob, dp, 8)
     pb32 = phase_bytes(prob, dp, 4)
@@ -533,6 +589,7 @@ def run_ours(args, rank, world, local):
                                   for k in phases32}},
         "davidson": dav,
         "batched": batched,
+        "stored_hamiltonian": stored,
         "cpu_baseline": cpu,
     }
     if rank == 0:

@@ -108,6 +108,20 @@ int sbdx_connectivity_size(sbdx_ctx* ctx, int spin, uint64_t* n_entries);
  * doubles, ascending ket index; slen/dlen: per-bra list lengths. */
 int sbdx_get_connectivity(sbdx_ctx* ctx, int spin, uint64_t* slen, uint64_t* dlen, uint64_t* idx);
 
+/* Stored Hamiltonian, the reference's method 1 (chemistry/tpb/sbdiag.h:275-330:
+ * makeQCham, chemistry/tpb/qcham.h:10-312, then the stored-element mult,
+ * chemistry/tpb/mult.h:13-123). Builds every off-diagonal H_IJ on the device
+ * (CSR over determinant rows, FP64 values with the determinant phases, 32-bit
+ * columns: 12 bytes per element) after the connectivity and the diagonal;
+ * from then on every FP64 sigma of this context (sbdx_sigma, sbdx_sigma_device
+ * with SBDX_FP64, the Davidson solvers' FP64 products) is its sparse product,
+ * and FP32 sigmas stay on the fly. *nnz (may be NULL) receives the number of
+ * stored elements. SBDX_ERR_NOMEM, with the size in the message, when the
+ * matrix does not fit. New strings, integrals or connectivity drop it. */
+int sbdx_build_hamiltonian(sbdx_ctx* ctx, uint64_t* nnz);
+/* Frees the stored matrix; FP64 sigmas go back to the on-the-fly kernels. */
+int sbdx_release_hamiltonian(sbdx_ctx* ctx);
+
 /* Diagonal H_II for all determinants. Replaces makeQChamDiagTerms
  * (chemistry/tpb/qcham.h:314-366). hii: host buffer of na*nb doubles (may be
  * NULL to only compute the device copy). */

@@ -430,8 +430,8 @@ void diag(const Comm& /*comm*/, const SBD& sbd_data, const FCIDump& fcidump,
           std::vector<std::vector<double>>& two_p_rdm) {
   if (sbd_data.adet_comm_size * sbd_data.bdet_comm_size * sbd_data.task_comm_size != 1)
     throw std::invalid_argument("sbd::tpb::diag (GPU): the basis runs at world size 1 on one GPU");
-  if (sbd_data.method != 0)
-    throw std::invalid_argument("sbd::tpb::diag (GPU): method 0 (on-the-fly sigma) is the supported method");
+  if (sbd_data.method != 0 && sbd_data.method != 1)
+    throw std::invalid_argument("sbd::tpb::diag (GPU): method must be 0 (on-the-fly sigma) or 1 (stored Hamiltonian)");
   if (adet.empty() || bdet.empty()) throw std::invalid_argument("sbd::tpb::diag: empty string set");
   int L = 0, N = 0;
   double I0 = 0.0;
@@ -447,6 +447,13 @@ void diag(const Comm& /*comm*/, const SBD& sbd_data, const FCIDump& fcidump,
   ctx.check(sbdx_set_strings(ctx.h, a.data(), a.size(), b.data(), b.size()));
   ctx.check(sbdx_build_connectivity(ctx.h));
   if (detail::env_int("SBDX_AUTOTUNE", 0)) ctx.check(sbdx_autotune(ctx.h, nullptr, nullptr));
+  if (sbd_data.method == 1) {  // method 1 (sbdiag.h:275-300): store H, then the same Davidson
+    const auto t0 = std::chrono::high_resolution_clock::now();
+    uint64_t nnz = 0;
+    ctx.check(sbdx_build_hamiltonian(ctx.h, &nnz));
+    const double sec = std::chrono::duration<double>(std::chrono::high_resolution_clock::now() - t0).count();
+    std::cout << " Elapsed time for make Hamiltonian " << sec << " (sec) " << std::endl;
+  }
 
   const size_t D = a.size() * b.size();
   std::vector<double> W(D, 0.0);

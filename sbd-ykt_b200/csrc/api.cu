@@ -316,6 +316,25 @@ int sbdx_build_connectivity(sbdx_ctx* ctx) {
   });
 }
 
+int sbdx_build_hamiltonian(sbdx_ctx* ctx, uint64_t* nnz) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    int rc = sbdx::ready(c, "build_hamiltonian");
+    if (rc) return rc;
+    if ((rc = sbdx::build_stored(c))) return rc;
+    if (nnz) *nnz = c->stored.nnz;
+    return SBDX_OK;
+  });
+}
+
+int sbdx_release_hamiltonian(sbdx_ctx* ctx) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    sbdx::release_stored(c);
+    sbdx::clear_sigma_graphs(c);
+    return SBDX_OK;
+  });
+}
+
 int sbdx_connectivity_size(sbdx_ctx* ctx, int spin, uint64_t* n_entries) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {
     if (spin != 0 && spin != 1) { c->err = "connectivity_size: spin must be 0 or 1"; return SBDX_ERR_ARG; }

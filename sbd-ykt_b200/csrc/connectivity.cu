@@ -605,6 +605,7 @@ int build_one(Ctx* c, int spin) {
 
 void free_connectivity(Ctx* c) {
   clear_sigma_graphs(c);
+  release_stored(c);  // its elements come from the connectivity
   free_conn(c->conn[0]);
   free_conn(c->conn[1]);
   cudaFree(c->d_Da); cudaFree(c->d_Db); cudaFree(c->d_Da32); cudaFree(c->d_Db32);

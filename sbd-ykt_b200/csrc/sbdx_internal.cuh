@@ -128,6 +128,15 @@ constexpr size_t kAbSmemBudget = 227 * 1024 - 1024;
 // n rounded up to a multiple of 8 (row strides of padded vectors and tables).
 constexpr size_t pad8(size_t n) { return (n + 7) / 8 * 8; }
 
+// Stored Hamiltonian (the reference's method 1): off-diagonal elements in CSR
+// over determinant rows, basis phases folded into the values (stored.cu).
+struct StoredH {
+  uint64_t* rowptr = nullptr;  // [D + 1]
+  uint32_t* col = nullptr;     // [nnz] determinant index ja*nb + jb
+  double* val = nullptr;       // [nnz] H_IJ
+  uint64_t nnz = 0;
+};
+
 // Launch shape of the sigma kernels. Codes (also the C-ABI encoding):
 //   same-spin: 1/2/4/8 = columns per thread of the prefix-parity-table kernel,
 //              11/12/14 = 1/2/4 columns of the popcount kernel
@@ -170,6 +179,8 @@ struct Ctx {
   // diagonal
   double* d_hii = nullptr;
   bool have_hii = false;
+  // stored Hamiltonian; when present, every FP64 sigma is its sparse product
+  StoredH stored;
   // opposite-spin Coulomb term of single excitations in the alpha-first
   // sigma: Db[pq * db_stride + ib] = sum_{q in beta(ib)} (pq|qq) (alpha
   // singles), Da[pq * da_stride + ia] = sum_{p in alpha(ia)} (pq|pp) (beta
@@ -316,6 +327,11 @@ int build_coulomb_tables(Ctx* c);
 int diag_terms(Ctx* c);
 // sigma: X (na x nb, type by precision: 0 = FP64, 1 = FP32) -> S (same type)
 int sigma_device(Ctx* c, int precision, const void* X, void* S);
+// Stored Hamiltonian (stored.cu): build (connectivity and diagonal first),
+// release, and its product S = H X in FP64.
+int build_stored(Ctx* c);
+void release_stored(Ctx* c);
+int stored_sigma(Ctx* c, const double* X, double* S);
 int ensure_sigma_scratch(Ctx* c);
 void clear_sigma_graphs(Ctx* c);
 int ensure_reduction(Ctx* c, size_t n);

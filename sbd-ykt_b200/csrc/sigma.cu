@@ -2039,6 +2039,8 @@ int sigma_device(Ctx* c, int precision, const void* X, void* S) {
     c->err = "sigma: precision must be SBDX_FP64 or SBDX_FP32";
     return 1;
   }
+  if (precision == 0 && c->stored.val != nullptr)
+    return stored_sigma(c, static_cast<const double*>(X), static_cast<double*>(S));
   if (c->use_graphs && !c->profiling && c->stream != nullptr) {
     rc = sigma_graph(c, precision, X, S);
     if (rc >= 0) return rc;

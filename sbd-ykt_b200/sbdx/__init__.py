@@ -32,6 +32,7 @@ EXPORTS = [
     "sbdx_get_connectivity", "sbdx_diag_terms", "sbdx_sigma", "sbdx_sigma_device", "sbdx_davidson",
     "sbdx_rdm", "sbdx_occupation", "sbdx_alpha_weights", "sbdx_energy_backward", "sbdx_set_profiling",
     "sbdx_phase_times", "sbdx_set_tuning", "sbdx_autotune", "sbdx_davidson_roots",
+    "sbdx_build_hamiltonian", "sbdx_release_hamiltonian",
 ]
 PHASES = ["alpha_same_spin", "transpose", "beta_same_spin", "alpha_beta", "combine"]
 
@@ -161,6 +162,16 @@ class Context:
 
     def build_connectivity(self):
         self._check(self.lib.sbdx_build_connectivity(self.h))
+
+    def build_hamiltonian(self) -> int:
+        """Stores H on the device (the reference's method 1); FP64 sigmas then
+        use it. Returns the number of stored off-diagonal elements."""
+        n = ctypes.c_uint64(0)
+        self._check(self.lib.sbdx_build_hamiltonian(self.h, ctypes.byref(n)))
+        return int(n.value)
+
+    def release_hamiltonian(self):
+        self._check(self.lib.sbdx_release_hamiltonian(self.h))
 
     def connectivity(self, spin):
         n = ctypes.c_uint64(0)

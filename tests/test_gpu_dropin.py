@@ -45,14 +45,18 @@ def energy(stdout, label="Sample-based diagonalization: Energy"):
     return float(re.search(label + r" = (\S+)", stdout).group(1))
 
 
+@pytest.mark.parametrize("method", [0, 1])
 @pytest.mark.parametrize("mol, readme", [("h2o", -76.2359376), ("n2", -109.041511)])
-def test_file_path_known_answer(tmp_path, mol, readme):
+def test_file_path_known_answer(tmp_path, mol, readme, method):
+    """Both diag methods: 0 evaluates H on the fly, 1 stores it first
+    (sbdiag.h:275-330); the energies are the reference's."""
     g, fd, ad = write_inputs(tmp_path, mol)
-    out = run(["--fcidump", fd, "--adetfile", ad, "--iteration", "10", "--block", "10", "--tolerance", "1e-8"],
-              str(tmp_path))
+    out = run(["--fcidump", fd, "--adetfile", ad, "--iteration", "10", "--block", "10", "--tolerance", "1e-8",
+               "--method", str(method)], str(tmp_path))
     E = energy(out)
     assert abs(E - float(g["E_file"])) < 1e-9
     assert abs(E - readme) < 1e-6
+    assert ("make Hamiltonian" in out) == (method == 1)
 
 
 def test_struct_path_and_rdm_identity(tmp_path):

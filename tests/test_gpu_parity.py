@@ -151,6 +151,44 @@ def test_edge_shapes(name, spec, port):
         assert np.abs(S32 - ref32).max() <= 2e-6 * np.abs(ref32).max()
 
 
+@pytest.mark.parametrize("spec", PROBLEMS + [e[1] for e in EDGE])
+def test_stored_hamiltonian_sigma(spec, port):
+    """The stored Hamiltonian (method 1): its product equals the oracle's
+    sigma (1e-12 relative); releasing it returns to the on-the-fly kernels;
+    the element count is the reference's per-row count (same-spin lists of
+    the row's alpha and beta strings plus singles x singles)."""
+    prob = _prob(spec)
+    C = np.random.default_rng(6).standard_normal(prob.D)
+    ref = port.sigma(prob, C)
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        nnz = ctx.build_hamiltonian()
+        sa, da, _ = ctx.connectivity(0)
+        sb, db, _ = ctx.connectivity(1)
+        na_e, nb_e = (sa + da).astype(np.int64), (sb + db).astype(np.int64)
+        expect = len(prob.beta) * na_e.sum() + len(prob.alpha) * nb_e.sum() + \
+            int(sa.astype(np.int64).sum()) * int(sb.astype(np.int64).sum())
+        assert nnz == expect
+        S = ctx.sigma(C)
+        assert np.abs(S - ref).max() <= 1e-12 * np.abs(ref).max()
+        ctx.release_hamiltonian()
+        S2 = ctx.sigma(C)
+        assert np.abs(S2 - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("spec", PROBLEMS[1:4])
+def test_stored_hamiltonian_davidson(spec, port):
+    """FP64 Davidson on the stored matrix: the oracle's energy (1e-9 Ha) and
+    the on-the-fly solve's."""
+    prob = _prob(spec)
+    E_ref, _, _ = port.davidson(prob, max_it=6, max_nb=10, eps=1e-9)
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        ctx.build_hamiltonian()
+        info, W = ctx.davidson(max_it=6, max_nb=10, eps=1e-9)
+    assert abs(info.energy - E_ref) < 1e-9
+
+
 @pytest.mark.parametrize("spec", PROBLEMS[1:4])
 def test_davidson_fp64_energy(spec, port):
     prob = _prob(spec)
