@@ -64,6 +64,9 @@ def parse_args():
     ap.add_argument("--roots", type=int, default=2, help="roots of the multi-root Davidson runs (0 = skip them)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-subspace runs")
     ap.add_argument("--batch-threads", type=int, default=16)
+    ap.add_argument("--diff", default="cfg4", metavar="WORKLOAD",
+                    help="workload of the differentiation measurement ('' = skip)")
+    ap.add_argument("--diff-entries", type=int, default=4, help="entries checked by central differences")
     ap.add_argument("--stored", default="cfg4", metavar="WORKLOAD",
                     help="workload of the stored-Hamiltonian (method 1) measurement ('' = skip)")
     ap.add_argument("--tune", default=None, metavar="SAME,AB",
@@ -363,6 +366,53 @@ def run_stored(args, hbm: float) -> dict:
             "max_rel_diff_vs_on_the_fly": rel}
 
 
+def run_differentiation(args) -> dict:
+    """Energy adjoint on the differentiation workload (L=32, 6+6 electrons,
+    2000x2000 strings): FP64 forward solve to 1e-10, the backward kernel
+    (dE/dh and dE/d(pq|rs) from the 1-/2-RDM of the converged vector, the
+    connectivity recomputed) and, on a few seeded entries, central
+    differences of the forward solve (step 1e-5) against it."""
+    import torch
+
+    import sbdx
+    from sbdx import autograd as sag
+    from sbdx import synth
+
+    w, _, sc = args.diff.partition("@")
+    prob = synth.config(w, float(sc) if sc else 1.0)
+    L = prob.L
+    out = {"workload": args.diff, "desc": workload_desc(args.diff), "dets": int(prob.D)}
+    with sbdx.Context(torch.cuda.current_device()) as ctx:
+        ctx.set_strings(prob.alpha, prob.beta)
+        h_tri = torch.tensor(sag.tril_pack(prob.h.reshape(L, L)), requires_grad=True)
+        eri = torch.tensor(prob.eri, requires_grad=True)
+        t0 = time.perf_counter()
+        E = sag.energy(ctx, h_tri, eri, L, prob.I0)
+        out["forward_seconds"] = time.perf_counter() - t0
+        out["energy"] = float(E.detach())
+        t0 = time.perf_counter()
+        E.backward()
+        out["backward_seconds"] = time.perf_counter() - t0
+        gh, ge = h_tri.grad.numpy(), eri.grad.numpy()
+        rng = np.random.default_rng(9)
+        k = max(args.diff_entries, 0)
+        picks = [("h", int(i)) for i in rng.choice(len(gh), k // 2, replace=False)]
+        nz = np.flatnonzero(np.abs(prob.eri) > 1e-3)
+        picks += [("eri", int(i)) for i in rng.choice(nz, k - k // 2, replace=False)]
+        worst, step = 0.0, 1e-5
+        for kind, i in picks:
+            vals = []
+            for sgn in (+1, -1):
+                ht, et = h_tri.detach().clone(), eri.detach().clone()
+                (ht if kind == "h" else et)[i] += sgn * step
+                vals.append(float(sag.energy(ctx, ht, et, L, prob.I0)))
+            fd = (vals[0] - vals[1]) / (2 * step)
+            an = float(gh[i] if kind == "h" else ge[i])
+            worst = max(worst, abs(fd - an) / max(1.0, abs(an)))
+        out.update({"fd_entries": len(picks), "fd_step": step, "max_rel_err_vs_central_differences": worst})
+    return out
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -554,6 +604,9 @@ def run_ours(args, rank, world, local):
     stored = None
     if args.stored and world == 1:
         stored = run_stored(args, hbm)
+    diff = None
+    if args.diff and world == 1 and not args.no_davidson:
+        diff = run_differentiation(args)
     B = roofline_bytes(prob, dp, 8)
     pb = phase_bytes(prob, dp, 8)
     pb32 = phase_bytes(prob, dp, 4)
@@ -590,6 +643,7 @@ def run_ours(args, rank, world, local):
         "davidson": dav,
         "batched": batched,
         "stored_hamiltonian": stored,
+        "differentiation": diff,
         "cpu_baseline": cpu,
     }
     if rank == 0:

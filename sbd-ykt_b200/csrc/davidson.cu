@@ -335,18 +335,34 @@ struct Work {
 // Device scalar slots
 enum { kE0 = 0, kNW = 1, kNR = 2, kOlap = 3, kNV = 4, kE = 5, kAB = 6, kDots = 8 };
 
+// CTAs of one full wave of a reduction kernel of kRedThreads threads, at most
+// kRedBlocks (the row length of the partial buffer). The reduction kernels
+// stride over D with their whole grid; the wider ones (more than 64 registers
+// per thread) fit 3 CTAs per SM, and a grid of kRedBlocks then ran a second,
+// one-third-full wave: their bandwidth halved.
+template <typename K>
+unsigned wave_of(K kernel) {
+  int dev = 0, nsm = 0, occ = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) nsm = 148;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kRedThreads, 0) != cudaSuccess || occ < 1) occ = 1;
+  return (unsigned)std::min(kRedBlocks, nsm * occ);
+}
+
 template <typename TV, typename TX>
 int multidot(Ctx* c, Work& wk, const TV* V, size_t ldv, int m, const TX* x, size_t D, double* out) {
-  dim3 grid(kRedBlocks, (unsigned)((m + kDotChunk - 1) / kDotChunk));
+  static const unsigned g = wave_of(multidot_kernel<TV, TX>);
+  dim3 grid(g, (unsigned)((m + kDotChunk - 1) / kDotChunk));
   multidot_kernel<TV, TX><<<grid, kRedThreads, 0, c->stream>>>(V, ldv, m, x, D, wk.partial);
   SBDX_LAUNCHED(c);
-  finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, kRedBlocks, m, out);
+  finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, (int)g, m, out);
   SBDX_LAUNCHED(c);
   return 0;
 }
 
-int finalize(Ctx* c, Work& wk, int m, double* out) {
-  finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, kRedBlocks, m, out);
+// out[k] = sum of the nblk partials of row k (nblk = the producing grid).
+int finalize(Ctx* c, Work& wk, int m, double* out, unsigned nblk = kRedBlocks) {
+  finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, (int)nblk, m, out);
   SBDX_LAUNCHED(c);
   return 0;
 }
@@ -546,7 +562,23 @@ olsen_precond_kernel(const double* __restrict__ R, const double* __restrict__ W,
   const double E0 = *E0p;
   const double inv = 1.0 / sqrt(*nr2);
   double a = 0.0, b = 0.0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nq = quads(D);
+  for (size_t q = t0; q < nq; q += st) {
+    double r[4], w[4], d[4], x[4];
+    ld4(R + 4 * q, r);
+    ld4(W + 4 * q, w);
+    ld4(dii + 4 * q, d);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const double p = precond_inv(E0, d[e]);
+      x[e] = r[e] * inv * p;
+      a = fma(w[e], x[e], a);
+      b = fma(w[e] * w[e], p, b);
+    }
+    st4(v + 4 * q, x);
+  }
+  for (size_t s = 4 * nq + t0; s < D; s += st) {
     const double p = precond_inv(E0, dii[s]);
     const double x = R[s] * inv * p;
     const double w = W[s];
@@ -570,7 +602,22 @@ olsen_apply_kernel(double* __restrict__ v, const double* __restrict__ W, const d
   const double E0 = *E0p;
   const double eps = ab[1] != 0.0 ? ab[0] / ab[1] : 0.0;
   double acc = 0.0, nn = 0.0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nq = quads(D);
+  for (size_t q = t0; q < nq; q += st) {
+    double x[4], w[4], d[4];
+    ld4_rw(v + 4 * q, x);
+    ld4(W + 4 * q, w);
+    ld4(dii + 4 * q, d);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      x[e] -= eps * precond_inv(E0, d[e]) * w[e];
+      acc = fma(w[e], x[e], acc);
+      nn = fma(x[e], x[e], nn);
+    }
+    st4(v + 4 * q, x);
+  }
+  for (size_t s = 4 * nq + t0; s < D; s += st) {
     const double w = W[s];
     const double x = v[s] - eps * precond_inv(E0, dii[s]) * w;
     v[s] = x;
@@ -889,10 +936,11 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
       ++since;
       // (<C_k|HC_j>, <C_k|C_j>) for k <= j with one read of C; <W|C_j>, <HW|C_j>
       {
-        dim3 grid(kRedBlocks, (unsigned)((nv + kDotChunk - 1) / kDotChunk));
+        static const unsigned g2 = wave_of(multidot2_kernel<float, float>);
+        dim3 grid(g2, (unsigned)((nv + kDotChunk - 1) / kDotChunk));
         multidot2_kernel<float, float><<<grid, kRedThreads, 0, c->stream>>>(C, D, nv, HCb, Cb, D, wk.partial);
         SBDX_LAUNCHED(c);
-        if ((rc = finalize(c, wk, 2 * nv, s + kDots))) return rc;
+        if ((rc = finalize(c, wk, 2 * nv, s + kDots, g2))) return rc;
       }
       if ((rc = multidot<double, float>(c, wk, AW, D, 2, Cb, D, s + kDots + 2 * nv))) return rc;
       SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kDots, sizeof(double) * (2 * nv + 2), cudaMemcpyDeviceToHost,
@@ -913,12 +961,13 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
       // the anchor becomes the Ritz vector: W <- x0 W + sum x_k C_k (same for HW)
       SBDX_CUDA(c, cudaMemcpyAsync(wk.u, x.data() + 1, sizeof(double) * nv, cudaMemcpyHostToDevice, c->stream));
       SBDX_CUDA(c, cudaMemcpyAsync(s + kE0, &theta, sizeof(double), cudaMemcpyHostToDevice, c->stream));
-      update_anchor_kernel<float><<<kRedBlocks, kRedThreads, 0, c->stream>>>(C, HC, D, nv, wk.u, x[0], s + kE0, D,
-                                                                             W, HW, R, wk.partial);
+      static const unsigned gu = wave_of(update_anchor_kernel<float>);
+      update_anchor_kernel<float><<<gu, kRedThreads, 0, c->stream>>>(C, HC, D, nv, wk.u, x[0], s + kE0, D, W, HW, R,
+                                                                     wk.partial);
       SBDX_LAUNCHED(c);
       // |W|^2 (kNW) and |R|^2 (kNR). x is S-normalised and S holds the exact dots
       // of the stored vectors, so the new anchor has unit norm to rounding.
-      if ((rc = finalize(c, wk, 2, s + kNW))) return rc;
+      if ((rc = finalize(c, wk, 2, s + kNW, gu))) return rc;
       double nrm[2];
       SBDX_CUDA(c, cudaMemcpyAsync(nrm, s + kNW, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
       SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1058,7 +1107,59 @@ update_anchors_kernel(const double* __restrict__ W, const double* __restrict__ H
   double nw[K], nr[K];
 #pragma unroll
   for (int r = 0; r < K; ++r) nw[r] = nr[r] = 0.0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nq = quads(D);
+  for (size_t q = t0; q < nq; q += st) {
+    double w[K][4], hw[K][4];
+#pragma unroll
+    for (int r = 0; r < K; ++r)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) w[r][e] = hw[r][e] = 0.0;
+#pragma unroll
+    for (int a = 0; a < K; ++a) {
+      double wa[4], ha[4];
+      ld4(W + (size_t)a * D + 4 * q, wa);
+      ld4(HW + (size_t)a * D + 4 * q, ha);
+#pragma unroll
+      for (int r = 0; r < K; ++r) {
+        const double xa = sx[a + n * r];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          w[r][e] = fma(xa, wa[e], w[r][e]);
+          hw[r][e] = fma(xa, ha[e], hw[r][e]);
+        }
+      }
+    }
+#pragma unroll 2
+    for (int j = 0; j < m; ++j) {
+      double cj[4], hj[4];
+      ld4(C + (size_t)j * D + 4 * q, cj);
+      ld4(HC + (size_t)j * D + 4 * q, hj);
+#pragma unroll
+      for (int r = 0; r < K; ++r) {
+        const double xj = sx[K + j + n * r];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          w[r][e] = fma(xj, cj[e], w[r][e]);
+          hw[r][e] = fma(xj, hj[e], hw[r][e]);
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < K; ++r) {
+      double rr[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        rr[e] = th[r] * w[r][e] - hw[r][e];
+        nw[r] = fma(w[r][e], w[r][e], nw[r]);
+        nr[r] = fma(rr[e], rr[e], nr[r]);
+      }
+      st4(Wn + (size_t)r * D + 4 * q, w[r]);
+      st4(HWn + (size_t)r * D + 4 * q, hw[r]);
+      st4(R + (size_t)r * D + 4 * q, rr);
+    }
+  }
+  for (size_t s = 4 * nq + t0; s < D; s += st) {
     double w[K], hw[K];
 #pragma unroll
     for (int r = 0; r < K; ++r) w[r] = hw[r] = 0.0;
@@ -1196,14 +1297,26 @@ int expand_block(Ctx* c, Work& wk, const double* Rr, const double* Wr, const dou
   return 0;
 }
 
+// Returns the grid used (the partial rows' length) in *nblk.
+template <typename TC, int K>
+void launch_update_anchors_k(Ctx* c, Work& wk, const double* W, const double* HW, const TC* C, const TC* HC, int m,
+                             const double* X, const double* theta, size_t D, double* Wn, double* HWn, double* R,
+                             unsigned* nblk) {
+  static const unsigned g = wave_of(update_anchors_kernel<TC, K>);
+  update_anchors_kernel<TC, K><<<g, kRedThreads, 0, c->stream>>>(W, HW, C, HC, m, X, theta, D, Wn, HWn, R,
+                                                                 wk.partial);
+  *nblk = g;
+}
+
 template <typename TC>
 int launch_update_anchors(Ctx* c, Work& wk, int k, const double* W, const double* HW, const TC* C, const TC* HC,
-                          int m, const double* X, const double* theta, size_t D, double* Wn, double* HWn, double* R) {
+                          int m, const double* X, const double* theta, size_t D, double* Wn, double* HWn, double* R,
+                          unsigned* nblk) {
   switch (k) {
-    case 1: update_anchors_kernel<TC, 1><<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, C, HC, m, X, theta, D, Wn, HWn, R, wk.partial); break;
-    case 2: update_anchors_kernel<TC, 2><<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, C, HC, m, X, theta, D, Wn, HWn, R, wk.partial); break;
-    case 3: update_anchors_kernel<TC, 3><<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, C, HC, m, X, theta, D, Wn, HWn, R, wk.partial); break;
-    default: update_anchors_kernel<TC, 4><<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, C, HC, m, X, theta, D, Wn, HWn, R, wk.partial); break;
+    case 1: launch_update_anchors_k<TC, 1>(c, wk, W, HW, C, HC, m, X, theta, D, Wn, HWn, R, nblk); break;
+    case 2: launch_update_anchors_k<TC, 2>(c, wk, W, HW, C, HC, m, X, theta, D, Wn, HWn, R, nblk); break;
+    case 3: launch_update_anchors_k<TC, 3>(c, wk, W, HW, C, HC, m, X, theta, D, Wn, HWn, R, nblk); break;
+    default: launch_update_anchors_k<TC, 4>(c, wk, W, HW, C, HC, m, X, theta, D, Wn, HWn, R, nblk); break;
   }
   SBDX_LAUNCHED(c);
   return 0;
@@ -1372,10 +1485,11 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
         ++added;
         // (<C_i|HC_j>, <C_i|C_j>) for i <= j; <W_r|C_j>, <HW_r|C_j>
         {
-          dim3 grid(kRedBlocks, (unsigned)((nv + kDotChunk - 1) / kDotChunk));
+          static const unsigned g2 = wave_of(multidot2_kernel<TC, TC>);
+          dim3 grid(g2, (unsigned)((nv + kDotChunk - 1) / kDotChunk));
           multidot2_kernel<TC, TC><<<grid, kRedThreads, 0, c->stream>>>(C, D, nv, HCb, Cb, D, wk.partial);
           SBDX_LAUNCHED(c);
-          if ((rc = finalize(c, wk, 2 * nv, s + kbDots))) return rc;
+          if ((rc = finalize(c, wk, 2 * nv, s + kbDots, g2))) return rc;
         }
         // W and HW are contiguous (HW = W + k*D) in either half of A
         if ((rc = multidot<double, TC>(c, wk, W, D, 2 * k, Cb, D, s + kbDots + 2 * nv))) return rc;
@@ -1404,11 +1518,12 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
       }
       SBDX_CUDA(c, cudaMemcpyAsync(Xd, X.data(), sizeof(double) * n * k, cudaMemcpyHostToDevice, c->stream));
       SBDX_CUDA(c, cudaMemcpyAsync(s + kbTheta, theta.data(), sizeof(double) * k, cudaMemcpyHostToDevice, c->stream));
-      if ((rc = launch_update_anchors<TC>(c, wk, k, W, HW, C, HC, nv, Xd, s + kbTheta, D, Wn, HWn, R))) return rc;
+      unsigned ga = kRedBlocks;
+      if ((rc = launch_update_anchors<TC>(c, wk, k, W, HW, C, HC, nv, Xd, s + kbTheta, D, Wn, HWn, R, &ga))) return rc;
       // |W'_r|^2 -> kbNW2 + r, |R_r|^2 -> kbNR2 + r
-      finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, kRedBlocks, k, s + kbNW2);
+      finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, (int)ga, k, s + kbNW2);
       SBDX_LAUNCHED(c);
-      finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial + (size_t)k * kRedBlocks, kRedBlocks, k, s + kbNR2);
+      finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial + (size_t)k * ga, (int)ga, k, s + kbNR2);
       SBDX_LAUNCHED(c);
       // A holds [W | HW | W' | HW']; the swaps exchange the halves, HW = W + k*D
       std::swap(W, Wn);
