@@ -51,6 +51,28 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return t;  // valid in thread 0
 }
 
+// Block sums of n <= N values with one barrier: every warp reduces all its
+// values by shuffles, then thread t < n adds value t over the warps (fixed
+// order) and writes partial[(row0 + t) * gridDim.x + blockIdx.x]. sh holds
+// N * (blockDim.x / 32) doubles.
+template <int N>
+__device__ __forceinline__ void block_sums(const double (&v)[N], int n, double* sh, double* __restrict__ partial,
+                                           size_t row0) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = (int)(blockDim.x >> 5);
+#pragma unroll
+  for (int t = 0; t < N; ++t) {
+    double x = v[t];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[t * nw + warp] = x;
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < n) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += sh[threadIdx.x * nw + w];
+    partial[(row0 + threadIdx.x) * gridDim.x + blockIdx.x] = s;
+  }
+}
+
 // Four consecutive elements as doubles. The vector kernels below take this
 // path for element quads when D % 4 == 0: every vector of the solvers starts
 // at a cudaMalloc base plus a multiple of D elements, so quads are 16-byte
@@ -81,7 +103,7 @@ template <typename TV, typename TX>
 __global__ void __launch_bounds__(kRedThreads)
 multidot_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restrict__ x, size_t D,
                 double* __restrict__ partial) {
-  __shared__ double sh[kRedThreads / 32];
+  __shared__ double sh[kDotChunk * (kRedThreads / 32)];
   const int k0 = blockIdx.y * kDotChunk;
   const int mc = min(kDotChunk, m - k0);
   double acc[kDotChunk];
@@ -106,10 +128,7 @@ multidot_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restric
     for (int k = 0; k < kDotChunk; ++k)
       if (k < mc) acc[k] = fma((double)V[(size_t)(k0 + k) * ldv + s], xv, acc[k]);
   }
-  for (int k = 0; k < mc; ++k) {
-    const double t = block_sum(acc[k], sh);
-    if (threadIdx.x == 0) partial[(size_t)(k0 + k) * gridDim.x + blockIdx.x] = t;
-  }
+  block_sums<kDotChunk>(acc, mc, sh, partial, (size_t)k0);
 }
 
 // out[k] = sum_b partial[k * nblk + b] (fixed order, deterministic)
@@ -636,7 +655,7 @@ template <typename TV, typename TX>
 __global__ void __launch_bounds__(kRedThreads)
 multidot2_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restrict__ x0, const TX* __restrict__ x1,
                  size_t D, double* __restrict__ partial) {
-  __shared__ double sh[kRedThreads / 32];
+  __shared__ double sh[2 * kDotChunk * (kRedThreads / 32)];
   const int k0 = blockIdx.y * kDotChunk;
   const int mc = min(kDotChunk, m - k0);
   double a0[kDotChunk], a1[kDotChunk];
@@ -667,12 +686,10 @@ multidot2_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restri
         a1[k] = fma(v, y1, a1[k]);
       }
   }
-  for (int k = 0; k < mc; ++k) {
-    double t = block_sum(a0[k], sh);
-    if (threadIdx.x == 0) partial[(size_t)(2 * (k0 + k)) * gridDim.x + blockIdx.x] = t;
-    t = block_sum(a1[k], sh);
-    if (threadIdx.x == 0) partial[(size_t)(2 * (k0 + k) + 1) * gridDim.x + blockIdx.x] = t;
-  }
+  double both[2 * kDotChunk];  // rows 2k (x0) and 2k + 1 (x1)
+#pragma unroll
+  for (int k = 0; k < kDotChunk; ++k) { both[2 * k] = a0[k]; both[2 * k + 1] = a1[k]; }
+  block_sums<2 * kDotChunk>(both, 2 * mc, sh, partial, (size_t)(2 * k0));
 }
 
 // Classical Gram-Schmidt update: v -= o[0] W + sum_k o[k+1] V_k; partial |v|^2.
