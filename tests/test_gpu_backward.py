@@ -57,9 +57,9 @@ def test_autograd_matches_central_differences():
         E.backward()
         gh, ge = h_tri.grad.numpy().copy(), eri.grad.numpy().copy()
         rng = np.random.default_rng(5)
-        picks = [("h", int(i)) for i in rng.choice(len(h_tri), 16, replace=False)]
+        picks = [("h", int(i)) for i in rng.choice(len(h_tri), 32, replace=False)]
         nz = np.flatnonzero(np.abs(prob.eri) > 1e-3)
-        picks += [("e", int(i)) for i in rng.choice(nz, 16, replace=False)]
+        picks += [("e", int(i)) for i in rng.choice(nz, 32, replace=False)]  # 64 entries in all
         step = 1e-5
         for kind, i in picks:
             vals = []
