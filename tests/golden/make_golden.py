@@ -13,6 +13,9 @@ Every array in the fixtures is an output of the UNMODIFIED reference headers
                   one sigma (mult), Davidson energy and vector, 1-/2-RDM
                   (Correlation), and the tpb::diag outputs (energy, density,
                   carry-over strings) on the struct path;
+  * cfg1.npz : the CPU-runnable synthetic workload (400 x 400 strings,
+                  L = 24): the tpb::diag energy and density, and seeded
+                  projections and entries of one sigma (mult);
   * h2o_1em3.npz / n2_1em3.npz : the reference's own known-answer inputs
                   (data/h2o, data/n2 with the 1e-3 string files) as parsed by
                   LoadFCIDump/LoadAlphaDets, the integrals after the file path's
@@ -106,12 +109,30 @@ def kat(ref: Ref, mol, fcidump, adet, L):
     print(mol, len(alpha), "E_file", file_path["energy"], "E_struct", struct["energy"])
 
 
+def cfg1(ref: Ref):
+    """The CPU-runnable plain-FP64 workload (L=24, 5+5 electrons, 400 x 400
+    strings): tpb::diag energy (max subspace 16, tolerance 1e-8) and one
+    sigma of a seeded vector, kept as size-independent checks (seeded
+    projections and seeded entries) so that the fixture stays small."""
+    prob = synth.config("cfg1")
+    rng = np.random.default_rng(2024)
+    C = rng.standard_normal(prob.D)
+    S = ref.sigma(prob, C)
+    R = np.random.default_rng(2025).standard_normal((8, prob.D))
+    idx = np.random.default_rng(2026).choice(prob.D, 256, replace=False)
+    struct = ref.tpb_diag(prob, max_it=20, max_nb=16, eps=1e-8, do_rdm=0)
+    np.savez_compressed(os.path.join(HERE, "cfg1.npz"), proj=R @ S, norm=np.linalg.norm(S), idx=idx, entries=S[idx],
+                        E=struct["energy"], density=struct["density"])
+    print("cfg1", prob.D, "E", struct["energy"])
+
+
 def main():
     if not Ref.available():
         raise SystemExit("oracle/_ref/libsbdref.so missing: run make -C oracle ref")
     ref = Ref()
     for name, spec in SMALL.items():
         small(ref, name, spec)
+    cfg1(ref)
     kat(ref, "h2o", f"{REF}/data/h2o/fcidump.txt", f"{REF}/data/h2o/h2o-1em3-alpha.txt", 24)
     kat(ref, "n2", f"{REF}/data/n2/fcidump.txt", f"{REF}/data/n2/1em3-alpha.txt", 18)
 

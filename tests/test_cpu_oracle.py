@@ -70,6 +70,23 @@ def test_davidson_and_rdm_match_reference(name, port):
         assert abs(port.rdm_energy(prob, one, two) - float(g["E"])) < 1e-9
 
 
+def test_cfg1_sigma_and_energy_match_reference(port):
+    """The CPU-runnable workload (400 x 400 strings, L = 24): the oracle's
+    sigma of the seeded vector against the reference's seeded projections
+    and entries (1e-12 relative to |S|), and its FP64 Davidson energy (max
+    subspace 16, tolerance 1e-8) against the reference's tpb::diag (1e-9 Ha)."""
+    g = dict(np.load(os.path.join(GOLD, "cfg1.npz")))
+    prob = synth.config("cfg1")
+    C = np.random.default_rng(2024).standard_normal(prob.D)
+    R = np.random.default_rng(2025).standard_normal((8, prob.D))
+    norm = float(g["norm"])
+    S = port.sigma(prob, C)
+    assert np.abs(S[g["idx"]] - g["entries"]).max() <= 1e-12 * norm
+    assert np.abs(R @ S - g["proj"]).max() <= 1e-12 * norm * np.sqrt(prob.D)
+    E, _, _ = port.davidson(prob, max_it=20, max_nb=16, eps=1e-8)
+    assert abs(E - float(g["E"])) < 1e-9
+
+
 @pytest.mark.parametrize("name", SMALL)
 def test_tpb_diag_outputs(name, port):
     prob, g = load(name)

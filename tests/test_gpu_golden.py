@@ -53,6 +53,29 @@ def test_cuda_matches_reference_golden(name):
     assert set(prob.alpha[order[:kept]].tolist()) == set(g["diag_carry"].tolist())
 
 
+def test_cfg1_workload_against_reference():
+    """The CPU-runnable workload (L=24, 5+5 electrons, 400 x 400 strings)
+    against the compiled reference: one sigma of a seeded vector through 8
+    seeded projections and 256 seeded entries (1e-12 relative to |S|), the
+    plain FP64 Davidson energy (max subspace 16, tolerance 1e-8; 1e-9 Ha) and
+    the mixed-precision one (1e-8 Ha)."""
+    g = dict(np.load(os.path.join(GOLD, "cfg1.npz")))
+    prob = synth.config("cfg1")
+    C = np.random.default_rng(2024).standard_normal(prob.D)
+    R = np.random.default_rng(2025).standard_normal((8, prob.D))
+    norm = float(g["norm"])
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        S = ctx.sigma(C)
+        assert abs(np.linalg.norm(S) - norm) <= 1e-12 * norm
+        assert np.abs(S[g["idx"]] - g["entries"]).max() <= 1e-12 * norm
+        assert np.abs(R @ S - g["proj"]).max() <= 1e-12 * norm * np.sqrt(prob.D)
+        info, _ = ctx.davidson(max_it=20, max_nb=16, eps=1e-8)
+        assert info.converged == 1 and abs(info.energy - float(g["E"])) < 1e-9
+        info32, _ = ctx.davidson(max_it=20, max_nb=16, eps=1e-8, precision=sbdx.SBDX_FP32)
+        assert info32.converged == 1 and abs(info32.energy - float(g["E"])) < 1e-8
+
+
 @pytest.mark.parametrize("mol", ["h2o", "n2"])
 def test_known_answer_energies_cabi(mol):
     g = dict(np.load(os.path.join(GOLD, f"{mol}_1em3.npz")))
