@@ -198,6 +198,21 @@ class Ref:
                                       ctypes.c_int(threads), ctypes.byref(pairs))
         return t, pairs.value, S
 
+    def sigma_rows(self, prob, C, row0, rows, threads=0, bit_length=20):
+        """Off-diagonal part of the reference mult on the bra alpha rows
+        [row0, row0 + rows) with all kets (ref_sigma_sample_range: the
+        diagonal is zero there): rows x nb values, row-major."""
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        S = np.zeros(rows * prob.nb)
+        sec = np.zeros(1)
+        pairs = ctypes.c_double(0.0)
+        self.lib.ref_sigma_sample_range.restype = ctypes.c_double
+        self.lib.ref_sigma_sample_range(*self._ham(prob), ctypes.c_int(bit_length), _u(prob.alpha),
+                                        ctypes.c_size_t(prob.na), _u(prob.beta), ctypes.c_size_t(prob.nb), _d(C),
+                                        _d(S), ctypes.c_size_t(row0), ctypes.c_size_t(rows), ctypes.c_int(threads),
+                                        ctypes.c_int(1), _d(sec), ctypes.byref(pairs))
+        return S
+
     def rdm(self, prob, W, bit_length=20):
         L = prob.L
         one = np.zeros(2 * L * L)

@@ -16,6 +16,11 @@ Every array in the fixtures is an output of the UNMODIFIED reference headers
   * cfg1.npz : the CPU-runnable synthetic workload (400 x 400 strings,
                   L = 24): the tpb::diag energy and density, and seeded
                   projections and entries of one sigma (mult);
+  * cfg2_rows.npz : the headline workload (8000 x 8000 strings, L = 58):
+                  the reference mult on 16 bra alpha rows of a seeded vector,
+                  as seeded projections and entries;
+  * cfg4_rdm.npz : the differentiation workload (2000 x 2000 strings,
+                  L = 32): the Correlation 1-/2-RDM of a seeded unit vector;
   * h2o_1em3.npz / n2_1em3.npz : the reference's own known-answer inputs
                   (data/h2o, data/n2 with the 1e-3 string files) as parsed by
                   LoadFCIDump/LoadAlphaDets, the integrals after the file path's
@@ -126,6 +131,37 @@ def cfg1(ref: Ref):
     print("cfg1", prob.D, "E", struct["energy"])
 
 
+def cfg2_rows(ref: Ref, row0=3992, rows=16):
+    """The headline workload (L=58, 7+7 electrons, 8000 x 8000 strings, 64 M
+    determinants): the reference mult on bra alpha rows [row0, row0 + rows)
+    of a seeded vector (off-diagonal part; a whole sigma takes about an hour
+    on the host), kept as seeded projections and entries of those rows."""
+    prob = synth.config("cfg2")
+    C = np.random.default_rng(2027).standard_normal(prob.D)
+    S = ref.sigma_rows(prob, C, row0, rows)
+    R = np.random.default_rng(2028).standard_normal((8, S.size))
+    idx = np.random.default_rng(2029).choice(S.size, 256, replace=False)
+    np.savez_compressed(os.path.join(HERE, "cfg2_rows.npz"), row0=row0, rows=rows, proj=R @ S,
+                        norm=np.linalg.norm(S), idx=idx, entries=S[idx])
+    print("cfg2 rows", row0, rows, "norm", np.linalg.norm(S))
+
+
+def cfg4_rdm(ref: Ref):
+    """The differentiation workload (L=32, 6+6 electrons, 2000 x 2000
+    strings): the reference Correlation 1-/2-RDM of a seeded unit vector
+    (the RDMs are bilinear in W, so any vector tests the kernels): the
+    1-RDM whole, the 2-RDM as seeded projections and entries."""
+    prob = synth.config("cfg4")
+    W = np.random.default_rng(2030).standard_normal(prob.D)
+    W /= np.linalg.norm(W)
+    one, two = ref.rdm(prob, W)
+    R = np.random.default_rng(2031).standard_normal((8, two.size))
+    idx = np.random.default_rng(2032).choice(two.size, 512, replace=False)
+    np.savez_compressed(os.path.join(HERE, "cfg4_rdm.npz"), one=one, two_norm=np.linalg.norm(two), two_proj=R @ two,
+                        two_idx=idx, two_entries=two[idx])
+    print("cfg4 rdm", np.abs(one).max(), np.linalg.norm(two))
+
+
 def main():
     if not Ref.available():
         raise SystemExit("oracle/_ref/libsbdref.so missing: run make -C oracle ref")
@@ -133,6 +169,8 @@ def main():
     for name, spec in SMALL.items():
         small(ref, name, spec)
     cfg1(ref)
+    cfg2_rows(ref)
+    cfg4_rdm(ref)
     kat(ref, "h2o", f"{REF}/data/h2o/fcidump.txt", f"{REF}/data/h2o/h2o-1em3-alpha.txt", 24)
     kat(ref, "n2", f"{REF}/data/n2/fcidump.txt", f"{REF}/data/n2/1em3-alpha.txt", 18)
 

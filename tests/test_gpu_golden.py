@@ -76,6 +76,30 @@ def test_cfg1_workload_against_reference():
         assert info32.converged == 1 and abs(info32.energy - float(g["E"])) < 1e-8
 
 
+def test_cfg2_rows_against_reference():
+    """The headline workload (L=58, 7+7 electrons, 8000 x 8000 strings):
+    the FP64 sigma of a seeded 64 M-element vector, off-diagonal part of 16
+    bra alpha rows from the middle of the list, against the reference mult
+    on those rows (seeded projections and entries, 1e-12 relative to the
+    rows' norm)."""
+    g = dict(np.load(os.path.join(GOLD, "cfg2_rows.npz")))
+    row0, rows = int(g["row0"]), int(g["rows"])
+    prob = synth.config("cfg2")
+    C = np.random.default_rng(2027).standard_normal(prob.D)
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        S = ctx.sigma(C)
+        hii = ctx.diag_terms()
+    blk = slice(row0 * prob.nb, (row0 + rows) * prob.nb)
+    off = S[blk] - hii[blk] * C[blk]
+    del S, hii, C
+    norm = float(g["norm"])
+    R = np.random.default_rng(2028).standard_normal((8, off.size))
+    assert abs(np.linalg.norm(off) - norm) <= 1e-12 * norm
+    assert np.abs(off[g["idx"]] - g["entries"]).max() <= 1e-12 * norm
+    assert np.abs(R @ off - g["proj"]).max() <= 1e-12 * norm * np.sqrt(off.size)
+
+
 @pytest.mark.parametrize("mol", ["h2o", "n2"])
 def test_known_answer_energies_cabi(mol):
     g = dict(np.load(os.path.join(GOLD, f"{mol}_1em3.npz")))
