@@ -100,6 +100,25 @@ def test_cfg2_rows_against_reference():
     assert np.abs(R @ off - g["proj"]).max() <= 1e-12 * norm * np.sqrt(off.size)
 
 
+def test_cfg4_rdm_against_reference():
+    """The differentiation workload (L=32, 6+6 electrons, 2000 x 2000
+    strings): 1-/2-RDM of a seeded unit vector against the reference
+    Correlation (1-RDM whole, 2-RDM through seeded projections and entries;
+    1e-8 max-abs)."""
+    g = dict(np.load(os.path.join(GOLD, "cfg4_rdm.npz")))
+    prob = synth.config("cfg4")
+    W = np.random.default_rng(2030).standard_normal(prob.D)
+    W /= np.linalg.norm(W)
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        one, two = ctx.rdm(W)
+    assert np.abs(one - g["one"]).max() < 1e-8
+    assert np.abs(two[g["two_idx"]] - g["two_entries"]).max() < 1e-8
+    assert abs(np.linalg.norm(two) - float(g["two_norm"])) < 1e-8
+    R = np.random.default_rng(2031).standard_normal((8, two.size))
+    assert np.abs(R @ two - g["two_proj"]).max() < 1e-8 * np.sqrt(two.size)
+
+
 @pytest.mark.parametrize("mol", ["h2o", "n2"])
 def test_known_answer_energies_cabi(mol):
     g = dict(np.load(os.path.join(GOLD, f"{mol}_1em3.npz")))
