@@ -370,6 +370,7 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
   // ket index, so the kernels' shared-memory index stays in range
   const uint64_t kPad = (1ull << 41) | (uint64_t)jb0;
   std::vector<uint64_t> sell(soff[ns] ? soff[ns] : 1, kPad);
+  std::vector<uint8_t> vcopy(sell.size(), 0);  // integral copy of each record (packed kernel)
   std::vector<uint32_t> vrow(nv ? nv : 1, 0);
   // Record order inside each virtual row is free (it only changes the order of
   // the sum). Per slice, step m and quarter-warp (8 lanes, one 128-byte
@@ -447,9 +448,41 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
             }
           if (!better) break;
         }
+        // integral copy per pick: copy c puts pair index p in slot (p + 4c) mod 8
+        // (the packed kernel stages the integral row twice, four slots apart);
+        // the assignment with the fewest wavefronts of the quarter's integral
+        // gather, fewest copy-1 reads on ties
+        unsigned best_mask = 0;
+        {
+          int best_w = 1 << 30, best_ones = 99;
+          for (unsigned mask = 0; mask < (1u << nl); ++mask) {
+            int worst = 0;
+            for (int slot = 0; slot < 8; ++slot) {
+              uint32_t seen[8];
+              int nd = 0;
+              for (size_t i = 0; i < nl; ++i) {
+                const uint32_t c = (mask >> i) & 1u;
+                const uint32_t pq = (uint32_t)((left[lanes[i]][pick[i]] >> 16) & 0xfffu);
+                if (((pq + 4u * c) & 7u) != (uint32_t)slot) continue;
+                const uint32_t key = pq | (c << 12);
+                bool dup = false;
+                for (int d = 0; d < nd; ++d) dup |= seen[d] == key;
+                if (!dup) seen[nd++] = key;
+              }
+              worst = std::max(worst, nd);
+            }
+            const int ones = __builtin_popcount(mask);
+            if (worst < best_w || (worst == best_w && ones < best_ones)) {
+              best_w = worst;
+              best_ones = ones;
+              best_mask = mask;
+            }
+          }
+        }
         for (size_t i = 0; i < nl; ++i) {
           std::vector<uint64_t>& lst = left[lanes[i]];
           sell[soff[sl] + 32ull * m + lanes[i]] = lst[pick[i]];
+          vcopy[soff[sl] + 32ull * m + lanes[i]] = (uint8_t)((best_mask >> i) & 1u);
           lst.erase(lst.begin() + (std::ptrdiff_t)pick[i]);
         }
       }
@@ -476,7 +509,7 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
         const uint64_t r = sell[soff[sl] + 32ull * m + l];
         sell32[soff4[sl] + 128ull * (m >> 2) + 4 * l + (m & 3u)] =
             (uint32_t)(r & 0xffffu) | (uint32_t)(((r >> 16) & 0xfffu) << 16) | (uint32_t)(((r >> 40) & 1u) << 28) |
-            (uint32_t)(((r >> 41) & 1u) << 29);
+            (uint32_t)(((r >> 41) & 1u) << 29) | ((uint32_t)vcopy[soff[sl] + 32ull * m + l] << 30);
       }
   SBDX_CUDA(c, cudaMalloc(&P.sell32, sizeof(uint32_t) * sell32.size()));
   SBDX_CUDA(c, cudaMalloc(&P.soff4, sizeof(uint64_t) * (ns + 1)));
@@ -583,8 +616,9 @@ int build_one(Ctx* c, int spin) {
       if (rc) return rc;
       // ket-range panels when the packed alpha-beta kernel (16 bytes per ket
       // and per pair index, 8 per split slot) cannot stage a whole ket row
-      const size_t fixed = 16 * c->npair + sizeof(double) * kMaxSplitSlots;
-      if (16 * (n + c->npair) + sizeof(double) * (size_t)cn.bal.nslot > kAbSmemBudget && fixed < kAbSmemBudget) {
+      const size_t er = ab7_er_packs(c->npair);
+      const size_t fixed = 16 * er + sizeof(double) * kMaxSplitSlots;
+      if (16 * (n + er) + sizeof(double) * (size_t)cn.bal.nslot > kAbSmemBudget && fixed < kAbSmemBudget) {
         const size_t width = ((kAbSmemBudget - fixed) / 16) & ~(size_t)1;
         const size_t np = (n + width - 1) / width;
         const size_t w = (n + np - 1) / np;

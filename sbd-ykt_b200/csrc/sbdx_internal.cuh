@@ -46,7 +46,8 @@ constexpr uint32_t kInfoSingle = 1u << 30;
 struct SellPanel {
   uint64_t* sell = nullptr;        // [soff[nslice]]
   // the same records in 32 bits (bits 0-15 ket, 16-27 pair index, 28 sign,
-  // 29 padding), read by the packed alpha-beta kernel in blocks of 4 per lane:
+  // 29 padding, 30 integral copy), read by the packed alpha-beta kernel in
+  // blocks of 4 per lane:
   // record m of lane l of slice s at sell32[soff4[s] + 128*(m/4) + 4*l + m%4],
   // slen4[s] = slen[s] rounded up to a multiple of 4 (padding records)
   uint32_t* sell32 = nullptr;      // [soff4[nslice]]
@@ -127,6 +128,13 @@ constexpr int kMaxSplitSlots = 2048;
 constexpr size_t kAbSmemBudget = 227 * 1024 - 1024;
 // n rounded up to a multiple of 8 (row strides of padded vectors and tables).
 constexpr size_t pad8(size_t n) { return (n + 7) / 8 * 8; }
+// The packed alpha-beta kernel stages its integral row twice: copy 0 at pack
+// index pq, copy 1 at ab7_epad(npair) + pq with ab7_epad = 4 (mod 8), i.e.
+// four 16-byte bank slots further on, so that a record can read whichever
+// copy collides less with the other lanes of its quarter-warp (bit 30 of
+// the 32-bit record). Packs of both copies: ab7_er_packs.
+constexpr size_t ab7_epad(size_t npair) { return (npair + 3) / 8 * 8 + 4; }
+constexpr size_t ab7_er_packs(size_t npair) { return ab7_epad(npair) + npair; }
 
 // Stored Hamiltonian (the reference's method 1): off-diagonal elements in CSR
 // over determinant rows, basis phases folded into the values (stored.cu).

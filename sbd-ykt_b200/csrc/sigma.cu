@@ -1407,7 +1407,7 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
                    const uint64_t* __restrict__ soff4, const uint32_t* __restrict__ slen4, size_t nslice,
                    const uint32_t* __restrict__ vrow, size_t nv, const uint32_t* __restrict__ split_row,
                    const uint32_t* __restrict__ split_slot, int nsplit, const T* __restrict__ Vt, size_t vstride,
-                   int npair, uint32_t jb0, size_t nbp, const uint4* __restrict__ items,
+                   int npair, uint32_t epad, uint32_t jb0, size_t nbp, const uint4* __restrict__ items,
                    double* __restrict__ ypart, double* __restrict__ Y) {
   using RP = RowPack<T>;
   using P = typename RP::P;
@@ -1415,8 +1415,8 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
   constexpr int kWarps = kAb6Threads / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   P* xs = reinterpret_cast<P*>(smem);   // [nbp]: ket indices jb0 .. jb0 + nbp - 1
-  P* er = xs + nbp;                     // [npair]
-  double* part = reinterpret_cast<double*>(er + npair);
+  P* er = xs + nbp;                     // [epad + npair]: copy 0 at pq, copy 1 at epad + pq
+  double* part = reinterpret_cast<double*>(er + epad + npair);
   // work item: bra alpha string, range of its singles, output row
   const uint4 item = items[blockIdx.x];
   const size_t ia = item.x;
@@ -1459,13 +1459,14 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
         RP::set(p, e, neg[e] ? -v : v);
       }
       er[t] = p;
+      er[epad + t] = p;
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < KS; ++k) {
       const size_t sl = slice_of(k);
       if (sl >= nslice) continue;
-      // 32-bit records (bits 0-15 ket, 16-27 pair, 28 sign, 29 pad), four per
+      // 32-bit records (bits 0-15 ket, 16-27 pair, 28 sign, 29 pad, 30 integral copy), four per
       // lane per 16-byte load, the next block in flight
       const uint32_t nblk = slen4[sl] >> 2;
       const uint4* rp = reinterpret_cast<const uint4*>(sell + soff4[sl]) + lane;
@@ -1478,7 +1479,7 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
         for (int q = 0; q < 4; ++q) {
           const uint32_t rec = recs[q];
           const P x = xs[(rec & 0xffffu) - jb0];  // pad records: ket = jb0
-          const P ev = er[(rec >> 16) & 0xfffu];
+          const P ev = er[((rec >> 16) & 0xfffu) + ((rec >> 30) & 1u) * epad];
           double d = RP::dot(ev, x);
           d = ((rec >> 29) & 1u) ? 0.0 : d;
           s += flip_sign(d, (rec >> 28) & 1u);
@@ -1509,12 +1510,12 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
   }
 }
 
-// Shared memory of v7 on one panel: its ket range and npair 16-byte packs
-// plus its split slots. (The kernels' dynamic shared-memory limit is always set
+// Shared memory of v7 on one panel: its ket range, the two copies of the
+// integral row (ab7_er_packs 16-byte packs) and its split slots. (The kernels' dynamic shared-memory limit is always set
 // to the full budget: the attribute is global per kernel, and contexts on
 // other host threads launch the same kernel with other sizes.)
 size_t ab7_smem_bytes(const Ctx* c, const SellPanel& p) {
-  return 16 * ((size_t)(p.jb1 - p.jb0) + c->npair) + sizeof(double) * (size_t)p.nslot;
+  return 16 * ((size_t)(p.jb1 - p.jb0) + ab7_er_packs(c->npair)) + sizeof(double) * (size_t)p.nslot;
 }
 
 // The panels v7 runs on: the whole ket range, or the ket-range slices.
@@ -1546,8 +1547,8 @@ int launch_ab_v7(Ctx* c, const T* Xp, const SellPanel& bp) {
   if (grid.y == 0) grid.y = 1;
   sigma_ab_v7_kernel<T, KS><<<grid, kAb6Threads, smem, c->stream>>>(
       Xp, c->xsa, ca.off, ca.ket, ca.info, bp.sell32, bp.soff4, bp.slen4, bp.nslice, bp.vrow, bp.nv,
-      bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, (int)c->npair, bp.jb0, (size_t)(bp.jb1 - bp.jb0),
-      ca.ab_item, ca.ypart, c->d_y);
+      bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, (int)c->npair, (uint32_t)ab7_epad(c->npair), bp.jb0,
+      (size_t)(bp.jb1 - bp.jb0), ca.ab_item, ca.ypart, c->d_y);
   SBDX_LAUNCHED(c);
   return 0;
 }
