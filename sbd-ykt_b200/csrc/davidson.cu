@@ -651,8 +651,11 @@ olsen_apply_kernel(double* __restrict__ v, const double* __restrict__ W, const d
 
 // partial[(2k + i) * gridDim.x + blk] = partial sums of <V_k, x_i>, i = 0, 1,
 // k in [k0, k0+mc): two projections with one read of V.
+// FP32 vectors: held to 4 CTAs per SM (64 registers) for more loads in
+// flight; it is bound by load latency (measured: 3 CTAs per SM at 80
+// registers, 36% of warps active, long-scoreboard stalls).
 template <typename TV, typename TX>
-__global__ void __launch_bounds__(kRedThreads)
+__global__ void __launch_bounds__(kRedThreads, sizeof(TV) == 4 ? 4 : 1)
 multidot2_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restrict__ x0, const TX* __restrict__ x1,
                  size_t D, double* __restrict__ partial) {
   __shared__ double sh[2 * kDotChunk * (kRedThreads / 32)];
