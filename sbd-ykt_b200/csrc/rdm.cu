@@ -415,7 +415,7 @@ int occupation_device(Ctx* c, const double* dW, double* d_density) {
   const size_t na = c->na, nb = c->nb, L = (size_t)c->L, L2 = L * L;
   Scratch sc;
   SBDX_CUDA(c, cudaMalloc(&sc.p, sizeof(double) * (na + nb + 3 * L2)));
-  double *wa = sc.p, *wb = wa + na, *Pa = wb + nb, *Pb = Pa + L2, *X = Pb + L2;
+  double *wa = sc.p, *wb = wa + na, *Pa = wb + nb, *Pb = Pa + L2;  // (the third L2 block is unused here)
   SBDX_CUDA(c, cudaMemsetAsync(Pa, 0, sizeof(double) * 3 * L2, c->stream));
   if ((rc = weights(c, dW, wa, wb, Pa, Pb, nullptr, reinterpret_cast<double*>(c->d_xt)))) return rc;
   // density[2p] = Pa[p][p], density[2p+1] = Pb[p][p]
@@ -424,7 +424,6 @@ int occupation_device(Ctx* c, const double* dW, double* d_density) {
   SBDX_CUDA(c, cudaMemcpyAsync(pb.data(), Pb, sizeof(double) * L2, cudaMemcpyDeviceToHost, c->stream));
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
   for (size_t p = 0; p < L; ++p) { dens[2 * p] = pa[p * L + p]; dens[2 * p + 1] = pb[p * L + p]; }
-  (void)X;
   SBDX_CUDA(c, cudaMemcpyAsync(d_density, dens.data(), sizeof(double) * 2 * L, cudaMemcpyHostToDevice, c->stream));
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
   return 0;
