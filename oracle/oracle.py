@@ -97,6 +97,17 @@ class Port:
                            _d(hii), _d(C), _d(out))
         return out
 
+    def sigma_rows(self, prob, C, row0, rows):
+        """Off-diagonal part of the bra alpha rows [row0, row0 + rows) of
+        sigma: rows x nb values, row-major."""
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        rows = min(rows, prob.na - row0)
+        out = np.zeros(rows * prob.nb)
+        self.lib.sbo_sigma_rows(ctypes.c_int(prob.L), ctypes.c_double(prob.I0), _d(prob.h), _d(prob.eri),
+                                _u(prob.alpha), ctypes.c_size_t(prob.na), _u(prob.beta), ctypes.c_size_t(prob.nb),
+                                _d(C), ctypes.c_size_t(row0), ctypes.c_size_t(rows), _d(out))
+        return out
+
     def davidson(self, prob, max_it=1, max_nb=10, eps=1e-4, W=None):
         D = prob.na * prob.nb
         if W is None:

@@ -193,15 +193,18 @@ void sbo_diag_terms(int L, double I0, const double* h, const double* eri, const 
 /* mult (mult.h:376-632) at world size 1: diagonal, then task type 2 (alpha
  * singles, alpha doubles), type 1 (beta singles, beta doubles), type 0
  * (alpha single x beta single), accumulated per bra element in that order. */
+/* Rows [ia0, ia1) of sigma into S[(ia - ia0) * nb + ib]; hii == NULL leaves
+ * out the diagonal term. */
 static void sigma_conn(int L, double I0, const double* h, const double* eri, const uint64_t* a, size_t na,
                        const uint64_t* b, size_t nb, const conn_t* ca, const conn_t* cb, const double* hii,
-                       const double* C, double* S) {
+                       const double* C, double* S, size_t ia0, size_t ia1) {
+  (void)na;
 #pragma omp parallel for schedule(dynamic, 1)
-  for (long long ia = 0; ia < (long long)na; ++ia) {
+  for (long long ia = (long long)ia0; ia < (long long)ia1; ++ia) {
     for (size_t ib = 0; ib < nb; ++ib) {
       size_t bra = (size_t)ia * nb + ib;
       u128 DI = interleave(a[ia], b[ib]);
-      double acc = hii[bra] * C[bra];
+      double acc = hii ? hii[bra] * C[bra] : 0.0;
       for (uint64_t k = ca->off[ia]; k < ca->off[ia + 1]; ++k) {
         size_t ja = ca->idx[k];
         acc += hij128(DI, interleave(a[ja], b[ib]), L, I0, h, eri) * C[ja * nb + ib];
@@ -217,7 +220,7 @@ static void sigma_conn(int L, double I0, const double* h, const double* eri, con
           acc += hij128(DI, interleave(a[ja], b[jb]), L, I0, h, eri) * C[ja * nb + jb];
         }
       }
-      S[bra] = acc;
+      S[bra - ia0 * nb] = acc;
     }
   }
 }
@@ -231,8 +234,22 @@ void sbo_sigma(int L, double I0, const double* h, const double* eri, const uint6
     sbo_diag_terms(L, I0, h, eri, a, na, b, nb, d);
     hii = d;
   }
-  sigma_conn(L, I0, h, eri, a, na, b, nb, &ca, &cb, hii, C, S);
+  sigma_conn(L, I0, h, eri, a, na, b, nb, &ca, &cb, hii, C, S, 0, na);
   free(d);
+  free_conn(&ca);
+  free_conn(&cb);
+}
+
+/* Off-diagonal part of the bra alpha rows [row0, row0 + rows) of sigma (all
+ * kets), rows x nb values: what the reference mult computes for a bra block
+ * with a zero diagonal (checks of large problems one block of rows at a
+ * time). */
+void sbo_sigma_rows(int L, double I0, const double* h, const double* eri, const uint64_t* a, size_t na,
+                    const uint64_t* b, size_t nb, const double* C, size_t row0, size_t rows, double* S) {
+  if (row0 >= na) return;
+  if (rows > na - row0) rows = na - row0;
+  conn_t ca = make_conn(a, na), cb = make_conn(b, nb);
+  sigma_conn(L, I0, h, eri, a, na, b, nb, &ca, &cb, NULL, C, S, row0, row0 + rows);
   free_conn(&ca);
   free_conn(&cb);
 }
@@ -335,7 +352,7 @@ double sbo_davidson(int L, double I0, const double* h, const double* eri, const 
     for (int ib = 0; ib < nbk; ++ib) {
       double* Cb = C + (size_t)ib * D;
       double* HCb = HC + (size_t)ib * D;
-      sigma_conn(L, I0, h, eri, a, na, b, nb, &ca, &cb, hii, Cb, HCb);
+      sigma_conn(L, I0, h, eri, a, na, b, nb, &ca, &cb, hii, Cb, HCb, 0, na);
       ++nsig;
       for (int jb = 0; jb <= ib; ++jb) {
         Hs[jb + nbk * ib] = kdot(C + (size_t)jb * D, HCb, D);
@@ -376,7 +393,7 @@ double sbo_davidson(int L, double I0, const double* h, const double* eri, const 
     memcpy(C, w, sizeof(double) * D);
   }
   double* S = HC; /* reuse */
-  sigma_conn(L, I0, h, eri, a, na, b, nb, &ca, &cb, hii, w, S);
+  sigma_conn(L, I0, h, eri, a, na, b, nb, &ca, &cb, hii, w, S, 0, na);
   ++nsig;
   double Efin = kdot(w, S, D);
   if (n_sigma) *n_sigma = nsig;

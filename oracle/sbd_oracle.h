@@ -45,6 +45,11 @@ void sbo_diag_terms(int L, double I0, const double* h, const double* eri, const 
 void sbo_sigma(int L, double I0, const double* h, const double* eri, const uint64_t* a, size_t na,
                const uint64_t* b, size_t nb, const double* hii, const double* C, double* S);
 
+/* Off-diagonal part of the bra alpha rows [row0, row0 + rows) of sigma,
+ * rows x nb values (the reference mult on a bra block with zero diagonal). */
+void sbo_sigma_rows(int L, double I0, const double* h, const double* eri, const uint64_t* a, size_t na,
+                    const uint64_t* b, size_t nb, const double* C, size_t row0, size_t rows, double* S);
+
 /* Davidson (davidson.h:661-924) + final <W|HW> (sbdiag.h:250-273).
  * W: in = start vector (NULL -> e_0), out = final normalised vector.
  * Returns the energy; *n_sigma receives the number of sigma products. */

@@ -87,6 +87,23 @@ def test_cfg1_sigma_and_energy_match_reference(port):
     assert abs(E - float(g["E"])) < 1e-9
 
 
+def test_cfg2_rows_match_reference(port):
+    """The headline workload (L=58, 7+7 electrons, 8000 x 8000 strings): the
+    oracle's off-diagonal sigma on 16 bra alpha rows of the seeded vector
+    against the reference mult on the same rows (seeded projections and
+    entries, 1e-12 relative to the rows' norm)."""
+    g = dict(np.load(os.path.join(GOLD, "cfg2_rows.npz")))
+    prob = synth.config("cfg2")
+    C = np.random.default_rng(2027).standard_normal(prob.D)
+    S = port.sigma_rows(prob, C, int(g["row0"]), int(g["rows"]))
+    del C
+    norm = float(g["norm"])
+    R = np.random.default_rng(2028).standard_normal((8, S.size))
+    assert abs(np.linalg.norm(S) - norm) <= 1e-12 * norm
+    assert np.abs(S[g["idx"]] - g["entries"]).max() <= 1e-12 * norm
+    assert np.abs(R @ S - g["proj"]).max() <= 1e-12 * norm * np.sqrt(S.size)
+
+
 @pytest.mark.parametrize("name", SMALL)
 def test_tpb_diag_outputs(name, port):
     prob, g = load(name)
