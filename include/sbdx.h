@@ -146,7 +146,10 @@ int sbdx_diag_terms(sbdx_ctx* ctx, double* hii);
  * each call writes every scratch word before reading it.
  * The first call on each device (with that device current) looks up the
  * array's device address with cudaGetSymbolAddress, which may initialise the
- * CUDA context; make that first call before any stream capture begins.
+ * CUDA context; make that first call before any stream capture begins. The
+ * address is cached per device ordinal, so the entry point assumes the
+ * device's primary context (the one the CUDA runtime uses); a caller that
+ * switches between its own driver contexts on one device must not use it.
  * All calls on one device share the array: calls that can overlap (on
  * different streams, or from several host threads) race and give wrong
  * results; serialise them on one stream. Asynchronous: synchronise the stream

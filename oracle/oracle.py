@@ -42,8 +42,14 @@ def build_port() -> str:
     return PORT_SO
 
 
-def build_ref(ref_root: str = "/root/reference") -> str | None:
+def reference_root() -> str:
+    """Root of the reference tree: $SBD_REFERENCE, else this container's mount."""
+    return os.environ.get("SBD_REFERENCE", "/root/reference")
+
+
+def build_ref(ref_root: str | None = None) -> str | None:
     """Compile the reference checker when the reference tree is present."""
+    ref_root = ref_root or reference_root()
     if not os.path.isdir(os.path.join(ref_root, "include", "sbd")):
         return None
     subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"], check=True)
@@ -281,3 +287,23 @@ class Ref:
         self.lib.ref_fcidump_roundtrip(path.encode(), ctypes.byref(Lv), ctypes.byref(Nv), ctypes.byref(I0), _d(h), _d(eri),
                                        ctypes.c_longlong(n))
         return L, Nv.value, I0.value, h, eri
+
+    def save_wavefunction(self, file, alpha, beta, L, W, bit_length=20):
+        """Reference SaveWavefunction (restart.h:20-67): writes file + '000000'."""
+        a = np.ascontiguousarray(alpha, dtype=np.uint64)
+        b = np.ascontiguousarray(beta, dtype=np.uint64)
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        assert W.size == len(a) * len(b)
+        self.lib.ref_save_wavefunction(file.encode(), _u(a), ctypes.c_size_t(len(a)), _u(b), ctypes.c_size_t(len(b)),
+                                       ctypes.c_int(L), ctypes.c_int(bit_length), _d(W))
+
+    def load_wavefunction(self, file, alpha, beta, L, bit_length=20):
+        """Reference LoadWavefunction (restart.h:414-657) onto the basis (alpha, beta)."""
+        a = np.ascontiguousarray(alpha, dtype=np.uint64)
+        b = np.ascontiguousarray(beta, dtype=np.uint64)
+        W = np.zeros(len(a) * len(b))
+        rc = self.lib.ref_load_wavefunction(file.encode(), _u(a), ctypes.c_size_t(len(a)), _u(b),
+                                            ctypes.c_size_t(len(b)), ctypes.c_int(L), ctypes.c_int(bit_length), _d(W))
+        if rc != 0:
+            raise RuntimeError("reference LoadWavefunction returned a vector of the wrong size")
+        return W

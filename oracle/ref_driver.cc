@@ -382,4 +382,30 @@ int ref_fcidump_roundtrip(const char* path, int* L_out, int* nelec_out, double* 
   return (int)I2.store.size();
 }
 
+// Reference SaveWavefunction (chemistry/tpb/restart.h:20-67) at world size 1:
+// writes file + "000000".
+int ref_save_wavefunction(const char* file, const uint64_t* astr, size_t na, const uint64_t* bstr, size_t nb,
+                          int L, int bit_length, const double* W) {
+  const size_t bl = (size_t)bit_length;
+  Dets a = to_words(astr, na, L, bl), b = to_words(bstr, nb, L, bl);
+  std::vector<double> w(W, W + na * nb);
+  MPI_Comm h_comm = 0, b_comm = 0, t_comm = 0;
+  sbd::SaveWavefunction(std::string(file), a, b, 1, 1, h_comm, b_comm, t_comm, w);
+  return 0;
+}
+
+// Reference LoadWavefunction (chemistry/tpb/restart.h:414-657) at world size 1
+// onto the basis (astr, bstr): W receives na*nb doubles.
+int ref_load_wavefunction(const char* file, const uint64_t* astr, size_t na, const uint64_t* bstr, size_t nb,
+                          int L, int bit_length, double* W) {
+  const size_t bl = (size_t)bit_length;
+  Dets a = to_words(astr, na, L, bl), b = to_words(bstr, nb, L, bl);
+  std::vector<double> w;
+  MPI_Comm h_comm = 0, b_comm = 0, t_comm = 0;
+  sbd::LoadWavefunction(std::string(file), a, b, 1, 1, h_comm, b_comm, t_comm, w);
+  if (w.size() != na * nb) return 1;
+  std::memcpy(W, w.data(), sizeof(double) * na * nb);
+  return 0;
+}
+
 }  // extern "C"

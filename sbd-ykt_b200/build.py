@@ -38,13 +38,28 @@ def _stale(target: str, sources: list[str]) -> bool:
 
 
 def build_lib(force: bool = False) -> str:
+    """Compiles every csrc/*.cu to an object (in parallel, under _build/) and
+    links libsbdx.so; sources whose object is newer than them and than the
+    shared headers are not recompiled."""
     srcs = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
-    deps = srcs + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [os.path.join(ROOT, "include", "sbdx.h")]
-    if not force and not _stale(LIB, deps):
+    hdrs = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [os.path.join(ROOT, "include", "sbdx.h")]
+    if not force and not _stale(LIB, srcs + hdrs):
         return LIB
-    cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-ccbin", host_cxx(), "-I" + os.path.join(ROOT, "include"), "-o", LIB, *srcs]
-    subprocess.run(cmd, check=True)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", host_cxx(),
+             "-I" + os.path.join(ROOT, "include")]
+    objs, jobs = [], []
+    for src in srcs:
+        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [src] + hdrs):
+            jobs.append([nvcc(), *flags, "-c", "-o", obj, src])
+    procs = [subprocess.Popen(cmd) for cmd in jobs]
+    failed = [cmd[-1] for cmd, p in zip(jobs, procs) if p.wait() != 0]
+    if failed:
+        raise RuntimeError("nvcc failed on " + ", ".join(os.path.basename(f) for f in failed))
+    subprocess.run([nvcc(), *ARCH, "-shared", "-ccbin", host_cxx(), "-o", LIB, *objs], check=True)
     return LIB
 
 

@@ -250,15 +250,29 @@ inline void LoadWavefunction(const std::string& file, const std::vector<std::vec
                              const std::vector<std::vector<size_t>>& bdet, std::vector<double>& W) {
   std::ifstream in(file + to_padded_string(0, 6), std::ios::binary);
   if (!in.is_open()) throw std::runtime_error("failed to open input file " + file + to_padded_string(0, 6));
+  const std::string name = file + to_padded_string(0, 6);
+  auto need = [&](bool ok, const char* what) {
+    if (!ok) throw std::runtime_error("LoadWavefunction: " + name + ": " + what);
+  };
   size_t na = 0, nb = 0, len = 0;
   in.read(reinterpret_cast<char*>(&na), sizeof(size_t));
   in.read(reinterpret_cast<char*>(&nb), sizeof(size_t));
   in.read(reinterpret_cast<char*>(&len), sizeof(size_t));
+  need((bool)in, "file shorter than its 3-word header");
+  // the header must describe exactly the bytes that follow
+  in.seekg(0, std::ios::end);
+  const std::streamoff total = in.tellg();
+  in.seekg((std::streamoff)(3 * sizeof(size_t)), std::ios::beg);
+  const long double body = (long double)(na + nb) * len * sizeof(size_t) + (long double)na * nb * sizeof(double);
+  need(len >= 1 && len <= 64 && body == (long double)(total - (std::streamoff)(3 * sizeof(size_t))),
+       "header (alpha count, beta count, words per string) does not match the file size");
   std::vector<std::vector<size_t>> la(na, std::vector<size_t>(len)), lb(nb, std::vector<size_t>(len));
   for (auto& d : la) in.read(reinterpret_cast<char*>(d.data()), (std::streamsize)(sizeof(size_t) * len));
   for (auto& d : lb) in.read(reinterpret_cast<char*>(d.data()), (std::streamsize)(sizeof(size_t) * len));
+  need((bool)in, "short read of the strings");
   std::vector<double> lw(na * nb);
   in.read(reinterpret_cast<char*>(lw.data()), (std::streamsize)(sizeof(double) * lw.size()));
+  need((bool)in, "short read of the wavefunction");
   W.assign(adet.size() * bdet.size(), 0.0);
   std::vector<long long> ma(na, -1), mb(nb, -1);
   for (size_t i = 0; i < na; ++i) {

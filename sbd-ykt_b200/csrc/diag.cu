@@ -251,6 +251,11 @@ extern "C" int sbdx_diag_terms_noalloc(int norb, double I0, const double* d_h, c
     double* Eb = Ea + na;
     double* Jb = Eb + nb;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // A launch error that unrelated earlier work left pending on this host
+    // thread would otherwise be reported as ours by the check after the
+    // launches: clear it first (an error that ruined the context persists and
+    // is still reported).
+    (void)cudaGetLastError();
     string_energy_masked_kernel<<<(unsigned)((na + 127) / 128), 128, 0, st>>>(d_alpha, na, norb, d_h, d_eri, Ea);
     string_energy_masked_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, st>>>(d_beta, nb, norb, d_h, d_eri, Eb);
     const size_t nj = nb * (size_t)norb;

@@ -599,6 +599,7 @@ sigma_ab_v4_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
   double acc[kAb2Slots];
 #pragma unroll
   for (int k = 0; k < kAb2Slots; ++k) acc[k] = 0.0;
+  int g_abort = -1;  // group whose wait timed out (the same in every thread)
   for (int g = 0; g < ngroups; ++g) {
     const int b = g & 1;
     const int nr = min(R, ns - g * R);
@@ -607,7 +608,7 @@ sigma_ab_v4_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
       s_abort = 1;
     }
     __syncthreads();
-    if (s_abort) break;
+    if (s_abort) { g_abort = g; break; }
     const T* xs = reinterpret_cast<const T*>(smem + (size_t)b * bufbytes);
     const V* erow = reinterpret_cast<const V*>(smem + (size_t)b * bufbytes + (size_t)R * xbytes);
     uint64_t P[R], M[R];
@@ -656,10 +657,15 @@ sigma_ab_v4_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
       issue(g + 2);
     }
   }
-  if (s_abort) {
-    // leave no bulk copy in flight into this CTA's shared memory
+  if (g_abort >= 0) {
+    // Leave no bulk copy in flight into this CTA's shared memory. The groups
+    // still outstanding are g_abort (its wait timed out) and g_abort + 1 when
+    // it was issued; group q completes phase (q >> 1) & 1 of barrier q & 1.
+    // Groups before g_abort were all waited for, and g_abort + 2 was never
+    // issued (issue(g + 2) follows a completed group g).
     if (threadIdx.x == 0)
-      for (int b = 0; b < 2; ++b) mbar_wait_bounded(&bar[b], 0u, kWaitLimit);
+      for (int q = g_abort; q < min(g_abort + 2, ngroups); ++q)
+        mbar_wait_bounded(&bar[q & 1], (uint32_t)((q >> 1) & 1), kWaitLimit);
     return;
   }
 #pragma unroll

@@ -150,6 +150,11 @@ int build_stored(Ctx* c) {
   if (!c->have_hii) { int rc = diag_terms(c); if (rc) return rc; }
   release_stored(c);
   const size_t na = c->na, nb = c->nb, D = na * nb;
+  if (D > (size_t)UINT32_MAX) {  // the columns are 32-bit determinant indices
+    c->err = "build_hamiltonian: " + std::to_string(D) +
+             " determinants exceed the 32-bit column indices of the stored matrix (at most 4294967295)";
+    return SBDX_ERR_ARG;
+  }
   const Conn& ca = c->conn[0];
   const Conn& cb = c->conn[1];
   StoredH& H = c->stored;

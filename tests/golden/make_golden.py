@@ -37,10 +37,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path[:0] = [os.path.join(ROOT, "oracle"), os.path.join(ROOT, "sbd-ykt_b200")]
 
-from oracle import Ref  # noqa: E402
+from oracle import Ref, reference_root  # noqa: E402
 from sbdx import synth  # noqa: E402
 
-REF = "/root/reference"
+REF = reference_root()  # $SBD_REFERENCE, else the mounted tree
 
 SMALL = {
     # name: (L, n_alpha, n_beta, Na, Nb, seed)
