@@ -13,12 +13,19 @@ C (512 MB) is larger than the 126 MB L2, so no flush is needed between steps.
 `e2e` times the same product through the C-ABI call sbdx_sigma with pinned
 host buffers, the host->device copy of C and the device->host copy of S inside
 every step. `roofline` describes the dominant kernel of the sigma (the
-alpha-beta kernel): its algorithmic bytes per launch, one vector gather per
-alpha-single x beta-single pair plus the read-modify-write of the partial
-sigma (P_ab*s_c + 16*D), over its CUDA-event time, against the measured HBM
-copy bandwidth; `roofline.sigma` gives the same for the whole sigma with
+alpha-beta kernel), which gathers from rows staged in shared memory and is
+bound by the shared-memory pipe: its conflict-free shared bytes per launch
+(one ket and one integral element per alpha-single x beta-single det-pair,
+2*s_c*P_ab) over its CUDA-event time, against 128 bytes per clock per SM at
+the sampled SM clock. `roofline.hbm` keeps the SpMV byte model (one vector
+gather per pair plus the partial-sigma read-modify-write, P_ab*s_c + 16*D)
+against the measured HBM copy bandwidth, and the DRAM bytes ncu measured;
+`roofline.sigma` gives the model for the whole sigma,
 B = P*s_c + D*(2*s_c + s_h) + 4*(connectivity entries) + 8*(na + nb). The CPU baseline is the reference's own
 OpenMP mult (compiled in oracle/_ref) on a bounded sample of bra alpha rows.
+`mixed_precision` runs the 400 M-determinant workload (2 roots) in FP64 and
+mixed precision with energy and 1-RDM errors; `summary`, printed last, holds
+the headline figures.
 
 Multi-GPU: the path is run at MPI world size 1; --gpus N runs N independent
 replicas (one process per GPU) and reports the whole-job det-pairs/s.
@@ -69,6 +76,9 @@ def parse_args():
     ap.add_argument("--diff-entries", type=int, default=4, help="entries checked by central differences")
     ap.add_argument("--stored", default="cfg4", metavar="WORKLOAD",
                     help="workload of the stored-Hamiltonian (method 1) measurement ('' = skip)")
+    ap.add_argument("--mixed", default="cfg3", metavar="WORKLOAD",
+                    help="workload of the mixed-precision measurement (2 roots, FP64 block solve vs mixed with "
+                         "refresh every 4 steps and adaptive; '' = skip)")
     ap.add_argument("--tune", default=None, metavar="SAME,AB",
                     help="fixed sigma launch codes for both precisions instead of the autotuner (profiling runs)")
     return ap.parse_args()
@@ -88,6 +98,16 @@ def peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def smem_peak_gbs(sm_mhz: float) -> float:
+    """Shared-memory bandwidth of the whole GPU: 128 bytes per clock per SM
+    (one 128-byte wavefront per cycle) x SMs x the SM clock sampled during
+    the timed region."""
+    import torch
+
+    nsm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    return 128.0 * nsm * sm_mhz * 1e6 / 1e9
 
 
 class ClockSampler:
@@ -194,7 +214,15 @@ def roofline_bytes(prob, dp, s_c: int, s_h: int = 8) -> float:
 
 # CUDA kernel of each sigma phase (alpha-first path) and its ncu summary file
 PHASE_KERNELS = {"alpha_same_spin": "sigma_same_v6", "transpose": "phase_split", "beta_same_spin": "sigma_same_v6",
-                 "alpha_beta": "sigma_ab_v6", "combine": "combine_phase"}
+                 "alpha_beta": "sigma_ab_v7", "combine": "combine_phase"}
+
+
+def ab_smem_bytes(dp, s_c: int) -> float:
+    """Shared-memory bytes the alpha-beta kernel must load: per alpha-single x
+    beta-single det-pair one element of the staged ket row and one of the
+    staged integral row (2 * s_c), at one 128-byte wavefront per 8 lanes of a
+    16-byte load, i.e. without bank conflicts."""
+    return 2.0 * s_c * dp["alpha_beta"]
 
 
 def phase_bytes(prob, dp, s_c: int) -> dict:
@@ -413,6 +441,53 @@ def run_differentiation(args) -> dict:
     return out
 
 
+def run_mixed(args) -> dict:
+    """The mixed-precision workload (L=58, 7+7 electrons, 20000 x 20000
+    strings, 400 M determinants): the 2 lowest roots to the Davidson tolerance
+    with the FP64 block solver (FP64 corrections) and with the mixed solver
+    (FP32-stored corrections, FP32-storage sigmas with FP64 row accumulation,
+    FP64 anchors refreshed by exact FP64 sigmas every 4 steps, and with the
+    adaptive refresh). Per root: |dE| and the max-abs difference of the 1-RDM
+    of the mixed vector against the 1-RDM of the FP64 vector, all on the
+    device (the vectors never leave it)."""
+    import torch
+
+    import sbdx
+    from sbdx import synth
+
+    w, _, sc = args.mixed.partition("@")
+    prob = synth.config(w, float(sc) if sc else 1.0)
+    out = {"workload": args.mixed, "desc": workload_desc(args.mixed), "dets": int(prob.D), "nroots": 2,
+           "tol": args.davidson_tol, "max_nb": 12}
+    with sbdx.Context(torch.cuda.current_device()) as ctx:
+        ctx.load(prob)
+        t0 = time.perf_counter()
+        ctx.build_connectivity()
+        out["connectivity_seconds"] = time.perf_counter() - t0
+        out["tuning"] = ctx.autotune()
+        sa, da, _ = ctx.connectivity(0)
+        sb, db, _ = ctx.connectivity(1)
+        out["det_pairs_per_sigma"] = synth.det_pairs(sa, da, sb, db)["total"]
+
+        def solve(precision, defect_every):
+            info, E, R, _ = ctx.davidson_roots(2, max_it=100, max_nb=12, eps=args.davidson_tol, precision=precision,
+                                               defect_every=defect_every, to_host=False)
+            one = [ctx.rdm_device(ctx.wavefunction_device(r), two=False)[0] for r in range(2)]
+            return info, E, R, one
+
+        f64, E64, R64, one64 = solve(sbdx.SBDX_FP64, 0)
+        out["fp64"] = {"seconds": f64.seconds, "sigmas": f64.n_sigma64, "energies": E64.tolist(),
+                       "residuals": R64.tolist(), "converged": bool(f64.converged)}
+        for label, every in (("mixed_every4", 4), ("mixed_adaptive", 0)):
+            f32, E32, R32, one32 = solve(sbdx.SBDX_FP32, every)
+            out[label] = {"seconds": f32.seconds, "sigmas_fp32": f32.n_sigma, "sigmas_fp64": f32.n_sigma64,
+                          "energies": E32.tolist(), "residuals": R32.tolist(), "converged": bool(f32.converged),
+                          "dE_vs_fp64": (E32 - E64).tolist(),
+                          "rdm1_maxabs_vs_fp64": [float(np.abs(one32[r] - one64[r]).max()) for r in range(2)],
+                          "speedup_vs_fp64": f64.seconds / f32.seconds if f32.seconds > 0 else None}
+    return out
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -580,6 +655,11 @@ def run_ours(args, rank, world, local):
                                       "dE_vs_fp64": (E32 - E64).tolist()},
                             "speedup_mixed_vs_fp64": f64.seconds / f32.seconds if f32.seconds > 0 else None}
 
+    # ---- mixed precision on the 400 M-determinant workload, 2 roots -----------------
+    mixed = None
+    if not args.no_davidson and args.mixed and world == 1:
+        mixed = run_mixed(args)
+
     # ---- batched subspaces (64 independent solves sharing one Hamiltonian) ---------
     batched = None
     if not args.no_davidson and not args.no_batched and world == 1:
@@ -611,18 +691,39 @@ def run_ours(args, rank, world, local):
     pb = phase_bytes(prob, dp, 8)
     pb32 = phase_bytes(prob, dp, 4)
     kern = PHASE_KERNELS[dominant]
-    if dominant == "alpha_beta" and tune[1] // 10 == 7:
-        kern = "sigma_ab_v7"  # code 71: packed staged rows
-    achieved = pb[dominant] / (phases[dominant] * 1e-3) / 1e9
-    roofline = {
-        "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-        "traffic": traffic_per_launch(kern, args.workload), "kernel": kern, "phase": dominant,
-        "algorithmic_bytes_per_launch": pb[dominant], "ms_per_launch": phases[dominant], "peak_kind": peak_kind,
-        "phases": {k: {"ms": phases[k], "bytes": pb[k], "gbs": pb[k] / (phases[k] * 1e-3) / 1e9,
-                       "frac": pb[k] / (phases[k] * 1e-3) / 1e9 / hbm} for k in phases},
-        "sigma": {"algorithmic_bytes": B, "ms": ms, "gbs": B / (ms * 1e-3) / 1e9,
-                  "frac": B / (ms * 1e-3) / 1e9 / hbm},
-    }
+    if dominant == "alpha_beta" and tune[1] // 10 != 7:
+        kern = "sigma_ab_v6"  # codes 61-64: unpacked staged rows
+    # The alpha-beta kernel gathers from rows staged in shared memory; DRAM
+    # moves a few percent of the SpMV byte model (profiles/sigma_ab_v7_cfg2.md),
+    # so its bound is the shared-memory pipe: frac = conflict-free shared bytes
+    # (two 8-byte elements per det-pair) / time / (128 B per clock per SM).
+    sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    smem_peak = smem_peak_gbs(sm_mhz)
+    traffic = traffic_per_launch(kern, args.workload)
+    t_dom = phases[dominant] * 1e-3
+    hbm_model = {"algorithmic_bytes_per_launch": pb[dominant], "gbs": pb[dominant] / t_dom / 1e9,
+                 "model_frac": pb[dominant] / t_dom / 1e9 / hbm,
+                 "dram_gbs": traffic / t_dom / 1e9 if traffic else None,
+                 "dram_frac": traffic / t_dom / 1e9 / hbm if traffic else None, "peak_gbs": hbm,
+                 "peak_kind": peak_kind}
+    if dominant == "alpha_beta":
+        sbytes = ab_smem_bytes(dp, 8)
+        achieved = sbytes / t_dom / 1e9
+        roofline = {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
+                    "frac": achieved / smem_peak, "traffic": traffic, "kernel": kern, "phase": dominant,
+                    "smem_bytes_per_launch": sbytes, "ms_per_launch": phases[dominant],
+                    "peak_kind": f"128 B/clk/SM x SMs x {sm_mhz:.0f} MHz (sampled)", "hbm": hbm_model}
+    else:
+        achieved = pb[dominant] / t_dom / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                    "traffic": traffic, "kernel": kern, "phase": dominant,
+                    "algorithmic_bytes_per_launch": pb[dominant], "ms_per_launch": phases[dominant],
+                    "peak_kind": peak_kind}
+    roofline["phases"] = {k: {"ms": phases[k], "bytes": pb[k], "gbs": pb[k] / (phases[k] * 1e-3) / 1e9,
+                              "model_frac": pb[k] / (phases[k] * 1e-3) / 1e9 / hbm} for k in phases}
+    roofline["phases"]["alpha_beta"]["smem_frac"] = ab_smem_bytes(dp, 8) / (phases["alpha_beta"] * 1e-3) / 1e9 / smem_peak
+    roofline["sigma"] = {"algorithmic_bytes": B, "ms": ms, "gbs": B / (ms * 1e-3) / 1e9,
+                         "model_frac": B / (ms * 1e-3) / 1e9 / hbm}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -639,13 +740,17 @@ def run_ours(args, rank, world, local):
         "clocks": clocks,
         "fp32_sigma": {"value": world * dp["total"] / (ms32 * 1e-3), "ms_per_step": ms32,
                        "phases": {k: {"ms": phases32[k], "gbs": pb32[k] / (phases32[k] * 1e-3) / 1e9}
-                                  for k in phases32}},
+                                  for k in phases32},
+                       "alpha_beta_smem_frac": ab_smem_bytes(dp, 4) / (phases32["alpha_beta"] * 1e-3) / 1e9
+                       / smem_peak},
         "davidson": dav,
+        "mixed_precision": mixed,
         "batched": batched,
         "stored_hamiltonian": stored,
         "differentiation": diff,
         "cpu_baseline": cpu,
     }
+    line["summary"] = summary(line)
     if rank == 0:
         print(json.dumps(line))
     ctx.close()
@@ -653,6 +758,34 @@ def run_ours(args, rank, world, local):
         pg.barrier()
         pg.destroy_process_group()
     return 0
+
+
+def summary(line) -> dict:
+    """The headline figures in one short object, printed last on the line."""
+    def get(*keys):
+        d = line
+        for k in keys:
+            if not isinstance(d, dict) or d.get(k) is None:
+                return None
+            d = d[k]
+        return d
+
+    out = {"sigma_fp64_ms": line["ms_per_step"], "sigma_fp32_ms": get("fp32_sigma", "ms_per_step"),
+           "alpha_beta_smem_frac": get("roofline", "phases", "alpha_beta", "smem_frac"),
+           "mixed_vs_fp64_cfg2_1root": get("davidson", "speedup_mixed_vs_fp64"),
+           "mixed_vs_fp64_cfg2_2roots": get("davidson", "roots", "speedup_mixed_vs_fp64")}
+    m = line.get("mixed_precision")
+    if m:
+        for lab in ("mixed_every4", "mixed_adaptive"):
+            out[f"{lab}_vs_fp64_cfg3_2roots"] = m[lab]["speedup_vs_fp64"]
+            out[f"{lab}_cfg3_max_abs_dE"] = max(abs(x) for x in m[lab]["dE_vs_fp64"])
+            out[f"{lab}_cfg3_max_rdm1_err"] = max(m[lab]["rdm1_maxabs_vs_fp64"])
+    out["batched_mixed_vs_sequential_fp64"] = get("batched", "speedup_batched_mixed_vs_sequential_fp64")
+    d = line.get("differentiation")
+    if d:
+        out["backward_over_forward"] = d["backward_seconds"] / d["forward_seconds"]
+        out["backward_fd_rel_err"] = d["max_rel_err_vs_central_differences"]
+    return out
 
 
 def main():

@@ -192,7 +192,10 @@ typedef struct {
  * chemistry/tpb/davidson.h:661-924), BasisInitVector (:101-140) and the energy
  * evaluation of tpb::diag (sbdiag.h:246-273). W: host buffer of na*nb doubles;
  * on input the start vector if init_from_W != 0, else W[0] = 1 (Hartree-Fock);
- * on output the normalised ground-state vector. */
+ * on output the normalised ground-state vector. W may be NULL when
+ * init_from_W == 0: the vector then stays on the device only. Either way the
+ * result stays resident in the context (sbdx_wavefunction_device) until the
+ * next solve or new strings. */
 int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_from_W, double* W,
                   sbdx_davidson_info* info);
 
@@ -200,7 +203,8 @@ int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_fr
  * single-root. W: host buffer of nroots*na*nb doubles (root r at offset
  * r*na*nb); on input the start vectors if init_from_W != 0, else unit vectors
  * on the nroots lowest diagonal elements; on output the orthonormal Ritz
- * vectors. energies and residuals (may be NULL): nroots doubles each, the
+ * vectors (W may be NULL when init_from_W == 0; the vectors stay resident as
+ * for sbdx_davidson). energies and residuals (may be NULL): nroots doubles each, the
  * Rayleigh quotients and exact residual norms |H W_r - E_r W_r|. 1 <= nroots
  * <= 4. SBDX_FP64: block Davidson whose subspace holds the nroots Ritz
  * vectors plus max_nb FP64 corrections; SBDX_FP32: the mixed-precision solver
@@ -209,6 +213,28 @@ int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_fr
  * Converged when every exact residual is below eps. */
 int sbdx_davidson_roots(sbdx_ctx* ctx, const sbdx_davidson_params* params, int nroots, int init_from_W,
                         double* W, double* energies, double* residuals, sbdx_davidson_info* info);
+
+/* ---- the converged vector on the device (no device-host round trip) -------
+ * The reference reduces its distributed vector where it lies: the density
+ * (OccupationDensity, chemistry/tpb/occupation.h:10-95), the alpha weights of
+ * the carry-over (DiagonalReducedDensityMatrix, chemistry/tpb/rdmat.h:10-58)
+ * and the RDMs (Correlation, chemistry/tpb/correlation.h:194-444) run on the
+ * W that Davidson left in memory. These entry points do the same with device
+ * vectors: dW is any device buffer of na*nb doubles on the context's device,
+ * usually the resident result of the last solve. */
+/* Device address of root `root` of the last sbdx_davidson /
+ * sbdx_davidson_roots solve of this context (SBDX_ERR_STATE before any solve;
+ * invalidated by the next solve or new strings). */
+int sbdx_wavefunction_device(sbdx_ctx* ctx, int root, const double** dW);
+/* Copies that root to the host buffer W (na*nb doubles), e.g. to save it
+ * (SaveWavefunction, chemistry/tpb/restart.h:20-67). */
+int sbdx_get_wavefunction(sbdx_ctx* ctx, int root, double* W);
+/* As sbdx_rdm, sbdx_occupation, sbdx_alpha_weights and sbdx_energy_backward
+ * (below) on a device vector; outputs are host buffers of the same sizes. */
+int sbdx_rdm_device(sbdx_ctx* ctx, const double* dW, double* one, double* two);
+int sbdx_occupation_device(sbdx_ctx* ctx, const double* dW, double* density);
+int sbdx_alpha_weights_device(sbdx_ctx* ctx, const double* dW, double* weights);
+int sbdx_energy_backward_device(sbdx_ctx* ctx, const double* dW, double* dE_dh, double* dE_deri);
 
 /* 1-/2-RDM of a vector W (host, na*nb doubles). Replaces Correlation
  * (chemistry/tpb/correlation.h:194-444). one: 2*L*L doubles; two: 4*L^4

@@ -470,7 +470,7 @@ void diag(const Comm& /*comm*/, const SBD& sbd_data, const FCIDump& fcidump,
   }
 
   const size_t D = a.size() * b.size();
-  std::vector<double> W(D, 0.0);
+  std::vector<double> W;
   int init_from_W = 0;
   if (!loadname.empty()) {
     LoadWavefunction(loadname, adet, bdet, W);
@@ -486,7 +486,13 @@ void diag(const Comm& /*comm*/, const SBD& sbd_data, const FCIDump& fcidump,
   p.defect_every = 0;
   p.verbose = detail::env_int("SBDX_VERBOSE", 1);
   sbdx_davidson_info info{};
-  ctx.check(sbdx_davidson(ctx.h, &p, init_from_W, W.data(), &info));
+  // the converged vector stays on the device: the density, the RDMs and the
+  // carry-over weights reduce it there (occupation.h:10-95, rdmat.h:10-58 act
+  // on the distributed vector in place); it comes to the host only when a file
+  // has to be written
+  ctx.check(sbdx_davidson(ctx.h, &p, init_from_W, init_from_W ? W.data() : nullptr, &info));
+  const double* dW = nullptr;
+  ctx.check(sbdx_wavefunction_device(ctx.h, 0, &dW));
   energy = info.energy;
   std::cout.precision(16);
   std::cout << " Energy = " << energy << std::endl;
@@ -494,10 +500,10 @@ void diag(const Comm& /*comm*/, const SBD& sbd_data, const FCIDump& fcidump,
   const size_t Lz = (size_t)L;
   if (sbd_data.do_rdm == 0) {
     density.assign(2 * Lz, 0.0);
-    ctx.check(sbdx_occupation(ctx.h, W.data(), density.data()));
+    ctx.check(sbdx_occupation_device(ctx.h, dW, density.data()));
   } else {
     std::vector<double> one(2 * Lz * Lz), two(4 * Lz * Lz * Lz * Lz);
-    ctx.check(sbdx_rdm(ctx.h, W.data(), one.data(), two.data()));
+    ctx.check(sbdx_rdm_device(ctx.h, dW, one.data(), two.data()));
     one_p_rdm.assign(2, std::vector<double>());
     two_p_rdm.assign(4, std::vector<double>());
     for (int s = 0; s < 2; ++s) one_p_rdm[s].assign(one.begin() + s * Lz * Lz, one.begin() + (s + 1) * Lz * Lz);
@@ -511,11 +517,15 @@ void diag(const Comm& /*comm*/, const SBD& sbd_data, const FCIDump& fcidump,
   }
 
   std::vector<double> wa(a.size());
-  ctx.check(sbdx_alpha_weights(ctx.h, W.data(), wa.data()));
+  ctx.check(sbdx_alpha_weights_device(ctx.h, dW, wa.data()));
   double truncated = 0.0;
   detail::carry_over(wa, adet, sbd_data.ratio, sbd_data.threshold, carryover_bitstrings, truncated);
   if (sbd_data.ratio != 0.0) std::cout << " truncated weight in carry-over = " << truncated << std::endl;
 
+  if (!savename.empty() || !sbd_data.dump_matrix_form_wf.empty()) {
+    W.resize(D);
+    ctx.check(sbdx_get_wavefunction(ctx.h, 0, W.data()));
+  }
   if (!savename.empty()) SaveWavefunction(savename, adet, bdet, W);
   if (!sbd_data.dump_matrix_form_wf.empty())
     SaveMatrixFormWF(sbd_data.dump_matrix_form_wf, bl, Lz, adet, bdet, W);

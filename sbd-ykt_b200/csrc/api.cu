@@ -77,6 +77,27 @@ void free_vector_state(Ctx* c) {
   cudaFree(c->d_yt); c->d_yt = nullptr;
   cudaFree(c->d_io_in); c->d_io_in = nullptr;
   cudaFree(c->d_io_out); c->d_io_out = nullptr;
+  cudaFree(c->d_wf); c->d_wf = nullptr; c->wf_roots = 0; c->wf_cap = 0;
+}
+
+// Room for k resident result vectors (contents of earlier solves are dropped).
+int ensure_wf(Ctx* c, int k) {
+  const size_t D = c->na * c->nb;
+  c->wf_roots = 0;
+  if (c->wf_cap < k) {
+    cudaFree(c->d_wf);
+    c->d_wf = nullptr;
+    c->wf_cap = 0;
+    cudaError_t e = cudaMalloc(&c->d_wf, sizeof(double) * D * (size_t)k);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      c->err = "davidson: no device memory for " + std::to_string(k) + " result vector(s) of " + std::to_string(D) +
+               " doubles";
+      return SBDX_ERR_NOMEM;
+    }
+    c->wf_cap = k;
+  }
+  return 0;
 }
 
 int ensure_io(Ctx* c) {
@@ -404,15 +425,15 @@ int sbdx_sigma_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS) {
 int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_from_W, double* W,
                   sbdx_davidson_info* info) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {
-    if (!params || !W) { c->err = "davidson: null pointer"; return SBDX_ERR_ARG; }
+    if (!params || (!W && init_from_W)) { c->err = "davidson: null pointer"; return SBDX_ERR_ARG; }
     int rc = sbdx::ready(c, "davidson");
     if (rc) return rc;
     const size_t D = c->na * c->nb;
     if (init_from_W)
       for (size_t k = 0; k < D; ++k)
         if (!std::isfinite(W[k])) { c->err = "davidson: non-finite start vector"; return SBDX_ERR_NUMERIC; }
-    if ((rc = sbdx::ensure_io(c))) return rc;
-    double* dW = (double*)c->d_io_in;
+    if ((rc = sbdx::ensure_wf(c, 1))) return rc;
+    double* dW = c->d_wf;
     if (init_from_W) {
       SBDX_CUDA(c, cudaMemcpyAsync(dW, W, sizeof(double) * D, cudaMemcpyHostToDevice, c->stream));
     } else {
@@ -425,7 +446,8 @@ int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_fr
     rc = sbdx::davidson(c, *params, dW, inf);
     if (rc) return rc;
     if ((rc = sbdx::check_device_error(c))) return rc;
-    SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * D, cudaMemcpyDeviceToHost, c->stream));
+    c->wf_roots = 1;
+    if (W) SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * D, cudaMemcpyDeviceToHost, c->stream));
     SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
     if (info) *info = inf;
     return SBDX_OK;
@@ -435,7 +457,7 @@ int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_fr
 int sbdx_davidson_roots(sbdx_ctx* ctx, const sbdx_davidson_params* params, int nroots, int init_from_W,
                         double* W, double* energies, double* residuals, sbdx_davidson_info* info) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {
-    if (!params || !W || !energies) { c->err = "davidson_roots: null pointer"; return SBDX_ERR_ARG; }
+    if (!params || (!W && init_from_W) || !energies) { c->err = "davidson_roots: null pointer"; return SBDX_ERR_ARG; }
     if (nroots < 1 || nroots > 4) { c->err = "davidson_roots: nroots must be in [1, 4]"; return SBDX_ERR_ARG; }
     int rc = sbdx::ready(c, "davidson_roots");
     if (rc) return rc;
@@ -444,13 +466,12 @@ int sbdx_davidson_roots(sbdx_ctx* ctx, const sbdx_davidson_params* params, int n
     if (init_from_W)
       for (size_t q = 0; q < D * nroots; ++q)
         if (!std::isfinite(W[q])) { c->err = "davidson_roots: non-finite start vector"; return SBDX_ERR_NUMERIC; }
-    double* dW = nullptr;
-    SBDX_CUDA(c, sbdx::pool_alloc(c, (void**)&dW, sizeof(double) * D * nroots));
+    if ((rc = sbdx::ensure_wf(c, nroots))) return rc;
+    double* dW = c->d_wf;
     struct Guard {
       Ctx* c;
-      double* p;
-      ~Guard() { cudaFreeAsync(p, c->stream); sbdx::pool_trim(c); }
-    } g{c, dW};
+      ~Guard() { sbdx::pool_trim(c); }
+    } g{c};
     if (init_from_W) {
       SBDX_CUDA(c, cudaMemcpyAsync(dW, W, sizeof(double) * D * nroots, cudaMemcpyHostToDevice, c->stream));
     } else {  // unit vectors on the nroots lowest diagonal elements
@@ -466,7 +487,8 @@ int sbdx_davidson_roots(sbdx_ctx* ctx, const sbdx_davidson_params* params, int n
     sbdx_davidson_info inf{};
     if ((rc = sbdx::davidson_roots(c, *params, nroots, dW, e.data(), res.data(), inf))) return rc;
     if ((rc = sbdx::check_device_error(c))) return rc;
-    SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * D * nroots, cudaMemcpyDeviceToHost, c->stream));
+    c->wf_roots = nroots;
+    if (W) SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * D * nroots, cudaMemcpyDeviceToHost, c->stream));
     SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
     for (int r = 0; r < nroots; ++r) {
       energies[r] = e[r];
@@ -545,6 +567,95 @@ int sbdx_energy_backward(sbdx_ctx* ctx, const double* W, double* dE_dh, double* 
     const size_t D = c->na * c->nb;
     SBDX_CUDA(c, cudaMemcpyAsync(c->d_io_in, W, sizeof(double) * D, cudaMemcpyHostToDevice, c->stream));
     return sbdx::backward_device(c, (const double*)c->d_io_in, dE_dh, dE_deri);
+  });
+}
+
+// ---- reductions on device-resident vectors ----------------------------------------
+
+int sbdx_wavefunction_device(sbdx_ctx* ctx, int root, const double** dW) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!dW) { c->err = "wavefunction_device: null pointer"; return SBDX_ERR_ARG; }
+    if (c->wf_roots == 0) { c->err = "wavefunction_device: no Davidson solve has run on this basis"; return SBDX_ERR_STATE; }
+    if (root < 0 || root >= c->wf_roots) {
+      c->err = "wavefunction_device: root " + std::to_string(root) + " outside [0, " + std::to_string(c->wf_roots) + ")";
+      return SBDX_ERR_ARG;
+    }
+    *dW = c->d_wf + (size_t)root * c->na * c->nb;
+    return SBDX_OK;
+  });
+}
+
+int sbdx_get_wavefunction(sbdx_ctx* ctx, int root, double* W) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    const double* dW = nullptr;
+    int rc = sbdx_wavefunction_device(ctx, root, &dW);
+    if (rc) return rc;
+    if (!W) { c->err = "get_wavefunction: null pointer"; return SBDX_ERR_ARG; }
+    SBDX_CUDA(c, cudaMemcpyAsync(W, dW, sizeof(double) * c->na * c->nb, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SBDX_OK;
+  });
+}
+
+int sbdx_rdm_device(sbdx_ctx* ctx, const double* dW, double* one, double* two) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!dW || !one) { c->err = "rdm_device: null pointer"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "rdm_device");
+    if (rc) return rc;
+    const size_t L = (size_t)c->L, L2 = L * L, L4 = L2 * L2;
+    double *d_one = nullptr, *d_two = nullptr;
+    SBDX_CUDA(c, cudaMalloc(&d_one, sizeof(double) * 2 * L2));
+    if (two) {
+      cudaError_t e = cudaMalloc(&d_two, sizeof(double) * 4 * L4);
+      if (e != cudaSuccess) { cudaFree(d_one); sbdx::set_cuda_err(c, e, "cudaMalloc(2-RDM)"); return SBDX_ERR_NOMEM; }
+    }
+    rc = sbdx::rdm_device(c, dW, d_one, d_two);
+    if (!rc) {
+      cudaError_t e = cudaMemcpyAsync(one, d_one, sizeof(double) * 2 * L2, cudaMemcpyDeviceToHost, c->stream);
+      if (e == cudaSuccess && two) e = cudaMemcpyAsync(two, d_two, sizeof(double) * 4 * L4, cudaMemcpyDeviceToHost, c->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) { sbdx::set_cuda_err(c, e, "rdm copy-out"); rc = SBDX_ERR_CUDA; }
+    }
+    cudaFree(d_one);
+    cudaFree(d_two);
+    return rc;
+  });
+}
+
+int sbdx_occupation_device(sbdx_ctx* ctx, const double* dW, double* density) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!dW || !density) { c->err = "occupation_device: null pointer"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "occupation_device");
+    if (rc) return rc;
+    if ((rc = sbdx::ensure_io(c))) return rc;
+    double* d = (double*)c->d_io_out;
+    if ((rc = sbdx::occupation_device(c, dW, d))) return rc;
+    SBDX_CUDA(c, cudaMemcpyAsync(density, d, sizeof(double) * 2 * c->L, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SBDX_OK;
+  });
+}
+
+int sbdx_alpha_weights_device(sbdx_ctx* ctx, const double* dW, double* weights) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!dW || !weights) { c->err = "alpha_weights_device: null pointer"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "alpha_weights_device");
+    if (rc) return rc;
+    if ((rc = sbdx::ensure_io(c))) return rc;
+    double* d = (double*)c->d_io_out;
+    if ((rc = sbdx::alpha_weights_device(c, dW, d))) return rc;
+    SBDX_CUDA(c, cudaMemcpyAsync(weights, d, sizeof(double) * c->na, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SBDX_OK;
+  });
+}
+
+int sbdx_energy_backward_device(sbdx_ctx* ctx, const double* dW, double* dE_dh, double* dE_deri) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!dW || !dE_dh || !dE_deri) { c->err = "energy_backward_device: null pointer"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "energy_backward_device");
+    if (rc) return rc;
+    return sbdx::backward_device(c, dW, dE_dh, dE_deri);
   });
 }
 

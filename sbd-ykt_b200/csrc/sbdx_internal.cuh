@@ -208,6 +208,13 @@ struct Ctx {
   size_t xsa = 0, xsb = 0;
   void* d_io_in = nullptr;  // D FP64 staging for host-buffer entry points
   void* d_io_out = nullptr;
+  // the wavefunction of the last Davidson solve, resident on the device:
+  // wf_roots vectors of D FP64 (root r at d_wf + r*D), kept until the next
+  // solve or until the strings change, so the density, RDM, carry-over
+  // weights and adjoint run on it without a device-host round trip
+  double* d_wf = nullptr;
+  int wf_roots = 0;     // vectors the last solve left (0 = none)
+  int wf_cap = 0;       // vectors allocated
   // reductions
   double* d_red = nullptr;  // partial sums
   size_t red_cap = 0;

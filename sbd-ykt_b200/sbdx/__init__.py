@@ -32,7 +32,8 @@ EXPORTS = [
     "sbdx_get_connectivity", "sbdx_diag_terms", "sbdx_sigma", "sbdx_sigma_device", "sbdx_davidson",
     "sbdx_rdm", "sbdx_occupation", "sbdx_alpha_weights", "sbdx_energy_backward", "sbdx_set_profiling",
     "sbdx_phase_times", "sbdx_set_tuning", "sbdx_autotune", "sbdx_davidson_roots",
-    "sbdx_build_hamiltonian", "sbdx_release_hamiltonian",
+    "sbdx_build_hamiltonian", "sbdx_release_hamiltonian", "sbdx_wavefunction_device", "sbdx_get_wavefunction",
+    "sbdx_rdm_device", "sbdx_occupation_device", "sbdx_alpha_weights_device", "sbdx_energy_backward_device",
 ]
 PHASES = ["alpha_same_spin", "transpose", "beta_same_spin", "alpha_beta", "combine"]
 
@@ -204,29 +205,76 @@ class Context:
                                                ctypes.c_void_p(s_ptr)))
 
     def davidson(self, max_it=1, max_nb=10, eps=1e-4, max_time=86400.0, precision=SBDX_FP64, defect_every=0,
-                 verbose=0, W=None):
+                 verbose=0, W=None, to_host=True):
+        """sbdx_davidson. Returns (info, W); with to_host=False (and no start
+        vector) W is None and the result stays on the device only
+        (wavefunction_device)."""
         p = DavidsonParams(max_it, max_nb, eps, max_time, precision, defect_every, verbose)
         D = self.na * self.nb
         init = 1 if W is not None else 0
-        W = np.zeros(D) if W is None else np.ascontiguousarray(W, dtype=np.float64).copy()
+        if W is not None:
+            W = np.ascontiguousarray(W, dtype=np.float64).copy()
+        elif to_host:
+            W = np.zeros(D)
         info = DavidsonInfo()
-        self._check(self.lib.sbdx_davidson(self.h, ctypes.byref(p), ctypes.c_int(init), _d(W), ctypes.byref(info)))
+        self._check(self.lib.sbdx_davidson(self.h, ctypes.byref(p), ctypes.c_int(init), _d(W) if W is not None else None,
+                                           ctypes.byref(info)))
         return info, W
 
     def davidson_roots(self, nroots, max_it=1, max_nb=10, eps=1e-4, max_time=86400.0, precision=SBDX_FP64,
-                       defect_every=0, verbose=0, W=None):
+                       defect_every=0, verbose=0, W=None, to_host=True):
         """sbdx_davidson_roots: the nroots lowest eigenpairs. Returns
         (info, energies[nroots], residuals[nroots], W[nroots, D])."""
         p = DavidsonParams(max_it, max_nb, eps, max_time, precision, defect_every, verbose)
         D = self.na * self.nb
         init = 1 if W is not None else 0
-        Wb = np.zeros((nroots, D)) if W is None else np.ascontiguousarray(W, dtype=np.float64).reshape(nroots, D).copy()
+        if W is not None:
+            Wb = np.ascontiguousarray(W, dtype=np.float64).reshape(nroots, D).copy()
+        else:
+            Wb = np.zeros((nroots, D)) if to_host else None
         E = np.zeros(nroots)
         res = np.zeros(nroots)
         info = DavidsonInfo()
         self._check(self.lib.sbdx_davidson_roots(self.h, ctypes.byref(p), ctypes.c_int(nroots), ctypes.c_int(init),
-                                                 _d(Wb), _d(E), _d(res), ctypes.byref(info)))
+                                                 _d(Wb) if Wb is not None else None, _d(E), _d(res),
+                                                 ctypes.byref(info)))
         return info, E, res, Wb
+
+    # ---- the resident result of the last solve and reductions on device vectors ----
+    def wavefunction_device(self, root=0) -> int:
+        """Device address of root `root` of the last solve (sbdx_wavefunction_device)."""
+        ptr = ctypes.c_void_p()
+        self._check(self.lib.sbdx_wavefunction_device(self.h, ctypes.c_int(root), ctypes.byref(ptr)))
+        return int(ptr.value)
+
+    def get_wavefunction(self, root=0):
+        W = np.zeros(self.na * self.nb)
+        self._check(self.lib.sbdx_get_wavefunction(self.h, ctypes.c_int(root), _d(W)))
+        return W
+
+    def rdm_device(self, w_ptr: int, two=True):
+        L = self.L
+        one = np.zeros(2 * L * L)
+        tw = np.zeros(4 * L ** 4) if two else None
+        self._check(self.lib.sbdx_rdm_device(self.h, ctypes.c_void_p(w_ptr), _d(one), _d(tw) if two else None))
+        return one, tw
+
+    def occupation_device(self, w_ptr: int):
+        out = np.zeros(2 * self.L)
+        self._check(self.lib.sbdx_occupation_device(self.h, ctypes.c_void_p(w_ptr), _d(out)))
+        return out
+
+    def alpha_weights_device(self, w_ptr: int):
+        out = np.zeros(self.na)
+        self._check(self.lib.sbdx_alpha_weights_device(self.h, ctypes.c_void_p(w_ptr), _d(out)))
+        return out
+
+    def energy_backward_device(self, w_ptr: int):
+        L = self.L
+        dh = np.zeros(L * L)
+        deri = np.zeros(synth.neri(L))
+        self._check(self.lib.sbdx_energy_backward_device(self.h, ctypes.c_void_p(w_ptr), _d(dh), _d(deri)))
+        return dh, deri
 
     def rdm(self, W, two=True):
         L = self.L
