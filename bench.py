@@ -27,8 +27,10 @@ OpenMP mult (compiled in oracle/_ref) on a bounded sample of bra alpha rows.
 mixed precision with energy and 1-RDM errors; `summary`, printed last, holds
 the headline figures.
 
-Multi-GPU: the path is run at MPI world size 1; --gpus N runs N independent
-replicas (one process per GPU) and reports the whole-job det-pairs/s.
+Multi-GPU (--gpus N under torchrun): one sigma of the same workload split by
+alpha-row shards over the N GPUs (sbdx/shard.py: the whole C gathered on every
+GPU by NCCL, each GPU evaluating its own rows), strong scaling; value = the
+det-pairs of the whole sigma over the slowest rank's step time.
 """
 from __future__ import annotations
 
@@ -79,6 +81,8 @@ def parse_args():
     ap.add_argument("--mixed", default="cfg3", metavar="WORKLOAD",
                     help="workload of the mixed-precision measurement (2 roots, FP64 block solve vs mixed with "
                          "refresh every 4 steps and adaptive; '' = skip)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="run the alpha-row-shard path (the N > 1 path) also at N = 1")
     ap.add_argument("--tune", default=None, metavar="SAME,AB",
                     help="fixed sigma launch codes for both precisions instead of the autotuner (profiling runs)")
     return ap.parse_args()
@@ -265,7 +269,7 @@ def max_over_ranks(x: float, pg=None, device: str = "cuda") -> float:
 
 
 def replica_throughput(pairs_per_step: float, ms_local: float, world: int, pg=None, device: str = "cuda"):
-    """Whole-job det-pairs/s of N independent replicas: every rank evaluates
+    """Whole-job det-pairs/s when every one of `world` ranks evaluates
     pairs_per_step per step; the job's step time is the slowest rank's."""
     ms = max_over_ranks(ms_local, pg, device)
     return ms, world * pairs_per_step / (ms * 1e-3)
@@ -507,13 +511,138 @@ def run_reference_arm(args, rank, world):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / len(timed),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "desc": workload_desc(args.workload), "parallelism": "replicas",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": workload_desc(args.workload),
+                   "parallelism": "reference at MPI world size 1, OpenMP threads",
                    "sample_rows": rows},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+    return 0
+
+
+def run_sharded(args, rank, world, local):
+    """N > 1: one sigma of the workload split over the GPUs by alpha-row
+    shards (sbdx/shard.py): each step gathers the whole C on every GPU (one
+    NCCL broadcast per rank) and evaluates the rank's rows
+    (sbdx_sigma_rows_device). value = det-pairs of the whole sigma / the
+    slowest rank's step time (strong scaling: the work is fixed as N grows).
+    Also the sharded FP64 Davidson to the tolerance (time to solution)."""
+    import torch
+    import torch.distributed as dist
+
+    import sbdx
+    from sbdx import shard, synth
+
+    torch.cuda.set_device(local)
+    if world == 1 and "MASTER_ADDR" not in os.environ:  # --sharded without torchrun
+        import socket
+
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK="0", WORLD_SIZE="1")
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    comm = shard.Comm(dist.group.WORLD)
+    prob = load_workload(args.workload)
+    ctx = sbdx.Context(local)
+    ctx.load(prob)
+    ctx.build_connectivity()
+    if args.tune:
+        tune = tuple(int(x) for x in args.tune.split(","))
+        ctx.set_tuning(*tune)
+    else:
+        tune = ctx.autotune()
+    sa, da, _ = ctx.connectivity(0)
+    sb, db, _ = ctx.connectivity(1)
+    dp = synth.det_pairs(sa, da, sb, db)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    bounds = shard.partition(shard.row_work(ctx), world)
+    a0, a1 = bounds[rank]
+    nb = prob.nb
+    n_loc = (a1 - a0) * nb
+    op = shard.ShardedSigma(ctx, comm, bounds)
+    gen = torch.Generator(device="cuda").manual_seed(1234)
+    C = torch.randn(prob.D, dtype=torch.float64, device="cuda", generator=gen)
+    C_loc = C[a0 * nb:a1 * nb].clone()
+    del C
+    S_loc = torch.empty_like(C_loc)
+
+    def barrier():
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        op(C_loc, S_loc)
+    barrier()
+    sampler = ClockSampler(gpu_index(local))
+    sampler.start()
+    launches0 = ctx.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        op(C_loc, S_loc)
+    e1.record(stream)
+    barrier()
+    clocks = sampler.stop()
+    launches = ctx.launches - launches0
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist)
+    value = dp["total"] / (ms * 1e-3)
+    # end to end: the rank's rows from pinned host memory and back, every step
+    hC = C_loc.cpu().pin_memory()
+    hS = torch.empty(n_loc, dtype=torch.float64).pin_memory()
+    barrier()
+    n_e2e = max(2, min(args.steps, 5))
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(n_e2e):
+        C_loc.copy_(hC, non_blocking=True)
+        op(C_loc, S_loc)
+        hS.copy_(S_loc, non_blocking=True)
+        stream.synchronize()
+    e1.record(stream)
+    barrier()
+    ms_e2e = max_over_ranks(max(e0.elapsed_time(e1) / n_e2e, 1e3 * (time.perf_counter() - t0) / n_e2e), dist)
+    dav = None
+    if not args.no_davidson:
+        hii = torch.from_numpy(ctx.diag_terms()[a0 * nb:a1 * nb]).cuda()
+        W0 = torch.zeros(n_loc, dtype=torch.float64, device="cuda")
+        if a0 == 0 and n_loc > 0:
+            W0[0] = 1.0
+        E, _, inf = shard.davidson(op, hii, comm, W0, max_it=100, max_nb=12, eps=args.davidson_tol)
+        dav = {"tol": args.davidson_tol, "max_nb": 12, "seconds": max_over_ranks(inf["seconds"], dist),
+               "sigmas": inf["sigmas"], "energy": E, "residual": inf["residual"], "converged": inf["converged"]}
+    hbm, peak_kind = peaks()
+    B = roofline_bytes(prob, dp, 8)
+    gbs = B / world / (ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded integrals and string samples of the stated law)",
+        "config": {"workload": args.workload, "desc": workload_desc(args.workload), "dets": prob.D, "na": prob.na,
+                   "nb": nb, "norb": prob.L, "det_pairs_per_sigma": dp["total"],
+                   "parallelism": f"alpha-row shards x{world} (whole C gathered per step)",
+                   "shards": bounds, "tuning": {"same_vec": tune[0], "ab_rows": tune[1]},
+                   "l2": f"inputs larger than L2 (C = {8 * prob.D / 1e6:.0f} MB > 126 MB), no flush"},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                     "traffic": None, "kernel": "whole sigma of a row shard (SpMV byte model / N per GPU)",
+                     "peak_kind": peak_kind},
+        "e2e": {"value": dp["total"] / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 8 * prob.D,
+                "d2h_bytes_per_step": 8 * prob.D, "ms_per_step": ms_e2e},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "davidson_sharded": dav,
+        "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    del op
+    ctx.close()
+    dist.barrier()
+    dist.destroy_process_group()
     return 0
 
 
@@ -523,13 +652,10 @@ def run_ours(args, rank, world, local):
     import sbdx
     from sbdx import synth
 
+    if world > 1 or args.sharded:
+        return run_sharded(args, rank, world, local)
     torch.cuda.set_device(local)
     pg = None
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-        pg = dist
     prob = load_workload(args.workload)
     ctx = sbdx.Context(local)
     ctx.load(prob)
@@ -726,10 +852,10 @@ def run_ours(args, rank, world, local):
                          "model_frac": B / (ms * 1e-3) / 1e9 / hbm}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded integrals and string samples of the stated law)",
         "config": {"workload": args.workload, "desc": workload_desc(args.workload), "dets": D, "na": prob.na, "nb": prob.nb,
-                   "norb": prob.L, "det_pairs_per_sigma": dp["total"], "parallelism": f"replicas x{world}",
+                   "norb": prob.L, "det_pairs_per_sigma": dp["total"], "parallelism": "one GPU (alpha-row shards x1)",
                    "tuning": {"same_vec": tune[0], "ab_rows": tune[1]},
                    "l2": f"inputs larger than L2 (C = {8 * D / 1e6:.0f} MB > 126 MB), no flush"
                          if 8 * D > 126e6 else "C fits in L2: timings include L2 reuse"},

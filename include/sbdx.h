@@ -167,6 +167,20 @@ int sbdx_sigma(sbdx_ctx* ctx, const double* C, double* S);
  * on the context stream. */
 int sbdx_sigma_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS);
 
+/* One shard of the product for a distributed solve: output rows [a0, a1) of
+ * S = H C, i.e. the determinants of alpha strings a0 .. a1-1. dC is the whole
+ * vector (na*nb elements of the given precision, the ket side); dS receives
+ * (a1-a0)*nb elements (its element 0 is determinant (a0, 0)). a0 must be a
+ * multiple of 8 (or a0 == a1). The reference distributes the vector in 2-D
+ * blocks, rotates ket blocks between ranks (Mpi2dSlide,
+ * framework/mpi_utility.h:441-515; chemistry/tpb/mult.h:429-432, 599-607) and
+ * sums partial products (MpiAllreduce, mult.h:614-615); here each GPU owns a
+ * block of alpha rows, gathers the whole C into its HBM (one all-gather per
+ * product) and evaluates its own rows completely, so no partial products are
+ * summed. Evaluated on the fly (SBDX_ERR_STATE while a stored Hamiltonian is
+ * held). The rows' work items are built on first use of a range. */
+int sbdx_sigma_rows_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS, size_t a0, size_t a1);
+
 typedef struct {
   int max_it;          /* outer restarts (SBD::max_it, sbdiag.h:19)            */
   int max_nb;          /* subspace size (SBD::max_nb, sbdiag.h:20)            */

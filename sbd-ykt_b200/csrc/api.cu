@@ -422,6 +422,22 @@ int sbdx_sigma_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS) {
   });
 }
 
+int sbdx_sigma_rows_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS, size_t a0, size_t a1) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (!dC || (!dS && a1 > a0)) { c->err = "sigma_rows_device: null pointer"; return SBDX_ERR_ARG; }
+    int rc = sbdx::ready(c, "sigma_rows_device");
+    if (rc) return rc;
+    const size_t es = precision == SBDX_FP32 ? sizeof(float) : sizeof(double);
+    const char* C0 = static_cast<const char*>(dC);
+    const char* S0 = static_cast<const char*>(dS);
+    if (S0 && S0 < C0 + es * c->na * c->nb && C0 < S0 + es * (a1 - a0) * c->nb) {
+      c->err = "sigma_rows_device: input and output must not overlap";
+      return SBDX_ERR_ARG;
+    }
+    return sbdx::sigma_rows_device(c, precision, dC, dS, a0, a1);
+  });
+}
+
 int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_from_W, double* W,
                   sbdx_davidson_info* info) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {

@@ -21,7 +21,10 @@
 #include "sbdx.h"
 
 #include <algorithm>
+#include <array>
 #include <cstdint>
+#include <random>
+#include <thread>
 #include <vector>
 
 namespace sbdx {
@@ -29,6 +32,8 @@ namespace sbdx {
 namespace {
 
 constexpr int kConnThreads = 256;
+// Move budget of the record-order descent, per step of a quarter-warp.
+constexpr int kOrderEffort = 3000;
 
 __global__ void __launch_bounds__(kConnThreads)
 conn_count_kernel(const uint64_t* __restrict__ s, size_t n, uint32_t* __restrict__ nsing,
@@ -183,7 +188,7 @@ void free_conn(Conn& c) {
   cudaFree(c.nsing); cudaFree(c.ndoub); cudaFree(c.off); cudaFree(c.ket);
   cudaFree(c.val); cudaFree(c.val32); cudaFree(c.omask); cudaFree(c.info);
   cudaFree(c.srec); cudaFree(c.order); cudaFree(c.spos);
-  cudaFree(c.sell); cudaFree(c.soff); cudaFree(c.slen);
+  cudaFree(c.sell); cudaFree(c.soff); cudaFree(c.slen); cudaFree(c.kpos);
   auto free_panel = [](SellPanel& p) {
     cudaFree(p.sell); cudaFree(p.sell32); cudaFree(p.soff4); cudaFree(p.slen4);
     cudaFree(p.soff); cudaFree(p.slen); cudaFree(p.vrow);
@@ -200,20 +205,22 @@ void free_conn(Conn& c) {
 // Conn::ab_item): {row, first unit, one past the last, 1 + slot or 0},
 // longest first; split rows as {row, first slot, parts, 0}. Empty rows get an
 // item only with keep_empty (a kernel that assigns its output row).
+// Rows are numbered from row0 (len[i] belongs to row row0 + i).
 void split_rows(const std::vector<uint32_t>& len, uint32_t cap, bool keep_empty, std::vector<uint4>& items,
-                std::vector<uint4>& split, int& nslot) {
+                std::vector<uint4>& split, int& nslot, size_t row0 = 0) {
   items.clear();
   split.clear();
   nslot = 0;
-  for (size_t r = 0; r < len.size(); ++r) {
-    if (len[r] <= cap) {
-      if (len[r] || keep_empty) items.push_back(make_uint4((uint32_t)r, 0u, len[r], 0u));
+  for (size_t i = 0; i < len.size(); ++i) {
+    const uint32_t r = (uint32_t)(row0 + i);
+    if (len[i] <= cap) {
+      if (len[i] || keep_empty) items.push_back(make_uint4(r, 0u, len[i], 0u));
       continue;
     }
-    const uint32_t parts = (len[r] + cap - 1) / cap;
-    split.push_back(make_uint4((uint32_t)r, (uint32_t)nslot, parts, 0u));
+    const uint32_t parts = (len[i] + cap - 1) / cap;
+    split.push_back(make_uint4(r, (uint32_t)nslot, parts, 0u));
     for (uint32_t q = 0; q < parts; ++q)
-      items.push_back(make_uint4((uint32_t)r, q * cap, std::min(len[r], (q + 1) * cap), (uint32_t)(nslot + q + 1)));
+      items.push_back(make_uint4(r, q * cap, std::min(len[i], (q + 1) * cap), (uint32_t)(nslot + q + 1)));
     nslot += (int)parts;
   }
   std::stable_sort(items.begin(), items.end(), [](const uint4& x, const uint4& y) { return x.z - x.y > y.z - y.y; });
@@ -245,7 +252,9 @@ int sm_count(Ctx* c) {
 // strip of 1024 columns (4 per thread); an item longer than the mean work of
 // a CTA slot (8 resident CTAs per SM) would set the kernel's duration, so
 // rows with more entries are split (at least 64 entries per item).
-int build_same_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const std::vector<uint32_t>& hd, size_t ncol) {
+// Rows row0 .. row0 + hs.size() - 1 (all rows, or one shard of them).
+int build_same_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const std::vector<uint32_t>& hd, size_t ncol,
+                     size_t row0 = 0) {
   std::vector<uint32_t> len(hs.size());
   uint64_t total = 0;
   for (size_t r = 0; r < hs.size(); ++r) total += (len[r] = hs[r] + hd[r]);
@@ -254,7 +263,7 @@ int build_same_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const st
   const uint32_t cap = (uint32_t)std::max<uint64_t>(64, (total * strips + slots - 1) / slots);
   std::vector<uint4> items, split;
   int nslot = 0;
-  split_rows(len, cap, true, items, split, nslot);  // every row's output is assigned
+  split_rows(len, cap, true, items, split, nslot, row0);  // every row's output is assigned
   cn.same_cap = (int)cap;
   cn.n_same_item = items.size();
   cn.n_same_split = (int)split.size();
@@ -270,7 +279,7 @@ int build_same_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const st
 // into items of at most cap singles, cap = a quarter of the mean work per SM
 // (rounded up to a multiple of 4, at least 8), and items run longest first.
 // Large samples have many strings per SM and split nothing.
-int build_ab_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, size_t nb) {
+int build_ab_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, size_t nb, size_t row0 = 0) {
   const uint64_t nsm = (uint64_t)sm_count(c);
   uint64_t total = 0;
   for (uint32_t h : hs) total += h;
@@ -278,12 +287,78 @@ int build_ab_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, size_t nb)
   const uint32_t cap = (uint32_t)std::max<uint64_t>(8, (quarter + 3) & ~3ull);
   std::vector<uint4> items, split;
   int slot = 0;
-  split_rows(hs, cap, false, items, split, slot);  // the kernel adds to its output
+  split_rows(hs, cap, false, items, split, slot, row0);  // the kernel adds to its output
   cn.item_cap = (int)cap;
   cn.n_item = items.size();
   cn.n_split = (int)split.size();
   cn.n_part = slot;
   return upload_items(c, items, split, slot, nb, &cn.ab_item, &cn.ab_split, &cn.ypart);
+}
+
+// Position of each ket string in the packed alpha-beta kernel's staged rows
+// (Conn::kpos). A string keeps its aligned group of 8 positions (8*(k/8) ..
+// 8*(k/8)+7, a 128-byte row of 16-byte packs) and gets the slot in it that
+// spreads the singles of every bra string most evenly over the 8 bank slots:
+// a descent on the sum over bra strings of the squared per-slot counts,
+// exchanging the slots of two strings of one group. With the singles of each
+// bra string spread evenly, every quarter-warp's ket slots are balanced and
+// its records can be ordered with few bank conflicts. A quarter-warp's
+// staging stores still hit 8 different slots (the group is permuted within
+// itself), so staging stays conflict-free.
+std::vector<uint32_t> ket_positions(size_t n, const std::vector<uint32_t>& hs, const std::vector<uint64_t>& off,
+                                    const std::vector<uint64_t>& rec) {
+  std::vector<uint32_t> pos(n);
+  for (size_t k = 0; k < n; ++k) pos[k] = (uint32_t)k;
+  if (n < 16) return pos;
+  // bra strings whose singles include ket k (CSR)
+  std::vector<uint64_t> roff(n + 1, 0);
+  for (size_t r = 0; r < n; ++r)
+    for (uint32_t e = 0; e < hs[r]; ++e) ++roff[(rec[off[r] + e] & 0xffffu) + 1];
+  for (size_t k = 0; k < n; ++k) roff[k + 1] += roff[k];
+  std::vector<uint32_t> rows(roff[n]);
+  {
+    std::vector<uint64_t> fill(roff.begin(), roff.end() - 1);
+    for (size_t r = 0; r < n; ++r)
+      for (uint32_t e = 0; e < hs[r]; ++e) rows[fill[rec[off[r] + e] & 0xffffu]++] = (uint32_t)r;
+  }
+  std::vector<std::array<int16_t, 8>> h(n);
+  for (size_t r = 0; r < n; ++r) {
+    h[r].fill(0);
+    for (uint32_t e = 0; e < hs[r]; ++e) ++h[r][pos[rec[off[r] + e] & 0xffffu] & 7u];
+  }
+  for (int sweep = 0; sweep < 8; ++sweep) {
+    long long gain = 0;
+    for (size_t g0 = 0; g0 < n; g0 += 8) {
+      const size_t g1 = std::min(n, g0 + 8);
+      for (size_t a = g0; a < g1; ++a)
+        for (size_t b = a + 1; b < g1; ++b) {
+          const uint32_t sa = pos[a] & 7u, sb = pos[b] & 7u;
+          long long d = 0;
+          // ket a moves from slot sa to sb, ket b from sb to sa
+          for (uint64_t t = roff[a]; t < roff[a + 1]; ++t) {
+            auto& x = h[rows[t]];
+            d += 2 * (x[sb] - x[sa]) + 2;
+            --x[sa];
+            ++x[sb];
+          }
+          for (uint64_t t = roff[b]; t < roff[b + 1]; ++t) {
+            auto& x = h[rows[t]];
+            d += 2 * (x[sa] - x[sb]) + 2;
+            --x[sb];
+            ++x[sa];
+          }
+          if (d < 0) {
+            std::swap(pos[a], pos[b]);
+            gain += d;
+          } else {
+            for (uint64_t t = roff[b]; t < roff[b + 1]; ++t) { ++h[rows[t]][sb]; --h[rows[t]][sa]; }
+            for (uint64_t t = roff[a]; t < roff[a + 1]; ++t) { ++h[rows[t]][sa]; --h[rows[t]][sb]; }
+          }
+        }
+    }
+    if (gain == 0) break;
+  }
+  return pos;
 }
 
 // Balanced SELL-32 of the single records (see Conn::bsell). The cap starts at
@@ -292,8 +367,8 @@ int build_ab_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, size_t nb)
 // fit the kernel's shared-memory budget. The slices per warp are the smallest
 // of 8, 12, 16 that cover the virtual rows in the fewest CTAs.
 int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32_t>& hs_all,
-                        const std::vector<uint64_t>& off_all, const std::vector<uint64_t>& rec, uint32_t jb0,
-                        uint32_t jb1) {
+                        const std::vector<uint64_t>& off_all, const std::vector<uint64_t>& rec,
+                        const std::vector<uint32_t>& kpos, uint32_t jb0, uint32_t jb1) {
   // the singles of row r are rec[off_all[r] .. off_all[r] + hs_all[r]), ascending
   // ket index: the ones in [jb0, jb1) are a contiguous sub-range
   std::vector<uint32_t> hs(n);
@@ -370,131 +445,11 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
   // ket index, so the kernels' shared-memory index stays in range
   const uint64_t kPad = (1ull << 41) | (uint64_t)jb0;
   std::vector<uint64_t> sell(soff[ns] ? soff[ns] : 1, kPad);
-  std::vector<uint8_t> vcopy(sell.size(), 0);  // integral copy of each record (packed kernel)
   std::vector<uint32_t> vrow(nv ? nv : 1, 0);
-  // Record order inside each virtual row is free (it only changes the order of
-  // the sum). Per slice, step m and quarter-warp (8 lanes, one 128-byte
-  // shared-memory wavefront of 16-byte loads), pick for every lane the record
-  // whose ket index and pair index fall in the least used of the 8 bank slots
-  // (index mod 8), most constrained lane first, then improve the picks by
-  // local search on the quarter's wavefront count (distinct indices per slot;
-  // equal indices are broadcast): fewer bank conflicts on the two
-  // shared-memory loads of each record.
-  std::vector<std::vector<uint64_t>> left(32);
-  for (size_t sl = 0; sl < ns; ++sl) {
-    const size_t l_end = std::min<size_t>(32, nv - sl * 32);
-    for (size_t l = 0; l < l_end; ++l) {
-      const VRow& w = vr[sl * 32 + l];
-      left[l].assign(rec.begin() + w.beg, rec.begin() + w.beg + w.len);
-      vrow[sl * 32 + l] = w.r | (w.slot1 << 16);
-    }
-    for (uint32_t m = 0; m < slen[sl]; ++m)
-      for (size_t q = 0; q * 8 < l_end; ++q) {
-        size_t lanes[8];
-        size_t nl = 0;
-        for (size_t l = q * 8; l < std::min(l_end, q * 8 + 8); ++l)
-          if (!left[l].empty()) lanes[nl++] = l;
-        std::sort(lanes, lanes + nl, [&](size_t x, size_t y) { return left[x].size() < left[y].size(); });
-        // greedy start: least used slots first, most constrained lane first
-        size_t pick[8];
-        {
-          int cj[8] = {0}, cp[8] = {0};
-          for (size_t i = 0; i < nl; ++i) {
-            const std::vector<uint64_t>& lst = left[lanes[i]];
-            size_t best = 0;
-            int bc = 1 << 30;
-            for (size_t t = 0; t < lst.size(); ++t) {
-              const int c = cj[lst[t] & 7u] + cp[(lst[t] >> 16) & 7u];
-              if (c < bc) { bc = c; best = t; }
-            }
-            pick[i] = best;
-            ++cj[lst[best] & 7u];
-            ++cp[(lst[best] >> 16) & 7u];
-          }
-        }
-        // local search on the wavefront count of the quarter: per slot, the
-        // number of distinct ket (and pair) indices, maximum over slots
-        auto wavefronts = [&]() {
-          int w = 0;
-          for (int field = 0; field < 2; ++field) {
-            int worst = 0;
-            for (int slot = 0; slot < 8; ++slot) {
-              uint32_t seen[8];
-              int nd = 0;
-              for (size_t i = 0; i < nl; ++i) {
-                const uint64_t r = left[lanes[i]][pick[i]];
-                const uint32_t idx = field == 0 ? (uint32_t)(r & 0xffffu) : (uint32_t)((r >> 16) & 0xfffu);
-                if ((idx & 7u) != (uint32_t)slot) continue;
-                bool dup = false;
-                for (int d = 0; d < nd; ++d) dup |= seen[d] == idx;
-                if (!dup) seen[nd++] = idx;
-              }
-              worst = std::max(worst, nd);
-            }
-            w += worst;
-          }
-          return w;
-        };
-        int cur = wavefronts();
-        for (int pass = 0; pass < 3; ++pass) {
-          bool better = false;
-          for (size_t i = 0; i < nl; ++i)
-            for (size_t t = 0; t < left[lanes[i]].size(); ++t) {
-              if (t == pick[i]) continue;
-              const size_t old = pick[i];
-              pick[i] = t;
-              const int w = wavefronts();
-              if (w < cur) { cur = w; better = true; } else { pick[i] = old; }
-            }
-          if (!better) break;
-        }
-        // integral copy per pick: copy c puts pair index p in slot (p + 4c) mod 8
-        // (the packed kernel stages the integral row twice, four slots apart);
-        // the assignment with the fewest wavefronts of the quarter's integral
-        // gather, fewest copy-1 reads on ties
-        unsigned best_mask = 0;
-        {
-          int best_w = 1 << 30, best_ones = 99;
-          for (unsigned mask = 0; mask < (1u << nl); ++mask) {
-            int worst = 0;
-            for (int slot = 0; slot < 8; ++slot) {
-              uint32_t seen[8];
-              int nd = 0;
-              for (size_t i = 0; i < nl; ++i) {
-                const uint32_t c = (mask >> i) & 1u;
-                const uint32_t pq = (uint32_t)((left[lanes[i]][pick[i]] >> 16) & 0xfffu);
-                if (((pq + 4u * c) & 7u) != (uint32_t)slot) continue;
-                const uint32_t key = pq | (c << 12);
-                bool dup = false;
-                for (int d = 0; d < nd; ++d) dup |= seen[d] == key;
-                if (!dup) seen[nd++] = key;
-              }
-              worst = std::max(worst, nd);
-            }
-            const int ones = __builtin_popcount(mask);
-            if (worst < best_w || (worst == best_w && ones < best_ones)) {
-              best_w = worst;
-              best_ones = ones;
-              best_mask = mask;
-            }
-          }
-        }
-        for (size_t i = 0; i < nl; ++i) {
-          std::vector<uint64_t>& lst = left[lanes[i]];
-          sell[soff[sl] + 32ull * m + lanes[i]] = lst[pick[i]];
-          vcopy[soff[sl] + 32ull * m + lanes[i]] = (uint8_t)((best_mask >> i) & 1u);
-          lst.erase(lst.begin() + (std::ptrdiff_t)pick[i]);
-        }
-      }
-  }
-  P.nslice = ns;
-  P.nv = nv;
-  P.nsplit = (int)split_row.size();
-  P.nslot = (int)split_slot.back();
-  P.cap = (int)cap;
-  P.slices_per_warp = ks;
-  if (split_row.empty()) split_row.push_back(0);
-  // 32-bit records in blocks of 4 per lane (see SellPanel::sell32)
+  for (size_t v = 0; v < nv; ++v) vrow[v] = vr[v].r | (vr[v].slot1 << 16);
+  // 32-bit records of the packed kernel in blocks of 4 per lane (see
+  // SellPanel::sell32); the steps that round a slice up to a multiple of 4
+  // are padding at the panel's first staged position
   std::vector<uint64_t> soff4(ns + 1, 0);
   std::vector<uint32_t> slen4(ns ? ns : 1, 0);
   for (size_t sl = 0; sl < ns; ++sl) {
@@ -503,14 +458,163 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
   }
   const uint32_t kPad32 = (1u << 29) | jb0;
   std::vector<uint32_t> sell32(soff4[ns] ? soff4[ns] : 4, kPad32);
-  for (size_t sl = 0; sl < ns; ++sl)
-    for (uint32_t m = 0; m < slen[sl]; ++m)
-      for (size_t l = 0; l < 32; ++l) {
-        const uint64_t r = sell[soff[sl] + 32ull * m + l];
-        sell32[soff4[sl] + 128ull * (m >> 2) + 4 * l + (m & 3u)] =
-            (uint32_t)(r & 0xffffu) | (uint32_t)(((r >> 16) & 0xfffu) << 16) | (uint32_t)(((r >> 40) & 1u) << 28) |
-            (uint32_t)(((r >> 41) & 1u) << 29) | ((uint32_t)vcopy[soff[sl] + 32ull * m + l] << 30);
+  // Record order inside each virtual row is free (it only changes the order
+  // of the sum) and decides the bank conflicts of the packed kernel's two
+  // 16-byte shared-memory gathers per record. The 8 lanes of a quarter-warp
+  // are served together: one 128-byte wavefront when their 16-byte slots
+  // differ, one more per further distinct address in a slot. A record's ket
+  // slot is kpos[ket] mod 8 (the staged ket rows are permuted within aligned
+  // groups of 8, see ket_positions); its integral slot is pq mod 8 or
+  // (pq + 4) mod 8 (two staged copies), so the distinct pairs of one class
+  // pq mod 4 cost ceil(count / 2) wavefronts. Per quarter: a greedy start
+  // (per step, each lane takes the record whose ket slot and pair class are
+  // least used in the step, most constrained lane first), then a descent on
+  // the quarter's estimate (per step, the largest ket-slot count plus half the
+  // largest pair-class count, rounded up) by exchanging the steps of two
+  // records of one lane, until the estimate reaches the quarter's lower bound
+  // or the move budget runs out. The integral copies then alternate over the
+  // distinct pairs of a class in each step, and pad records repeat the
+  // addresses of a real record of their step (a broadcast costs nothing).
+  // Slices are ordered on several host threads, each slice with its own
+  // seeded generator, so the result does not depend on the thread count.
+  auto kslot = [&](uint64_t r) { return (uint32_t)(kpos[r & 0xffffu] & 7u); };
+  auto pcls = [](uint64_t r) { return (uint32_t)((r >> 16) & 3u); };
+  auto order_slice = [&](size_t sl) {
+    const size_t l_end = std::min<size_t>(32, nv - sl * 32);
+    const uint32_t m_len = slen[sl];
+    constexpr uint64_t kEmpty = ~0ull;
+    std::vector<uint64_t> grid;
+    std::vector<std::vector<uint64_t>> left(8);
+    std::vector<std::array<int8_t, 8>> ck;
+    std::vector<std::array<int8_t, 4>> cp;
+    std::vector<int> sc;
+    for (size_t q = 0; q * 8 < l_end; ++q) {
+      const int nl = (int)std::min<size_t>(8, l_end - q * 8);
+      grid.assign((size_t)m_len * 8, kEmpty);
+      uint32_t lmax = 0;
+      int deg[8] = {0}, pdeg[4] = {0};
+      for (int i = 0; i < nl; ++i) {
+        const VRow& w = vr[sl * 32 + q * 8 + i];
+        left[i].assign(rec.begin() + w.beg, rec.begin() + w.beg + w.len);
+        lmax = std::max(lmax, w.len);
+        for (uint64_t r : left[i]) { ++deg[kslot(r)]; ++pdeg[pcls(r)]; }
       }
+      // greedy start
+      for (uint32_t m = 0; m < m_len; ++m) {
+        int lanes[8], n_act = 0;
+        for (int i = 0; i < nl; ++i)
+          if (!left[i].empty()) lanes[n_act++] = i;
+        std::sort(lanes, lanes + n_act, [&](int x, int y) { return left[x].size() < left[y].size(); });
+        int cj[8] = {0}, cq[4] = {0};
+        for (int a = 0; a < n_act; ++a) {
+          std::vector<uint64_t>& lst = left[lanes[a]];
+          size_t best = 0;
+          int bc = 1 << 30;
+          for (size_t t = 0; t < lst.size(); ++t) {
+            const int cc = cj[kslot(lst[t])] + cq[pcls(lst[t])];
+            if (cc < bc) { bc = cc; best = t; }
+          }
+          grid[(size_t)m * 8 + lanes[a]] = lst[best];
+          ++cj[kslot(lst[best])];
+          ++cq[pcls(lst[best])];
+          lst.erase(lst.begin() + (std::ptrdiff_t)best);
+        }
+      }
+      // descent
+      ck.assign(m_len, std::array<int8_t, 8>{});
+      cp.assign(m_len, std::array<int8_t, 4>{});
+      for (uint32_t m = 0; m < m_len; ++m)
+        for (int i = 0; i < nl; ++i) {
+          const uint64_t r = grid[(size_t)m * 8 + i];
+          if (r != kEmpty) { ++ck[m][kslot(r)]; ++cp[m][pcls(r)]; }
+        }
+      auto cost = [&](uint32_t m) {
+        int a = 0, b = 0;
+        for (int x = 0; x < 8; ++x) a = std::max(a, (int)ck[m][x]);
+        for (int x = 0; x < 4; ++x) b = std::max(b, (int)cp[m][x]);
+        return a + (b + 1) / 2;
+      };
+      sc.assign(m_len, 0);
+      long long cur = 0;
+      for (uint32_t m = 0; m < m_len; ++m) cur += (sc[m] = cost(m));
+      const long long lb = (long long)std::max<int>((int)lmax, *std::max_element(deg, deg + 8)) +
+                           std::max<int>((int)lmax, (*std::max_element(pdeg, pdeg + 4) + 1) / 2);
+      std::mt19937 rng((uint32_t)(sl * 4 + q) * 2654435761u + 12345u);
+      const long long budget = (long long)kOrderEffort * m_len;
+      for (long long it = 0; it < budget && cur > lb && m_len > 1; ++it) {
+        const int i = (int)(rng() % (uint32_t)nl);
+        const uint32_t m1 = rng() % m_len, m2 = rng() % m_len;
+        if (m1 == m2) continue;
+        uint64_t& A = grid[(size_t)m1 * 8 + i];
+        uint64_t& B = grid[(size_t)m2 * 8 + i];
+        if (A == kEmpty && B == kEmpty) continue;
+        auto move = [&](uint64_t r, uint32_t from, uint32_t to) {
+          if (r == kEmpty) return;
+          --ck[from][kslot(r)]; --cp[from][pcls(r)];
+          ++ck[to][kslot(r)]; ++cp[to][pcls(r)];
+        };
+        move(A, m1, m2);
+        move(B, m2, m1);
+        const int c1 = cost(m1), c2 = cost(m2);
+        const int d = c1 + c2 - sc[m1] - sc[m2];
+        if (d <= 0) {
+          std::swap(A, B);
+          cur += d;
+          sc[m1] = c1;
+          sc[m2] = c2;
+        } else {
+          move(A, m2, m1);
+          move(B, m1, m2);
+        }
+      }
+      // emit: 64-bit records (original ket index) and 32-bit packed records
+      for (uint32_t m = 0; m < m_len; ++m) {
+        uint32_t seen[8], seen_copy[8], nseen = 0, cls_count[4] = {0, 0, 0, 0};
+        uint32_t src32 = kPad32;
+        bool have_src = false;
+        for (int i = 0; i < nl; ++i) {
+          const uint64_t r = grid[(size_t)m * 8 + i];
+          if (r == kEmpty) continue;
+          const size_t lane = q * 8 + (size_t)i;
+          sell[soff[sl] + 32ull * m + lane] = r;
+          const uint32_t pq = (uint32_t)((r >> 16) & 0xfffu);
+          uint32_t copy = 0;
+          bool dup = false;
+          for (uint32_t t = 0; t < nseen; ++t)
+            if (seen[t] == pq) { copy = seen_copy[t]; dup = true; }
+          if (!dup) {
+            copy = cls_count[pq & 3u]++ & 1u;
+            seen[nseen] = pq;
+            seen_copy[nseen++] = copy;
+          }
+          const uint32_t w32 = (kpos[r & 0xffffu] & 0xffffu) | (pq << 16) | ((uint32_t)((r >> 40) & 1u) << 28) |
+                               (copy << 30);
+          sell32[soff4[sl] + 128ull * (m >> 2) + 4 * lane + (m & 3u)] = w32;
+          if (!have_src) { src32 = w32 | (1u << 29); have_src = true; }
+        }
+        for (int i = 0; i < nl; ++i)
+          if (grid[(size_t)m * 8 + i] == kEmpty)
+            sell32[soff4[sl] + 128ull * (m >> 2) + 4 * (q * 8 + (size_t)i) + (m & 3u)] = src32;
+      }
+    }
+  };
+  {
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const unsigned nt = (unsigned)std::min<size_t>(hw, std::max<size_t>(1, ns));
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nt; ++t)
+      pool.emplace_back([&, t]() {
+        for (size_t sl = t; sl < ns; sl += nt) order_slice(sl);
+      });
+    for (auto& th : pool) th.join();
+  }
+  P.nslice = ns;
+  P.nv = nv;
+  P.nsplit = (int)split_row.size();
+  P.nslot = (int)split_slot.back();
+  P.cap = (int)cap;
+  P.slices_per_warp = ks;
+  if (split_row.empty()) split_row.push_back(0);
   SBDX_CUDA(c, cudaMalloc(&P.sell32, sizeof(uint32_t) * sell32.size()));
   SBDX_CUDA(c, cudaMalloc(&P.soff4, sizeof(uint64_t) * (ns + 1)));
   SBDX_CUDA(c, cudaMalloc(&P.slen4, sizeof(uint32_t) * slen4.size()));
@@ -612,20 +716,24 @@ int build_one(Ctx* c, int spin) {
     if (ns) SBDX_CUDA(c, cudaMemcpyAsync(cn.slen, slen.data(), sizeof(uint32_t) * ns, cudaMemcpyHostToDevice, c->stream));
     SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
     if (spin == 1) {
-      int rc = build_balanced_sell(c, cn.bal, n, hs, off, rec, 0, (uint32_t)n);
+      const std::vector<uint32_t> kpos = ket_positions(n, hs, off, rec);
+      SBDX_CUDA(c, cudaMalloc(&cn.kpos, sizeof(uint32_t) * n));
+      SBDX_CUDA(c, cudaMemcpyAsync(cn.kpos, kpos.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream));
+      int rc = build_balanced_sell(c, cn.bal, n, hs, off, rec, kpos, 0, (uint32_t)n);
       if (rc) return rc;
       // ket-range panels when the packed alpha-beta kernel (16 bytes per ket
       // and per pair index, 8 per split slot) cannot stage a whole ket row
       const size_t er = ab7_er_packs(c->npair);
       const size_t fixed = 16 * er + sizeof(double) * kMaxSplitSlots;
       if (16 * (n + er) + sizeof(double) * (size_t)cn.bal.nslot > kAbSmemBudget && fixed < kAbSmemBudget) {
-        const size_t width = ((kAbSmemBudget - fixed) / 16) & ~(size_t)1;
+        // panel widths are multiples of 8: the ket permutation keeps groups of 8
+        const size_t width = ((kAbSmemBudget - fixed) / 16) & ~(size_t)7;
         const size_t np = (n + width - 1) / width;
-        const size_t w = (n + np - 1) / np;
-        cn.panels.resize(np);
-        for (size_t q = 0; q < np; ++q) {
+        const size_t w = ((n + np - 1) / np + 7) & ~(size_t)7;
+        for (size_t q = 0; q < np && q * w < n; ++q) {
           const uint32_t lo = (uint32_t)(q * w), hi = (uint32_t)std::min(n, (q + 1) * w);
-          if ((rc = build_balanced_sell(c, cn.panels[q], n, hs, off, rec, lo, hi))) return rc;
+          cn.panels.emplace_back();
+          if ((rc = build_balanced_sell(c, cn.panels.back(), n, hs, off, rec, kpos, lo, hi))) return rc;
         }
       }
     }
@@ -637,9 +745,48 @@ int build_one(Ctx* c, int spin) {
 
 }  // namespace
 
+void free_row_range(Ctx* c) {
+  Conn& r = c->range_conn;
+  cudaFree(r.same_item); cudaFree(r.same_split); cudaFree(r.same_ypart);
+  cudaFree(r.ab_item); cudaFree(r.ab_split); cudaFree(r.ypart);
+  r.same_item = r.same_split = r.ab_item = r.ab_split = nullptr;
+  r.same_ypart = r.ypart = nullptr;
+  r.n_same_item = r.n_item = 0;
+  r.n_same_split = r.n_same_part = r.n_split = r.n_part = 0;
+  c->range_a0 = c->range_a1 = 0;
+  c->have_range = false;
+}
+
+// Work items of the alpha rows [a0, a1) only, for a sigma that writes those
+// output rows (one shard of the alpha strings): the same-spin and alpha-beta
+// items of build_same_items / build_ab_items over that range, their caps
+// derived from the range's own work.
+int build_row_range(Ctx* c, size_t a0, size_t a1) {
+  free_row_range(c);
+  const Conn& ca = c->conn[0];
+  const size_t n = a1 - a0;
+  std::vector<uint32_t> hs(n ? n : 1), hd(n ? n : 1);
+  if (n) {
+    SBDX_CUDA(c, cudaMemcpyAsync(hs.data(), ca.nsing + a0, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaMemcpyAsync(hd.data(), ca.ndoub + a0, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  hs.resize(n);
+  hd.resize(n);
+  Conn& r = c->range_conn;
+  int rc = build_same_items(c, r, hs, hd, c->nb, a0);
+  if (rc) return rc;
+  if ((rc = build_ab_items(c, r, hs, c->nb, a0))) return rc;
+  c->range_a0 = a0;
+  c->range_a1 = a1;
+  c->have_range = true;
+  return 0;
+}
+
 void free_connectivity(Ctx* c) {
   clear_sigma_graphs(c);
   release_stored(c);  // its elements come from the connectivity
+  free_row_range(c);
   free_conn(c->conn[0]);
   free_conn(c->conn[1]);
   cudaFree(c->d_Da); cudaFree(c->d_Db); cudaFree(c->d_Da32); cudaFree(c->d_Db32);

@@ -1530,7 +1530,7 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
         break;
       }
       steps += added;
-      since += added;
+      ++since;  // Davidson iterations since the last exact refresh (defect_every counts these)
       const int n = k + nv;
       if (!gen_eigen_k(n, k, M, S, ld, theta, X)) {
         c->err = "davidson: projected overlap matrix is not positive definite";

@@ -45,9 +45,10 @@ constexpr uint32_t kInfoSingle = 1u << 30;
 // bit 41 set.
 struct SellPanel {
   uint64_t* sell = nullptr;        // [soff[nslice]]
-  // the same records in 32 bits (bits 0-15 ket, 16-27 pair index, 28 sign,
-  // 29 padding, 30 integral copy), read by the packed alpha-beta kernel in
-  // blocks of 4 per lane:
+  // the same records in 32 bits (bits 0-15 position of the ket in the staged
+  // rows, Conn::kpos; 16-27 pair index, 28 sign, 29 padding, 30 integral
+  // copy), read by the packed alpha-beta kernel in blocks of 4 per lane (a
+  // padding record repeats the addresses of a real record of its step):
   // record m of lane l of slice s at sell32[soff4[s] + 128*(m/4) + 4*l + m%4],
   // slen4[s] = slen[s] rounded up to a multiple of 4 (padding records)
   uint32_t* sell32 = nullptr;      // [soff4[nslice]]
@@ -98,6 +99,12 @@ struct Conn {
   // shared memory) split the ket range into slices that it can.
   SellPanel bal;
   std::vector<SellPanel> panels;
+  // (beta spin only) position of ket string k in the packed alpha-beta
+  // kernel's staged ket rows: a permutation within aligned groups of 8 chosen
+  // to spread every bra string's singles over the shared-memory bank slots;
+  // the 32-bit records (SellPanel::sell32) hold positions, the 64-bit ones
+  // ket indices
+  uint32_t* kpos = nullptr;   // [n]
   // work items of the packed alpha-beta kernel (alpha spin only), one CTA
   // each, longest first: {bra alpha string, first single, one past the last
   // single, 1 + partial-row slot or 0}. A string with more singles than the
@@ -184,6 +191,12 @@ struct Ctx {
   // connectivity (0 = alpha, 1 = beta)
   Conn conn[2];
   bool have_conn = false;
+  // a shard of the alpha strings: the work items (same-spin and alpha-beta
+  // fields of a Conn, nothing else set) of the output rows [range_a0,
+  // range_a1) of a row-range sigma (sigma_rows_device)
+  Conn range_conn;
+  size_t range_a0 = 0, range_a1 = 0;
+  bool have_range = false;
   // diagonal
   double* d_hii = nullptr;
   bool have_hii = false;
@@ -337,6 +350,12 @@ __host__ __device__ __forceinline__ uint64_t other_range(int spin, int x, int y)
 // ---- internal entry points shared between translation units ------------------
 int build_connectivity(Ctx* c);
 void free_connectivity(Ctx* c);
+// Work items of the output rows [a0, a1) (Ctx::range_conn) and their release.
+int build_row_range(Ctx* c, size_t a0, size_t a1);
+void free_row_range(Ctx* c);
+// Rows [a0, a1) of S = H X: X the whole vector (na x nb), S the (a1 - a0) x nb
+// output rows; a0 a multiple of 8 (or a0 == a1).
+int sigma_rows_device(Ctx* c, int precision, const void* X, void* S, size_t a0, size_t a1);
 int build_g_table(Ctx* c);
 int build_coulomb_tables(Ctx* c);
 int diag_terms(Ctx* c);

@@ -1413,14 +1413,14 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
                    const uint64_t* __restrict__ soff4, const uint32_t* __restrict__ slen4, size_t nslice,
                    const uint32_t* __restrict__ vrow, size_t nv, const uint32_t* __restrict__ split_row,
                    const uint32_t* __restrict__ split_slot, int nsplit, const T* __restrict__ Vt, size_t vstride,
-                   int npair, uint32_t epad, uint32_t jb0, size_t nbp, const uint4* __restrict__ items,
-                   double* __restrict__ ypart, double* __restrict__ Y) {
+                   int npair, uint32_t epad, uint32_t jb0, size_t nbp, const uint32_t* __restrict__ kpos,
+                   const uint4* __restrict__ items, double* __restrict__ ypart, double* __restrict__ Y) {
   using RP = RowPack<T>;
   using P = typename RP::P;
   constexpr int VR = RP::kRows;
   constexpr int kWarps = kAb6Threads / 32;
   extern __shared__ __align__(16) unsigned char smem[];
-  P* xs = reinterpret_cast<P*>(smem);   // [nbp]: ket indices jb0 .. jb0 + nbp - 1
+  P* xs = reinterpret_cast<P*>(smem);   // [nbp]: ket jb at kpos[jb] - jb0 (jb in jb0 .. jb0 + nbp - 1)
   P* er = xs + nbp;                     // [epad + npair]: copy 0 at pq, copy 1 at epad + pq
   double* part = reinterpret_cast<double*>(er + epad + npair);
   // work item: bra alpha string, range of its singles, output row
@@ -1451,11 +1451,13 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
       neg[e] = (inf >> 31) != 0;
     }
     __syncthreads();
+    // ket jb goes to position kpos[jb] - jb0, a permutation within aligned
+    // groups of 8: the 8 lanes of a quarter-warp store to 8 different slots
     for (size_t t = threadIdx.x; t < nbp; t += kAb6Threads) {
       P p;
 #pragma unroll
       for (int e = 0; e < VR; ++e) RP::set(p, e, e < nr ? __ldg(xrow[e] + t) : (T)0);
-      xs[t] = p;
+      xs[__ldg(kpos + jb0 + t) - jb0] = p;
     }
     for (int t = threadIdx.x; t < npair; t += kAb6Threads) {
       P p;
@@ -1472,8 +1474,8 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
     for (int k = 0; k < KS; ++k) {
       const size_t sl = slice_of(k);
       if (sl >= nslice) continue;
-      // 32-bit records (bits 0-15 ket, 16-27 pair, 28 sign, 29 pad, 30 integral copy), four per
-      // lane per 16-byte load, the next block in flight
+      // 32-bit records (bits 0-15 staged ket position, 16-27 pair, 28 sign, 29 pad, 30 integral
+      // copy), four per lane per 16-byte load, the next block in flight
       const uint32_t nblk = slen4[sl] >> 2;
       const uint4* rp = reinterpret_cast<const uint4*>(sell + soff4[sl]) + lane;
       double s = acc[k];
@@ -1484,7 +1486,7 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const uint32_t rec = recs[q];
-          const P x = xs[(rec & 0xffffu) - jb0];  // pad records: ket = jb0
+          const P x = xs[(rec & 0xffffu) - jb0];  // pad records repeat a real record's addresses
           const P ev = er[((rec >> 16) & 0xfffu) + ((rec >> 30) & 1u) * epad];
           double d = RP::dot(ev, x);
           d = ((rec >> 29) & 1u) ? 0.0 : d;
@@ -1539,8 +1541,10 @@ bool ab7_fits(const Ctx* c) {
   return true;
 }
 
+// `it` supplies the work items: the alpha connectivity itself, or the items
+// of a row range (Ctx::range_conn).
 template <typename T, int KS>
-int launch_ab_v7(Ctx* c, const T* Xp, const SellPanel& bp) {
+int launch_ab_v7(Ctx* c, const T* Xp, const SellPanel& bp, const Conn& it) {
   const Conn& ca = c->conn[0];
   const bool f64 = std::is_same<T, double>::value;
   const T* Vt = f64 ? (const T*)c->d_V : (const T*)c->d_V32;
@@ -1549,12 +1553,12 @@ int launch_ab_v7(Ctx* c, const T* Xp, const SellPanel& bp) {
   SBDX_CUDA(c, cudaFuncSetAttribute(sigma_ab_v7_kernel<T, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kAbSmemBudget));
   const size_t per_cta = (size_t)(kAb6Threads / 32) * KS;
-  dim3 grid((unsigned)ca.n_item, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
+  dim3 grid((unsigned)it.n_item, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
   if (grid.y == 0) grid.y = 1;
   sigma_ab_v7_kernel<T, KS><<<grid, kAb6Threads, smem, c->stream>>>(
       Xp, c->xsa, ca.off, ca.ket, ca.info, bp.sell32, bp.soff4, bp.slen4, bp.nslice, bp.vrow, bp.nv,
       bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, (int)c->npair, (uint32_t)ab7_epad(c->npair), bp.jb0,
-      (size_t)(bp.jb1 - bp.jb0), ca.ab_item, ca.ypart, c->d_y);
+      (size_t)(bp.jb1 - bp.jb0), c->conn[1].kpos, it.ab_item, it.ypart, c->d_y);
   SBDX_LAUNCHED(c);
   return 0;
 }
@@ -1573,17 +1577,17 @@ __global__ void ab_split_fixup_kernel(const uint4* __restrict__ split, const dou
 }
 
 template <typename T>
-int run_ab_v7(Ctx* c, const T* Xp) {
-  const Conn& ca = c->conn[0];
+int run_ab_v7(Ctx* c, const T* Xp, const Conn* items = nullptr) {
+  const Conn& ca = items ? *items : c->conn[0];
   if (ca.n_item == 0) return 0;  // no alpha string has a single excitation
   if (ca.n_part > 0)
     SBDX_CUDA(c, cudaMemsetAsync(ca.ypart, 0, sizeof(double) * (size_t)ca.n_part * c->xsa, c->stream));
   std::vector<SellPanel> one;
   for (const SellPanel& bp : *ab7_panels(c, one)) {
     int rc;
-    if (bp.slices_per_warp >= 16) rc = launch_ab_v7<T, 16>(c, Xp, bp);
-    else if (bp.slices_per_warp >= 12) rc = launch_ab_v7<T, 12>(c, Xp, bp);
-    else rc = launch_ab_v7<T, 8>(c, Xp, bp);
+    if (bp.slices_per_warp >= 16) rc = launch_ab_v7<T, 16>(c, Xp, bp, ca);
+    else if (bp.slices_per_warp >= 12) rc = launch_ab_v7<T, 12>(c, Xp, bp, ca);
+    else rc = launch_ab_v7<T, 8>(c, Xp, bp, ca);
     if (rc) return rc;
   }
   if (ca.n_split > 0) {
@@ -1843,6 +1847,57 @@ int run_sigma(Ctx* c, const T* X, T* S) {
   return run_sigma_v5<T>(c, X, S);
 }
 
+// Output rows [a0, a1) of the alpha-first sigma (one shard of the alpha
+// strings; the reference's bra block of a rank, chemistry/tpb/mult.h:429-432).
+// The phase split covers the whole input (every ket row may be read); the
+// alpha same-spin and alpha-beta kernels run the range's work items
+// (Ctx::range_conn); the beta same-spin kernel runs on the range's columns of
+// the transposed input (its output and Coulomb-table columns offset by a0,
+// a multiple of 8 so that the vector loads stay aligned); the combine writes
+// the range's rows into S, whose row 0 is alpha string a0.
+template <typename T>
+int run_sigma_rows(Ctx* c, const Tune& tune, const T* X, T* S, size_t a0, size_t a1) {
+  using V = typename Prec<T>::V;
+  const size_t na = c->na, nb = c->nb, nr = a1 - a0;
+  const bool f64 = std::is_same<T, double>::value;
+  const Conn& ca = c->conn[0];
+  const Conn& cb = c->conn[1];
+  const Conn& rc_items = c->range_conn;
+  Conn ra = ca;  // the alpha lists with the range's same-spin work items
+  ra.same_item = rc_items.same_item;
+  ra.n_same_item = rc_items.n_same_item;
+  ra.same_split = rc_items.same_split;
+  ra.n_same_split = rc_items.n_same_split;
+  ra.n_same_part = rc_items.n_same_part;
+  ra.same_ypart = rc_items.same_ypart;
+  const V* valA = f64 ? (const V*)ca.val : (const V*)ca.val32;
+  const V* valB = f64 ? (const V*)cb.val : (const V*)cb.val32;
+  const V* Db = f64 ? (const V*)c->d_Db : (const V*)c->d_Db32;
+  const V* Da = f64 ? (const V*)c->d_Da : (const V*)c->d_Da32;
+  T* xp = reinterpret_cast<T*>(c->d_xp);
+  T* xpt = reinterpret_cast<T*>(c->d_xt);
+  int rc = 0;
+  {
+    dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((na + 31) / 32));
+    phase_split_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(X, na, nb, c->d_a, c->d_b, xp, xpt, c->xsa, c->xsb);
+    SBDX_LAUNCHED(c);
+  }
+  if (nr == 0) return 0;
+  if ((rc = run_same_v6<T>(c, tune.same_code, xp, na, nb, c->xsa, ra, valA, Db, c->db_stride, c->d_hii, c->d_y)))
+    return rc;
+  if ((rc = run_same_v6<T>(c, tune.same_code, xpt + a0, nb, nr, c->xsb, cb, valB, Da + a0, c->da_stride, nullptr,
+                           c->d_yt + a0)))
+    return rc;
+  if ((rc = run_ab_v7<T>(c, xp, &rc_items))) return rc;
+  {
+    dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((nr + 31) / 32));
+    combine_phase_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(c->d_y + a0 * c->xsa, c->d_yt + a0, nr, nb,
+                                                                 c->d_a + a0, c->d_b, S, c->xsa, c->xsb);
+    SBDX_LAUNCHED(c);
+  }
+  return 0;
+}
+
 }  // namespace
 
 int build_coulomb_tables(Ctx* c) {
@@ -2030,6 +2085,47 @@ int sigma_graph(Ctx* c, int precision, const void* X, void* S) {
 }
 
 }  // namespace
+
+int sigma_rows_device(Ctx* c, int precision, const void* X, void* S, size_t a0, size_t a1) {
+  if (a0 > a1 || a1 > c->na) {
+    c->err = "sigma_rows: need a0 <= a1 <= na";
+    return SBDX_ERR_ARG;
+  }
+  if (a0 % 8 != 0 && a0 != a1) {
+    c->err = "sigma_rows: the first row must be a multiple of 8";
+    return SBDX_ERR_ARG;
+  }
+  if (precision != 0 && precision != 1) {
+    c->err = "sigma_rows: precision must be SBDX_FP64 or SBDX_FP32";
+    return SBDX_ERR_ARG;
+  }
+  if (precision == 0 && c->stored.val != nullptr) {
+    c->err = "sigma_rows: a row range is evaluated on the fly; release the stored Hamiltonian first";
+    return SBDX_ERR_STATE;
+  }
+  if (!c->have_conn) {
+    int rc = build_connectivity(c);
+    if (rc) return rc;
+  }
+  if (!c->have_hii) {
+    int rc = diag_terms(c);
+    if (rc) return rc;
+  }
+  int rc = ensure_sigma_scratch(c);
+  if (rc) return rc;
+  const bool f64 = precision == 0;
+  Tune t = effective_tune(c, f64);
+  if (!is_v6(t)) t = kDefaultTune[f64 ? 0 : 1];  // the row range runs the alpha-first kernels
+  if (!ab7_fits(c)) {
+    c->err = "sigma_rows: the packed alpha-beta kernel cannot stage this problem's rows";
+    return SBDX_ERR_ARG;
+  }
+  if (!c->have_range || c->range_a0 != a0 || c->range_a1 != a1) {
+    if ((rc = build_row_range(c, a0, a1))) return rc;
+  }
+  if (f64) return run_sigma_rows<double>(c, t, static_cast<const double*>(X), static_cast<double*>(S), a0, a1);
+  return run_sigma_rows<float>(c, t, static_cast<const float*>(X), static_cast<float*>(S), a0, a1);
+}
 
 int sigma_device(Ctx* c, int precision, const void* X, void* S) {
   if (!c->have_conn) {

@@ -34,6 +34,7 @@ EXPORTS = [
     "sbdx_phase_times", "sbdx_set_tuning", "sbdx_autotune", "sbdx_davidson_roots",
     "sbdx_build_hamiltonian", "sbdx_release_hamiltonian", "sbdx_wavefunction_device", "sbdx_get_wavefunction",
     "sbdx_rdm_device", "sbdx_occupation_device", "sbdx_alpha_weights_device", "sbdx_energy_backward_device",
+    "sbdx_sigma_rows_device",
 ]
 PHASES = ["alpha_same_spin", "transpose", "beta_same_spin", "alpha_beta", "combine"]
 
@@ -203,6 +204,12 @@ class Context:
     def sigma_device(self, precision, c_ptr: int, s_ptr: int):
         self._check(self.lib.sbdx_sigma_device(self.h, ctypes.c_int(precision), ctypes.c_void_p(c_ptr),
                                                ctypes.c_void_p(s_ptr)))
+
+    def sigma_rows_device(self, precision, c_ptr: int, s_ptr: int, a0: int, a1: int):
+        """Rows [a0, a1) of S = H C (sbdx_sigma_rows_device): c_ptr the whole
+        input, s_ptr the (a1 - a0) * nb output rows."""
+        self._check(self.lib.sbdx_sigma_rows_device(self.h, ctypes.c_int(precision), ctypes.c_void_p(c_ptr),
+                                                    ctypes.c_void_p(s_ptr), ctypes.c_size_t(a0), ctypes.c_size_t(a1)))
 
     def davidson(self, max_it=1, max_nb=10, eps=1e-4, max_time=86400.0, precision=SBDX_FP64, defect_every=0,
                  verbose=0, W=None, to_host=True):

@@ -1,8 +1,8 @@
-"""The multi-GPU path of bench.py runs N independent replicas (one process per
-GPU, no data-path collective); its only collective is the max over ranks of
-the step time. This checks that aggregation with world size 2 over gloo on
-the CPU: both ranks see the slowest rank's time, and the whole-job
-throughput is N x the per-replica work over that time."""
+"""bench.py times every multi-rank measurement as the maximum over ranks of
+the device-timed step (one all-reduce of the step time). This checks that
+aggregation with world size 2 over gloo on the CPU: both ranks see the
+slowest rank's time, and the whole-job throughput of ranks that each do the
+same work is N x that work over that time."""
 import os
 import socket
 
