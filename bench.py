@@ -327,9 +327,13 @@ def run_batched(args) -> dict:
         out["tuning"] = batch.tune()
         runs = {}
         ref_E = None
-        for label, prec, threads in (("sequential_fp64", sbdx.SBDX_FP64, 1), ("sequential_mixed", sbdx.SBDX_FP32, 1),
-                                     ("batched_fp64", sbdx.SBDX_FP64, args.batch_threads),
-                                     ("batched_mixed", sbdx.SBDX_FP32, args.batch_threads)):
+        for label, prec, threads, graphs in (("sequential_fp64", sbdx.SBDX_FP64, 1, False),
+                                             ("sequential_mixed", sbdx.SBDX_FP32, 1, False),
+                                             ("batched_fp64", sbdx.SBDX_FP64, args.batch_threads, False),
+                                             ("batched_mixed", sbdx.SBDX_FP32, args.batch_threads, False),
+                                             ("batched_mixed_graph_steps", sbdx.SBDX_FP32, args.batch_threads, True),
+                                             ("sequential_mixed_graph_steps", sbdx.SBDX_FP32, 1, True)):
+            batch.set_graph_steps(graphs)
             E, R, infos, sec = batch.solve(nroots=2, max_it=100, max_nb=12, eps=args.davidson_tol, precision=prec,
                                            nthreads=threads)
             if ref_E is None:
@@ -342,8 +346,11 @@ def run_batched(args) -> dict:
                            "sigma_det_pairs_per_s": float(sum(n * q for n, q in zip(nsig, pairs)) / sec),
                            "subspace_seconds_median": float(np.median(t_sub)),
                            "subspace_seconds_max": float(np.max(t_sub))}
+        batch.set_graph_steps(False)
         out["runs"] = runs
         out["speedup_batched_mixed_vs_sequential_fp64"] = runs["sequential_fp64"]["seconds"] / runs["batched_mixed"]["seconds"]
+        out["speedup_batched_mixed_graph_steps_vs_sequential_fp64"] = (
+            runs["sequential_fp64"]["seconds"] / runs["batched_mixed_graph_steps"]["seconds"])
     return out
 
 
@@ -907,6 +914,8 @@ def summary(line) -> dict:
             out[f"{lab}_cfg3_max_abs_dE"] = max(abs(x) for x in m[lab]["dE_vs_fp64"])
             out[f"{lab}_cfg3_max_rdm1_err"] = max(m[lab]["rdm1_maxabs_vs_fp64"])
     out["batched_mixed_vs_sequential_fp64"] = get("batched", "speedup_batched_mixed_vs_sequential_fp64")
+    out["batched_mixed_graph_steps_vs_sequential_fp64"] = get("batched",
+                                                              "speedup_batched_mixed_graph_steps_vs_sequential_fp64")
     d = line.get("differentiation")
     if d:
         out["backward_over_forward"] = d["backward_seconds"] / d["forward_seconds"]

@@ -250,6 +250,18 @@ int sbdx_occupation_device(sbdx_ctx* ctx, const double* dW, double* density);
 int sbdx_alpha_weights_device(sbdx_ctx* ctx, const double* dW, double* weights);
 int sbdx_energy_backward_device(sbdx_ctx* ctx, const double* dW, double* dE_dh, double* dE_deri);
 
+/* Solver of sbdx_davidson_roots (no counterpart in the reference, whose
+ * Davidson steps are host loops over distributed vectors, davidson.h:661-924):
+ * on != 0 runs the device-driven form, in which an iteration (expansion of
+ * every root, its products, the projections, the generalised Rayleigh-Ritz
+ * problem solved on the device, the anchor update) is one CUDA graph launched
+ * without a host round trip; the host reads each iteration's residual
+ * estimates one iteration later and launches the exact FP64 refreshes from
+ * them. Same algorithm and results as the host-driven form (every root is
+ * expanded in every iteration, Gram-Schmidt always makes two passes). Needs a
+ * non-default stream for the graphs (else the same kernels run unrecorded). */
+int sbdx_set_graph_steps(sbdx_ctx* ctx, int on);
+
 /* 1-/2-RDM of a vector W (host, na*nb doubles). Replaces Correlation
  * (chemistry/tpb/correlation.h:194-444). one: 2*L*L doubles; two: 4*L^4
  * doubles (may be NULL to skip the 2-RDM). */
@@ -291,6 +303,8 @@ int sbdx_batch_add(sbdx_batch* batch, const uint64_t* alpha, size_t na, const ui
                    int* index);
 int sbdx_batch_size(const sbdx_batch* batch);
 int sbdx_batch_dims(const sbdx_batch* batch, int index, size_t* na, size_t* nb);
+/* sbdx_set_graph_steps for every subspace of the batch (and those added later). */
+int sbdx_batch_set_graph_steps(sbdx_batch* batch, int on);
 /* Tunes the sigma launch shapes on the largest subspace (sbdx_autotune) and
  * applies them to all subspaces. */
 int sbdx_batch_tune(sbdx_batch* batch, int* same_code, int* ab_code);

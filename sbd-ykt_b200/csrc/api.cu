@@ -422,6 +422,13 @@ int sbdx_sigma_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS) {
   });
 }
 
+int sbdx_set_graph_steps(sbdx_ctx* ctx, int on) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    c->graph_steps = on != 0;
+    return SBDX_OK;
+  });
+}
+
 int sbdx_sigma_rows_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS, size_t a0, size_t a1) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {
     if (!dC || (!dS && a1 > a0)) { c->err = "sigma_rows_device: null pointer"; return SBDX_ERR_ARG; }

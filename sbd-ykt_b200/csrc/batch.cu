@@ -44,6 +44,7 @@ struct sbdx_batch {
     int nroots = 0;
   };
   std::vector<Sub> subs;
+  bool graph_steps = false;  // the subspaces' solves run one CUDA graph per iteration
 };
 
 namespace {
@@ -126,6 +127,7 @@ int sbdx_batch_add(sbdx_batch* b, const uint64_t* alpha, size_t na, const uint64
     if ((rc = sbdx_diag_terms(ctx, nullptr))) return drop(rc);
     if ((rc = sbdx::ensure_sigma_scratch(c))) return drop(rc);
     c->use_graphs = true;
+    c->graph_steps = b->graph_steps;
     b->subs.push_back({ctx, nullptr, 0});
     if (index) *index = (int)b->subs.size() - 1;
     return SBDX_OK;
@@ -134,6 +136,13 @@ int sbdx_batch_add(sbdx_batch* b, const uint64_t* alpha, size_t na, const uint64
   } catch (...) {
     return fail(b, SBDX_ERR_ARG, "batch_add: unexpected host exception");
   }
+}
+
+int sbdx_batch_set_graph_steps(sbdx_batch* b, int on) {
+  if (!b) return SBDX_ERR_ARG;
+  for (auto& sub : b->subs) sub.ctx->c.graph_steps = on != 0;
+  b->graph_steps = on != 0;
+  return SBDX_OK;
 }
 
 int sbdx_batch_tune(sbdx_batch* b, int* same_code, int* ab_code) {

@@ -583,7 +583,11 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
           for (uint32_t t = 0; t < nseen; ++t)
             if (seen[t] == pq) { copy = seen_copy[t]; dup = true; }
           if (!dup) {
-            copy = cls_count[pq & 3u]++ & 1u;
+            // the distinct pairs of class pq mod 4 go alternately to bank
+            // slots (pq mod 4) and (pq mod 4) + 4: copy 0 reads slot pq mod 8,
+            // copy 1 the slot four further on
+            const uint32_t target = (pq & 3u) + 4u * (cls_count[pq & 3u]++ & 1u);
+            copy = (pq & 7u) == target ? 0u : 1u;
             seen[nseen] = pq;
             seen_copy[nseen++] = copy;
           }

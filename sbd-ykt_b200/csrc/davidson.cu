@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdio>
 #include <algorithm>
+#include <map>
 #include <type_traits>
 
 namespace sbdx {
@@ -1634,6 +1635,698 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
   return 0;
 }
 
+// ---- device-driven block Davidson: one CUDA graph per iteration ---------------
+//
+// The algorithm of davidson_block (FP64 anchors plus corrections of type TC,
+// Olsen expansion, classical Gram-Schmidt, generalised Rayleigh-Ritz, thick
+// restart, exact FP64 refresh of the anchors) with every decision inside an
+// iteration taken on the device, so that an iteration is one graph launch
+// with no host round trip:
+//  - the projected matrices M and S stay on the device and kernels update
+//    them; one CTA solves the generalised eigenproblem (ritz_kernel:
+//    Cholesky of S, parallel cyclic Jacobi, back-substitution);
+//  - every root adds a correction in every iteration; a correction that
+//    Gram-Schmidt annihilates is stored as zero and its basis slot is left
+//    out of the Rayleigh-Ritz problem;
+//  - Gram-Schmidt always makes two passes;
+//  - the anchors' renormalisation is a kernel that skips factors of 1.
+// The host launches iteration t + 1 before it reads the status that
+// iteration t copied to pinned memory (residual estimates, energies, error
+// word), and decides there whether to refresh the anchors with exact FP64
+// products (the criteria of davidson_block, one iteration later) or stop.
+// Graphs are captured on first use, one per kind (iteration or refresh),
+// number of corrections and current anchor buffer, and replayed after that.
+
+constexpr int kStatusSlots = 3;  // two iterations in flight + one refresh
+
+struct GStatus {
+  double theta[kMaxRoots];
+  double r_est[kMaxRoots];
+  int err;     // 1: S not positive definite, 2: a Ritz vector lost its norm
+  int ndead;   // corrections of the last iteration that Gram-Schmidt removed
+};
+
+// Lowest k eigenpairs of M x = theta S x over the basis slots in use (the k
+// anchors and the corrections not removed by Gram-Schmidt, of the first
+// n_all slots of the ld-strided symmetric arrays, at most 64), on one CTA:
+// S = L L^T (right-looking Cholesky), A = L^-1 M L^-T, parallel cyclic Jacobi
+// on A (round-robin pairs: n/2 disjoint rotations per round), ascending
+// order, X = L^-T Y (column-major n_all x k, zero at removed slots). The same
+// steps as the host solver gen_eigen_k, in another rotation order.
+__global__ void __launch_bounds__(256)
+ritz_kernel(int n_all, int k, int ld, const double* __restrict__ M, const double* __restrict__ S,
+            const int* __restrict__ dead, double* __restrict__ theta, double* __restrict__ X,
+            GStatus* __restrict__ st) {
+  extern __shared__ double sm[];
+  __shared__ double s_cs[32], s_sn[32], s_red[8];
+  __shared__ int s_pa[32], s_pb[32], s_bad, s_ord[64], s_map[64], s_n;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (tid == 0) {
+    int m = 0;
+    for (int i = 0; i < n_all; ++i)
+      if (i < k || !dead[i - k]) s_map[m++] = i;
+    s_n = m;
+    s_bad = 0;
+  }
+  __syncthreads();
+  const int n = s_n;
+  double* Lf = sm;            // n x n, lower triangle used
+  double* A = Lf + n * n;     // n x n
+  double* V = A + n * n;      // n x n eigenvectors
+  for (int t = tid; t < n * n; t += nt) {
+    const int i = t % n, j = t / n;
+    Lf[t] = S[s_map[i] + (size_t)ld * s_map[j]];
+    A[t] = M[s_map[i] + (size_t)ld * s_map[j]];
+    V[t] = i == j ? 1.0 : 0.0;
+  }
+  for (int t = tid; t < n_all * k; t += nt) X[t] = 0.0;
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    if (tid == 0) {
+      const double d = Lf[j + n * j];
+      if (!(d > 0.0)) s_bad = 1;
+      Lf[j + n * j] = d > 0.0 ? sqrt(d) : 1.0;
+    }
+    __syncthreads();
+    const double d = Lf[j + n * j];
+    for (int i = j + 1 + tid; i < n; i += nt) Lf[i + n * j] /= d;
+    __syncthreads();
+    const int m = n - j - 1;
+    for (int t = tid; t < m * m; t += nt) {
+      const int i = j + 1 + t % m, l = j + 1 + t / m;
+      if (i >= l) Lf[i + n * l] -= Lf[i + n * j] * Lf[l + n * j];
+    }
+    __syncthreads();
+  }
+  if (s_bad) {
+    if (tid == 0) st->err = 1;
+    return;
+  }
+  for (int col = tid; col < n; col += nt)  // T = L^-1 M, in A
+    for (int i = 0; i < n; ++i) {
+      double v = A[i + n * col];
+      for (int q = 0; q < i; ++q) v -= Lf[i + n * q] * A[q + n * col];
+      A[i + n * col] = v / Lf[i + n * i];
+    }
+  __syncthreads();
+  for (int row = tid; row < n; row += nt)  // A = T L^-T
+    for (int i = 0; i < n; ++i) {
+      double v = A[row + n * i];
+      for (int q = 0; q < i; ++q) v -= Lf[i + n * q] * A[row + n * q];
+      A[row + n * i] = v / Lf[i + n * i];
+    }
+  __syncthreads();
+  for (int t = tid; t < n * n; t += nt) {
+    const int i = t % n, j = t / n;
+    if (i < j) {
+      const double a = 0.5 * (A[i + n * j] + A[j + n * i]);
+      A[i + n * j] = a;
+      A[j + n * i] = a;
+    }
+  }
+  __syncthreads();
+  const int nn = n + (n & 1);  // players of the round-robin (index n is a bye when n is odd)
+  const int npairs = nn / 2;
+  for (int sweep = 0; sweep < 60 && n > 1; ++sweep) {
+    double off = 0.0, dg = 0.0;
+    for (int t = tid; t < n * n; t += nt) {
+      const int i = t % n, j = t / n;
+      const double a = A[t] * A[t];
+      if (i < j) off += a;
+      else if (i == j) dg += a;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_down_sync(0xffffffffu, off, o);
+      dg += __shfl_down_sync(0xffffffffu, dg, o);
+    }
+    __syncthreads();
+    if ((tid & 31) == 0) { s_red[tid >> 5] = off; }
+    __syncthreads();
+    double off_all = 0.0;
+    for (int w = 0; w < (nt >> 5); ++w) off_all += s_red[w];
+    __syncthreads();
+    if ((tid & 31) == 0) { s_red[tid >> 5] = dg; }
+    __syncthreads();
+    double dg_all = 0.0;
+    for (int w = 0; w < (nt >> 5); ++w) dg_all += s_red[w];
+    __syncthreads();
+    if (off_all <= 1e-32 * dg_all || off_all < 1e-300) break;
+    for (int round = 0; round < nn - 1; ++round) {
+      for (int pr = tid; pr < npairs; pr += nt) {
+        int a, b;
+        if (pr == 0) { a = round; b = nn - 1; }
+        else { a = (round + pr) % (nn - 1); b = (round - pr + (nn - 1)) % (nn - 1); }
+        if (a > b) { const int x = a; a = b; b = x; }
+        double cs = 1.0, sn = 0.0;
+        if (b < n) {
+          const double apq = A[a + n * b];
+          if (apq != 0.0) {
+            const double th = (A[b + n * b] - A[a + n * a]) / (2.0 * apq);
+            const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+            cs = 1.0 / sqrt(t * t + 1.0);
+            sn = t * cs;
+          }
+        }
+        s_pa[pr] = a;
+        s_pb[pr] = b;
+        s_cs[pr] = cs;
+        s_sn[pr] = sn;
+      }
+      __syncthreads();
+      for (int t = tid; t < npairs * n; t += nt) {  // columns a, b of A and V
+        const int pr = t / n, row = t % n, a = s_pa[pr], b = s_pb[pr];
+        if (b >= n || s_sn[pr] == 0.0) continue;
+        const double cs = s_cs[pr], sn = s_sn[pr];
+        const double akp = A[row + n * a], akq = A[row + n * b];
+        A[row + n * a] = cs * akp - sn * akq;
+        A[row + n * b] = sn * akp + cs * akq;
+        const double vkp = V[row + n * a], vkq = V[row + n * b];
+        V[row + n * a] = cs * vkp - sn * vkq;
+        V[row + n * b] = sn * vkp + cs * vkq;
+      }
+      __syncthreads();
+      for (int t = tid; t < npairs * n; t += nt) {  // rows a, b of A
+        const int pr = t / n, col = t % n, a = s_pa[pr], b = s_pb[pr];
+        if (b >= n || s_sn[pr] == 0.0) continue;
+        const double cs = s_cs[pr], sn = s_sn[pr];
+        const double apk = A[a + n * col], aqk = A[b + n * col];
+        A[a + n * col] = cs * apk - sn * aqk;
+        A[b + n * col] = sn * apk + cs * aqk;
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0) {  // ascending order of the eigenvalues
+    for (int i = 0; i < n; ++i) s_ord[i] = i;
+    for (int i = 1; i < n; ++i) {
+      const int x = s_ord[i];
+      int j = i - 1;
+      while (j >= 0 && A[s_ord[j] + n * s_ord[j]] > A[x + n * x]) { s_ord[j + 1] = s_ord[j]; --j; }
+      s_ord[j + 1] = x;
+    }
+  }
+  __syncthreads();
+  for (int r = tid; r < k; r += nt) {  // x = L^-T y for the k lowest, at the slots in use
+    const int o = s_ord[r];
+    theta[r] = A[o + n * o];
+    for (int i = n - 1; i >= 0; --i) {
+      double v = V[i + n * o];
+      for (int q = i + 1; q < n; ++q) v -= Lf[q + n * i] * X[s_map[q] + (size_t)n_all * r];
+      X[s_map[i] + (size_t)n_all * r] = v / Lf[i + n * i];
+    }
+  }
+}
+
+// The new correction j (basis slot k + j): its row and column of M and S from
+// the dots <C_i|HC_j>, <C_i|C_j> (i <= j, interleaved) and <W_q|C_j>,
+// <HW_q|C_j> (q < k). (A removed correction is zero, so are its dots; the
+// Rayleigh-Ritz kernel leaves its slot out.)
+__global__ void scatter_new_kernel(int k, int j, int ld, const double* __restrict__ d, double* __restrict__ M,
+                                   double* __restrict__ S) {
+  const int bj = k + j;
+  for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+    const int bi = k + i;
+    M[bi + (size_t)ld * bj] = M[bj + (size_t)ld * bi] = d[2 * i];
+    S[bi + (size_t)ld * bj] = S[bj + (size_t)ld * bi] = d[2 * i + 1];
+  }
+  for (int q = threadIdx.x; q < k; q += blockDim.x) {
+    S[q + (size_t)ld * bj] = S[bj + (size_t)ld * q] = d[2 * (j + 1) + q];
+    M[q + (size_t)ld * bj] = M[bj + (size_t)ld * q] = d[2 * (j + 1) + k + q];
+  }
+}
+
+// Stores v / |v| into the correction slot, or zeros (and marks the slot
+// removed) when Gram-Schmidt left less than 1e-24 of the norm it started with.
+template <typename TC>
+__global__ void store_correction_kernel(const double* __restrict__ v, const double* __restrict__ nv2,
+                                        const double* __restrict__ before, size_t D, TC* __restrict__ dst,
+                                        int* __restrict__ dead) {
+  const double a = *nv2;
+  const bool ok = a > 1e-24 * *before;
+  const double f = ok ? 1.0 / sqrt(a) : 0.0;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x)
+    dst[s] = (TC)(v[s] * f);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *dead = ok ? 0 : 1;
+}
+
+// After the anchors moved to the Ritz vectors: normalisation factors fs
+// (|W'_r|^2 in nw2), residual estimates, the new anchors' rows of M and S
+// (X^T M and X^T S scaled by fs, read before they are overwritten), the
+// anchor block (diag(theta), I), and the status.
+__global__ void __launch_bounds__(256)
+post_update_kernel(int k, int nv, int nact, int ld, double* __restrict__ M, double* __restrict__ S,
+                   const double* __restrict__ X,
+                   const double* __restrict__ theta, const double* __restrict__ nw2, double* __restrict__ nr2,
+                   double* __restrict__ fs, const int* __restrict__ dead, GStatus* __restrict__ st) {
+  __shared__ double rowM[kMaxRoots * 64], rowS[kMaxRoots * 64], s_fs[kMaxRoots];
+  const int n = k + nv;
+  if (threadIdx.x < k) {
+    const int r = threadIdx.x;
+    const double h = nw2[r];
+    if (!(h > 0.5 && h < 2.0)) st->err = 2;
+    const double f = fabs(h - 1.0) > 1e-13 ? 1.0 / sqrt(h) : 1.0;
+    const double re = sqrt(nr2[r]) * f;
+    s_fs[r] = f;
+    fs[r] = f;
+    nr2[r] = re * re;
+    st->theta[r] = theta[r];
+    st->r_est[r] = re;
+  }
+  if (threadIdx.x == 0) {
+    int nd = 0;
+    for (int j = nv - nact; j < nv; ++j) nd += j >= 0 ? dead[j] : 0;
+    st->ndead = nd;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < k * nv; t += blockDim.x) {
+    const int r = t / nv, q = k + t % nv;
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < n; ++i) {
+      a += X[i + (size_t)n * r] * M[i + (size_t)ld * q];
+      b += X[i + (size_t)n * r] * S[i + (size_t)ld * q];
+    }
+    rowM[t] = a * s_fs[r];
+    rowS[t] = b * s_fs[r];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < k * nv; t += blockDim.x) {
+    const int r = t / nv, q = k + t % nv;
+    M[r + (size_t)ld * q] = M[q + (size_t)ld * r] = rowM[t];
+    S[r + (size_t)ld * q] = S[q + (size_t)ld * r] = rowS[t];
+  }
+  for (int t = threadIdx.x; t < k * k; t += blockDim.x) {
+    const int r = t % k, q = t / k;
+    M[r + (size_t)ld * q] = r == q ? theta[r] : 0.0;
+    S[r + (size_t)ld * q] = r == q ? 1.0 : 0.0;
+  }
+}
+
+// Exact refresh, part 1: the anchor block of M and S from the dots
+// <W_q|HW_r> (d[2kr + q]) and <W_q|W_r> (d[2kr + k + q]), q <= r; theta_r =
+// M_rr / S_rr (the Rayleigh quotients).
+__global__ void refresh_block_kernel(int k, int ld, const double* __restrict__ d, double* __restrict__ M,
+                                     double* __restrict__ S, double* __restrict__ theta, GStatus* __restrict__ st) {
+  for (int t = threadIdx.x; t < k * k; t += blockDim.x) {
+    const int q = t % k, r = t / k;
+    if (q > r) continue;
+    M[q + (size_t)ld * r] = M[r + (size_t)ld * q] = d[2 * k * r + q];
+    S[q + (size_t)ld * r] = S[r + (size_t)ld * q] = d[2 * k * r + k + q];
+  }
+  __syncthreads();
+  if (threadIdx.x < k) {
+    const int r = threadIdx.x;
+    theta[r] = M[r + (size_t)ld * r] / S[r + (size_t)ld * r];
+    st->theta[r] = theta[r];
+  }
+}
+
+// Exact refresh, part 2: the exact residual norms (|R_r|^2 in nr2) are the
+// new estimates; <HW_r|C_j> (d[r * nv + j]) into M.
+__global__ void refresh_tail_kernel(int k, int nv, int ld, const double* __restrict__ nr2, const double* __restrict__ d,
+                                    double* __restrict__ M, GStatus* __restrict__ st) {
+  if (threadIdx.x < k) st->r_est[threadIdx.x] = sqrt(nr2[threadIdx.x]);
+  if (threadIdx.x == 0) st->ndead = 0;
+  for (int t = threadIdx.x; t < k * nv; t += blockDim.x) {
+    const int r = t / nv, q = k + t % nv;
+    M[r + (size_t)ld * q] = M[q + (size_t)ld * r] = d[t];
+  }
+}
+
+// Thick restart of M, S and the removed-slot flags: keep the anchors and the
+// corrections drop .. drop + keep - 1 (moved to slots 0 .. keep - 1). The
+// sources lie at or after their destinations, so one ordered pass suffices.
+__global__ void restart_kernel(int k, int keep, int drop, int ld, double* __restrict__ M, double* __restrict__ S,
+                               int* __restrict__ dead) {
+  const int n = k + keep;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        const int si = i < k ? i : i + drop, sj = j < k ? j : j + drop;
+        M[i + (size_t)ld * j] = M[si + (size_t)ld * sj];
+        S[i + (size_t)ld * j] = S[si + (size_t)ld * sj];
+      }
+    for (int j = 0; j < keep; ++j) dead[j] = dead[j + drop];
+  }
+}
+
+template <typename TC>
+int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, double* E, double* res,
+                         sbdx_davidson_info& info) {
+  constexpr bool kMixed = std::is_same<TC, float>::value;
+  const size_t D = c->na * c->nb;
+  const int nc = std::max(std::min(kMixed ? 2 * p.max_nb : p.max_nb, 64 - k), 2 * k);
+  const int keep = std::max(k, nc / 3);
+  const int period = p.defect_every > 0 ? p.defect_every : 0;
+  const int ld = k + nc;
+  struct AsyncGuard {
+    Ctx* c;
+    std::vector<void*> p;
+    void* host = nullptr;
+    std::vector<cudaGraphExec_t> execs;
+    ~AsyncGuard() {
+      cudaStreamSynchronize(c->stream);
+      for (cudaGraphExec_t e : execs) cudaGraphExecDestroy(e);
+      for (void* q : p) cudaFreeAsync(q, c->stream);
+      if (host) cudaFreeHost(host);
+      pool_trim(c);
+    }
+  } g{c, {}};
+  auto alloc = [&](void** ptr, size_t bytes) -> cudaError_t {
+    const cudaError_t e = pool_alloc(c, ptr, bytes);
+    if (e == cudaSuccess) g.p.push_back(*ptr);
+    return e;
+  };
+  Work wk;
+  double *wpartial = nullptr, *wscal = nullptr, *wu = nullptr;
+  SBDX_CUDA(c, alloc((void**)&wpartial, sizeof(double) * kRedBlocks * (2 * nc + 2 * kMaxRoots + 4)));
+  SBDX_CUDA(c, alloc((void**)&wscal, sizeof(double) * (kbDots + (size_t)(k + 2) * (nc + 2 * k) + 64)));
+  SBDX_CUDA(c, alloc((void**)&wu, sizeof(double) * ((size_t)(k + nc) * k + k + nc + 8)));
+  TC *C = nullptr, *HC = nullptr;
+  double *A = nullptr, *R = nullptr, *V = nullptr, *dM = nullptr, *dS = nullptr, *misc = nullptr;
+  int* dead = nullptr;
+  GStatus* dst = nullptr;
+  SBDX_CUDA(c, alloc((void**)&C, sizeof(TC) * D * nc));
+  SBDX_CUDA(c, alloc((void**)&HC, sizeof(TC) * D * nc));
+  SBDX_CUDA(c, alloc((void**)&A, sizeof(double) * D * 4 * k));  // anchors: [W | HW] twice, the current by parity
+  SBDX_CUDA(c, alloc((void**)&R, sizeof(double) * D * k));
+  SBDX_CUDA(c, alloc((void**)&V, sizeof(double) * D));
+  SBDX_CUDA(c, alloc((void**)&dM, sizeof(double) * ld * ld));
+  SBDX_CUDA(c, alloc((void**)&dS, sizeof(double) * ld * ld));
+  SBDX_CUDA(c, alloc((void**)&misc, sizeof(double) * 16));  // fs[4], before
+  SBDX_CUDA(c, alloc((void**)&dead, sizeof(int) * nc));
+  SBDX_CUDA(c, alloc((void**)&dst, sizeof(GStatus)));
+  GStatus* hst = nullptr;
+  SBDX_CUDA(c, cudaMallocHost((void**)&hst, sizeof(GStatus) * kStatusSlots));
+  g.host = hst;
+  struct Borrow {
+    Work& w;
+    ~Borrow() { w.partial = w.scal = w.u = nullptr; }
+  } borrow{wk};
+  wk.partial = wpartial;
+  wk.scal = wscal;
+  wk.u = wu;
+  double* s = wk.scal;
+  double* gso = wk.u;
+  double* Xd = wk.u + k + nc + 8;
+  double* fs = misc;
+  double* before = misc + 8;
+  SBDX_CUDA(c, cudaMemsetAsync(dM, 0, sizeof(double) * ld * ld, c->stream));
+  SBDX_CUDA(c, cudaMemsetAsync(dS, 0, sizeof(double) * ld * ld, c->stream));
+  SBDX_CUDA(c, cudaMemsetAsync(dead, 0, sizeof(int) * nc, c->stream));
+  SBDX_CUDA(c, cudaMemsetAsync(dst, 0, sizeof(GStatus), c->stream));
+  const size_t ritz_smem = sizeof(double) * 3 * 64 * 64;
+  SBDX_CUDA(c, cudaFuncSetAttribute(ritz_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ritz_smem));
+  const auto t0 = std::chrono::steady_clock::now();
+  int rc = 0;
+  double* W0 = A;  // parity 0: [W | HW] in A[0 .. 2kD), parity 1 in A[2kD .. 4kD)
+  SBDX_CUDA(c, cudaMemcpyAsync(W0, dW, sizeof(double) * D * k, cudaMemcpyDeviceToDevice, c->stream));
+  for (int r = 0; r < k; ++r) {  // start vectors: MGS-orthonormalised in FP64
+    double* wr = W0 + (size_t)r * D;
+    for (int pass = 0; pass < 2 && r > 0; ++pass) {
+      if ((rc = multidot<double, double>(c, wk, W0, D, r, wr, D, gso))) return rc;
+      gs_subtract_block_kernel<double><<<kRedBlocks, kRedThreads, 0, c->stream>>>(wr, W0, r, (const double*)nullptr, 0,
+                                                                                gso, D, wk.partial);
+      SBDX_LAUNCHED(c);
+    }
+    if ((rc = multidot<double, double>(c, wk, wr, D, 1, wr, D, s + kbNV))) return rc;
+    scale_store_kernel<double, double><<<kRedBlocks, kRedThreads, 0, c->stream>>>(wr, s + kbNV, D, wr);
+    SBDX_LAUNCHED(c);
+  }
+  auto anchors = [&](int par) { return A + (size_t)par * 2 * k * D; };
+  auto next_nv = [&](int nv, int nact) { return (nv + nact > nc ? keep : nv) + nact; };
+  // one exact refresh of the anchors of buffer `par` (nv corrections)
+  auto enqueue_refresh = [&](int nv, int par, int slot) -> int {
+    double* W = anchors(par);
+    double* HW = W + (size_t)k * D;
+    int r2;
+    for (int r = 0; r < k; ++r) {
+      if ((r2 = sigma_typed<double>(c, W + (size_t)r * D, HW + (size_t)r * D))) return r2;
+    }
+    for (int r = 0; r < k; ++r) {
+      if ((r2 = multidot<double, double>(c, wk, W, D, k, HW + (size_t)r * D, D, s + kbDots + 2 * k * r))) return r2;
+      if ((r2 = multidot<double, double>(c, wk, W, D, k, W + (size_t)r * D, D, s + kbDots + 2 * k * r + k))) return r2;
+    }
+    refresh_block_kernel<<<1, 64, 0, c->stream>>>(k, ld, s + kbDots, dM, dS, s + kbTheta, dst);
+    SBDX_LAUNCHED(c);
+    residual_block_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, s + kbTheta, k, D, R, wk.partial);
+    SBDX_LAUNCHED(c);
+    if ((r2 = finalize(c, wk, k, s + kbNR2))) return r2;
+    for (int r = 0; r < k && nv > 0; ++r)
+      if ((r2 = multidot<TC, double>(c, wk, C, D, nv, HW + (size_t)r * D, D, s + kbDots + (size_t)r * nv))) return r2;
+    refresh_tail_kernel<<<1, 256, 0, c->stream>>>(k, nv, ld, s + kbNR2, s + kbDots, dM, dst);
+    SBDX_LAUNCHED(c);
+    SBDX_CUDA(c, cudaMemcpyAsync(hst + slot, dst, sizeof(GStatus), cudaMemcpyDeviceToHost, c->stream));
+    return 0;
+  };
+  // one iteration from anchor buffer `par` with nv corrections, expanding the
+  // roots of `mask` (those whose residual estimate was not below eps); the new
+  // anchors go to buffer 1 - par
+  auto enqueue_step = [&](int nv, int par, int slot, int mask) -> int {
+    double* W = anchors(par);
+    double* HW = W + (size_t)k * D;
+    double* Wn = anchors(1 - par);
+    double* HWn = Wn + (size_t)k * D;
+    int r2;
+    const int nact = __builtin_popcount((unsigned)mask);
+    if (nv + nact > nc) {  // thick restart: keep the newest corrections beside the anchors
+      const int drop = nv - keep;
+      for (int j = 0; j < keep; ++j) {  // ascending: a source slot is read before it can be overwritten
+        SBDX_CUDA(c, cudaMemcpyAsync(C + (size_t)j * D, C + (size_t)(drop + j) * D, sizeof(TC) * D,
+                                     cudaMemcpyDeviceToDevice, c->stream));
+        SBDX_CUDA(c, cudaMemcpyAsync(HC + (size_t)j * D, HC + (size_t)(drop + j) * D, sizeof(TC) * D,
+                                     cudaMemcpyDeviceToDevice, c->stream));
+      }
+      restart_kernel<<<1, 32, 0, c->stream>>>(k, keep, drop, ld, dM, dS, dead);
+      SBDX_LAUNCHED(c);
+      nv = keep;
+    }
+    for (int r = 0; r < k; ++r) {
+      if (!((mask >> r) & 1)) continue;
+      const double* Rr = R + (size_t)r * D;
+      const double* Wr = W + (size_t)r * D;
+      olsen_precond_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(Rr, Wr, c->d_hii, s + kbTheta + r,
+                                                                      s + kbNR2 + r, D, V, wk.partial);
+      SBDX_LAUNCHED(c);
+      if ((r2 = finalize(c, wk, 2, s + kbAB))) return r2;
+      olsen_apply_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(V, Wr, c->d_hii, s + kbTheta + r, s + kbAB, D,
+                                                                    wk.partial);
+      SBDX_LAUNCHED(c);
+      if ((r2 = finalize(c, wk, 2, s + kbOlap))) return r2;  // kbOlap, kbNV
+      SBDX_CUDA(c, cudaMemcpyAsync(before, s + kbNV, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+      for (int pass = 0; pass < 2; ++pass) {
+        if ((r2 = multidot<double, double>(c, wk, W, D, k, V, D, gso))) return r2;
+        if (nv > 0 && (r2 = multidot<TC, double>(c, wk, C, D, nv, V, D, gso + k))) return r2;
+        gs_subtract_block_kernel<TC><<<kRedBlocks, kRedThreads, 0, c->stream>>>(V, W, k, C, nv, gso, D, wk.partial);
+        SBDX_LAUNCHED(c);
+        if ((r2 = finalize(c, wk, 1, s + kbNV))) return r2;
+      }
+      const int j = nv;
+      TC* Cb = C + (size_t)j * D;
+      TC* HCb = HC + (size_t)j * D;
+      store_correction_kernel<TC><<<kRedBlocks, kRedThreads, 0, c->stream>>>(V, s + kbNV, before, D, Cb, dead + j);
+      SBDX_LAUNCHED(c);
+      if ((r2 = sigma_typed<TC>(c, Cb, HCb))) return r2;
+      ++nv;
+      {
+        static const unsigned g2 = wave_of(multidot2_kernel<TC, TC>);
+        dim3 grid(g2, (unsigned)((nv + kDotChunk - 1) / kDotChunk));
+        multidot2_kernel<TC, TC><<<grid, kRedThreads, 0, c->stream>>>(C, D, nv, HCb, Cb, D, wk.partial);
+        SBDX_LAUNCHED(c);
+        if ((r2 = finalize(c, wk, 2 * nv, s + kbDots, g2))) return r2;
+      }
+      if ((r2 = multidot<double, TC>(c, wk, W, D, 2 * k, Cb, D, s + kbDots + 2 * nv))) return r2;
+      scatter_new_kernel<<<1, 64, 0, c->stream>>>(k, j, ld, s + kbDots, dM, dS);
+      SBDX_LAUNCHED(c);
+    }
+    ritz_kernel<<<1, 256, ritz_smem, c->stream>>>(k + nv, k, ld, dM, dS, dead, s + kbTheta, Xd, dst);
+    SBDX_LAUNCHED(c);
+    unsigned ga = kRedBlocks;
+    if ((r2 = launch_update_anchors<TC>(c, wk, k, W, HW, C, HC, nv, Xd, s + kbTheta, D, Wn, HWn, R, &ga))) return r2;
+    finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, (int)ga, k, s + kbNW2);
+    SBDX_LAUNCHED(c);
+    finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial + (size_t)k * ga, (int)ga, k, s + kbNR2);
+    SBDX_LAUNCHED(c);
+    post_update_kernel<<<1, 256, 0, c->stream>>>(k, nv, nact, ld, dM, dS, Xd, s + kbTheta, s + kbNW2, s + kbNR2, fs,
+                                                 dead, dst);
+    SBDX_LAUNCHED(c);
+    scale_anchors_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(Wn, HWn, R, fs, k, D);
+    SBDX_LAUNCHED(c);
+    SBDX_CUDA(c, cudaMemcpyAsync(hst + slot, dst, sizeof(GStatus), cudaMemcpyDeviceToHost, c->stream));
+    return 0;
+  };
+  // launches: the first iteration and the first refresh run eagerly (they set
+  // up the kernels' launch shapes outside any capture); after that each
+  // (kind, corrections, anchor buffer, status slot) is captured into a graph on
+  // first use and replayed
+  struct Cached {
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long kernels = 0;
+  };
+  std::map<long long, Cached> cache;
+  const bool capture_ok = c->stream != nullptr;
+  bool warm[2] = {false, false};
+  auto launch = [&](int kind, int nv, int par, int slot, int mask) -> int {
+    const long long key = (((long long)kind * 128 + nv) * 8 + par * 4 + slot) * 16 + mask;
+    Cached& e = cache[key];
+    if (e.exec) {
+      SBDX_CUDA(c, cudaGraphLaunch(e.exec, c->stream));
+      c->launches += e.kernels;
+      return 0;
+    }
+    const bool cap = capture_ok && warm[kind];
+    warm[kind] = true;
+    const unsigned long long l0 = c->launches;
+    const bool ug = c->use_graphs;
+    if (cap) {
+      c->use_graphs = false;  // the sigma's kernels go into this graph, not a graph of their own
+      SBDX_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    }
+    int r2 = kind == 0 ? enqueue_step(nv, par, slot, mask) : enqueue_refresh(nv, par, slot);
+    if (!cap) return r2;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+    c->use_graphs = ug;
+    if (r2) { if (graph) cudaGraphDestroy(graph); return r2; }
+    if (ce != cudaSuccess) { set_cuda_err(c, ce, "davidson graph capture"); return SBDX_ERR_CUDA; }
+    const cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) { e.exec = nullptr; set_cuda_err(c, ie, "davidson graph instantiate"); return SBDX_ERR_CUDA; }
+    g.execs.push_back(e.exec);
+    e.kernels = c->launches - l0;
+    SBDX_CUDA(c, cudaGraphLaunch(e.exec, c->stream));
+    return 0;
+  };
+  auto all_below = [&](const double* x) {
+    for (int r = 0; r < k; ++r) if (!(x[r] < p.eps)) return false;
+    return true;
+  };
+  auto worst = [&](const double* x) {
+    double w = 0.0;
+    for (int r = 0; r < k; ++r) w = std::max(w, x[r]);
+    return w;
+  };
+  int nv = 0, par = 0, steps = 0, since = 0, stale = 0;
+  double r_exact[kMaxRoots], best = 1e300;
+  auto refresh = [&]() -> int {
+    int r2 = launch(1, nv, par, 2, 0);
+    if (r2) return r2;
+    for (int r = 0; r < k; ++r) info.n_sigma64++;
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    const GStatus& h = hst[2];
+    for (int r = 0; r < k; ++r) {
+      r_exact[r] = h.r_est[r];
+      E[r] = h.theta[r];
+    }
+    since = 0;
+    best = 1e300;
+    stale = 0;
+    return 0;
+  };
+  if ((rc = refresh())) return rc;
+  double r_ref = worst(r_exact);
+  const int max_steps = p.max_it * p.max_nb;
+  // iterations launched and not yet read: their status slots and numbers of
+  // expanded roots, in order
+  std::vector<std::pair<int, int>> inflight;
+  std::vector<cudaEvent_t> evs(2);
+  for (auto& ev : evs) SBDX_CUDA(c, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  struct EvGuard {
+    std::vector<cudaEvent_t>& e;
+    ~EvGuard() { for (auto x : e) cudaEventDestroy(x); }
+  } evg{evs};
+  int it_slot = 0, last_ndead = 0, last_nact = k;
+  bool converged = all_below(r_exact), stalled = false;
+  // roots to expand: those whose newest known residual is not below eps
+  int mask = 0;
+  auto set_mask = [&](const double* x) {
+    mask = 0;
+    for (int r = 0; r < k; ++r)
+      if (!(x[r] < p.eps)) mask |= 1 << r;
+    if (mask == 0) mask = (1 << k) - 1;
+  };
+  set_mask(r_exact);
+  auto launch_step = [&]() -> int {
+    int r2 = launch(0, nv, par, it_slot, mask);
+    if (r2) return r2;
+    SBDX_CUDA(c, cudaEventRecord(evs[it_slot], c->stream));
+    const int nact = __builtin_popcount((unsigned)mask);
+    inflight.emplace_back(it_slot, nact);
+    it_slot ^= 1;
+    nv = next_nv(nv, nact);
+    par ^= 1;
+    steps += nact;
+    ++since;
+    if (kMixed) info.n_sigma += nact; else info.n_sigma64 += nact;
+    return 0;
+  };
+  while (!converged && !stalled) {
+    if (p.verbose) {
+      std::printf(" Davidson graph step %d: E0=%.12f max exact residual %.6e\n", steps, E[0], worst(r_exact));
+      std::fflush(stdout);
+    }
+    if (steps >= max_steps || seconds_since(t0) > p.max_time) break;
+    if (inflight.empty() && (rc = launch_step())) return rc;
+    const bool more = steps < max_steps;
+    if (more && (rc = launch_step())) return rc;  // iteration t + 1 queued before t is read
+    const int slot = inflight.front().first;
+    last_nact = inflight.front().second;
+    inflight.erase(inflight.begin());
+    SBDX_CUDA(c, cudaEventSynchronize(evs[slot]));
+    const GStatus h = hst[slot];
+    if (h.err == 1) { c->err = "davidson: projected overlap matrix is not positive definite"; return 5; }
+    if (h.err == 2) { c->err = "davidson: Ritz vector lost its normalisation"; return 5; }
+    last_ndead = h.ndead;
+    for (int r = 0; r < k; ++r) E[r] = h.theta[r];
+    set_mask(h.r_est);
+    const double w = worst(h.r_est);
+    bool due;
+    if (!kMixed) {
+      due = all_below(h.r_est);  // exact products: the estimates are exact residuals
+    } else {
+      if (w < kStallGain * best) { best = w; stale = 0; } else { ++stale; }
+      due = period > 0 ? since >= period
+                       : (w < kRefreshDrop * r_ref || all_below(h.r_est) || stale >= kStallSteps);
+    }
+    if (last_ndead >= last_nact) due = true;  // nothing new: refresh (or stop when that changes nothing)
+    if (!due && more && steps < max_steps && seconds_since(t0) <= p.max_time) continue;
+    // drain the queued iteration, then refresh from the newest anchors
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (!inflight.empty()) {
+      last_ndead = hst[inflight.back().first].ndead;
+      last_nact = inflight.back().second;
+      inflight.clear();
+    }
+    const int since_before = since;
+    const bool nothing_new = last_ndead >= last_nact;
+    if (kMixed || nothing_new) {
+      if ((rc = refresh())) return rc;
+    } else {  // the newest iteration's residuals are exact
+      for (int r = 0; r < k; ++r) {
+        r_exact[r] = hst[it_slot ^ 1].r_est[r];
+        E[r] = hst[it_slot ^ 1].theta[r];
+      }
+    }
+    r_ref = worst(r_exact);
+    converged = all_below(r_exact);
+    set_mask(r_exact);
+    if (nothing_new && since_before <= 2) stalled = true;
+  }
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (!inflight.empty() && !converged) {  // stopped on a limit: take the newest anchors exactly
+    inflight.clear();
+    if ((rc = refresh())) return rc;
+  }
+  if (converged) info.converged = 1;
+  SBDX_CUDA(c, cudaMemcpyAsync(dW, anchors(par), sizeof(double) * D * k, cudaMemcpyDeviceToDevice, c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int r = 0; r < k; ++r) res[r] = r_exact[r];
+  info.energy = E[0];
+  info.residual = worst(r_exact);
+  info.seconds = seconds_since(t0);
+  return 0;
+}
+
+
 }  // namespace
 
 int davidson(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info) {
@@ -1731,6 +2424,10 @@ int davidson_roots(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
   }
   if (!c->have_conn) { int rc = build_connectivity(c); if (rc) return rc; }
   if (!c->have_hii) { int rc = diag_terms(c); if (rc) return rc; }
+  if (c->graph_steps) {
+    if (p.precision == 0) return davidson_block_graph<double>(c, p, k, dW, E, res, info);
+    if (p.precision == 1) return davidson_block_graph<float>(c, p, k, dW, E, res, info);
+  }
   if (p.precision == 0) return davidson_block<double>(c, p, k, dW, E, res, info);
   if (p.precision == 1) return davidson_block<float>(c, p, k, dW, E, res, info);
   c->err = "davidson_roots: precision must be SBDX_FP64 or SBDX_FP32";

@@ -20,6 +20,9 @@
 // Layout: one[s*L^2 + p + L q], two[(s + 2t)*L^4 + i + L j + L^2 k + L^3 l].
 #include "sbdx_internal.cuh"
 
+#include <algorithm>
+#include <vector>
+
 namespace sbdx {
 
 int ensure_sigma_scratch(Ctx* c);
@@ -97,7 +100,9 @@ __global__ void diag_finalize_kernel(int L, const double* __restrict__ Pa, const
   if (p == q) {
     one[(size_t)p + L * p] += Pa[t];
     one[L2 + (size_t)p + L * p] += Pb[t];
-  } else {
+  }
+  if (two == nullptr) return;  // the 1-RDM alone
+  if (p != q) {
     two[0 * L4 + d] += Pa[t];
     two[0 * L4 + x] -= Pa[t];
     two[3 * L4 + d] += Pb[t];
@@ -172,7 +177,7 @@ rdm_same_kernel(int spin, const double* __restrict__ W, size_t rows, size_t cols
     const uint32_t neg = (sbit ^ (uint32_t)popc64(o & om)) & 1u;
     const double t = neg ? -x : x;
     s += t;
-    if (single) {
+    if (single && two != nullptr) {
       uint64_t bits = o;
       while (bits) {
         const int q = __ffsll((long long)bits) - 1;
@@ -189,6 +194,7 @@ rdm_same_kernel(int spin, const double* __restrict__ W, size_t rows, size_t cols
   const int so = spin + 2 * (1 - spin), os = (1 - spin) + 2 * spin;
   if (single) {
     if (lane == 0) atomicAdd(&one[(size_t)spin * L2 + oi + (size_t)L * oa], s);
+    if (two == nullptr) return;  // the 1-RDM alone
     // same-spin occupied orbitals of the bra (including oi itself, whose
     // four terms cancel exactly as in the reference)
     uint64_t bits = sr;
@@ -210,7 +216,7 @@ rdm_same_kernel(int spin, const double* __restrict__ W, size_t rows, size_t cols
         atomicAdd(&two[os * L4 + q + (size_t)L * oa + L2 * q + L3 * oi], v);
       }
     }
-  } else if (lane == 0 && s != 0.0) {
+  } else if (lane == 0 && s != 0.0 && two != nullptr) {
     // oi = a_e, oj = b_e (bra-only); oa = i_e, ob = j_e (ket-only); same spin
     atomicAdd(&two[ss * L4 + i_e + (size_t)L * j_e + L2 * (a_e + (size_t)L * b_e)], s);
     atomicAdd(&two[ss * L4 + j_e + (size_t)L * i_e + L2 * (b_e + (size_t)L * a_e)], s);
@@ -283,6 +289,114 @@ rdm_ab_kernel(const double* __restrict__ W, size_t nb, const uint64_t* __restric
         atomicAdd(&two[(sj + 2 * si) * L4 + ob + (size_t)L * oa + L2 * (oi + (size_t)L * oj)], -sg);
       }
     }
+  }
+}
+
+// Alpha single x beta single pairs (task type 0), without atomics: the
+// singles of each spin are grouped by their excitation pattern (hole, particle),
+// and the contribution of a pair depends on the pair of patterns only through
+// the two reference parities, which split into an alpha-string part and a
+// beta-string part. A CTA takes a chunk of at most kAbChunk alpha singles of
+// one alpha pattern; per alpha single (bra ia -> ket ja) it stages the rows
+// W[ia, :] and W[ja, :] in shared memory, and warp w sums, for the beta
+// patterns w, w + 16, ..., all their beta singles (bra ib -> ket jb) of
+// +-W[ia, ib] W[ja, jb] in a fixed lane order and shuffle tree; the warp owns
+// those patterns' accumulators, so every sum has one fixed order. The chunk's
+// sums go to partial[chunk][beta pattern]; rdm_ab_finalize_kernel adds the
+// chunks of one alpha pattern in order and writes the two 2-RDM elements of
+// each pattern pair (no other kernel writes them).
+constexpr int kAbChunk = 32;
+constexpr int kAbDetThreads = 512;
+
+// Combined parity mask of the two reference parity() calls of a pair (one
+// per spin of the string): parity(det, s, e) on the interleaved determinant
+// counts alpha orbitals in [(s+1)/2, (e+1)/2), beta orbitals in [s/2, e/2) and
+// the spin-orbital s itself; the parity of a sum of popcounts is the popcount
+// of the XOR of the masks.
+__device__ __forceinline__ void pair_parity_masks(int s1, int e1, int s2, int e2, uint64_t& ma, uint64_t& mb) {
+  ma = range_mask((s1 + 1) >> 1, (e1 + 1) >> 1) ^ range_mask((s2 + 1) >> 1, (e2 + 1) >> 1);
+  mb = range_mask(s1 >> 1, e1 >> 1) ^ range_mask(s2 >> 1, e2 >> 1);
+  if (s1 & 1) mb ^= 1ull << (s1 >> 1); else ma ^= 1ull << (s1 >> 1);
+  if (s2 & 1) mb ^= 1ull << (s2 >> 1); else ma ^= 1ull << (s2 >> 1);
+}
+
+__global__ void __launch_bounds__(kAbDetThreads)
+rdm_ab_det_kernel(const double* __restrict__ W, size_t nb, const uint64_t* __restrict__ astr,
+                  const uint64_t* __restrict__ bstr, const uint4* __restrict__ chunks,
+                  const uint32_t* __restrict__ arec, const uint32_t* __restrict__ bpat_off,
+                  const uint32_t* __restrict__ bpat_key, const uint32_t* __restrict__ brec, int npb,
+                  double* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* wi = reinterpret_cast<double*>(smem);  // [nb] row ia
+  double* wj = wi + nb;                          // [nb] row ja
+  double* acc = wj + nb;                         // [npb]
+  const uint4 ch = chunks[blockIdx.x];           // {alpha pattern key, first single, count, 0}
+  const int ia_h = (int)(ch.x >> 6), ia_p = (int)(ch.x & 63u);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int kWarps = kAbDetThreads / 32;
+  for (int p = threadIdx.x; p < npb; p += kAbDetThreads) acc[p] = 0.0;
+  for (uint32_t q = 0; q < ch.z; ++q) {
+    const uint32_t ar = arec[ch.y + q];
+    const size_t ia = ar & 0xffffu, ja = ar >> 16;
+    __syncthreads();
+    for (size_t t = threadIdx.x; t < nb; t += kAbDetThreads) {
+      wi[t] = W[ia * nb + t];
+      wj[t] = W[ja * nb + t];
+    }
+    __syncthreads();
+    const uint64_t alpha_bra = astr[ia];
+    for (int p = warp; p < npb; p += kWarps) {
+      const uint32_t key = bpat_key[p];
+      const int ib_h = (int)(key >> 6), ib_p = (int)(key & 63u);
+      const int c0 = 2 * ia_p, c1 = 2 * ib_p + 1, d0 = 2 * ia_h, d1 = 2 * ib_h + 1;
+      const int I = c0 < c1 ? c0 : c1, J = c0 < c1 ? c1 : c0;
+      const int A = d0 < d1 ? d0 : d1, B = d0 < d1 ? d1 : d0;
+      uint64_t ma, mb;
+      pair_parity_masks(I < A ? I : A, I < A ? A : I, J < B ? J : B, J < B ? B : J, ma, mb);
+      const uint32_t pa = (uint32_t)popc64(alpha_bra & ma) & 1u;
+      double s = 0.0;
+      for (uint32_t m = bpat_off[p] + lane; m < bpat_off[p + 1]; m += 32) {
+        const uint32_t br = brec[m];
+        const uint32_t ib = br & 0xffffu, jb = br >> 16;
+        const double v = wi[ib] * wj[jb];
+        const uint32_t par = (pa + (uint32_t)popc64(bstr[ib] & mb)) & 1u;
+        s += par ? -v : v;
+      }
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (lane == 0) acc[p] += s;
+    }
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < npb; p += kAbDetThreads) partial[(size_t)blockIdx.x * npb + p] = acc[p];
+}
+
+// Sum of the chunks of each alpha pattern (in chunk order) for every beta
+// pattern, written to the two 2-RDM elements of the pattern pair (the
+// reference's TwoDiffCorrelation indices and operator-order sign).
+__global__ void rdm_ab_finalize_kernel(const uint4* __restrict__ apat, int npa, const uint32_t* __restrict__ bpat_key,
+                                       int npb, const double* __restrict__ partial, int L, double* __restrict__ two) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)npa * npb) return;
+  const int pa = (int)(t / npb), p = (int)(t % npb);
+  const uint4 ap = apat[pa];  // {alpha pattern key, first chunk, chunks, 0}
+  double v0 = 0.0;
+  for (uint32_t q = 0; q < ap.z; ++q) v0 += partial[(size_t)(ap.y + q) * npb + p];
+  if (v0 == 0.0) return;
+  const int ia_h = (int)(ap.x >> 6), ia_p = (int)(ap.x & 63u);
+  const uint32_t key = bpat_key[p];
+  const int ib_h = (int)(key >> 6), ib_p = (int)(key & 63u);
+  const size_t L2 = (size_t)L * L, L3 = L2 * L, L4 = L3 * L;
+  const int c0 = 2 * ia_p, c1 = 2 * ib_p + 1, d0 = 2 * ia_h, d1 = 2 * ib_h + 1;
+  const int I = c0 < c1 ? c0 : c1, J = c0 < c1 ? c1 : c0;
+  const int A = d0 < d1 ? d0 : d1, B = d0 < d1 ? d1 : d0;
+  const double sg = (A > J || B < I) ? -v0 : v0;
+  const int oi = I >> 1, si = I & 1, oa = A >> 1, sa = A & 1, oj = J >> 1, sj = J & 1, ob = B >> 1;
+  if (si == sa) {
+    two[(si + 2 * sj) * L4 + oa + (size_t)L * ob + L2 * (oi + (size_t)L * oj)] += sg;
+    two[(sj + 2 * si) * L4 + ob + (size_t)L * oa + L2 * (oj + (size_t)L * oi)] += sg;
+  } else {
+    two[(si + 2 * sj) * L4 + oa + (size_t)L * ob + L2 * (oj + (size_t)L * oi)] -= sg;
+    two[(sj + 2 * si) * L4 + ob + (size_t)L * oa + L2 * (oi + (size_t)L * oj)] -= sg;
   }
 }
 
@@ -365,22 +479,119 @@ static int weights(Ctx* c, const double* dW, double* wa, double* wb, double* Pa,
   return 0;
 }
 
+// The single excitations of one spin grouped by pattern key = hole << 6 |
+// particle (hole: the ket's orbital, particle: the bra's), each group in
+// ascending bra then ket order: keys, group offsets and records bra | ket << 16.
+static int singles_by_pattern(Ctx* c, int spin, std::vector<uint32_t>& keys, std::vector<uint32_t>& goff,
+                              std::vector<uint32_t>& recs) {
+  const Conn& cn = c->conn[spin];
+  const size_t n = cn.n;
+  std::vector<uint64_t> off(n + 1);
+  std::vector<uint32_t> ns(n), ket(cn.total ? cn.total : 1), info(cn.total ? cn.total : 1);
+  SBDX_CUDA(c, cudaMemcpyAsync(off.data(), cn.off, sizeof(uint64_t) * (n + 1), cudaMemcpyDeviceToHost, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(ns.data(), cn.nsing, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c->stream));
+  if (cn.total) {
+    SBDX_CUDA(c, cudaMemcpyAsync(ket.data(), cn.ket, sizeof(uint32_t) * cn.total, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaMemcpyAsync(info.data(), cn.info, sizeof(uint32_t) * cn.total, cudaMemcpyDeviceToHost, c->stream));
+  }
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  std::vector<uint32_t> count(64 * 64, 0);
+  for (size_t r = 0; r < n; ++r)
+    for (uint32_t e = 0; e < ns[r]; ++e) ++count[info[off[r] + e] & 0xfffu];
+  std::vector<uint32_t> start(64 * 64 + 1, 0), where(64 * 64, 0);
+  keys.clear();
+  goff.assign(1, 0);
+  for (uint32_t k = 0; k < 64 * 64; ++k) {
+    start[k + 1] = start[k] + count[k];
+    if (count[k]) {
+      where[k] = (uint32_t)keys.size();
+      // info bits 0-5 hole, 6-11 particle -> key hole << 6 | particle
+      keys.push_back(((k & 63u) << 6) | (k >> 6));
+      goff.push_back(start[k + 1]);
+    }
+  }
+  recs.assign(start[64 * 64] ? start[64 * 64] : 1, 0);
+  std::vector<uint32_t> fill(start.begin(), start.end() - 1);
+  for (size_t r = 0; r < n; ++r)
+    for (uint32_t e = 0; e < ns[r]; ++e) {
+      const uint32_t k = info[off[r] + e] & 0xfffu;
+      recs[fill[k]++] = (uint32_t)r | (ket[off[r] + e] << 16);
+    }
+  (void)where;
+  return 0;
+}
+
+// The alpha-single x beta-single 2-RDM contributions without atomics
+// (rdm_ab_det_kernel, rdm_ab_finalize_kernel); returns 1 when the two staged
+// rows do not fit in shared memory (the caller then uses rdm_ab_kernel).
+static int rdm_ab_deterministic(Ctx* c, const double* dW, double* two, bool& done) {
+  done = false;
+  const size_t nb = c->nb;
+  std::vector<uint32_t> akeys, agoff, arecs, bkeys, bgoff, brecs;
+  int rc;
+  if ((rc = singles_by_pattern(c, 0, akeys, agoff, arecs))) return rc;
+  if ((rc = singles_by_pattern(c, 1, bkeys, bgoff, brecs))) return rc;
+  const int npb = (int)bkeys.size(), npa = (int)akeys.size();
+  const size_t smem = sizeof(double) * (2 * nb + (size_t)npb);
+  if (smem > kAbSmemBudget) return 0;
+  done = true;
+  if (npa == 0 || npb == 0) return 0;
+  // chunks of at most kAbChunk alpha singles of one pattern; per pattern its chunk range
+  std::vector<uint4> chunks, apat;
+  for (int q = 0; q < npa; ++q) {
+    const uint32_t first = (uint32_t)chunks.size();
+    for (uint32_t b = agoff[q]; b < agoff[q + 1]; b += kAbChunk)
+      chunks.push_back(make_uint4(akeys[q], b, std::min<uint32_t>(kAbChunk, agoff[q + 1] - b), 0u));
+    apat.push_back(make_uint4(akeys[q], first, (uint32_t)chunks.size() - first, 0u));
+  }
+  struct Bufs {
+    std::vector<void*> p;
+    ~Bufs() { for (void* q : p) cudaFree(q); }
+  } bufs;
+  auto up = [&](const void* h, size_t bytes, void** d) -> cudaError_t {
+    cudaError_t e = cudaMalloc(d, bytes ? bytes : 16);
+    if (e == cudaSuccess) bufs.p.push_back(*d);
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(*d, h, bytes, cudaMemcpyHostToDevice, c->stream);
+    return e;
+  };
+  uint4 *d_chunks = nullptr, *d_apat = nullptr;
+  uint32_t *d_arec = nullptr, *d_boff = nullptr, *d_bkey = nullptr, *d_brec = nullptr;
+  double* d_part = nullptr;
+  SBDX_CUDA(c, up(chunks.data(), sizeof(uint4) * chunks.size(), (void**)&d_chunks));
+  SBDX_CUDA(c, up(apat.data(), sizeof(uint4) * apat.size(), (void**)&d_apat));
+  SBDX_CUDA(c, up(arecs.data(), sizeof(uint32_t) * arecs.size(), (void**)&d_arec));
+  SBDX_CUDA(c, up(bgoff.data(), sizeof(uint32_t) * bgoff.size(), (void**)&d_boff));
+  SBDX_CUDA(c, up(bkeys.data(), sizeof(uint32_t) * bkeys.size(), (void**)&d_bkey));
+  SBDX_CUDA(c, up(brecs.data(), sizeof(uint32_t) * brecs.size(), (void**)&d_brec));
+  SBDX_CUDA(c, up(nullptr, sizeof(double) * chunks.size() * (size_t)npb, (void**)&d_part));
+  SBDX_CUDA(c, cudaFuncSetAttribute(rdm_ab_det_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAbSmemBudget));
+  rdm_ab_det_kernel<<<(unsigned)chunks.size(), kAbDetThreads, smem, c->stream>>>(
+      dW, nb, c->d_a, c->d_b, d_chunks, d_arec, d_boff, d_bkey, d_brec, npb, d_part);
+  SBDX_LAUNCHED(c);
+  const size_t npairs = (size_t)npa * npb;
+  rdm_ab_finalize_kernel<<<(unsigned)((npairs + 255) / 256), 256, 0, c->stream>>>(d_apat, npa, d_bkey, npb, d_part,
+                                                                                 c->L, two);
+  SBDX_LAUNCHED(c);
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // the host vectors and buffers die at return
+  return 0;
+}
+
 int rdm_device(Ctx* c, const double* dW, double* d_one, double* d_two) {
   if (!c->have_conn) { int rc = build_connectivity(c); if (rc) return rc; }
   int rc = ensure_sigma_scratch(c);
   if (rc) return rc;
   const size_t na = c->na, nb = c->nb, L = (size_t)c->L, L2 = L * L, L4 = L2 * L2;
   Scratch sc;
-  SBDX_CUDA(c, cudaMalloc(&sc.p, sizeof(double) * (na + nb + 3 * L2 + (d_two ? 0 : 4 * L4))));
+  SBDX_CUDA(c, cudaMalloc(&sc.p, sizeof(double) * (na + nb + 3 * L2)));
   double* wa = sc.p;
   double* wb = wa + na;
   double* Pa = wb + nb;
   double* Pb = Pa + L2;
   double* X = Pb + L2;
-  double* two = d_two ? d_two : X + L2;  // the 1-RDM alone still needs a 2-RDM sink
+  double* two = d_two;  // null: the 1-RDM alone
   SBDX_CUDA(c, cudaMemsetAsync(Pa, 0, sizeof(double) * 3 * L2, c->stream));
   SBDX_CUDA(c, cudaMemsetAsync(d_one, 0, sizeof(double) * 2 * L2, c->stream));
-  SBDX_CUDA(c, cudaMemsetAsync(two, 0, sizeof(double) * 4 * L4, c->stream));
+  if (two) SBDX_CUDA(c, cudaMemsetAsync(two, 0, sizeof(double) * 4 * L4, c->stream));
   double* Wt = reinterpret_cast<double*>(c->d_xt);
   if ((rc = weights(c, dW, wa, wb, Pa, Pb, X, Wt))) return rc;
   diag_finalize_kernel<<<(unsigned)((L2 + 255) / 256), 256, 0, c->stream>>>(c->L, Pa, Pb, X, d_one, two);
@@ -395,7 +606,9 @@ int rdm_device(Ctx* c, const double* dW, double* d_one, double* d_two) {
         cn.info, cn.total, c->L, d_one, two);
     SBDX_LAUNCHED(c);
   }
-  {
+  bool done = d_two == nullptr;  // the alpha-beta pairs only add to the 2-RDM
+  if (!done && (rc = rdm_ab_deterministic(c, dW, two, done))) return rc;
+  if (!done) {
     const size_t smem = sizeof(double) * (L2 + nb);
     if (smem > 220 * 1024) { c->err = "rdm: beta dimension too large for the shared-memory row"; return 1; }
     SBDX_CUDA(c, cudaFuncSetAttribute(rdm_ab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAbSmemBudget));

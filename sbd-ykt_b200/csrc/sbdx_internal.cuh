@@ -246,6 +246,9 @@ struct Ctx {
     unsigned long long kernels;
   };
   bool use_graphs = false;
+  // several-root solves (davidson_roots) run the device-driven solver, one
+  // CUDA graph per iteration (sbdx_set_graph_steps)
+  bool graph_steps = false;
   bool own_stream = false;  // stream created by the library (destroyed with the context)
   // pool of the solvers' stream-ordered scratch. It keeps its memory between
   // allocations (no unmap/map of gigabytes per solve, which stalls the other

@@ -34,7 +34,7 @@ EXPORTS = [
     "sbdx_phase_times", "sbdx_set_tuning", "sbdx_autotune", "sbdx_davidson_roots",
     "sbdx_build_hamiltonian", "sbdx_release_hamiltonian", "sbdx_wavefunction_device", "sbdx_get_wavefunction",
     "sbdx_rdm_device", "sbdx_occupation_device", "sbdx_alpha_weights_device", "sbdx_energy_backward_device",
-    "sbdx_sigma_rows_device",
+    "sbdx_sigma_rows_device", "sbdx_set_graph_steps",
 ]
 PHASES = ["alpha_same_spin", "transpose", "beta_same_spin", "alpha_beta", "combine"]
 
@@ -205,6 +205,10 @@ class Context:
         self._check(self.lib.sbdx_sigma_device(self.h, ctypes.c_int(precision), ctypes.c_void_p(c_ptr),
                                                ctypes.c_void_p(s_ptr)))
 
+    def set_graph_steps(self, on: bool = True):
+        """sbdx_set_graph_steps: several-root solves run one CUDA graph per iteration."""
+        self._check(self.lib.sbdx_set_graph_steps(self.h, ctypes.c_int(1 if on else 0)))
+
     def sigma_rows_device(self, precision, c_ptr: int, s_ptr: int, a0: int, a1: int):
         """Rows [a0, a1) of S = H C (sbdx_sigma_rows_device): c_ptr the whole
         input, s_ptr the (a1 - a0) * nb output rows."""
@@ -337,7 +341,8 @@ class Batch:
         lib.sbdx_batch_last_error.restype = ctypes.c_char_p
         lib.sbdx_batch_last_error.argtypes = [ctypes.c_void_p]
         for name in ("sbdx_batch_create", "sbdx_batch_destroy", "sbdx_batch_add", "sbdx_batch_size",
-                     "sbdx_batch_dims", "sbdx_batch_tune", "sbdx_batch_solve", "sbdx_batch_vector"):
+                     "sbdx_batch_dims", "sbdx_batch_tune", "sbdx_batch_solve", "sbdx_batch_vector",
+                     "sbdx_batch_set_graph_steps"):
             getattr(lib, name).restype = ctypes.c_int
         h = np.ascontiguousarray(h, dtype=np.float64)
         eri = np.ascontiguousarray(eri, dtype=np.float64)
@@ -378,6 +383,9 @@ class Batch:
                                             ctypes.byref(idx)))
         self.dims.append((len(a), len(b)))
         return idx.value
+
+    def set_graph_steps(self, on: bool = True):
+        self._check(self.lib.sbdx_batch_set_graph_steps(self.b, ctypes.c_int(1 if on else 0)))
 
     def tune(self):
         s, a = ctypes.c_int(0), ctypes.c_int(0)
