@@ -1666,13 +1666,18 @@ struct GStatus {
   int ndead;   // corrections of the last iteration that Gram-Schmidt removed
 };
 
-// Lowest k eigenpairs of M x = theta S x over the basis slots in use (the k
-// anchors and the corrections not removed by Gram-Schmidt, of the first
-// n_all slots of the ld-strided symmetric arrays, at most 64), on one CTA:
-// S = L L^T (right-looking Cholesky), A = L^-1 M L^-T, parallel cyclic Jacobi
-// on A (round-robin pairs: n/2 disjoint rotations per round), ascending
-// order, X = L^-T Y (column-major n_all x k, zero at removed slots). The same
-// steps as the host solver gen_eigen_k, in another rotation order.
+// Lowest k eigenpairs of M x = theta S x over the basis slots in use (of the
+// first n_all slots of the ld-strided symmetric arrays, at most 64), on one
+// CTA: the k anchors and the corrections that Gram-Schmidt kept, taken in
+// slot order by a bordered Cholesky factorisation S = L L^T that also leaves
+// out any correction whose component orthogonal to the slots before it has a
+// squared norm below kPivotFloor (a direction below FP32 resolution; without
+// this a nearly dependent basis gives spurious eigenvalues); then A =
+// L^-1 M L^-T, parallel cyclic Jacobi on A (round-robin pairs: n/2 disjoint
+// rotations per round), ascending order, X = L^-T Y (column-major n_all x k,
+// zero at slots left out). The same steps as the host solver gen_eigen_k, in
+// another rotation order.
+constexpr double kPivotFloor = 1e-8;
 __global__ void __launch_bounds__(256)
 ritz_kernel(int n_all, int k, int ld, const double* __restrict__ M, const double* __restrict__ S,
             const int* __restrict__ dead, double* __restrict__ theta, double* __restrict__ X,
@@ -1681,43 +1686,44 @@ ritz_kernel(int n_all, int k, int ld, const double* __restrict__ M, const double
   __shared__ double s_cs[32], s_sn[32], s_red[8];
   __shared__ int s_pa[32], s_pb[32], s_bad, s_ord[64], s_map[64], s_n;
   const int tid = threadIdx.x, nt = blockDim.x;
+  double* L64 = sm + 3 * 64 * 64;  // bordered factor, row stride 64
   if (tid == 0) {
     int m = 0;
-    for (int i = 0; i < n_all; ++i)
-      if (i < k || !dead[i - k]) s_map[m++] = i;
-    s_n = m;
     s_bad = 0;
+    for (int j = 0; j < n_all; ++j) {
+      if (j >= k && dead[j - k]) continue;
+      // row m of L: solve L[0..m) y = S[map, j], then the pivot
+      double d = S[j + (size_t)ld * j];
+      for (int q = 0; q < m; ++q) {
+        double v = S[s_map[q] + (size_t)ld * j];
+        for (int u = 0; u < q; ++u) v -= L64[q * 64 + u] * L64[m * 64 + u];
+        v /= L64[q * 64 + q];
+        L64[m * 64 + q] = v;
+        d -= v * v;
+      }
+      if (j < k) {
+        if (!(d > 0.0)) { s_bad = 1; break; }
+      } else if (!(d > kPivotFloor * S[j + (size_t)ld * j])) {
+        continue;  // left out: nearly dependent on the slots before it
+      }
+      L64[m * 64 + m] = sqrt(d);
+      s_map[m++] = j;
+    }
+    s_n = m;
   }
   __syncthreads();
   const int n = s_n;
-  double* Lf = sm;            // n x n, lower triangle used
+  double* Lf = sm;            // n x n, lower triangle used (column-major)
   double* A = Lf + n * n;     // n x n
   double* V = A + n * n;      // n x n eigenvectors
   for (int t = tid; t < n * n; t += nt) {
     const int i = t % n, j = t / n;
-    Lf[t] = S[s_map[i] + (size_t)ld * s_map[j]];
+    Lf[t] = i >= j ? L64[i * 64 + j] : 0.0;
     A[t] = M[s_map[i] + (size_t)ld * s_map[j]];
     V[t] = i == j ? 1.0 : 0.0;
   }
   for (int t = tid; t < n_all * k; t += nt) X[t] = 0.0;
   __syncthreads();
-  for (int j = 0; j < n; ++j) {
-    if (tid == 0) {
-      const double d = Lf[j + n * j];
-      if (!(d > 0.0)) s_bad = 1;
-      Lf[j + n * j] = d > 0.0 ? sqrt(d) : 1.0;
-    }
-    __syncthreads();
-    const double d = Lf[j + n * j];
-    for (int i = j + 1 + tid; i < n; i += nt) Lf[i + n * j] /= d;
-    __syncthreads();
-    const int m = n - j - 1;
-    for (int t = tid; t < m * m; t += nt) {
-      const int i = j + 1 + t % m, l = j + 1 + t / m;
-      if (i >= l) Lf[i + n * l] -= Lf[i + n * j] * Lf[l + n * j];
-    }
-    __syncthreads();
-  }
   if (s_bad) {
     if (tid == 0) st->err = 1;
     return;
@@ -1941,14 +1947,17 @@ __global__ void refresh_block_kernel(int k, int ld, const double* __restrict__ d
 }
 
 // Exact refresh, part 2: the exact residual norms (|R_r|^2 in nr2) are the
-// new estimates; <HW_r|C_j> (d[r * nv + j]) into M.
+// new estimates; <HW_r|C_j> (d[r * nv + j]) into M and <W_r|C_j>
+// (d[(k + r) * nv + j]) into S (recomputed: the solve may have gone back to
+// anchors whose rows a later iteration had replaced).
 __global__ void refresh_tail_kernel(int k, int nv, int ld, const double* __restrict__ nr2, const double* __restrict__ d,
-                                    double* __restrict__ M, GStatus* __restrict__ st) {
+                                    double* __restrict__ M, double* __restrict__ S, GStatus* __restrict__ st) {
   if (threadIdx.x < k) st->r_est[threadIdx.x] = sqrt(nr2[threadIdx.x]);
   if (threadIdx.x == 0) st->ndead = 0;
   for (int t = threadIdx.x; t < k * nv; t += blockDim.x) {
     const int r = t / nv, q = k + t % nv;
     M[r + (size_t)ld * q] = M[q + (size_t)ld * r] = d[t];
+    S[r + (size_t)ld * q] = S[q + (size_t)ld * r] = d[(size_t)k * nv + t];
   }
 }
 
@@ -1968,6 +1977,14 @@ __global__ void restart_kernel(int k, int keep, int drop, int ld, double* __rest
     for (int j = 0; j < keep; ++j) dead[j] = dead[j + drop];
   }
 }
+
+// Longest run of FP32 iterations between two exact refreshes in the
+// device-driven solver when no period is set. Its subspace matrices are
+// updated from single-precision products and never re-derived between
+// refreshes, so an uncapped run drifts: on a 90 x 60-determinant, 2-root test
+// the estimated Ritz values left the spectrum after six iterations, while
+// every schedule of four or fewer converged to the FP64 energies.
+constexpr int kGraphMaxSince = 4;
 
 template <typename TC>
 int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, double* E, double* res,
@@ -1999,7 +2016,7 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
   Work wk;
   double *wpartial = nullptr, *wscal = nullptr, *wu = nullptr;
   SBDX_CUDA(c, alloc((void**)&wpartial, sizeof(double) * kRedBlocks * (2 * nc + 2 * kMaxRoots + 4)));
-  SBDX_CUDA(c, alloc((void**)&wscal, sizeof(double) * (kbDots + (size_t)(k + 2) * (nc + 2 * k) + 64)));
+  SBDX_CUDA(c, alloc((void**)&wscal, sizeof(double) * (kbDots + 2 * (size_t)k * (nc + 2 * k) + 64)));
   SBDX_CUDA(c, alloc((void**)&wu, sizeof(double) * ((size_t)(k + nc) * k + k + nc + 8)));
   TC *C = nullptr, *HC = nullptr;
   double *A = nullptr, *R = nullptr, *V = nullptr, *dM = nullptr, *dS = nullptr, *misc = nullptr;
@@ -2034,7 +2051,7 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
   SBDX_CUDA(c, cudaMemsetAsync(dS, 0, sizeof(double) * ld * ld, c->stream));
   SBDX_CUDA(c, cudaMemsetAsync(dead, 0, sizeof(int) * nc, c->stream));
   SBDX_CUDA(c, cudaMemsetAsync(dst, 0, sizeof(GStatus), c->stream));
-  const size_t ritz_smem = sizeof(double) * 3 * 64 * 64;
+  const size_t ritz_smem = sizeof(double) * 4 * 64 * 64;
   SBDX_CUDA(c, cudaFuncSetAttribute(ritz_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ritz_smem));
   const auto t0 = std::chrono::steady_clock::now();
   int rc = 0;
@@ -2071,9 +2088,12 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
     residual_block_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(W, HW, s + kbTheta, k, D, R, wk.partial);
     SBDX_LAUNCHED(c);
     if ((r2 = finalize(c, wk, k, s + kbNR2))) return r2;
-    for (int r = 0; r < k && nv > 0; ++r)
+    for (int r = 0; r < k && nv > 0; ++r) {
       if ((r2 = multidot<TC, double>(c, wk, C, D, nv, HW + (size_t)r * D, D, s + kbDots + (size_t)r * nv))) return r2;
-    refresh_tail_kernel<<<1, 256, 0, c->stream>>>(k, nv, ld, s + kbNR2, s + kbDots, dM, dst);
+      if ((r2 = multidot<TC, double>(c, wk, C, D, nv, W + (size_t)r * D, D, s + kbDots + (size_t)(k + r) * nv)))
+        return r2;
+    }
+    refresh_tail_kernel<<<1, 256, 0, c->stream>>>(k, nv, ld, s + kbNR2, s + kbDots, dM, dS, dst);
     SBDX_LAUNCHED(c);
     SBDX_CUDA(c, cudaMemcpyAsync(hst + slot, dst, sizeof(GStatus), cudaMemcpyDeviceToHost, c->stream));
     return 0;
@@ -2140,6 +2160,38 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
     }
     ritz_kernel<<<1, 256, ritz_smem, c->stream>>>(k + nv, k, ld, dM, dS, dead, s + kbTheta, Xd, dst);
     SBDX_LAUNCHED(c);
+    if (p.verbose >= 2) {  // diagnostic (no capture at this level): the same problem on the host
+      const int n = k + nv;
+      std::vector<double> hM((size_t)ld * ld), hS((size_t)ld * ld), hX((size_t)n * k), dth(k), th, X;
+      SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+      SBDX_CUDA(c, cudaMemcpy(hM.data(), dM, sizeof(double) * ld * ld, cudaMemcpyDeviceToHost));
+      SBDX_CUDA(c, cudaMemcpy(hS.data(), dS, sizeof(double) * ld * ld, cudaMemcpyDeviceToHost));
+      SBDX_CUDA(c, cudaMemcpy(hX.data(), Xd, sizeof(double) * n * k, cudaMemcpyDeviceToHost));
+      SBDX_CUDA(c, cudaMemcpy(dth.data(), s + kbTheta, sizeof(double) * k, cudaMemcpyDeviceToHost));
+      double asym = 0.0;
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+          asym = std::max(asym, std::fabs(hM[i + (size_t)ld * j] - hM[j + (size_t)ld * i]));
+          asym = std::max(asym, std::fabs(hS[i + (size_t)ld * j] - hS[j + (size_t)ld * i]));
+        }
+      std::vector<double> Sc((size_t)n * n), ws(n);
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) Sc[i + (size_t)n * j] = hS[i + (size_t)ld * j];
+      jacobi_eigen(n, Sc.data(), n, ws.data());
+      const bool ok = gen_eigen_k(n, k, hM, hS, ld, th, X);
+      double dx = 0.0;
+      for (int r = 0; r < k && ok; ++r) {
+        double dp = 0.0, dm = 0.0;
+        for (int i = 0; i < n; ++i) {
+          dp = std::max(dp, std::fabs(hX[i + (size_t)n * r] - X[i + (size_t)n * r]));
+          dm = std::max(dm, std::fabs(hX[i + (size_t)n * r] + X[i + (size_t)n * r]));
+        }
+        dx = std::max(dx, std::min(dp, dm));
+      }
+      std::printf("     ritz n=%d device theta0=%.10f host=%.10f |dX|=%.2e min eig S=%.3e asym=%.1e\n", n, dth[0],
+                  ok ? th[0] : 0.0, dx, ws[0], asym);
+      std::fflush(stdout);
+    }
     unsigned ga = kRedBlocks;
     if ((r2 = launch_update_anchors<TC>(c, wk, k, W, HW, C, HC, nv, Xd, s + kbTheta, D, Wn, HWn, R, &ga))) return r2;
     finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, (int)ga, k, s + kbNW2);
@@ -2163,7 +2215,7 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
     unsigned long long kernels = 0;
   };
   std::map<long long, Cached> cache;
-  const bool capture_ok = c->stream != nullptr;
+  const bool capture_ok = c->stream != nullptr && p.verbose < 2;
   bool warm[2] = {false, false};
   auto launch = [&](int kind, int nv, int par, int slot, int mask) -> int {
     const long long key = (((long long)kind * 128 + nv) * 8 + par * 4 + slot) * 16 + mask;
@@ -2225,9 +2277,13 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
   if ((rc = refresh())) return rc;
   double r_ref = worst(r_exact);
   const int max_steps = p.max_it * p.max_nb;
-  // iterations launched and not yet read: their status slots and numbers of
-  // expanded roots, in order
-  std::vector<std::pair<int, int>> inflight;
+  // iterations launched and not yet read, in order: status slot, roots
+  // expanded, and the solver state after each (anchor buffer, corrections,
+  // iterations since the last refresh)
+  struct Flight {
+    int slot, nact, par, nv, since;
+  };
+  std::vector<Flight> inflight;
   std::vector<cudaEvent_t> evs(2);
   for (auto& ev : evs) SBDX_CUDA(c, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   struct EvGuard {
@@ -2250,13 +2306,13 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
     if (r2) return r2;
     SBDX_CUDA(c, cudaEventRecord(evs[it_slot], c->stream));
     const int nact = __builtin_popcount((unsigned)mask);
-    inflight.emplace_back(it_slot, nact);
-    it_slot ^= 1;
     nv = next_nv(nv, nact);
     par ^= 1;
     steps += nact;
     ++since;
     if (kMixed) info.n_sigma += nact; else info.n_sigma64 += nact;
+    inflight.push_back({it_slot, nact, par, nv, since});
+    it_slot ^= 1;
     return 0;
   };
   while (!converged && !stalled) {
@@ -2266,17 +2322,24 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
     }
     if (steps >= max_steps || seconds_since(t0) > p.max_time) break;
     if (inflight.empty() && (rc = launch_step())) return rc;
-    const bool more = steps < max_steps;
-    if (more && (rc = launch_step())) return rc;  // iteration t + 1 queued before t is read
-    const int slot = inflight.front().first;
-    last_nact = inflight.front().second;
+    // iteration t + 1 is queued before t is read, unless it would restart the
+    // subspace (the decision on t may undo t + 1, which a restart rules out)
+    const bool more = steps < max_steps && nv + __builtin_popcount((unsigned)mask) <= nc;
+    if (more && (rc = launch_step())) return rc;
+    const Flight f = inflight.front();
     inflight.erase(inflight.begin());
-    SBDX_CUDA(c, cudaEventSynchronize(evs[slot]));
-    const GStatus h = hst[slot];
+    SBDX_CUDA(c, cudaEventSynchronize(evs[f.slot]));
+    const GStatus h = hst[f.slot];
     if (h.err == 1) { c->err = "davidson: projected overlap matrix is not positive definite"; return 5; }
     if (h.err == 2) { c->err = "davidson: Ritz vector lost its normalisation"; return 5; }
     last_ndead = h.ndead;
+    last_nact = f.nact;
     for (int r = 0; r < k; ++r) E[r] = h.theta[r];
+    if (p.verbose) {
+      std::printf("   iteration (read one late): theta0=%.12f est.res0=%.3e est.res%d=%.3e removed %d of %d\n",
+                  h.theta[0], h.r_est[0], k - 1, h.r_est[k - 1], h.ndead, last_nact);
+      std::fflush(stdout);
+    }
     set_mask(h.r_est);
     const double w = worst(h.r_est);
     bool due;
@@ -2284,27 +2347,26 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
       due = all_below(h.r_est);  // exact products: the estimates are exact residuals
     } else {
       if (w < kStallGain * best) { best = w; stale = 0; } else { ++stale; }
-      due = period > 0 ? since >= period
-                       : (w < kRefreshDrop * r_ref || all_below(h.r_est) || stale >= kStallSteps);
+      due = period > 0 ? f.since >= period
+                       : (w < kRefreshDrop * r_ref || all_below(h.r_est) || stale >= kStallSteps ||
+                          f.since >= kGraphMaxSince);
     }
     if (last_ndead >= last_nact) due = true;  // nothing new: refresh (or stop when that changes nothing)
-    if (!due && more && steps < max_steps && seconds_since(t0) <= p.max_time) continue;
-    // drain the queued iteration, then refresh from the newest anchors
+    if (!due && steps < max_steps && seconds_since(t0) <= p.max_time) continue;
+    // act on iteration t, as the host-driven solver does: the iteration queued
+    // after it is dropped (its new anchors went to the other buffer, its
+    // corrections lie beyond t's count; a refresh recomputes the anchor rows)
     SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
-    if (!inflight.empty()) {
-      last_ndead = hst[inflight.back().first].ndead;
-      last_nact = inflight.back().second;
-      inflight.clear();
-    }
+    inflight.clear();
+    par = f.par;
+    nv = f.nv;
+    since = f.since;
     const int since_before = since;
     const bool nothing_new = last_ndead >= last_nact;
     if (kMixed || nothing_new) {
       if ((rc = refresh())) return rc;
-    } else {  // the newest iteration's residuals are exact
-      for (int r = 0; r < k; ++r) {
-        r_exact[r] = hst[it_slot ^ 1].r_est[r];
-        E[r] = hst[it_slot ^ 1].theta[r];
-      }
+    } else {  // exact products: t's residuals are exact
+      for (int r = 0; r < k; ++r) r_exact[r] = h.r_est[r];
     }
     r_ref = worst(r_exact);
     converged = all_below(r_exact);

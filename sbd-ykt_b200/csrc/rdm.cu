@@ -29,7 +29,6 @@ int ensure_sigma_scratch(Ctx* c);
 
 namespace {
 
-constexpr int kRowThreads = 256;
 
 // Reference parity(det, start, end) (determinants.h:228-279) on the
 // interleaved determinant of (alpha, beta): returns the sign bit (1 = -1).
@@ -40,29 +39,32 @@ __device__ __forceinline__ uint32_t ref_parity_bit(uint64_t a, uint64_t b, int s
   return (uint32_t)(popc64(a & ma) + popc64(b & mb) + (int)((sw >> (start >> 1)) & 1ull)) & 1u;
 }
 
-// Row weights and occupation profiles of one orientation of W (rows x cols):
-// wrow[r] = sum_c W^2; P[p][q] += wrow[r] for p, q in s_row[r];
-// X[p][q] += sum_c W[r,c]^2 n_q(s_col[c]) for p in s_row[r] (if X != null).
-__global__ void __launch_bounds__(kRowThreads)
-row_weight_kernel(const double* __restrict__ W, size_t rows, size_t cols, const uint64_t* __restrict__ s_row,
-                  const uint64_t* __restrict__ s_col, int L, double* __restrict__ wrow, double* __restrict__ P,
-                  double* __restrict__ X) {
-  __shared__ double vq[64];
-  __shared__ double red[kRowThreads / 32];
+// Row weights and occupation profiles of one orientation of W (rows x cols),
+// without atomics: wrow[r] = sum_c W[r,c]^2 (lane-strided sums, a fixed
+// shuffle tree, warps added in order) and, when vq is not null, the row's
+// opposite-spin occupation profile vq[r*L + q] = sum_c W[r,c]^2 n_q(s_col[c])
+// (per-thread shared accumulators of L doubles, added in thread order).
+constexpr int kRowWeightThreads = 64;
+__global__ void __launch_bounds__(kRowWeightThreads)
+row_weight_kernel(const double* __restrict__ W, size_t cols, const uint64_t* __restrict__ s_col, int L,
+                  double* __restrict__ wrow, double* __restrict__ vq) {
+  extern __shared__ double acc_q[];  // [thread][L] when vq != null
+  __shared__ double red[kRowWeightThreads / 32];
   const size_t r = blockIdx.x;
-  for (int q = threadIdx.x; q < 64; q += blockDim.x) vq[q] = 0.0;
-  __syncthreads();
+  double* mine = acc_q + (size_t)threadIdx.x * L;
+  if (vq != nullptr)
+    for (int q = 0; q < L; ++q) mine[q] = 0.0;
   double s = 0.0;
   for (size_t c = threadIdx.x; c < cols; c += blockDim.x) {
     const double w = W[r * cols + c];
     const double w2 = w * w;
     s += w2;
-    if (X != nullptr && w2 != 0.0) {
+    if (vq != nullptr && w2 != 0.0) {
       uint64_t bits = s_col[c];
       while (bits) {
         const int q = __ffsll((long long)bits) - 1;
         bits &= bits - 1;
-        atomicAdd(&vq[q], w2);
+        mine[q] += w2;
       }
     }
   }
@@ -71,21 +73,35 @@ row_weight_kernel(const double* __restrict__ W, size_t rows, size_t cols, const 
   __syncthreads();
   if (threadIdx.x == 0) {
     double t = 0.0;
-    for (int w = 0; w < kRowThreads / 32; ++w) t += red[w];
-    red[0] = t;
+    for (int w = 0; w < kRowWeightThreads / 32; ++w) t += red[w];
     wrow[r] = t;
   }
-  __syncthreads();
-  const double tot = red[0];
-  const uint64_t own = s_row[r];
-  // P: pairs of own orbitals; X: own orbital x opposite-spin profile
-  for (int t = threadIdx.x; t < L * L; t += blockDim.x) {
-    const int p = t / L, q = t % L;
-    if ((own >> p) & 1ull) {
-      if ((own >> q) & 1ull) atomicAdd(&P[t], tot);
-      if (X != nullptr && vq[q] != 0.0) atomicAdd(&X[t], vq[q]);
+  if (vq != nullptr)
+    for (int q = threadIdx.x; q < L; q += blockDim.x) {
+      double v = 0.0;
+      for (int t = 0; t < kRowWeightThreads; ++t) v += acc_q[(size_t)t * L + q];
+      vq[r * L + q] = v;
     }
+}
+
+// P[p][q] = sum_r wrow[r] over the rows whose string holds p and q, and (if X
+// is not null) X[p][q] = sum_r vq[r][q] over the rows whose string holds p:
+// one thread per (p, q), rows in order.
+__global__ void occupation_sums_kernel(size_t rows, const uint64_t* __restrict__ s_row, int L,
+                                       const double* __restrict__ wrow, const double* __restrict__ vq,
+                                       double* __restrict__ P, double* __restrict__ X) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= L * L) return;
+  const int p = t / L, q = t % L;
+  double a = 0.0, b = 0.0;
+  for (size_t r = 0; r < rows; ++r) {
+    const uint64_t own = s_row[r];
+    if (!((own >> p) & 1ull)) continue;
+    if ((own >> q) & 1ull) a += wrow[r];
+    if (X != nullptr) b += vq[r * L + q];
   }
+  P[t] = a;
+  if (X != nullptr) X[t] = b;
 }
 
 // Diagonal (ZeroDiffCorrelation) contributions from P_alpha, P_beta, X.
@@ -114,47 +130,47 @@ __global__ void diag_finalize_kernel(int L, const double* __restrict__ Pa, const
   two[1 * L4 + (size_t)q + L * p + L2 * q + L3 * p] += v;
 }
 
-__device__ __forceinline__ size_t find_row(const uint64_t* off, size_t n, uint64_t e) {
-  size_t lo = 0, hi = n;  // off[lo] <= e < off[hi]
-  while (hi - lo > 1) {
-    const size_t mid = (lo + hi) >> 1;
-    if (off[mid] <= e) lo = mid; else hi = mid;
-  }
-  return lo;
-}
+// Same-spin singles and doubles without atomics. The entries of one spin are
+// grouped by excitation pattern on the host (singles: hole, particle;
+// doubles: both holes and both particles), each group in ascending bra then
+// ket order. Pass 1 (rdm_same_values_kernel, one warp per entry) evaluates the
+// entry's value s = sum_c W[r,c] W[k,c] (-1)^{opposite-spin parity} over the
+// opposite-spin index c (lane c mod 32, then a fixed shuffle tree) and, for a
+// single when the 2-RDM is wanted, its opposite-spin occupation profile
+// prof[q] = sum_c (the same terms) n_q(c) (per-lane shared accumulators added
+// in lane order). Pass 2 (rdm_singles_finalize_kernel,
+// rdm_doubles_finalize_kernel) gives every output element one thread, which
+// adds its group's values in group order: the result does not depend on the
+// launch. Indices and signs are those of OneDiffCorrelation and
+// TwoDiffCorrelation (correlation.h:49-130).
+constexpr int kValWarps = 4;
 
-// Same-spin singles and doubles of spin `spin`, one warp per entry.
-__global__ void __launch_bounds__(256)
-rdm_same_kernel(int spin, const double* __restrict__ W, size_t rows, size_t cols, const uint64_t* __restrict__ s_row,
-                const uint64_t* __restrict__ s_col, const uint64_t* __restrict__ off, const uint32_t* __restrict__ ket,
-                const uint64_t* __restrict__ omask, const uint32_t* __restrict__ info, size_t total, int L,
-                double* __restrict__ one, double* __restrict__ two) {
-  __shared__ double vq_all[8][64];
+// Dynamic shared memory: kValWarps * 32 * L doubles when profile != 0.
+__global__ void __launch_bounds__(kValWarps * 32)
+rdm_same_values_kernel(const double* __restrict__ W, size_t cols, const uint64_t* __restrict__ s_row,
+                       const uint64_t* __restrict__ s_col, const uint32_t* __restrict__ ket,
+                       const uint64_t* __restrict__ omask, const uint32_t* __restrict__ info,
+                       const uint32_t* __restrict__ ent, const uint32_t* __restrict__ erow, size_t n, int L,
+                       int profile, double* __restrict__ sval, double* __restrict__ prof) {
+  extern __shared__ double vq_all[];  // [warp][lane][L]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const size_t e = (size_t)blockIdx.x * 8 + warp;
-  double* vq = vq_all[warp];
-  for (int q = lane; q < 64; q += 32) vq[q] = 0.0;
-  __syncwarp();
-  if (e >= total) return;
-  const size_t r = find_row(off, rows, e);
-  const size_t k = ket[e];
+  const size_t t = (size_t)blockIdx.x * kValWarps + warp;
+  double* vq = vq_all + ((size_t)warp * 32 + lane) * L;
+  if (profile)
+    for (int q = 0; q < L; ++q) vq[q] = 0.0;
+  if (t >= n) return;
+  const size_t e = ent[t], r = erow[t], k = ket[e];
   const uint32_t inf = info[e];
   const uint64_t om = omask[e];
   const uint64_t sr = s_row[r];
-  const bool single = (inf & kInfoSingle) != 0;
   uint32_t sbit;
-  int oi = 0, oa = 0, i_e = 0, j_e = 0, a_e = 0, b_e = 0;
-  if (single) {
+  if (inf & kInfoSingle) {
     sbit = inf >> 31;
-    i_e = (int)(inf & 63u);
-    a_e = (int)((inf >> 6) & 63u);
-    oi = a_e;  // bra-only orbital
-    oa = i_e;  // ket-only orbital
   } else {
-    i_e = (int)(inf & 63u); j_e = (int)((inf >> 6) & 63u);
-    a_e = (int)((inf >> 12) & 63u); b_e = (int)((inf >> 18) & 63u);
+    const int i_e = (int)(inf & 63u), j_e = (int)((inf >> 6) & 63u);
+    const int a_e = (int)((inf >> 12) & 63u), b_e = (int)((inf >> 18) & 63u);
     // TwoDiffCorrelation sign on the bra: I = a_e, J = b_e (bra-only), A = i_e,
-    // B = j_e (ket-only); same-spin part here, opposite-spin part via omask.
+    // B = j_e (ket-only); same-spin part here, opposite-spin part via omask
     int par = 0;
     {
       const int lo = a_e < i_e ? a_e : i_e, hi = a_e < i_e ? i_e : a_e;
@@ -174,55 +190,92 @@ rdm_same_kernel(int spin, const double* __restrict__ W, size_t rows, size_t cols
     const double x = wr[c] * wk[c];
     if (x == 0.0) continue;
     const uint64_t o = s_col[c];
-    const uint32_t neg = (sbit ^ (uint32_t)popc64(o & om)) & 1u;
-    const double t = neg ? -x : x;
-    s += t;
-    if (single && two != nullptr) {
+    const double v = ((sbit ^ (uint32_t)popc64(o & om)) & 1u) ? -x : x;
+    s += v;
+    if (profile) {
       uint64_t bits = o;
       while (bits) {
         const int q = __ffsll((long long)bits) - 1;
         bits &= bits - 1;
-        atomicAdd(&vq[q], t);
+        vq[q] += v;
       }
     }
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  s = __shfl_sync(0xffffffffu, s, 0);
-  __syncwarp();
-  const size_t L2 = (size_t)L * L, L3 = L2 * L, L4 = L3 * L;
-  const int ss = 3 * spin;           // same-spin block
-  const int so = spin + 2 * (1 - spin), os = (1 - spin) + 2 * spin;
-  if (single) {
-    if (lane == 0) atomicAdd(&one[(size_t)spin * L2 + oi + (size_t)L * oa], s);
-    if (two == nullptr) return;  // the 1-RDM alone
-    // same-spin occupied orbitals of the bra (including oi itself, whose
-    // four terms cancel exactly as in the reference)
-    uint64_t bits = sr;
-    int n = 0;
-    while (bits) {
-      const int oj = __ffsll((long long)bits) - 1;
-      bits &= bits - 1;
-      if ((n++ & 31) == lane) {
-        atomicAdd(&two[ss * L4 + oa + (size_t)L * oj + L2 * oi + L3 * oj], s);
-        atomicAdd(&two[ss * L4 + oj + (size_t)L * oa + L2 * oj + L3 * oi], s);
-        atomicAdd(&two[ss * L4 + oa + (size_t)L * oj + L2 * oj + L3 * oi], -s);
-        atomicAdd(&two[ss * L4 + oj + (size_t)L * oa + L2 * oi + L3 * oj], -s);
-      }
-    }
+  if (lane == 0) sval[t] = s;
+  if (profile) {
+    __syncwarp();
     for (int q = lane; q < L; q += 32) {
-      const double v = vq[q];
-      if (v != 0.0) {
-        atomicAdd(&two[so * L4 + oa + (size_t)L * q + L2 * oi + L3 * q], v);
-        atomicAdd(&two[os * L4 + q + (size_t)L * oa + L2 * q + L3 * oi], v);
-      }
+      double v = 0.0;
+      for (int l = 0; l < 32; ++l) v += vq_all[((size_t)warp * 32 + l) * L + q];
+      prof[t * (size_t)L + q] = v;
     }
-  } else if (lane == 0 && s != 0.0 && two != nullptr) {
-    // oi = a_e, oj = b_e (bra-only); oa = i_e, ob = j_e (ket-only); same spin
-    atomicAdd(&two[ss * L4 + i_e + (size_t)L * j_e + L2 * (a_e + (size_t)L * b_e)], s);
-    atomicAdd(&two[ss * L4 + j_e + (size_t)L * i_e + L2 * (b_e + (size_t)L * a_e)], s);
-    atomicAdd(&two[ss * L4 + i_e + (size_t)L * j_e + L2 * (b_e + (size_t)L * a_e)], -s);
-    atomicAdd(&two[ss * L4 + j_e + (size_t)L * i_e + L2 * (a_e + (size_t)L * b_e)], -s);
   }
+}
+
+// Singles of spin `spin`, one thread per (group, x): x = 0 the 1-RDM element
+// gamma[particle + L hole]; x = 1 + oj (oj < L) the four same-spin 2-RDM
+// elements of the bra orbital oj (oj = the particle: they cancel, skipped);
+// x = 1 + L + q the two opposite-spin elements of the profile orbital q.
+__global__ void rdm_singles_finalize_kernel(int spin, int L, const uint32_t* __restrict__ gkey,
+                                            const uint32_t* __restrict__ goff, size_t ngroups,
+                                            const uint32_t* __restrict__ erow, const uint64_t* __restrict__ s_row,
+                                            const double* __restrict__ sval, const double* __restrict__ prof,
+                                            double* __restrict__ one, double* __restrict__ two) {
+  const int nx = two ? 1 + 2 * L : 1;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ngroups * nx) return;
+  const size_t g = t / nx;
+  const int x = (int)(t % nx);
+  const uint32_t key = gkey[g];
+  const int oa = (int)(key & 63u), oi = (int)((key >> 6) & 63u);  // hole (ket-only), particle (bra-only)
+  const size_t L2 = (size_t)L * L, L3 = L2 * L, L4 = L3 * L;
+  if (x == 0) {
+    double v = 0.0;
+    for (uint32_t q = goff[g]; q < goff[g + 1]; ++q) v += sval[q];
+    one[(size_t)spin * L2 + oi + (size_t)L * oa] += v;
+    return;
+  }
+  const int ss = 3 * spin;
+  if (x <= L) {
+    const int oj = x - 1;
+    if (oj == oi) return;
+    double v = 0.0;
+    for (uint32_t q = goff[g]; q < goff[g + 1]; ++q)
+      if ((s_row[erow[q]] >> oj) & 1ull) v += sval[q];
+    if (v == 0.0) return;
+    two[ss * L4 + oa + (size_t)L * oj + L2 * oi + L3 * oj] += v;
+    two[ss * L4 + oj + (size_t)L * oa + L2 * oj + L3 * oi] += v;
+    two[ss * L4 + oa + (size_t)L * oj + L2 * oj + L3 * oi] -= v;
+    two[ss * L4 + oj + (size_t)L * oa + L2 * oi + L3 * oj] -= v;
+    return;
+  }
+  const int qo = x - 1 - L;
+  double v = 0.0;
+  for (uint32_t q = goff[g]; q < goff[g + 1]; ++q) v += prof[(size_t)q * L + qo];
+  if (v == 0.0) return;
+  const int so = spin + 2 * (1 - spin), os = (1 - spin) + 2 * spin;
+  two[so * L4 + oa + (size_t)L * qo + L2 * oi + L3 * qo] += v;
+  two[os * L4 + qo + (size_t)L * oa + L2 * qo + L3 * oi] += v;
+}
+
+// Doubles of spin `spin`, one thread per group (i, j ket-only; a, b bra-only).
+__global__ void rdm_doubles_finalize_kernel(int spin, int L, const uint32_t* __restrict__ gkey,
+                                            const uint32_t* __restrict__ goff, size_t ngroups,
+                                            const double* __restrict__ sval, double* __restrict__ two) {
+  const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  double s = 0.0;
+  for (uint32_t q = goff[g]; q < goff[g + 1]; ++q) s += sval[q];
+  if (s == 0.0) return;
+  const uint32_t key = gkey[g];
+  const size_t i_e = key & 63u, j_e = (key >> 6) & 63u, a_e = (key >> 12) & 63u, b_e = (key >> 18) & 63u;
+  const size_t L2 = (size_t)L * L, L4 = L2 * L2;
+  const int ss = 3 * spin;
+  two[ss * L4 + i_e + (size_t)L * j_e + L2 * (a_e + (size_t)L * b_e)] += s;
+  two[ss * L4 + j_e + (size_t)L * i_e + L2 * (b_e + (size_t)L * a_e)] += s;
+  two[ss * L4 + i_e + (size_t)L * j_e + L2 * (b_e + (size_t)L * a_e)] -= s;
+  two[ss * L4 + j_e + (size_t)L * i_e + L2 * (a_e + (size_t)L * b_e)] -= s;
 }
 
 // Alpha single x beta single pairs (task type 0). One CTA per bra alpha row.
@@ -302,9 +355,9 @@ rdm_ab_kernel(const double* __restrict__ W, size_t nb, const uint64_t* __restric
 // patterns w, w + 16, ..., all their beta singles (bra ib -> ket jb) of
 // +-W[ia, ib] W[ja, jb] in a fixed lane order and shuffle tree; the warp owns
 // those patterns' accumulators, so every sum has one fixed order. The chunk's
-// sums go to partial[chunk][beta pattern]; rdm_ab_finalize_kernel adds the
-// chunks of one alpha pattern in order and writes the two 2-RDM elements of
-// each pattern pair (no other kernel writes them).
+// sums go to partial[chunk][beta pattern]; rdm_ab_sum_kernel adds the chunks
+// of one alpha pattern in order and rdm_ab_write_kernel writes the 2-RDM
+// elements (no other kernel writes them).
 constexpr int kAbChunk = 32;
 constexpr int kAbDetThreads = 512;
 
@@ -371,32 +424,84 @@ rdm_ab_det_kernel(const double* __restrict__ W, size_t nb, const uint64_t* __res
 }
 
 // Sum of the chunks of each alpha pattern (in chunk order) for every beta
-// pattern, written to the two 2-RDM elements of the pattern pair (the
-// reference's TwoDiffCorrelation indices and operator-order sign).
-__global__ void rdm_ab_finalize_kernel(const uint4* __restrict__ apat, int npa, const uint32_t* __restrict__ bpat_key,
-                                       int npb, const double* __restrict__ partial, int L, double* __restrict__ two) {
+// pattern: G[alpha pattern][beta pattern].
+__global__ void rdm_ab_sum_kernel(const uint4* __restrict__ apat, int npa, int npb, const double* __restrict__ partial,
+                                  double* __restrict__ G) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (size_t)npa * npb) return;
   const int pa = (int)(t / npb), p = (int)(t % npb);
   const uint4 ap = apat[pa];  // {alpha pattern key, first chunk, chunks, 0}
-  double v0 = 0.0;
-  for (uint32_t q = 0; q < ap.z; ++q) v0 += partial[(size_t)(ap.y + q) * npb + p];
-  if (v0 == 0.0) return;
-  const int ia_h = (int)(ap.x >> 6), ia_p = (int)(ap.x & 63u);
-  const uint32_t key = bpat_key[p];
-  const int ib_h = (int)(key >> 6), ib_p = (int)(key & 63u);
+  double v = 0.0;
+  for (uint32_t q = 0; q < ap.z; ++q) v += partial[(size_t)(ap.y + q) * npb + p];
+  G[t] = v;
+}
+
+// The two 2-RDM elements of the pattern pair (alpha hole h1, particle p1;
+// beta hole h2, particle p2) and the sign with which its sum enters each: the
+// indices and operator-order sign of TwoDiffCorrelation (correlation.h:91-130).
+__device__ __forceinline__ void ab_targets(int h1, int p1, int h2, int p2, int L, size_t (&e)[2], double (&sg)[2]) {
   const size_t L2 = (size_t)L * L, L3 = L2 * L, L4 = L3 * L;
-  const int c0 = 2 * ia_p, c1 = 2 * ib_p + 1, d0 = 2 * ia_h, d1 = 2 * ib_h + 1;
+  const int c0 = 2 * p1, c1 = 2 * p2 + 1, d0 = 2 * h1, d1 = 2 * h2 + 1;
   const int I = c0 < c1 ? c0 : c1, J = c0 < c1 ? c1 : c0;
   const int A = d0 < d1 ? d0 : d1, B = d0 < d1 ? d1 : d0;
-  const double sg = (A > J || B < I) ? -v0 : v0;
+  const double s0 = (A > J || B < I) ? -1.0 : 1.0;
   const int oi = I >> 1, si = I & 1, oa = A >> 1, sa = A & 1, oj = J >> 1, sj = J & 1, ob = B >> 1;
   if (si == sa) {
-    two[(si + 2 * sj) * L4 + oa + (size_t)L * ob + L2 * (oi + (size_t)L * oj)] += sg;
-    two[(sj + 2 * si) * L4 + ob + (size_t)L * oa + L2 * (oj + (size_t)L * oi)] += sg;
+    e[0] = (si + 2 * sj) * L4 + oa + (size_t)L * ob + L2 * (oi + (size_t)L * oj);
+    e[1] = (sj + 2 * si) * L4 + ob + (size_t)L * oa + L2 * (oj + (size_t)L * oi);
+    sg[0] = sg[1] = s0;
   } else {
-    two[(si + 2 * sj) * L4 + oa + (size_t)L * ob + L2 * (oj + (size_t)L * oi)] -= sg;
-    two[(sj + 2 * si) * L4 + ob + (size_t)L * oa + L2 * (oi + (size_t)L * oj)] -= sg;
+    e[0] = (si + 2 * sj) * L4 + oa + (size_t)L * ob + L2 * (oj + (size_t)L * oi);
+    e[1] = (sj + 2 * si) * L4 + ob + (size_t)L * oa + L2 * (oi + (size_t)L * oj);
+    sg[0] = sg[1] = -s0;
+  }
+}
+
+// Writes the alpha-beta 2-RDM elements, one thread per pattern pair. Two
+// pattern pairs reach the same element exactly when they differ by exchanging
+// the particles (equal holes) or the holes (equal particles) of the two
+// spins; the element is then written once, by the pair that comes first in
+// (h1, p1, h2, p2) order, as its own term followed by its partner's, so every
+// element has one writer and one summation order. amap, bmap: pattern index
+// of (hole << 6 | particle), -1 when no single has that pattern.
+__global__ void rdm_ab_write_kernel(const uint32_t* __restrict__ akey, int npa, const uint32_t* __restrict__ bkey,
+                                    int npb, const int* __restrict__ amap, const int* __restrict__ bmap,
+                                    const double* __restrict__ G, int L, double* __restrict__ two) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)npa * npb) return;
+  const int pa = (int)(t / npb), p = (int)(t % npb);
+  const int h1 = (int)(akey[pa] >> 6), p1 = (int)(akey[pa] & 63u);
+  const int h2 = (int)(bkey[p] >> 6), p2 = (int)(bkey[p] & 63u);
+  const double v = G[t];
+  size_t e[2], ep[2] = {~(size_t)0, ~(size_t)0};
+  double sg[2], sgp[2] = {0.0, 0.0};
+  ab_targets(h1, p1, h2, p2, L, e, sg);
+  int q1 = -1, q2 = -1, x1 = 0, y1 = 0, x2 = 0, y2 = 0;  // partner (alpha x1 -> y1, beta x2 -> y2)
+  if (h1 == h2 && p1 != p2) { x1 = h1; y1 = p2; x2 = h2; y2 = p1; }
+  else if (p1 == p2 && h1 != h2) { x1 = h2; y1 = p1; x2 = h1; y2 = p2; }
+  else x1 = -1;
+  double vp = 0.0;
+  bool partner_first = false;
+  if (x1 >= 0) {
+    q1 = amap[(x1 << 6) | y1];
+    q2 = bmap[(x2 << 6) | y2];
+    if (q1 >= 0 && q2 >= 0) {
+      vp = G[(size_t)q1 * npb + q2];
+      ab_targets(x1, y1, x2, y2, L, ep, sgp);
+      partner_first = x1 < h1 || (x1 == h1 && (y1 < p1 || (y1 == p1 && (x2 < h2 || (x2 == h2 && y2 < p2)))));
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    double val = sg[i] * v;
+    bool skip = false;
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+      if (ep[j] == e[i]) {
+        if (partner_first) skip = true;
+        else val += sgp[j] * vp;
+      }
+    if (!skip && val != 0.0) two[e[i]] += val;
   }
 }
 
@@ -465,17 +570,28 @@ struct Scratch {
 }  // namespace
 
 // Row weights of both orientations: wa[na], wb[nb]; P_a, P_b, X (L*L each).
+// (P and X are written, not accumulated; the sums have a fixed order.)
 static int weights(Ctx* c, const double* dW, double* wa, double* wb, double* Pa, double* Pb, double* X, double* Wt) {
   const size_t na = c->na, nb = c->nb;
-  row_weight_kernel<<<(unsigned)na, kRowThreads, 0, c->stream>>>(dW, na, nb, c->d_a, c->d_b, c->L, wa, Pa, X);
+  const int L = c->L;
+  Scratch vq;
+  if (X) SBDX_CUDA(c, cudaMalloc(&vq.p, sizeof(double) * na * (size_t)L));
+  const size_t smem = X ? sizeof(double) * kRowWeightThreads * (size_t)L : 0;
+  row_weight_kernel<<<(unsigned)na, kRowWeightThreads, smem, c->stream>>>(dW, nb, c->d_b, L, wa, vq.p);
+  SBDX_LAUNCHED(c);
+  occupation_sums_kernel<<<(unsigned)((L * L + 127) / 128), 128, 0, c->stream>>>(na, c->d_a, L, wa, vq.p, Pa, X);
   SBDX_LAUNCHED(c);
   if (wb) {
     dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((na + 31) / 32));
     transpose_d_kernel<double><<<grid, dim3(32, 8), 0, c->stream>>>(dW, na, nb, Wt);
     SBDX_LAUNCHED(c);
-    row_weight_kernel<<<(unsigned)nb, kRowThreads, 0, c->stream>>>(Wt, nb, na, c->d_b, c->d_a, c->L, wb, Pb, nullptr);
+    row_weight_kernel<<<(unsigned)nb, kRowWeightThreads, 0, c->stream>>>(Wt, na, c->d_a, L, wb, nullptr);
+    SBDX_LAUNCHED(c);
+    occupation_sums_kernel<<<(unsigned)((L * L + 127) / 128), 128, 0, c->stream>>>(nb, c->d_b, L, wb, nullptr, Pb,
+                                                                                  nullptr);
     SBDX_LAUNCHED(c);
   }
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // the profile scratch dies at return
   return 0;
 }
 
@@ -521,8 +637,129 @@ static int singles_by_pattern(Ctx* c, int spin, std::vector<uint32_t>& keys, std
   return 0;
 }
 
+// The entries of one spin grouped by pattern, each group in CSR (bra, then
+// ket) order: singles by info bits 0-11 (hole, particle), doubles by info
+// bits 0-23 (both holes, both particles); per sorted position the entry and
+// its bra row.
+struct EntryGroups {
+  std::vector<uint32_t> key, off, ent, row;
+};
+static int group_entries(Ctx* c, int spin, EntryGroups& sg, EntryGroups& dg) {
+  const Conn& cn = c->conn[spin];
+  const size_t n = cn.n;
+  std::vector<uint64_t> off(n + 1);
+  std::vector<uint32_t> ns(n), info(cn.total ? cn.total : 1);
+  SBDX_CUDA(c, cudaMemcpyAsync(off.data(), cn.off, sizeof(uint64_t) * (n + 1), cudaMemcpyDeviceToHost, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(ns.data(), cn.nsing, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c->stream));
+  if (cn.total)
+    SBDX_CUDA(c, cudaMemcpyAsync(info.data(), cn.info, sizeof(uint32_t) * cn.total, cudaMemcpyDeviceToHost, c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  // stable counting sort by 12-bit digits, least significant first (one pass
+  // for singles, two for doubles)
+  auto sort_by = [&](std::vector<uint32_t> a, int digits, std::vector<uint32_t>& out) {
+    std::vector<uint32_t> b(a.size());
+    for (int d = 0; d < digits; ++d) {
+      std::vector<uint32_t> cnt(4097, 0);
+      for (uint32_t e : a) ++cnt[((info[e] >> (12 * d)) & 0xfffu) + 1];
+      for (int k = 0; k < 4096; ++k) cnt[k + 1] += cnt[k];
+      for (uint32_t e : a) b[cnt[(info[e] >> (12 * d)) & 0xfffu]++] = e;
+      a.swap(b);
+    }
+    out.swap(a);
+  };
+  std::vector<uint32_t> es, ed, rowof(cn.total ? cn.total : 1);
+  for (size_t r = 0; r < n; ++r)
+    for (uint64_t e = off[r]; e < off[r + 1]; ++e) {
+      rowof[e] = (uint32_t)r;
+      (e - off[r] < ns[r] ? es : ed).push_back((uint32_t)e);
+    }
+  auto finish = [&](const std::vector<uint32_t>& sorted, uint32_t mask, EntryGroups& g) {
+    g.ent = sorted;
+    g.row.resize(sorted.size());
+    g.key.clear();
+    g.off.assign(1, 0);
+    for (size_t t = 0; t < sorted.size(); ++t) {
+      g.row[t] = rowof[sorted[t]];
+      const uint32_t k = info[sorted[t]] & mask;
+      if (g.key.empty() || k != g.key.back()) {
+        if (!g.key.empty()) g.off.push_back((uint32_t)t);
+        g.key.push_back(k);
+      }
+    }
+    if (!g.key.empty()) g.off.push_back((uint32_t)sorted.size());
+  };
+  std::vector<uint32_t> ss, sd;
+  sort_by(es, 1, ss);
+  sort_by(ed, 2, sd);
+  finish(ss, 0xfffu, sg);
+  finish(sd, 0xffffffu, dg);
+  return 0;
+}
+
+// Same-spin 1-/2-RDM contributions of one spin without atomics (two may be
+// null: the 1-RDM alone, singles only). Wm: W (spin 0) or W^T (spin 1).
+static int rdm_same_deterministic(Ctx* c, int spin, const double* Wm, double* one, double* two) {
+  const Conn& cn = c->conn[spin];
+  if (cn.total == 0) return 0;
+  EntryGroups sg, dg;
+  int rc = group_entries(c, spin, sg, dg);
+  if (rc) return rc;
+  const size_t cols = spin == 0 ? c->nb : c->na;
+  const uint64_t* s_row = spin == 0 ? c->d_a : c->d_b;
+  const uint64_t* s_col = spin == 0 ? c->d_b : c->d_a;
+  const int L = c->L;
+  struct Bufs {
+    std::vector<void*> p;
+    ~Bufs() { for (void* q : p) cudaFree(q); }
+  } bufs;
+  auto dev = [&](const std::vector<uint32_t>& h, uint32_t** d) -> cudaError_t {
+    cudaError_t e = cudaMalloc(d, sizeof(uint32_t) * std::max<size_t>(1, h.size()));
+    if (e == cudaSuccess) bufs.p.push_back(*d);
+    if (e == cudaSuccess && !h.empty())
+      e = cudaMemcpyAsync(*d, h.data(), sizeof(uint32_t) * h.size(), cudaMemcpyHostToDevice, c->stream);
+    return e;
+  };
+  auto run = [&](const EntryGroups& g, bool singles) -> int {
+    const size_t n = g.ent.size();
+    if (n == 0 || (!singles && two == nullptr)) return 0;
+    uint32_t *d_ent = nullptr, *d_row = nullptr, *d_key = nullptr, *d_off = nullptr;
+    double *d_val = nullptr, *d_prof = nullptr;
+    SBDX_CUDA(c, dev(g.ent, &d_ent));
+    SBDX_CUDA(c, dev(g.row, &d_row));
+    SBDX_CUDA(c, dev(g.key, &d_key));
+    SBDX_CUDA(c, dev(g.off, &d_off));
+    SBDX_CUDA(c, cudaMalloc(&d_val, sizeof(double) * n));
+    bufs.p.push_back(d_val);
+    const int profile = singles && two != nullptr;
+    if (profile) {
+      SBDX_CUDA(c, cudaMalloc(&d_prof, sizeof(double) * n * (size_t)L));
+      bufs.p.push_back(d_prof);
+    }
+    const size_t smem = profile ? sizeof(double) * kValWarps * 32 * (size_t)L : 0;
+    SBDX_CUDA(c, cudaFuncSetAttribute(rdm_same_values_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(double) * kValWarps * 32 * 64)));
+    rdm_same_values_kernel<<<(unsigned)((n + kValWarps - 1) / kValWarps), kValWarps * 32, smem, c->stream>>>(
+        Wm, cols, s_row, s_col, cn.ket, cn.omask, cn.info, d_ent, d_row, n, L, profile, d_val, d_prof);
+    SBDX_LAUNCHED(c);
+    const size_t ng = g.key.size();
+    if (singles) {
+      const size_t nt = ng * (two ? 1 + 2 * (size_t)L : 1);
+      rdm_singles_finalize_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, c->stream>>>(
+          spin, L, d_key, d_off, ng, d_row, s_row, d_val, d_prof, one, two);
+    } else {
+      rdm_doubles_finalize_kernel<<<(unsigned)((ng + 255) / 256), 256, 0, c->stream>>>(spin, L, d_key, d_off, ng,
+                                                                                       d_val, two);
+    }
+    SBDX_LAUNCHED(c);
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // the host vectors and buffers die at return
+    return 0;
+  };
+  if ((rc = run(sg, true))) return rc;
+  return run(dg, false);
+}
+
 // The alpha-single x beta-single 2-RDM contributions without atomics
-// (rdm_ab_det_kernel, rdm_ab_finalize_kernel); returns 1 when the two staged
+// (rdm_ab_det_kernel, rdm_ab_sum_kernel, rdm_ab_write_kernel); returns 1 when the two staged
 // rows do not fit in shared memory (the caller then uses rdm_ab_kernel).
 static int rdm_ab_deterministic(Ctx* c, const double* dW, double* two, bool& done) {
   done = false;
@@ -551,7 +788,7 @@ static int rdm_ab_deterministic(Ctx* c, const double* dW, double* two, bool& don
   auto up = [&](const void* h, size_t bytes, void** d) -> cudaError_t {
     cudaError_t e = cudaMalloc(d, bytes ? bytes : 16);
     if (e == cudaSuccess) bufs.p.push_back(*d);
-    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(*d, h, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && h && bytes) e = cudaMemcpyAsync(*d, h, bytes, cudaMemcpyHostToDevice, c->stream);
     return e;
   };
   uint4 *d_chunks = nullptr, *d_apat = nullptr;
@@ -569,8 +806,21 @@ static int rdm_ab_deterministic(Ctx* c, const double* dW, double* two, bool& don
       dW, nb, c->d_a, c->d_b, d_chunks, d_arec, d_boff, d_bkey, d_brec, npb, d_part);
   SBDX_LAUNCHED(c);
   const size_t npairs = (size_t)npa * npb;
-  rdm_ab_finalize_kernel<<<(unsigned)((npairs + 255) / 256), 256, 0, c->stream>>>(d_apat, npa, d_bkey, npb, d_part,
-                                                                                 c->L, two);
+  std::vector<int> amap(64 * 64, -1), bmap(64 * 64, -1);
+  for (int q = 0; q < npa; ++q) amap[akeys[q]] = q;
+  for (int q = 0; q < npb; ++q) bmap[bkeys[q]] = q;
+  std::vector<uint32_t> akey_v(akeys.begin(), akeys.end());
+  int *d_amap = nullptr, *d_bmap = nullptr;
+  uint32_t* d_akey = nullptr;
+  double* d_G = nullptr;
+  SBDX_CUDA(c, up(amap.data(), sizeof(int) * amap.size(), (void**)&d_amap));
+  SBDX_CUDA(c, up(bmap.data(), sizeof(int) * bmap.size(), (void**)&d_bmap));
+  SBDX_CUDA(c, up(akey_v.data(), sizeof(uint32_t) * akey_v.size(), (void**)&d_akey));
+  SBDX_CUDA(c, up(nullptr, sizeof(double) * npairs, (void**)&d_G));
+  rdm_ab_sum_kernel<<<(unsigned)((npairs + 255) / 256), 256, 0, c->stream>>>(d_apat, npa, npb, d_part, d_G);
+  SBDX_LAUNCHED(c);
+  rdm_ab_write_kernel<<<(unsigned)((npairs + 255) / 256), 256, 0, c->stream>>>(d_akey, npa, d_bkey, npb, d_amap,
+                                                                               d_bmap, d_G, c->L, two);
   SBDX_LAUNCHED(c);
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // the host vectors and buffers die at return
   return 0;
@@ -596,16 +846,8 @@ int rdm_device(Ctx* c, const double* dW, double* d_one, double* d_two) {
   if ((rc = weights(c, dW, wa, wb, Pa, Pb, X, Wt))) return rc;
   diag_finalize_kernel<<<(unsigned)((L2 + 255) / 256), 256, 0, c->stream>>>(c->L, Pa, Pb, X, d_one, two);
   SBDX_LAUNCHED(c);
-  for (int spin = 0; spin < 2; ++spin) {
-    const Conn& cn = c->conn[spin];
-    if (cn.total == 0) continue;
-    const double* Wm = spin == 0 ? dW : Wt;
-    const size_t rows = spin == 0 ? na : nb, cols = spin == 0 ? nb : na;
-    rdm_same_kernel<<<(unsigned)((cn.total + 7) / 8), 256, 0, c->stream>>>(
-        spin, Wm, rows, cols, spin == 0 ? c->d_a : c->d_b, spin == 0 ? c->d_b : c->d_a, cn.off, cn.ket, cn.omask,
-        cn.info, cn.total, c->L, d_one, two);
-    SBDX_LAUNCHED(c);
-  }
+  for (int spin = 0; spin < 2; ++spin)
+    if ((rc = rdm_same_deterministic(c, spin, spin == 0 ? dW : Wt, d_one, two))) return rc;
   bool done = d_two == nullptr;  // the alpha-beta pairs only add to the 2-RDM
   if (!done && (rc = rdm_ab_deterministic(c, dW, two, done))) return rc;
   if (!done) {
