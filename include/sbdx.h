@@ -181,6 +181,18 @@ int sbdx_sigma_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS);
  * held). The rows' work items are built on first use of a range. */
 int sbdx_sigma_rows_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS, size_t a0, size_t a1);
 
+/* The subspace projection of every Davidson step: dP[i*nx + r] = <V_i, X_r>
+ * for m device vectors V_i (element stride ldv) and 1 <= nx <= 8 device
+ * vectors X_r (stride ldx), D elements each, of the given precision; dP holds
+ * m*nx doubles on the device. The reference forms these dots one pair at a
+ * time (InnerProduct, framework/dm_vector.h:179-243, called from
+ * chemistry/tpb/davidson.h:756-797 and 865-873); here one pass over the
+ * vectors evaluates all of them as (m x D)(D x nx) tiles on the FP64 tensor
+ * pipe (FP32 vectors widened exactly), with a fixed-order reduction, on the
+ * context stream; returns after the result is written. */
+int sbdx_project_device(sbdx_ctx* ctx, int precision, const void* dV, size_t ldv, int m, const void* dX, size_t ldx,
+                        int nx, size_t D, double* dP);
+
 typedef struct {
   int max_it;          /* outer restarts (SBD::max_it, sbdiag.h:19)            */
   int max_nb;          /* subspace size (SBD::max_nb, sbdiag.h:20)            */

@@ -445,6 +445,16 @@ int sbdx_sigma_rows_device(sbdx_ctx* ctx, int precision, const void* dC, void* d
   });
 }
 
+int sbdx_project_device(sbdx_ctx* ctx, int precision, const void* dV, size_t ldv, int m, const void* dX, size_t ldx,
+                        int nx, size_t D, double* dP) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (m < 0 || nx < 1 || nx > 8) { c->err = "project_device: need m >= 0 and 1 <= nx <= 8"; return SBDX_ERR_ARG; }
+    if (m > 0 && (!dV || !dX || !dP)) { c->err = "project_device: null pointer"; return SBDX_ERR_ARG; }
+    if ((m > 1 && ldv < D) || (nx > 1 && ldx < D)) { c->err = "project_device: stride below D"; return SBDX_ERR_ARG; }
+    return sbdx::project_device(c, precision, dV, ldv, m, dX, ldx, nx, D, dP);
+  });
+}
+
 int sbdx_davidson(sbdx_ctx* ctx, const sbdx_davidson_params* params, int init_from_W, double* W,
                   sbdx_davidson_info* info) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {

@@ -38,7 +38,6 @@ namespace {
 
 constexpr int kRedThreads = 256;
 constexpr int kRedBlocks = 4 * 148;
-constexpr int kDotChunk = 8;
 
 __device__ __forceinline__ double block_sum(double v, double* sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -99,10 +98,16 @@ __device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
 }
 __device__ __forceinline__ size_t quads(size_t D) { return D % 4 == 0 ? D / 4 : 0; }
 
-// partial[k * gridDim.x + blk] = partial sums of <V_k, x>, k in [k0, k0+mc)
+// A few dots with one vector (m <= kCoreRows, one X) on the CUDA cores: an
+// 8 x 8 DMMA tile would leave all but m of its 8 A rows and 7 of its 8 B
+// columns empty, and with them the lanes that load them, so too few bytes
+// would be in flight. partial[k * gridDim.x + blk] = partial sums of
+// <V_k, x>, k in [k0, k0 + mc), four consecutive elements per thread.
+constexpr int kCoreRows = 4;
+constexpr int kDotChunk = 8;
 template <typename TV, typename TX>
 __global__ void __launch_bounds__(kRedThreads)
-multidot_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restrict__ x, size_t D,
+multidot_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restrict__ x, size_t D, int vec,
                 double* __restrict__ partial) {
   __shared__ double sh[kDotChunk * (kRedThreads / 32)];
   const int k0 = blockIdx.y * kDotChunk;
@@ -111,7 +116,7 @@ multidot_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restric
 #pragma unroll
   for (int k = 0; k < kDotChunk; ++k) acc[k] = 0.0;
   const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
-  const size_t nq = quads(D);
+  const size_t nq = vec ? D / 4 : 0;  // 16-byte quads when every row and x are 16-byte aligned
   for (size_t q = t0; q < nq; q += st) {
     double xv[4];
     ld4(x + 4 * q, xv);
@@ -130,6 +135,167 @@ multidot_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restric
       if (k < mc) acc[k] = fma((double)V[(size_t)(k0 + k) * ldv + s], xv, acc[k]);
   }
   block_sums<kDotChunk>(acc, mc, sh, partial, (size_t)k0);
+}
+
+// Projection on the FP64 tensor pipe: P[i][r] = <V_i, X_r> for i < m <= 64,
+// r < nx <= 8, with one read of every vector, as a skinny product
+// (m x D) * (D x nx) of DMMA tiles (mma.sync m8n8k4, FP64 in, FP64
+// accumulate). A tile's A operand is 8 rows of V over 4 k-slots, its B
+// operand the X vectors over the same 4 k-slots; the k-slot of lane l is
+// l & 3 in both, so lane l may bind its k-slot to any element index as long
+// as it uses the same index for its A and its B element. Each lane therefore
+// loads R elements of a chunk of 4R (row l >> 2 of every tile, X vector
+// l >> 2) and issues R DMMAs per tile, one per element; ld_lane interleaves
+// the lanes' pieces so that every load is coalesced. FP32 vectors are
+// widened exactly at the DMMA, so both storage types share the FP64 products
+// and accumulation. Lane l ends with P rows 8t + (l >> 2), columns
+// 2 (l & 3) + {0, 1} of tile t; the warps of a CTA are summed in a fixed
+// order into partial[(i * nx + r) * gridDim.x + blockIdx.x].
+constexpr int kProjCols = 8;
+template <typename T>
+struct XSet {
+  const T* p[kProjCols];
+};
+
+__device__ __forceinline__ void dmma_m8n8k4(double (&d)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
+
+// One piece of G consecutive elements in one load (8 or 16 bytes).
+template <int G, typename T>
+struct Piece;
+template <>
+struct Piece<2, double> {
+  __device__ static void load(const double* p, double* o) {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+  }
+};
+template <>
+struct Piece<2, float> {
+  __device__ static void load(const float* p, float* o) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+  }
+};
+template <>
+struct Piece<4, float> {
+  __device__ static void load(const float* p, float* o) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+  }
+};
+
+// The R elements of lane q in a chunk starting at element c0: pieces
+// 4i + q (i < R / G) of G elements, so the four lanes of a row read 4 G
+// consecutive elements per load and a warp's load touches 8 rows x 64 bytes
+// (whole sectors). Element j of the lane is chunk element
+// (4 (j / G) + q) G + j % G; the A and B operands use the same map.
+template <int R, int G, typename T>
+__device__ __forceinline__ void ld_lane(const T* p, size_t c0, int q, T (&o)[R]) {
+#pragma unroll
+  for (int i = 0; i < R / G; ++i) Piece<G, T>::load(p + c0 + (size_t)(4 * i + q) * G, o + i * G);
+}
+// same map, elements at or beyond D read as zero
+template <int R, int G, typename T>
+__device__ __forceinline__ void ld_lane_tail(const T* p, size_t c0, int q, size_t D, T (&o)[R]) {
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    const size_t d = c0 + (size_t)(4 * (j / G) + q) * G + j % G;
+    o[j] = d < D ? __ldg(p + d) : T(0);
+  }
+}
+
+// Elements per lane and chunk: 32 / 16 / 8 for one / two or three / more row tiles,
+// doubled when both operands are FP32, which keeps a warp's loads in flight
+// near 8 KB whatever m is.
+template <int MT, typename TV, typename TX>
+struct ProjRun {
+  static constexpr int value = (MT >= 4 ? 8 : (MT >= 2 ? 16 : 32)) * (sizeof(TV) == 4 && sizeof(TX) == 4 ? 2 : 1);
+};
+
+template <int MT, typename TV, typename TX>
+__global__ void __launch_bounds__(kRedThreads)
+project_kernel(const TV* __restrict__ V, size_t ldv, int m, XSet<TX> X, int nx, size_t D, int vec,
+               double* __restrict__ partial) {
+  constexpr int G = 16 / (sizeof(TV) > sizeof(TX) ? sizeof(TV) : sizeof(TX));  // piece: 16 bytes of the wider type
+  constexpr int R = ProjRun<MT, TV, TX>::value;
+  constexpr int kSpan = 4 * R;  // elements of one chunk
+  static_assert(R % G == 0, "a lane's run is whole pieces");
+  __shared__ double sh[(kRedThreads / 32) * 8 * MT * kProjCols];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+  const int row0 = 8 * MT * blockIdx.y;  // rows of V beyond 8 * MT go to further grid rows
+  V += (size_t)row0 * ldv;
+  m = min(m - row0, 8 * MT);
+  partial += (size_t)row0 * nx * gridDim.x;
+  double acc[MT][2];
+#pragma unroll
+  for (int t = 0; t < MT; ++t) acc[t][0] = acc[t][1] = 0.0;
+  const TX* xp = nullptr;  // selected without a dynamic index into the parameter block
+#pragma unroll
+  for (int r = 0; r < kProjCols; ++r)
+    if (r == g && r < nx) xp = X.p[r];
+  const TV* vp[MT];
+#pragma unroll
+  for (int t = 0; t < MT; ++t) vp[t] = 8 * t + g < m ? V + (size_t)(8 * t + g) * ldv : nullptr;
+  const size_t nchunk = (D + kSpan - 1) / kSpan;
+  const size_t wpb = blockDim.x >> 5;
+  for (size_t ch = (size_t)blockIdx.x * wpb + warp; ch < nchunk; ch += (size_t)gridDim.x * wpb) {
+    const size_t c0 = ch * kSpan;
+    const bool full = vec && c0 + kSpan <= D;  // warp-uniform
+    // operands stay in their storage type until the DMMA (FP32 runs take
+    // half the registers)
+    TX xv[R];
+    if (!xp) {
+#pragma unroll
+      for (int j = 0; j < R; ++j) xv[j] = TX(0);
+    } else if (full) {
+      ld_lane<R, G>(xp, c0, q, xv);
+    } else {
+      ld_lane_tail<R, G>(xp, c0, q, D, xv);
+    }
+    TV vv[MT][R];
+#pragma unroll
+    for (int t = 0; t < MT; ++t) {
+      if (!vp[t]) {
+#pragma unroll
+        for (int j = 0; j < R; ++j) vv[t][j] = TV(0);
+      } else if (full) {
+        ld_lane<R, G>(vp[t], c0, q, vv[t]);
+      } else {
+        ld_lane_tail<R, G>(vp[t], c0, q, D, vv[t]);
+      }
+    }
+    // element-major order: consecutive DMMAs go to different tiles
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const double xd = (double)xv[j];
+#pragma unroll
+      for (int t = 0; t < MT; ++t)
+        if (8 * t < m) dmma_m8n8k4(acc[t], (double)vv[t][j], xd);  // tiles without rows skipped (warp-uniform)
+    }
+  }
+  double* sw = sh + (size_t)warp * 8 * MT * kProjCols;
+#pragma unroll
+  for (int t = 0; t < MT; ++t) {
+    sw[(8 * t + g) * kProjCols + 2 * q] = acc[t][0];
+    sw[(8 * t + g) * kProjCols + 2 * q + 1] = acc[t][1];
+  }
+  __syncthreads();
+  const int nw = (int)wpb;
+  for (int e = threadIdx.x; e < m * nx; e += blockDim.x) {
+    const int i = e / nx, r = e - i * nx;
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += sh[((size_t)w * 8 * MT + i) * kProjCols + r];
+    partial[(size_t)e * gridDim.x + blockIdx.x] = s;
+  }
 }
 
 // out[k] = sum_b partial[k * nblk + b] (fixed order, deterministic)
@@ -219,7 +385,22 @@ precond_kernel(const double* R, const double* __restrict__ dii, const double* __
   const double inv = 1.0 / sqrt(*nrm2);
   const double eps_reg = 1.0e-12;
   double acc = 0.0;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < D; s += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nq = quads(D);
+  for (size_t q = t0; q < nq; q += st) {  // element quads (16-byte loads), then the rest one by one
+    double r[4], d[4], b[4], x[4];
+    ld4(R + 4 * q, r);
+    ld4(dii + 4 * q, d);
+    if (V0d != nullptr) ld4(V0d + 4 * q, b); else ld4(V0 + 4 * q, b);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const double rs = r[e] * inv, den = E0 - d[e];
+      x[e] = fabs(den) > eps_reg ? rs / den : rs / (den - eps_reg);
+      acc = fma(b[e], x[e], acc);
+    }
+    st4(v + 4 * q, x);
+  }
+  for (size_t s = 4 * nq + t0; s < D; s += st) {
     const double rs = R[s] * inv;
     const double den = E0 - dii[s];
     const double x = fabs(den) > eps_reg ? rs / den : rs / (den - eps_reg);
@@ -369,15 +550,67 @@ unsigned wave_of(K kernel) {
   return (unsigned)std::min(kRedBlocks, nsm * occ);
 }
 
+template <int MT, typename TV, typename TX>
+unsigned launch_project(Ctx* c, const TV* V, size_t ldv, int m, const XSet<TX>& X, int nx, size_t D, int vec,
+                        double* partial) {
+  static const unsigned g = wave_of(project_kernel<MT, TV, TX>);
+  const dim3 grid(g, (unsigned)((m + 8 * MT - 1) / (8 * MT)));
+  project_kernel<MT, TV, TX><<<grid, kRedThreads, 0, c->stream>>>(V, ldv, m, X, nx, D, vec, partial);
+  return g;
+}
+
+// out[i * nx + r] = <V_i, X_r>, i < m, r < nx <= 8 (project_kernel on the
+// tensor pipe, or multidot_kernel for a few dots with one vector; then the
+// fixed-order sum of the CTA partials). Needs kRedBlocks * m * nx partials.
 template <typename TV, typename TX>
-int multidot(Ctx* c, Work& wk, const TV* V, size_t ldv, int m, const TX* x, size_t D, double* out) {
-  static const unsigned g = wave_of(multidot_kernel<TV, TX>);
-  dim3 grid(g, (unsigned)((m + kDotChunk - 1) / kDotChunk));
-  multidot_kernel<TV, TX><<<grid, kRedThreads, 0, c->stream>>>(V, ldv, m, x, D, wk.partial);
+int project(Ctx* c, Work& wk, const TV* V, size_t ldv, int m, const XSet<TX>& X, int nx, size_t D, double* out) {
+  if (m <= 0) return 0;
+  if (nx < 1 || nx > kProjCols) {
+    c->err = "projection onto " + std::to_string(nx) + " vectors (1 .. 8)";
+    return SBDX_ERR_ARG;
+  }
+  int vec = reinterpret_cast<uintptr_t>(V) % 16 == 0 && (ldv * sizeof(TV)) % 16 == 0;
+  for (int r = 0; r < nx; ++r) vec = vec && reinterpret_cast<uintptr_t>(X.p[r]) % 16 == 0;
+  unsigned g;
+  if (nx == 1 && m <= kCoreRows) {
+    static const unsigned gc = wave_of(multidot_kernel<TV, TX>);
+    g = gc;
+    multidot_kernel<TV, TX><<<dim3(g, 1), kRedThreads, 0, c->stream>>>(V, ldv, m, X.p[0], D, vec, wk.partial);
+  } else {
+    // as many row tiles as m needs (a tile without rows would still cost its
+    // DMMAs: the FP32 form is within 1.5x of the DMMA rate at 8 tiles)
+    switch (std::min((m + 7) / 8, 8)) {
+      case 1: g = launch_project<1>(c, V, ldv, m, X, nx, D, vec, wk.partial); break;
+      case 2: g = launch_project<2>(c, V, ldv, m, X, nx, D, vec, wk.partial); break;
+      case 3: g = launch_project<3>(c, V, ldv, m, X, nx, D, vec, wk.partial); break;
+      case 4: g = launch_project<4>(c, V, ldv, m, X, nx, D, vec, wk.partial); break;
+      case 5: g = launch_project<5>(c, V, ldv, m, X, nx, D, vec, wk.partial); break;
+      case 6: g = launch_project<6>(c, V, ldv, m, X, nx, D, vec, wk.partial); break;
+      case 7: g = launch_project<7>(c, V, ldv, m, X, nx, D, vec, wk.partial); break;
+      default: g = launch_project<8>(c, V, ldv, m, X, nx, D, vec, wk.partial); break;
+    }
+  }
   SBDX_LAUNCHED(c);
-  finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, (int)g, m, out);
+  finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, (int)g, m * nx, out);
   SBDX_LAUNCHED(c);
   return 0;
+}
+
+// out[k] = <V_k, x>, k < m
+template <typename TV, typename TX>
+int multidot(Ctx* c, Work& wk, const TV* V, size_t ldv, int m, const TX* x, size_t D, double* out) {
+  XSet<TX> X{};
+  X.p[0] = x;
+  return project(c, wk, V, ldv, m, X, 1, D, out);
+}
+
+// out[2k + i] = <V_k, x_i>, i = 0, 1: two projections with one read of V
+template <typename TV, typename TX>
+int multidot2(Ctx* c, Work& wk, const TV* V, size_t ldv, int m, const TX* x0, const TX* x1, size_t D, double* out) {
+  XSet<TX> X{};
+  X.p[0] = x0;
+  X.p[1] = x1;
+  return project(c, wk, V, ldv, m, X, 2, D, out);
 }
 
 // out[k] = sum of the nblk partials of row k (nblk = the producing grid).
@@ -650,52 +883,6 @@ olsen_apply_kernel(double* __restrict__ v, const double* __restrict__ W, const d
   if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = t;
 }
 
-// partial[(2k + i) * gridDim.x + blk] = partial sums of <V_k, x_i>, i = 0, 1,
-// k in [k0, k0+mc): two projections with one read of V.
-// FP32 vectors: held to 4 CTAs per SM (64 registers) for more loads in
-// flight; it is bound by load latency (measured: 3 CTAs per SM at 80
-// registers, 36% of warps active, long-scoreboard stalls).
-template <typename TV, typename TX>
-__global__ void __launch_bounds__(kRedThreads, sizeof(TV) == 4 ? 4 : 1)
-multidot2_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restrict__ x0, const TX* __restrict__ x1,
-                 size_t D, double* __restrict__ partial) {
-  __shared__ double sh[2 * kDotChunk * (kRedThreads / 32)];
-  const int k0 = blockIdx.y * kDotChunk;
-  const int mc = min(kDotChunk, m - k0);
-  double a0[kDotChunk], a1[kDotChunk];
-#pragma unroll
-  for (int k = 0; k < kDotChunk; ++k) a0[k] = a1[k] = 0.0;
-  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
-  const size_t nq = quads(D);
-  for (size_t q = t0; q < nq; q += st) {
-    double y0[4], y1[4];
-    ld4(x0 + 4 * q, y0);
-    ld4(x1 + 4 * q, y1);
-#pragma unroll
-    for (int k = 0; k < kDotChunk; ++k)
-      if (k < mc) {
-        double v[4];
-        ld4(V + (size_t)(k0 + k) * ldv + 4 * q, v);
-        a0[k] = fma(v[0], y0[0], fma(v[1], y0[1], fma(v[2], y0[2], fma(v[3], y0[3], a0[k]))));
-        a1[k] = fma(v[0], y1[0], fma(v[1], y1[1], fma(v[2], y1[2], fma(v[3], y1[3], a1[k]))));
-      }
-  }
-  for (size_t s = 4 * nq + t0; s < D; s += st) {
-    const double y0 = (double)x0[s], y1 = (double)x1[s];
-#pragma unroll
-    for (int k = 0; k < kDotChunk; ++k)
-      if (k < mc) {
-        const double v = (double)V[(size_t)(k0 + k) * ldv + s];
-        a0[k] = fma(v, y0, a0[k]);
-        a1[k] = fma(v, y1, a1[k]);
-      }
-  }
-  double both[2 * kDotChunk];  // rows 2k (x0) and 2k + 1 (x1)
-#pragma unroll
-  for (int k = 0; k < kDotChunk; ++k) { both[2 * k] = a0[k]; both[2 * k + 1] = a1[k]; }
-  block_sums<2 * kDotChunk>(both, 2 * mc, sh, partial, (size_t)(2 * k0));
-}
-
 // Classical Gram-Schmidt update: v -= o[0] W + sum_k o[k+1] V_k; partial |v|^2.
 template <typename TV>
 __global__ void __launch_bounds__(kRedThreads)
@@ -956,13 +1143,7 @@ int davidson_mixed(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_david
       ++steps;
       ++since;
       // (<C_k|HC_j>, <C_k|C_j>) for k <= j with one read of C; <W|C_j>, <HW|C_j>
-      {
-        static const unsigned g2 = wave_of(multidot2_kernel<float, float>);
-        dim3 grid(g2, (unsigned)((nv + kDotChunk - 1) / kDotChunk));
-        multidot2_kernel<float, float><<<grid, kRedThreads, 0, c->stream>>>(C, D, nv, HCb, Cb, D, wk.partial);
-        SBDX_LAUNCHED(c);
-        if ((rc = finalize(c, wk, 2 * nv, s + kDots, g2))) return rc;
-      }
+      if ((rc = multidot2<float, float>(c, wk, C, D, nv, HCb, Cb, D, s + kDots))) return rc;
       if ((rc = multidot<double, float>(c, wk, AW, D, 2, Cb, D, s + kDots + 2 * nv))) return rc;
       SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kDots, sizeof(double) * (2 * nv + 2), cudaMemcpyDeviceToHost,
                                    c->stream));
@@ -1505,13 +1686,7 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
         if (kMixed) info.n_sigma++; else info.n_sigma64++;
         ++added;
         // (<C_i|HC_j>, <C_i|C_j>) for i <= j; <W_r|C_j>, <HW_r|C_j>
-        {
-          static const unsigned g2 = wave_of(multidot2_kernel<TC, TC>);
-          dim3 grid(g2, (unsigned)((nv + kDotChunk - 1) / kDotChunk));
-          multidot2_kernel<TC, TC><<<grid, kRedThreads, 0, c->stream>>>(C, D, nv, HCb, Cb, D, wk.partial);
-          SBDX_LAUNCHED(c);
-          if ((rc = finalize(c, wk, 2 * nv, s + kbDots, g2))) return rc;
-        }
+        if ((rc = multidot2<TC, TC>(c, wk, C, D, nv, HCb, Cb, D, s + kbDots))) return rc;
         // W and HW are contiguous (HW = W + k*D) in either half of A
         if ((rc = multidot<double, TC>(c, wk, W, D, 2 * k, Cb, D, s + kbDots + 2 * nv))) return rc;
         SBDX_CUDA(c, cudaMemcpyAsync(col.data(), s + kbDots, sizeof(double) * (2 * nv + 2 * k), cudaMemcpyDeviceToHost,
@@ -2147,13 +2322,7 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
       SBDX_LAUNCHED(c);
       if ((r2 = sigma_typed<TC>(c, Cb, HCb))) return r2;
       ++nv;
-      {
-        static const unsigned g2 = wave_of(multidot2_kernel<TC, TC>);
-        dim3 grid(g2, (unsigned)((nv + kDotChunk - 1) / kDotChunk));
-        multidot2_kernel<TC, TC><<<grid, kRedThreads, 0, c->stream>>>(C, D, nv, HCb, Cb, D, wk.partial);
-        SBDX_LAUNCHED(c);
-        if ((r2 = finalize(c, wk, 2 * nv, s + kbDots, g2))) return r2;
-      }
+      if ((r2 = multidot2<TC, TC>(c, wk, C, D, nv, HCb, Cb, D, s + kbDots))) return r2;
       if ((r2 = multidot<double, TC>(c, wk, W, D, 2 * k, Cb, D, s + kbDots + 2 * nv))) return r2;
       scatter_new_kernel<<<1, 64, 0, c->stream>>>(k, j, ld, s + kbDots, dM, dS);
       SBDX_LAUNCHED(c);
@@ -2390,6 +2559,27 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
 
 
 }  // namespace
+
+int project_device(Ctx* c, int precision, const void* V, size_t ldv, int m, const void* X, size_t ldx, int nx,
+                   size_t D, double* P) {
+  if (m <= 0) return 0;
+  Work wk;  // partials from the context's stream-ordered pool (no device-wide sync per call)
+  SBDX_CUDA(c, pool_alloc(c, reinterpret_cast<void**>(&wk.partial), sizeof(double) * kRedBlocks * (size_t)m * nx));
+  int rc;
+  if (precision == SBDX_FP32) {
+    XSet<float> xs{};
+    for (int r = 0; r < nx && r < kProjCols; ++r) xs.p[r] = static_cast<const float*>(X) + (size_t)r * ldx;
+    rc = project<float, float>(c, wk, static_cast<const float*>(V), ldv, m, xs, nx, D, P);
+  } else {
+    XSet<double> xs{};
+    for (int r = 0; r < nx && r < kProjCols; ++r) xs.p[r] = static_cast<const double*>(X) + (size_t)r * ldx;
+    rc = project<double, double>(c, wk, static_cast<const double*>(V), ldv, m, xs, nx, D, P);
+  }
+  cudaFreeAsync(wk.partial, c->stream);
+  wk.partial = nullptr;
+  if (!rc) SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  return rc;
+}
 
 int davidson(Ctx* c, const sbdx_davidson_params& p, double* dW, sbdx_davidson_info& info) {
   if (p.max_nb < 1 || p.max_nb > 60 || p.max_it < 1) {

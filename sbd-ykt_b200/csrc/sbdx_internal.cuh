@@ -359,6 +359,8 @@ void free_row_range(Ctx* c);
 // Rows [a0, a1) of S = H X: X the whole vector (na x nb), S the (a1 - a0) x nb
 // output rows; a0 a multiple of 8 (or a0 == a1).
 int sigma_rows_device(Ctx* c, int precision, const void* X, void* S, size_t a0, size_t a1);
+int project_device(Ctx* c, int precision, const void* V, size_t ldv, int m, const void* X, size_t ldx, int nx,
+                   size_t D, double* P);
 int build_g_table(Ctx* c);
 int build_coulomb_tables(Ctx* c);
 int diag_terms(Ctx* c);

@@ -34,7 +34,7 @@ EXPORTS = [
     "sbdx_phase_times", "sbdx_set_tuning", "sbdx_autotune", "sbdx_davidson_roots",
     "sbdx_build_hamiltonian", "sbdx_release_hamiltonian", "sbdx_wavefunction_device", "sbdx_get_wavefunction",
     "sbdx_rdm_device", "sbdx_occupation_device", "sbdx_alpha_weights_device", "sbdx_energy_backward_device",
-    "sbdx_sigma_rows_device", "sbdx_set_graph_steps",
+    "sbdx_sigma_rows_device", "sbdx_set_graph_steps", "sbdx_project_device",
 ]
 PHASES = ["alpha_same_spin", "transpose", "beta_same_spin", "alpha_beta", "combine"]
 
@@ -214,6 +214,14 @@ class Context:
         input, s_ptr the (a1 - a0) * nb output rows."""
         self._check(self.lib.sbdx_sigma_rows_device(self.h, ctypes.c_int(precision), ctypes.c_void_p(c_ptr),
                                                     ctypes.c_void_p(s_ptr), ctypes.c_size_t(a0), ctypes.c_size_t(a1)))
+
+    def project_device(self, precision, v_ptr: int, ldv: int, m: int, x_ptr: int, ldx: int, nx: int, D: int,
+                       p_ptr: int):
+        """sbdx_project_device: p[i * nx + r] = <V_i, X_r> on the device."""
+        self._check(self.lib.sbdx_project_device(self.h, ctypes.c_int(precision), ctypes.c_void_p(v_ptr),
+                                                 ctypes.c_size_t(ldv), ctypes.c_int(m), ctypes.c_void_p(x_ptr),
+                                                 ctypes.c_size_t(ldx), ctypes.c_int(nx), ctypes.c_size_t(D),
+                                                 ctypes.c_void_p(p_ptr)))
 
     def davidson(self, max_it=1, max_nb=10, eps=1e-4, max_time=86400.0, precision=SBDX_FP64, defect_every=0,
                  verbose=0, W=None, to_host=True):
