@@ -24,8 +24,9 @@ against the measured HBM copy bandwidth, and the DRAM bytes ncu measured;
 B = P*s_c + D*(2*s_c + s_h) + 4*(connectivity entries) + 8*(na + nb). The CPU baseline is the reference's own
 OpenMP mult (compiled in oracle/_ref) on a bounded sample of bra alpha rows.
 `mixed_precision` runs the 400 M-determinant workload (2 roots) in FP64 and
-mixed precision with energy and 1-RDM errors; `summary`, printed last, holds
-the headline figures.
+mixed precision with energy and 1-RDM errors; `projection` times the
+Davidson subspace projection (DMMA tiles on the FP64 tensor pipe) at the
+shapes the solvers issue; `summary`, printed last, holds the headline figures.
 
 Multi-GPU (--gpus N under torchrun): one sigma of the same workload split by
 alpha-row shards over the N GPUs (sbdx/shard.py: the whole C gathered on every
@@ -81,6 +82,8 @@ def parse_args():
     ap.add_argument("--mixed", default="cfg3", metavar="WORKLOAD",
                     help="workload of the mixed-precision measurement (2 roots, FP64 block solve vs mixed with "
                          "refresh every 4 steps and adaptive; '' = skip)")
+    ap.add_argument("--projection-d", type=int, default=None, metavar="D",
+                    help="vector length of the projection measurement (default: the workload's; 0 = skip)")
     ap.add_argument("--sharded", action="store_true",
                     help="run the alpha-row-shard path (the N > 1 path) also at N = 1")
     ap.add_argument("--tune", default=None, metavar="SAME,AB",
@@ -351,6 +354,61 @@ def run_batched(args) -> dict:
         out["speedup_batched_mixed_vs_sequential_fp64"] = runs["sequential_fp64"]["seconds"] / runs["batched_mixed"]["seconds"]
         out["speedup_batched_mixed_graph_steps_vs_sequential_fp64"] = (
             runs["sequential_fp64"]["seconds"] / runs["batched_mixed_graph_steps"]["seconds"])
+    return out
+
+
+def run_projection(args, hbm: float) -> dict:
+    """The Davidson subspace projection on the FP64 tensor pipe
+    (sbdx_project_device, DMMA tiles): P = V X^T at the shapes the solvers
+    issue, on vectors of `--projection-d` elements (default: the workload's
+    determinant count). First one call of each of three shapes (FP64 24 x 2,
+    FP32 24 x 2, FP32 62 x 2), so that an ncu capture of the first three
+    launches sees three kernels; then, shape by shape, one warm-up call and
+    10 timed calls (CUDA events). Bytes: one read of the m + nx vectors; they
+    are far larger than L2."""
+    import torch
+
+    import sbdx
+
+    D = args.projection_d
+    F64, F32 = sbdx.SBDX_FP64, sbdx.SBDX_FP32
+    first = [(F64, 24, 2), (F32, 24, 2), (F32, 62, 2)]
+    sweep = [(p, m, nx) for p in (F64, F32)
+             for m, nx in ((1, 1), (2, 1), (4, 4), (8, 2), (16, 2), (24, 2), (40, 2), (62, 2), (20, 1))]
+    out = {"kernel": "project_kernel (mma.sync m8n8k4 f64); m <= 4 with nx = 1: multidot_kernel (CUDA cores)",
+           "D": D, "cases": []}
+    with sbdx.Context(torch.cuda.current_device()) as ctx:
+        stream = torch.cuda.current_stream()
+        ctx.set_stream(stream.cuda_stream)
+
+        def operands(prec, m, nx):
+            dt = torch.float64 if prec == F64 else torch.float32
+            V = torch.randn(m, D, dtype=dt, device="cuda")
+            X = torch.randn(nx, D, dtype=dt, device="cuda")
+            P = torch.empty(m * nx, dtype=torch.float64, device="cuda")
+            return V, X, P, (lambda: ctx.project_device(prec, V.data_ptr(), D, m, X.data_ptr(), D, nx, D,
+                                                         P.data_ptr()))
+
+        for shape in first:
+            ops = operands(*shape)
+            ops[3]()
+            del ops
+        for prec, m, nx in sweep:
+            V, X, P, call = operands(prec, m, nx)
+            call()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(10):
+                call()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 10
+            gbs = (m + nx) * D * V.element_size() / (ms * 1e-3) / 1e9
+            out["cases"].append({"precision": "fp64" if prec == F64 else "fp32", "m": m, "nx": nx,
+                                 "ms": ms, "gbs": gbs, "frac_of_hbm": gbs / hbm})
+            del V, X, P, call
+            torch.cuda.empty_cache()
     return out
 
 
@@ -817,6 +875,11 @@ def run_ours(args, rank, world, local):
     stored = None
     if args.stored and world == 1:
         stored = run_stored(args, hbm)
+    proj = None
+    if args.projection_d is None:
+        args.projection_d = int(prob.D)
+    if args.projection_d and world == 1:
+        proj = run_projection(args, hbm)
     diff = None
     if args.diff and world == 1 and not args.no_davidson:
         diff = run_differentiation(args)
@@ -880,6 +943,7 @@ def run_ours(args, rank, world, local):
         "mixed_precision": mixed,
         "batched": batched,
         "stored_hamiltonian": stored,
+        "projection": proj,
         "differentiation": diff,
         "cpu_baseline": cpu,
     }
@@ -916,6 +980,10 @@ def summary(line) -> dict:
     out["batched_mixed_vs_sequential_fp64"] = get("batched", "speedup_batched_mixed_vs_sequential_fp64")
     out["batched_mixed_graph_steps_vs_sequential_fp64"] = get("batched",
                                                               "speedup_batched_mixed_graph_steps_vs_sequential_fp64")
+    pr = line.get("projection")
+    if pr:
+        out["projection_dmma_frac_of_hbm"] = {f"{c['precision']}_m{c['m']}_nx{c['nx']}": round(c["frac_of_hbm"], 3)
+                                               for c in pr["cases"] if (c["m"], c["nx"]) in ((24, 2), (62, 2))}
     d = line.get("differentiation")
     if d:
         out["backward_over_forward"] = d["backward_seconds"] / d["forward_seconds"]

@@ -1828,7 +1828,10 @@ int davidson_block(Ctx* c, const sbdx_davidson_params& p, int k, double* dW, dou
 // The host launches iteration t + 1 before it reads the status that
 // iteration t copied to pinned memory (residual estimates, energies, error
 // word), and decides there whether to refresh the anchors with exact FP64
-// products (the criteria of davidson_block, one iteration later) or stop.
+// products (the criteria of davidson_block, one iteration later, and at most
+// kGraphMaxSince iterations after the last refresh) or stop. On a decision
+// the iteration queued after t is dropped: the solver continues from t's
+// anchors and subspace, as the host-driven solver does.
 // Graphs are captured on first use, one per kind (iteration or refresh),
 // number of corrections and current anchor buffer, and replayed after that.
 
