@@ -102,39 +102,51 @@ __device__ __forceinline__ size_t quads(size_t D) { return D % 4 == 0 ? D / 4 : 
 // 8 x 8 DMMA tile would leave all but m of its 8 A rows and 7 of its 8 B
 // columns empty, and with them the lanes that load them, so too few bytes
 // would be in flight. partial[k * gridDim.x + blk] = partial sums of
-// <V_k, x>, k in [k0, k0 + mc), four consecutive elements per thread.
+// <V_k, x>, k < m, two quads of consecutive elements per thread in flight.
 constexpr int kCoreRows = 4;
-constexpr int kDotChunk = 8;
 template <typename TV, typename TX>
 __global__ void __launch_bounds__(kRedThreads)
 multidot_kernel(const TV* __restrict__ V, size_t ldv, int m, const TX* __restrict__ x, size_t D, int vec,
                 double* __restrict__ partial) {
-  __shared__ double sh[kDotChunk * (kRedThreads / 32)];
-  const int k0 = blockIdx.y * kDotChunk;
-  const int mc = min(kDotChunk, m - k0);
-  double acc[kDotChunk];
+  __shared__ double sh[kCoreRows * (kRedThreads / 32)];
+  double acc[kCoreRows];
 #pragma unroll
-  for (int k = 0; k < kDotChunk; ++k) acc[k] = 0.0;
+  for (int k = 0; k < kCoreRows; ++k) acc[k] = 0.0;
   const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
   const size_t nq = vec ? D / 4 : 0;  // 16-byte quads when every row and x are 16-byte aligned
-  for (size_t q = t0; q < nq; q += st) {
-    double xv[4];
-    ld4(x + 4 * q, xv);
+  size_t q = t0;
+  for (; q + st < nq; q += 2 * st) {  // two quads per thread in flight
+    double xa[4], xb[4];
+    ld4(x + 4 * q, xa);
+    ld4(x + 4 * (q + st), xb);
 #pragma unroll
-    for (int k = 0; k < kDotChunk; ++k)
-      if (k < mc) {
-        double vv[4];
-        ld4(V + (size_t)(k0 + k) * ldv + 4 * q, vv);
-        acc[k] = fma(vv[0], xv[0], fma(vv[1], xv[1], fma(vv[2], xv[2], fma(vv[3], xv[3], acc[k]))));
+    for (int k = 0; k < kCoreRows; ++k)
+      if (k < m) {
+        double va[4], vb[4];
+        ld4(V + (size_t)k * ldv + 4 * q, va);
+        ld4(V + (size_t)k * ldv + 4 * (q + st), vb);
+        acc[k] = fma(va[0], xa[0], fma(va[1], xa[1], fma(va[2], xa[2], fma(va[3], xa[3], acc[k]))));
+        acc[k] = fma(vb[0], xb[0], fma(vb[1], xb[1], fma(vb[2], xb[2], fma(vb[3], xb[3], acc[k]))));
       }
   }
-  for (size_t s = 4 * nq + t0; s < D; s += st) {
-    const double xv = (double)x[s];
+  if (q < nq) {
+    double xa[4];
+    ld4(x + 4 * q, xa);
 #pragma unroll
-    for (int k = 0; k < kDotChunk; ++k)
-      if (k < mc) acc[k] = fma((double)V[(size_t)(k0 + k) * ldv + s], xv, acc[k]);
+    for (int k = 0; k < kCoreRows; ++k)
+      if (k < m) {
+        double va[4];
+        ld4(V + (size_t)k * ldv + 4 * q, va);
+        acc[k] = fma(va[0], xa[0], fma(va[1], xa[1], fma(va[2], xa[2], fma(va[3], xa[3], acc[k]))));
+      }
   }
-  block_sums<kDotChunk>(acc, mc, sh, partial, (size_t)k0);
+  for (size_t e = 4 * nq + t0; e < D; e += st) {
+    const double xv = (double)x[e];
+#pragma unroll
+    for (int k = 0; k < kCoreRows; ++k)
+      if (k < m) acc[k] = fma((double)V[(size_t)k * ldv + e], xv, acc[k]);
+  }
+  block_sums<kCoreRows>(acc, m, sh, partial, 0);
 }
 
 // Projection on the FP64 tensor pipe: P[i][r] = <V_i, X_r> for i < m <= 64,
@@ -2332,38 +2344,6 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
     }
     ritz_kernel<<<1, 256, ritz_smem, c->stream>>>(k + nv, k, ld, dM, dS, dead, s + kbTheta, Xd, dst);
     SBDX_LAUNCHED(c);
-    if (p.verbose >= 2) {  // diagnostic (no capture at this level): the same problem on the host
-      const int n = k + nv;
-      std::vector<double> hM((size_t)ld * ld), hS((size_t)ld * ld), hX((size_t)n * k), dth(k), th, X;
-      SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
-      SBDX_CUDA(c, cudaMemcpy(hM.data(), dM, sizeof(double) * ld * ld, cudaMemcpyDeviceToHost));
-      SBDX_CUDA(c, cudaMemcpy(hS.data(), dS, sizeof(double) * ld * ld, cudaMemcpyDeviceToHost));
-      SBDX_CUDA(c, cudaMemcpy(hX.data(), Xd, sizeof(double) * n * k, cudaMemcpyDeviceToHost));
-      SBDX_CUDA(c, cudaMemcpy(dth.data(), s + kbTheta, sizeof(double) * k, cudaMemcpyDeviceToHost));
-      double asym = 0.0;
-      for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) {
-          asym = std::max(asym, std::fabs(hM[i + (size_t)ld * j] - hM[j + (size_t)ld * i]));
-          asym = std::max(asym, std::fabs(hS[i + (size_t)ld * j] - hS[j + (size_t)ld * i]));
-        }
-      std::vector<double> Sc((size_t)n * n), ws(n);
-      for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) Sc[i + (size_t)n * j] = hS[i + (size_t)ld * j];
-      jacobi_eigen(n, Sc.data(), n, ws.data());
-      const bool ok = gen_eigen_k(n, k, hM, hS, ld, th, X);
-      double dx = 0.0;
-      for (int r = 0; r < k && ok; ++r) {
-        double dp = 0.0, dm = 0.0;
-        for (int i = 0; i < n; ++i) {
-          dp = std::max(dp, std::fabs(hX[i + (size_t)n * r] - X[i + (size_t)n * r]));
-          dm = std::max(dm, std::fabs(hX[i + (size_t)n * r] + X[i + (size_t)n * r]));
-        }
-        dx = std::max(dx, std::min(dp, dm));
-      }
-      std::printf("     ritz n=%d device theta0=%.10f host=%.10f |dX|=%.2e min eig S=%.3e asym=%.1e\n", n, dth[0],
-                  ok ? th[0] : 0.0, dx, ws[0], asym);
-      std::fflush(stdout);
-    }
     unsigned ga = kRedBlocks;
     if ((r2 = launch_update_anchors<TC>(c, wk, k, W, HW, C, HC, nv, Xd, s + kbTheta, D, Wn, HWn, R, &ga))) return r2;
     finalize_kernel<<<1, kRedThreads, 0, c->stream>>>(wk.partial, (int)ga, k, s + kbNW2);
@@ -2387,7 +2367,7 @@ int davidson_block_graph(Ctx* c, const sbdx_davidson_params& p, int k, double* d
     unsigned long long kernels = 0;
   };
   std::map<long long, Cached> cache;
-  const bool capture_ok = c->stream != nullptr && p.verbose < 2;
+  const bool capture_ok = c->stream != nullptr;
   bool warm[2] = {false, false};
   auto launch = [&](int kind, int nv, int par, int slot, int mask) -> int {
     const long long key = (((long long)kind * 128 + nv) * 8 + par * 4 + slot) * 16 + mask;

@@ -6,8 +6,9 @@ chemistry/tpb/correlation.h:194-444).
 A solve run without a host vector leaves its result resident; the density,
 alpha weights, RDMs and adjoint computed from the device address must equal
 the same reductions of the host copy, and the vector must be the one the
-host path returns. Tolerances: 1e-13 (the same kernels on the same data;
-the RDM kernels add with atomics, so the order of the sums may differ)."""
+host path returns. Tolerances: 1e-13 (the same kernels on the same data in
+a fixed summation order, which agree bit for bit in practice; the tolerance
+is a margin)."""
 import numpy as np
 import pytest
 
