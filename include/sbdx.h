@@ -160,8 +160,17 @@ int sbdx_diag_terms_noalloc(int norb, double I0, const double* d_h, const double
                             double* d_hii, void* stream, char* errbuf, size_t errlen);
 
 /* One H*C product. Replaces mult (chemistry/tpb/mult.h:376-632). C and S are
- * host buffers of na*nb doubles (S is overwritten, not accumulated). */
+ * host buffers of na*nb doubles (S is overwritten, not accumulated). On large
+ * problems the copies run in chunks of alpha rows on a second stream,
+ * overlapped with the product's kernels (page-locked host buffers let them
+ * overlap; pageable ones give the same result, serialised). */
 int sbdx_sigma(sbdx_ctx* ctx, const double* C, double* S);
+/* Chunks of that pipeline: 0 = automatic (about 8 M determinants per chunk,
+ * at most 8; none below 16 M determinants), 1 = no pipeline (one copy in, the
+ * product, one copy out), K >= 2 = K chunks of equal alpha-row counts. The
+ * pipeline runs with the default alpha-first launch codes and no stored
+ * Hamiltonian; otherwise sbdx_sigma copies around one whole product. */
+int sbdx_set_io_chunks(sbdx_ctx* ctx, int chunks);
 /* Same on device buffers of na*nb elements of the given precision
  * (SBDX_FP64: double; SBDX_FP32: float storage with FP64 row accumulation),
  * on the context stream. */

@@ -404,10 +404,7 @@ int sbdx_sigma(sbdx_ctx* ctx, const double* C, double* S) {
     int rc = sbdx::ready(c, "sigma");
     if (rc) return rc;
     if ((rc = sbdx::ensure_io(c))) return rc;
-    const size_t D = c->na * c->nb;
-    SBDX_CUDA(c, cudaMemcpyAsync(c->d_io_in, C, sizeof(double) * D, cudaMemcpyHostToDevice, c->stream));
-    if ((rc = sbdx::sigma_device(c, SBDX_FP64, c->d_io_in, c->d_io_out))) return rc;
-    SBDX_CUDA(c, cudaMemcpyAsync(S, c->d_io_out, sizeof(double) * D, cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sbdx::sigma_host(c, C, S))) return rc;
     return sbdx::check_device_error(c);
   });
 }
@@ -419,6 +416,16 @@ int sbdx_sigma_device(sbdx_ctx* ctx, int precision, const void* dC, void* dS) {
     int rc = sbdx::ready(c, "sigma_device");
     if (rc) return rc;
     return sbdx::sigma_device(c, precision, dC, dS);
+  });
+}
+
+int sbdx_set_io_chunks(sbdx_ctx* ctx, int chunks) {
+  return sbdx::guarded(ctx, [&](Ctx* c) -> int {
+    if (chunks < 0) { c->err = "set_io_chunks: chunks must be >= 0"; return SBDX_ERR_ARG; }
+    cudaStreamSynchronize(c->stream);
+    sbdx::free_io_chunks(c);
+    c->io_chunks_req = chunks;
+    return SBDX_OK;
   });
 }
 

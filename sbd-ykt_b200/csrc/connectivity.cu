@@ -749,24 +749,28 @@ int build_one(Ctx* c, int spin) {
 
 }  // namespace
 
-void free_row_range(Ctx* c) {
-  Conn& r = c->range_conn;
+void free_range_items(Conn& r) {
   cudaFree(r.same_item); cudaFree(r.same_split); cudaFree(r.same_ypart);
   cudaFree(r.ab_item); cudaFree(r.ab_split); cudaFree(r.ypart);
   r.same_item = r.same_split = r.ab_item = r.ab_split = nullptr;
   r.same_ypart = r.ypart = nullptr;
   r.n_same_item = r.n_item = 0;
   r.n_same_split = r.n_same_part = r.n_split = r.n_part = 0;
+}
+
+void free_row_range(Ctx* c) {
+  free_range_items(c->range_conn);
   c->range_a0 = c->range_a1 = 0;
   c->have_range = false;
 }
 
 // Work items of the alpha rows [a0, a1) only, for a sigma that writes those
-// output rows (one shard of the alpha strings): the same-spin and alpha-beta
-// items of build_same_items / build_ab_items over that range, their caps
-// derived from the range's own work.
-int build_row_range(Ctx* c, size_t a0, size_t a1) {
-  free_row_range(c);
+// output rows (one shard of the alpha strings, or one chunk of a pipelined
+// product): the same-spin and alpha-beta items of build_same_items /
+// build_ab_items over that range, their caps derived from the range's own
+// work.
+int build_range_items(Ctx* c, size_t a0, size_t a1, Conn& r) {
+  free_range_items(r);
   const Conn& ca = c->conn[0];
   const size_t n = a1 - a0;
   std::vector<uint32_t> hs(n ? n : 1), hd(n ? n : 1);
@@ -777,10 +781,15 @@ int build_row_range(Ctx* c, size_t a0, size_t a1) {
   }
   hs.resize(n);
   hd.resize(n);
-  Conn& r = c->range_conn;
   int rc = build_same_items(c, r, hs, hd, c->nb, a0);
   if (rc) return rc;
-  if ((rc = build_ab_items(c, r, hs, c->nb, a0))) return rc;
+  return build_ab_items(c, r, hs, c->nb, a0);
+}
+
+int build_row_range(Ctx* c, size_t a0, size_t a1) {
+  free_row_range(c);
+  const int rc = build_range_items(c, a0, a1, c->range_conn);
+  if (rc) return rc;
   c->range_a0 = a0;
   c->range_a1 = a1;
   c->have_range = true;
@@ -791,6 +800,7 @@ void free_connectivity(Ctx* c) {
   clear_sigma_graphs(c);
   release_stored(c);  // its elements come from the connectivity
   free_row_range(c);
+  free_io_chunks(c);
   free_conn(c->conn[0]);
   free_conn(c->conn[1]);
   cudaFree(c->d_Da); cudaFree(c->d_Db); cudaFree(c->d_Da32); cudaFree(c->d_Db32);

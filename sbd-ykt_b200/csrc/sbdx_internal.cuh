@@ -220,6 +220,14 @@ struct Ctx {
   double* d_yt = nullptr;   // nb x xsb FP64: beta-major partial sigma
   size_t xsa = 0, xsb = 0;
   void* d_io_in = nullptr;  // D FP64 staging for host-buffer entry points
+  // the host-buffer sigma's pipeline: alpha-row chunks whose host<->device
+  // copies run on io_copy beside the chunks' kernels on the context stream
+  // (io_chunks_req: 0 automatic, 1 no pipeline, K >= 2 that many chunks)
+  int io_chunks_req = 0;
+  std::vector<size_t> io_bounds;  // chunk boundaries, multiples of 8
+  std::vector<Conn> io_items;     // work items of each chunk's output rows
+  cudaStream_t io_copy = nullptr;
+  std::vector<cudaEvent_t> io_events;  // per chunk: input copied, output ready; then one for the last copy
   void* d_io_out = nullptr;
   // the wavefunction of the last Davidson solve, resident on the device:
   // wf_roots vectors of D FP64 (root r at d_wf + r*D), kept until the next
@@ -356,6 +364,13 @@ void free_connectivity(Ctx* c);
 // Work items of the output rows [a0, a1) (Ctx::range_conn) and their release.
 int build_row_range(Ctx* c, size_t a0, size_t a1);
 void free_row_range(Ctx* c);
+// The work items of rows [a0, a1) into r, and their release.
+int build_range_items(Ctx* c, size_t a0, size_t a1, Conn& r);
+void free_range_items(Conn& r);
+// The host-buffer sigma's chunks (their work items, copy stream, events).
+void free_io_chunks(Ctx* c);
+// S = H C for host buffers (FP64), the copies overlapped with the kernels.
+int sigma_host(Ctx* c, const double* hC, double* hS);
 // Rows [a0, a1) of S = H X: X the whole vector (na x nb), S the (a1 - a0) x nb
 // output rows; a0 a multiple of 8 (or a0 == a1).
 int sigma_rows_device(Ctx* c, int precision, const void* X, void* S, size_t a0, size_t a1);

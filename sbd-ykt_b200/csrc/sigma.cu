@@ -2152,4 +2152,149 @@ int sigma_device(Ctx* c, int precision, const void* X, void* S) {
   return run_sigma_any(c, precision, X, S);
 }
 
+// ---- the host-buffer sigma, copies overlapped with the kernels ----------------
+//
+// S = H C from host C to host S in chunks of alpha rows, each one contiguous
+// block of both vectors (alpha-major layout). A copy stream brings chunk i in
+// while the context stream runs, for every chunk that has arrived, the phase
+// split of its rows and the beta same-spin product on its columns of the
+// transpose (which read that chunk only). Once every chunk is in, the context
+// stream runs per chunk the alpha same-spin and alpha-beta work items of its
+// rows (they read any ket row) and the combine of its rows, and the copy
+// stream takes each finished chunk out while the next one computes. Exposed:
+// the first chunk's copy in, the last chunk's beta same-spin product and the
+// last chunk's copy out.
+
+namespace {
+
+constexpr size_t kIoChunkDets = size_t(8) << 20;  // determinants per chunk in automatic mode
+constexpr int kIoMaxChunks = 8;
+
+int io_chunk_count(const Ctx* c) {
+  if (c->io_chunks_req == 1) return 1;
+  const size_t D = c->na * c->nb;
+  int k = c->io_chunks_req >= 2 ? c->io_chunks_req : (int)std::min<size_t>(kIoMaxChunks, D / kIoChunkDets);
+  k = std::min<int>(k, (int)(c->na / 8));  // at least 8 rows per chunk
+  return std::max(k, 1);
+}
+
+// chunk boundaries for K chunks: equal row counts, multiples of 8
+std::vector<size_t> io_bounds_for(const Ctx* c, int K) {
+  const size_t na = c->na;
+  std::vector<size_t> b{0};
+  for (int i = 1; i < K; ++i) {
+    const size_t x = na * (size_t)i / (size_t)K / 8 * 8;
+    if (x > b.back() && x < na) b.push_back(x);
+  }
+  b.push_back(na);
+  return b;
+}
+
+int build_io_chunks(Ctx* c, const std::vector<size_t>& bounds) {
+  free_io_chunks(c);
+  const size_t n = bounds.size() - 1;
+  c->io_items.resize(n);
+  for (size_t i = 0; i < n; ++i) {
+    const int rc = build_range_items(c, bounds[i], bounds[i + 1], c->io_items[i]);
+    if (rc) return rc;
+  }
+  SBDX_CUDA(c, cudaStreamCreateWithFlags(&c->io_copy, cudaStreamNonBlocking));
+  c->io_events.assign(2 * n + 2, nullptr);
+  for (auto& e : c->io_events) SBDX_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  c->io_bounds = bounds;  // last: a build that failed part way leaves no bounds, so the next call rebuilds
+  return 0;
+}
+
+}  // namespace
+
+void free_io_chunks(Ctx* c) {
+  for (auto& r : c->io_items) free_range_items(r);
+  c->io_items.clear();
+  c->io_bounds.clear();
+  for (auto e : c->io_events)
+    if (e) cudaEventDestroy(e);
+  c->io_events.clear();
+  if (c->io_copy) cudaStreamDestroy(c->io_copy);
+  c->io_copy = nullptr;
+}
+
+int sigma_host(Ctx* c, const double* hC, double* hS) {
+  const size_t na = c->na, nb = c->nb, D = na * nb;
+  int rc;
+  if (!c->have_conn && (rc = build_connectivity(c))) return rc;
+  if (!c->have_hii && (rc = diag_terms(c))) return rc;
+  if ((rc = ensure_sigma_scratch(c))) return rc;
+  double* din = static_cast<double*>(c->d_io_in);
+  double* dout = static_cast<double*>(c->d_io_out);
+  const Tune t = effective_tune(c, true);
+  const int K = io_chunk_count(c);
+  const bool pipe = K >= 2 && c->stored.val == nullptr && is_v6(t) && t.ab_code == 71 && ab7_fits(c) &&
+                    !c->profiling;
+  if (!pipe) {  // one copy in, the sigma, one copy out
+    SBDX_CUDA(c, cudaMemcpyAsync(din, hC, sizeof(double) * D, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = sigma_device(c, SBDX_FP64, din, dout))) return rc;
+    SBDX_CUDA(c, cudaMemcpyAsync(hS, dout, sizeof(double) * D, cudaMemcpyDeviceToHost, c->stream));
+    return 0;
+  }
+  const std::vector<size_t> want = io_bounds_for(c, K);
+  if (want != c->io_bounds) {
+    if ((rc = build_io_chunks(c, want))) return rc;
+  }
+  const size_t n = c->io_bounds.size() - 1;
+  const std::vector<size_t>& b = c->io_bounds;
+  cudaEvent_t* ev = c->io_events.data();  // [0, n): chunk in; [n, 2n): chunk out ready; 2n: start; 2n + 1: end
+  const Conn& ca = c->conn[0];
+  const Conn& cb = c->conn[1];
+  double* xp = static_cast<double*>(c->d_xp);
+  double* xpt = static_cast<double*>(c->d_xt);
+  // the copies in follow whatever the context stream was doing
+  SBDX_CUDA(c, cudaEventRecord(ev[2 * n], c->stream));
+  SBDX_CUDA(c, cudaStreamWaitEvent(c->io_copy, ev[2 * n], 0));
+  for (size_t i = 0; i < n; ++i) {
+    const size_t off = b[i] * nb, len = (b[i + 1] - b[i]) * nb;
+    SBDX_CUDA(c, cudaMemcpyAsync(din + off, hC + off, sizeof(double) * len, cudaMemcpyHostToDevice, c->io_copy));
+    SBDX_CUDA(c, cudaEventRecord(ev[i], c->io_copy));
+  }
+  for (size_t i = 0; i < n; ++i) {  // per arrived chunk: phase split, beta same-spin on its columns
+    const size_t a0 = b[i], nr = b[i + 1] - b[i];
+    SBDX_CUDA(c, cudaStreamWaitEvent(c->stream, ev[i], 0));
+    const dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((nr + 31) / 32));
+    phase_split_kernel<double><<<grid, dim3(32, 8), 0, c->stream>>>(din + a0 * nb, nr, nb, c->d_a + a0, c->d_b,
+                                                                     xp + a0 * c->xsa, xpt + a0, c->xsa, c->xsb);
+    SBDX_LAUNCHED(c);
+    if ((rc = run_same_v6<double>(c, t.same_code, xpt + a0, nb, nr, c->xsb, cb, cb.val, c->d_Da + a0, c->da_stride,
+                                  nullptr, c->d_yt + a0)))
+      return rc;
+  }
+  for (size_t i = 0; i < n; ++i) {  // per chunk: alpha same-spin and alpha-beta items of its rows, combine
+    const size_t a0 = b[i], nr = b[i + 1] - b[i];
+    const Conn& it = c->io_items[i];
+    Conn ra = ca;
+    ra.same_item = it.same_item;
+    ra.n_same_item = it.n_same_item;
+    ra.same_split = it.same_split;
+    ra.n_same_split = it.n_same_split;
+    ra.n_same_part = it.n_same_part;
+    ra.same_ypart = it.same_ypart;
+    if ((rc = run_same_v6<double>(c, t.same_code, xp, na, nb, c->xsa, ra, ca.val, c->d_Db, c->db_stride, c->d_hii,
+                                  c->d_y)))
+      return rc;
+    if ((rc = run_ab_v7<double>(c, xp, &it))) return rc;
+    const dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((nr + 31) / 32));
+    combine_phase_kernel<double><<<grid, dim3(32, 8), 0, c->stream>>>(c->d_y + a0 * c->xsa, c->d_yt + a0, nr, nb,
+                                                                       c->d_a + a0, c->d_b, dout + a0 * nb, c->xsa,
+                                                                       c->xsb);
+    SBDX_LAUNCHED(c);
+    SBDX_CUDA(c, cudaEventRecord(ev[n + i], c->stream));
+  }
+  for (size_t i = 0; i < n; ++i) {  // each chunk out as soon as it is ready
+    const size_t off = b[i] * nb, len = (b[i + 1] - b[i]) * nb;
+    SBDX_CUDA(c, cudaStreamWaitEvent(c->io_copy, ev[n + i], 0));
+    SBDX_CUDA(c, cudaMemcpyAsync(hS + off, dout + off, sizeof(double) * len, cudaMemcpyDeviceToHost, c->io_copy));
+  }
+  SBDX_CUDA(c, cudaEventRecord(ev[2 * n + 1], c->io_copy));
+  SBDX_CUDA(c, cudaStreamWaitEvent(c->stream, ev[2 * n + 1], 0));  // the call's work ends on the context stream
+  return 0;
+}
+
 }  // namespace sbdx

@@ -34,7 +34,7 @@ EXPORTS = [
     "sbdx_phase_times", "sbdx_set_tuning", "sbdx_autotune", "sbdx_davidson_roots",
     "sbdx_build_hamiltonian", "sbdx_release_hamiltonian", "sbdx_wavefunction_device", "sbdx_get_wavefunction",
     "sbdx_rdm_device", "sbdx_occupation_device", "sbdx_alpha_weights_device", "sbdx_energy_backward_device",
-    "sbdx_sigma_rows_device", "sbdx_set_graph_steps", "sbdx_project_device",
+    "sbdx_sigma_rows_device", "sbdx_set_graph_steps", "sbdx_project_device", "sbdx_set_io_chunks",
 ]
 PHASES = ["alpha_same_spin", "transpose", "beta_same_spin", "alpha_beta", "combine"]
 
@@ -204,6 +204,11 @@ class Context:
     def sigma_device(self, precision, c_ptr: int, s_ptr: int):
         self._check(self.lib.sbdx_sigma_device(self.h, ctypes.c_int(precision), ctypes.c_void_p(c_ptr),
                                                ctypes.c_void_p(s_ptr)))
+
+    def set_io_chunks(self, chunks: int = 0):
+        """sbdx_set_io_chunks: chunks of the host-buffer sigma's copy/compute
+        pipeline (0 automatic, 1 none, K >= 2 fixed)."""
+        self._check(self.lib.sbdx_set_io_chunks(self.h, ctypes.c_int(chunks)))
 
     def set_graph_steps(self, on: bool = True):
         """sbdx_set_graph_steps: several-root solves run one CUDA graph per iteration."""
