@@ -1103,7 +1103,8 @@ sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, size_t ldx, const uin
                      const uint32_t* __restrict__ nsing, const uint32_t* __restrict__ ket,
                      const typename Prec<T>::V* __restrict__ val, const uint32_t* __restrict__ info,
                      const typename Prec<T>::V* __restrict__ Dt, size_t dstride, const double* __restrict__ hii,
-                     const uint4* __restrict__ items, double* __restrict__ ypart, double* __restrict__ Y) {
+                     const uint4* __restrict__ items, double* __restrict__ ypart, double* __restrict__ Y,
+                     int accumulate) {
   __shared__ uint32_t s_ket[kSameThreads], s_pq[kSameThreads];
   __shared__ double s_val[kSameThreads];
   const uint4 item = items[blockIdx.x];  // bra string, entry range, output row
@@ -1155,8 +1156,13 @@ sigma_same_v6_kernel(const T* __restrict__ X, size_t ncol, size_t ldx, const uin
     }
   }
   if (active) {
+    if (accumulate && item.w == 0) {  // add to the row (a partial row of a split string is always written)
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) Yrow[c0 + v] = acc[v];
+      for (int v = 0; v < VEC; ++v) Yrow[c0 + v] += acc[v];
+    } else {
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) Yrow[c0 + v] = acc[v];
+    }
   }
 }
 
@@ -1195,7 +1201,7 @@ sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, size_t ldx, cons
                       const uint32_t* __restrict__ nsing, const uint32_t* __restrict__ ket,
                       const float* __restrict__ val, const uint32_t* __restrict__ info, const float* __restrict__ Dt,
                       size_t dstride, const double* __restrict__ hii, const uint4* __restrict__ items,
-                      double* __restrict__ ypart, double* __restrict__ Y) {
+                      double* __restrict__ ypart, double* __restrict__ Y, int accumulate) {
   __shared__ uint32_t s_ket[kSameThreads], s_pq[kSameThreads];
   __shared__ float s_val[kSameThreads];
   const uint4 item = items[blockIdx.x];  // bra string, entry range, output row
@@ -1263,8 +1269,13 @@ sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, size_t ldx, cons
     }
   }
   if (active) {
+    if (accumulate && item.w == 0) {
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) Yrow[c0 + v] = acc[v];
+      for (int v = 0; v < VEC; ++v) Yrow[c0 + v] += acc[v];
+    } else {
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) Yrow[c0 + v] = acc[v];
+    }
   }
 }
 
@@ -1599,23 +1610,24 @@ int run_ab_v7(Ctx* c, const T* Xp, const Conn* items = nullptr) {
   return 0;
 }
 
-// Assigns the sum of the partial rows of the bra strings split over several
-// same-spin work items, parts in slot order.
+// Assigns (or, with accumulate, adds) the sum of the partial rows of the bra
+// strings split over several same-spin work items, parts in slot order.
 __global__ void same_split_fixup_kernel(const uint4* __restrict__ split, const double* __restrict__ ypart,
-                                        size_t ncol, size_t ldx, double* __restrict__ Y) {
+                                        size_t ncol, size_t ldx, double* __restrict__ Y, int accumulate) {
   const uint4 sp = split[blockIdx.y];
   const double* part = ypart + (size_t)sp.y * ldx;
   for (size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x; col < ncol; col += (size_t)gridDim.x * blockDim.x) {
     double t = 0.0;
     for (uint32_t q = 0; q < sp.z; ++q) t += part[(size_t)q * ldx + col];
-    Y[(size_t)sp.x * ldx + col] = t;
+    double* y = Y + (size_t)sp.x * ldx + col;
+    *y = accumulate ? *y + t : t;
   }
 }
 
 template <typename T, int VEC>
 int launch_same_v6(Ctx* c, const T* X, size_t nrow, size_t ncol, size_t ldx, const Conn& cn,
                    const typename Prec<T>::V* val, const typename Prec<T>::V* Dt, size_t dstride, const double* hii,
-                   double* Y) {
+                   double* Y, int accumulate) {
   (void)nrow;
   if (cn.n_same_item > 0) {
     dim3 grid((unsigned)cn.n_same_item,
@@ -1623,18 +1635,18 @@ int launch_same_v6(Ctx* c, const T* X, size_t nrow, size_t ncol, size_t ldx, con
     if constexpr (std::is_same<T, float>::value) {
       sigma_same_v6f_kernel<VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, ldx, cn.off, cn.nsing, cn.ket, val,
                                                                         cn.info, Dt, dstride, hii, cn.same_item,
-                                                                        cn.same_ypart, Y);
+                                                                        cn.same_ypart, Y, accumulate);
     } else {
       sigma_same_v6_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(X, ncol, ldx, cn.off, cn.nsing, cn.ket, val,
                                                                          cn.info, Dt, dstride, hii, cn.same_item,
-                                                                         cn.same_ypart, Y);
+                                                                         cn.same_ypart, Y, accumulate);
     }
     SBDX_LAUNCHED(c);
   }
   if (cn.n_same_split > 0) {
     const unsigned bx = (unsigned)std::min<size_t>((ncol + 255) / 256, 64);
-    same_split_fixup_kernel<<<dim3(bx, (unsigned)cn.n_same_split), 256, 0, c->stream>>>(cn.same_split,
-                                                                                         cn.same_ypart, ncol, ldx, Y);
+    same_split_fixup_kernel<<<dim3(bx, (unsigned)cn.n_same_split), 256, 0, c->stream>>>(
+        cn.same_split, cn.same_ypart, ncol, ldx, Y, accumulate);
     SBDX_LAUNCHED(c);
   }
   return 0;
@@ -1644,17 +1656,19 @@ int launch_same_v6(Ctx* c, const T* X, size_t nrow, size_t ncol, size_t ldx, con
 // to the widest vector that divides the row stride and keeps 16-byte
 // alignment (the internal vectors have strides padded to 8 elements, so only
 // a misaligned base narrows).
+// accumulate: add to Y's rows instead of writing them (the pipelined
+// host-buffer sigma runs the alpha-beta kernel first).
 template <typename T>
 int run_same_v6(Ctx* c, int code, const T* X, size_t nrow, size_t ncol, size_t ldx, const Conn& cn,
                 const typename Prec<T>::V* val, const typename Prec<T>::V* Dt, size_t dstride, const double* hii,
-                double* Y) {
+                double* Y, int accumulate = 0) {
   int vec = code % 10;
   const bool aligned = (reinterpret_cast<uintptr_t>(X) % 16) == 0;
   while (vec > 1 && (!aligned || ldx % vec != 0 || dstride % vec != 0)) vec >>= 1;
-  if (vec >= 8) return launch_same_v6<T, 8>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y);
-  if (vec >= 4) return launch_same_v6<T, 4>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y);
-  if (vec == 2) return launch_same_v6<T, 2>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y);
-  return launch_same_v6<T, 1>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y);
+  if (vec >= 8) return launch_same_v6<T, 8>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y, accumulate);
+  if (vec >= 4) return launch_same_v6<T, 4>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y, accumulate);
+  if (vec == 2) return launch_same_v6<T, 2>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y, accumulate);
+  return launch_same_v6<T, 1>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y, accumulate);
 }
 
 template <typename T, int R, int KS>
@@ -2159,11 +2173,12 @@ int sigma_device(Ctx* c, int precision, const void* X, void* S) {
 // while the context stream runs, for every chunk that has arrived, the phase
 // split of its rows and the beta same-spin product on its columns of the
 // transpose (which read that chunk only). Once every chunk is in, the context
-// stream runs per chunk the alpha same-spin and alpha-beta work items of its
-// rows (they read any ket row) and the combine of its rows, and the copy
-// stream takes each finished chunk out while the next one computes. Exposed:
-// the first chunk's copy in, the last chunk's beta same-spin product and the
-// last chunk's copy out.
+// stream runs the alpha-beta product of all rows (it reads any ket row), then
+// per chunk the alpha same-spin work items of its rows, added to the
+// alpha-beta result, and the combine of its rows; the copy stream takes each
+// finished chunk out while the next one computes. Exposed: the first chunk's
+// copy in, the last chunk's beta same-spin product and the last chunk's copy
+// out.
 
 namespace {
 
@@ -2266,7 +2281,12 @@ int sigma_host(Ctx* c, const double* hC, double* hS) {
                                   nullptr, c->d_yt + a0)))
       return rc;
   }
-  for (size_t i = 0; i < n; ++i) {  // per chunk: alpha same-spin and alpha-beta items of its rows, combine
+  // the alpha-beta product of all rows in one launch (its work items keep
+  // the whole grid busy, longest first) into a zeroed Y, then per chunk the
+  // alpha same-spin items of its rows added to Y, and the combine
+  SBDX_CUDA(c, cudaMemsetAsync(c->d_y, 0, sizeof(double) * na * c->xsa, c->stream));
+  if ((rc = run_ab_v7<double>(c, xp))) return rc;
+  for (size_t i = 0; i < n; ++i) {
     const size_t a0 = b[i], nr = b[i + 1] - b[i];
     const Conn& it = c->io_items[i];
     Conn ra = ca;
@@ -2277,9 +2297,8 @@ int sigma_host(Ctx* c, const double* hC, double* hS) {
     ra.n_same_part = it.n_same_part;
     ra.same_ypart = it.same_ypart;
     if ((rc = run_same_v6<double>(c, t.same_code, xp, na, nb, c->xsa, ra, ca.val, c->d_Db, c->db_stride, c->d_hii,
-                                  c->d_y)))
+                                  c->d_y, 1)))
       return rc;
-    if ((rc = run_ab_v7<double>(c, xp, &it))) return rc;
     const dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((nr + 31) / 32));
     combine_phase_kernel<double><<<grid, dim3(32, 8), 0, c->stream>>>(c->d_y + a0 * c->xsa, c->d_yt + a0, nr, nb,
                                                                        c->d_a + a0, c->d_b, dout + a0 * nb, c->xsa,

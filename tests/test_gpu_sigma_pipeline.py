@@ -1,9 +1,9 @@
 """The host-buffer product (sbdx_sigma, the drop-in for mult,
 chemistry/tpb/mult.h:376-632) with its copies overlapped with the kernels:
 chunks of alpha rows copied in on a second stream, the phase split and the
-beta same-spin product per arrived chunk, then per chunk the alpha
-same-spin and alpha-beta work items of its rows, the combine and the copy
-out.
+beta same-spin product per arrived chunk, the alpha-beta product of all
+rows, then per chunk the alpha same-spin work items of its rows (added to
+the alpha-beta result), the combine and the copy out.
 
 Every chunking must give the oracle's sigma within 1e-12 relative to
 max |value| (the FP64 sigma tolerance) and the device-buffer product within
