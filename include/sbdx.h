@@ -95,7 +95,8 @@ int sbdx_set_integrals(sbdx_ctx* ctx, int norb, double I0, const double* h, cons
  * chemistry/tpb/sbdiag.h:116-117). Strings must be unique; sorted ascending for
  * index 0 to be the Aufbau start vector, as LoadAlphaDets leaves them
  * (chemistry/basic/makedeterminants.h:184). All alpha strings must have the
- * same popcount, and all beta strings likewise. */
+ * same popcount, and all beta strings likewise. At most 16,777,215 strings
+ * per spin (the excitation records hold 24-bit string indices). */
 int sbdx_set_strings(sbdx_ctx* ctx, const uint64_t* alpha, size_t na, const uint64_t* beta, size_t nb);
 
 /* Excitation connectivity. Replaces MakeHelpers/RemakeHelpers + GenerateExcitation

@@ -301,7 +301,10 @@ int sbdx_set_integrals(sbdx_ctx* ctx, int norb, double I0, const double* h, cons
 int sbdx_set_strings(sbdx_ctx* ctx, const uint64_t* alpha, size_t na, const uint64_t* beta, size_t nb) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {
     if (!alpha || !beta || na == 0 || nb == 0) { c->err = "set_strings: empty string set"; return SBDX_ERR_ARG; }
-    if (na > 65535 || nb > 65535) { c->err = "set_strings: at most 65535 strings per spin"; return SBDX_ERR_ARG; }
+    if (na > sbdx::kMaxStrings || nb > sbdx::kMaxStrings) {
+      c->err = "set_strings: at most 16777215 strings per spin";
+      return SBDX_ERR_ARG;
+    }
     const int pa = __builtin_popcountll(alpha[0]), pb = __builtin_popcountll(beta[0]);
     for (size_t k = 0; k < na; ++k)
       if (__builtin_popcountll(alpha[k]) != pa) { c->err = "set_strings: alpha strings differ in electron count"; return SBDX_ERR_ARG; }

@@ -174,7 +174,7 @@ conn_fill_kernel(int spin, const uint64_t* __restrict__ s, size_t n, const uint6
       if (is_s) {
         const uint32_t i = inf & 63u, a = (inf >> 6) & 63u;
         const uint64_t lo = i < a ? i : a, hi = i < a ? a : i;
-        srec[pos] = (uint64_t)k | ((uint64_t)((inf >> 12) & 0xfffu) << 16) | (lo << 28) | (hi << 34) |
+        srec[pos] = rec_ket_bits(k) | ((uint64_t)((inf >> 12) & 0xfffu) << 16) | (lo << 28) | (hi << 34) |
                     ((uint64_t)(inf >> 31) << 40);
       }
     }
@@ -191,7 +191,7 @@ void free_conn(Conn& c) {
   cudaFree(c.sell); cudaFree(c.soff); cudaFree(c.slen); cudaFree(c.kpos);
   auto free_panel = [](SellPanel& p) {
     cudaFree(p.sell); cudaFree(p.sell32); cudaFree(p.soff4); cudaFree(p.slen4);
-    cudaFree(p.soff); cudaFree(p.slen); cudaFree(p.vrow);
+    cudaFree(p.soff); cudaFree(p.slen); cudaFree(p.vrow); cudaFree(p.vslot);
     cudaFree(p.split_row); cudaFree(p.split_slot);
   };
   free_panel(c.bal);
@@ -313,18 +313,18 @@ std::vector<uint32_t> ket_positions(size_t n, const std::vector<uint32_t>& hs, c
   // bra strings whose singles include ket k (CSR)
   std::vector<uint64_t> roff(n + 1, 0);
   for (size_t r = 0; r < n; ++r)
-    for (uint32_t e = 0; e < hs[r]; ++e) ++roff[(rec[off[r] + e] & 0xffffu) + 1];
+    for (uint32_t e = 0; e < hs[r]; ++e) ++roff[rec_ket(rec[off[r] + e]) + 1];
   for (size_t k = 0; k < n; ++k) roff[k + 1] += roff[k];
   std::vector<uint32_t> rows(roff[n]);
   {
     std::vector<uint64_t> fill(roff.begin(), roff.end() - 1);
     for (size_t r = 0; r < n; ++r)
-      for (uint32_t e = 0; e < hs[r]; ++e) rows[fill[rec[off[r] + e] & 0xffffu]++] = (uint32_t)r;
+      for (uint32_t e = 0; e < hs[r]; ++e) rows[fill[rec_ket(rec[off[r] + e])]++] = (uint32_t)r;
   }
   std::vector<std::array<int16_t, 8>> h(n);
   for (size_t r = 0; r < n; ++r) {
     h[r].fill(0);
-    for (uint32_t e = 0; e < hs[r]; ++e) ++h[r][pos[rec[off[r] + e] & 0xffffu] & 7u];
+    for (uint32_t e = 0; e < hs[r]; ++e) ++h[r][pos[rec_ket(rec[off[r] + e])] & 7u];
   }
   for (int sweep = 0; sweep < 8; ++sweep) {
     long long gain = 0;
@@ -376,8 +376,8 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
   for (size_t r = 0; r < n; ++r) {
     const uint64_t* b = rec.data() + off_all[r];
     const uint64_t* e = b + hs_all[r];
-    const uint64_t* lo = std::lower_bound(b, e, jb0, [](uint64_t x, uint32_t v) { return (x & 0xffffu) < v; });
-    const uint64_t* hi = std::lower_bound(lo, e, jb1, [](uint64_t x, uint32_t v) { return (x & 0xffffu) < v; });
+    const uint64_t* lo = std::lower_bound(b, e, jb0, [](uint64_t x, uint32_t v) { return rec_ket(x) < v; });
+    const uint64_t* hi = std::lower_bound(lo, e, jb1, [](uint64_t x, uint32_t v) { return rec_ket(x) < v; });
     off[r] = (uint64_t)(lo - rec.data());
     hs[r] = (uint32_t)(hi - lo);
   }
@@ -443,10 +443,13 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
   }
   // padding records contribute nothing (bit 41) and point at the panel's first
   // ket index, so the kernels' shared-memory index stays in range
-  const uint64_t kPad = (1ull << 41) | (uint64_t)jb0;
+  const uint64_t kPad = (1ull << 41) | rec_ket_bits(jb0);
   std::vector<uint64_t> sell(soff[ns] ? soff[ns] : 1, kPad);
-  std::vector<uint32_t> vrow(nv ? nv : 1, 0);
-  for (size_t v = 0; v < nv; ++v) vrow[v] = vr[v].r | (vr[v].slot1 << 16);
+  std::vector<uint32_t> vrow(nv ? nv : 1, 0), vslot(nv ? nv : 1, 0);
+  for (size_t v = 0; v < nv; ++v) {
+    vrow[v] = vr[v].r;
+    vslot[v] = vr[v].slot1;
+  }
   // 32-bit records of the packed kernel in blocks of 4 per lane (see
   // SellPanel::sell32); the steps that round a slice up to a multiple of 4
   // are padding at the panel's first staged position
@@ -456,7 +459,7 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
     slen4[sl] = (slen[sl] + 3u) & ~3u;
     soff4[sl + 1] = soff4[sl] + 32ull * slen4[sl];
   }
-  const uint32_t kPad32 = (1u << 29) | jb0;
+  const uint32_t kPad32 = 1u << 29;  // position 0 of the panel
   std::vector<uint32_t> sell32(soff4[ns] ? soff4[ns] : 4, kPad32);
   // Record order inside each virtual row is free (it only changes the order
   // of the sum) and decides the bank conflicts of the packed kernel's two
@@ -477,7 +480,7 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
   // addresses of a real record of their step (a broadcast costs nothing).
   // Slices are ordered on several host threads, each slice with its own
   // seeded generator, so the result does not depend on the thread count.
-  auto kslot = [&](uint64_t r) { return (uint32_t)(kpos[r & 0xffffu] & 7u); };
+  auto kslot = [&](uint64_t r) { return (uint32_t)(kpos[rec_ket(r)] & 7u); };
   auto pcls = [](uint64_t r) { return (uint32_t)((r >> 16) & 3u); };
   auto order_slice = [&](size_t sl) {
     const size_t l_end = std::min<size_t>(32, nv - sl * 32);
@@ -591,7 +594,7 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
             seen[nseen] = pq;
             seen_copy[nseen++] = copy;
           }
-          const uint32_t w32 = (kpos[r & 0xffffu] & 0xffffu) | (pq << 16) | ((uint32_t)((r >> 40) & 1u) << 28) |
+          const uint32_t w32 = ((kpos[rec_ket(r)] - jb0) & 0xffffu) | (pq << 16) | ((uint32_t)((r >> 40) & 1u) << 28) |
                                (copy << 30);
           sell32[soff4[sl] + 128ull * (m >> 2) + 4 * lane + (m & 3u)] = w32;
           if (!have_src) { src32 = w32 | (1u << 29); have_src = true; }
@@ -632,12 +635,15 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
   SBDX_CUDA(c, cudaMalloc(&P.soff, sizeof(uint64_t) * (ns + 1)));
   SBDX_CUDA(c, cudaMalloc(&P.slen, sizeof(uint32_t) * slen.size()));
   SBDX_CUDA(c, cudaMalloc(&P.vrow, sizeof(uint32_t) * vrow.size()));
+  SBDX_CUDA(c, cudaMalloc(&P.vslot, sizeof(uint32_t) * vslot.size()));
   SBDX_CUDA(c, cudaMalloc(&P.split_row, sizeof(uint32_t) * split_row.size()));
   SBDX_CUDA(c, cudaMalloc(&P.split_slot, sizeof(uint32_t) * split_slot.size()));
   SBDX_CUDA(c, cudaMemcpyAsync(P.sell, sell.data(), sizeof(uint64_t) * sell.size(), cudaMemcpyHostToDevice, c->stream));
   SBDX_CUDA(c, cudaMemcpyAsync(P.soff, soff.data(), sizeof(uint64_t) * (ns + 1), cudaMemcpyHostToDevice, c->stream));
   SBDX_CUDA(c, cudaMemcpyAsync(P.slen, slen.data(), sizeof(uint32_t) * slen.size(), cudaMemcpyHostToDevice, c->stream));
   SBDX_CUDA(c, cudaMemcpyAsync(P.vrow, vrow.data(), sizeof(uint32_t) * vrow.size(), cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(P.vslot, vslot.data(), sizeof(uint32_t) * vslot.size(), cudaMemcpyHostToDevice,
+                               c->stream));
   SBDX_CUDA(c, cudaMemcpyAsync(P.split_row, split_row.data(), sizeof(uint32_t) * split_row.size(),
                                cudaMemcpyHostToDevice, c->stream));
   SBDX_CUDA(c, cudaMemcpyAsync(P.split_slot, split_slot.data(), sizeof(uint32_t) * split_slot.size(),

@@ -9,6 +9,8 @@
 // kernel then needs n_alpha table reads per element and is HBM-write bound
 // (8 bytes per determinant).
 #include "sbdx_internal.cuh"
+
+#include <algorithm>
 #include "sbdx.h"
 
 #include <cstring>
@@ -60,18 +62,19 @@ __global__ void coulomb_row_kernel(const uint64_t* __restrict__ s, size_t n, int
 __global__ void diag_kernel(const uint64_t* __restrict__ a, size_t na, size_t nb, int L, double I0,
                             const double* __restrict__ Ea, const double* __restrict__ Eb,
                             const double* __restrict__ Jb, double* __restrict__ hii) {
-  const size_t ia = blockIdx.y;
   const size_t ib = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ib >= nb) return;
   const double* jrow = Jb + ib * (size_t)L;
-  double v = 0.0;
-  uint64_t bp = a[ia];
-  while (bp) {
-    const int p = __ffsll((long long)bp) - 1;
-    bp &= bp - 1;
-    v += jrow[p];
+  for (size_t ia = blockIdx.y; ia < na; ia += gridDim.y) {  // grid rows stride over the alpha strings
+    double v = 0.0;
+    uint64_t bp = a[ia];
+    while (bp) {
+      const int p = __ffsll((long long)bp) - 1;
+      bp &= bp - 1;
+      v += jrow[p];
+    }
+    hii[ia * nb + ib] = I0 + Ea[ia] + Eb[ib] + v;
   }
-  hii[ia * nb + ib] = I0 + Ea[ia] + Eb[ib] + v;
 }
 
 }  // namespace
@@ -94,7 +97,7 @@ int diag_terms(Ctx* c) {
   const size_t nj = nb * (size_t)c->L;
   coulomb_row_kernel<<<(unsigned)((nj + 255) / 256), 256, 0, c->stream>>>(c->d_b, nb, c->L, c->d_eri, Jb);
   SBDX_LAUNCHED(c);
-  dim3 grid((unsigned)((nb + 255) / 256), (unsigned)na);
+  dim3 grid((unsigned)((nb + 255) / 256), (unsigned)std::min<size_t>(na, 65535));  // grid y is at most 65535
   diag_kernel<<<grid, 256, 0, c->stream>>>(c->d_a, na, nb, c->L, c->I0, Ea, Eb, Jb, c->d_hii);
   SBDX_LAUNCHED(c);
   SBDX_CUDA(c, cudaFreeAsync(Ea, c->stream));

@@ -285,10 +285,10 @@ rdm_ab_kernel(const double* __restrict__ W, size_t nb, const uint64_t* __restric
               const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
               const uint32_t* __restrict__ a_info, const uint64_t* __restrict__ b_off,
               const uint32_t* __restrict__ b_nsing, const uint32_t* __restrict__ b_ket,
-              const uint32_t* __restrict__ b_info, int L, double* __restrict__ two) {
+              const uint32_t* __restrict__ b_info, int L, double* __restrict__ two, int staged) {
   extern __shared__ __align__(16) unsigned char smem[];
   double* acc = reinterpret_cast<double*>(smem);  // [L*L] by (i_b, a_b)
-  double* ws = acc + (size_t)L * L;               // [nb]
+  double* ws = acc + (size_t)L * L;               // [nb] when staged
   const size_t ia = blockIdx.x;
   const uint64_t alpha_bra = astr[ia];
   const double* wbra = W + ia * nb;
@@ -302,7 +302,11 @@ rdm_ab_kernel(const double* __restrict__ W, size_t nb, const uint64_t* __restric
     const int ia_p = (int)((inf >> 6) & 63u);   // alpha bra-only orbital a_a
     __syncthreads();
     for (int t = threadIdx.x; t < L * L; t += blockDim.x) acc[t] = 0.0;
-    for (size_t t = threadIdx.x; t < nb; t += blockDim.x) ws[t] = W[ja * nb + t];
+    // the ket row W[ja, :] in shared memory, or read from global memory
+    // (L2) when a beta row does not fit
+    const double* wket = staged ? ws : W + ja * nb;
+    if (staged)
+      for (size_t t = threadIdx.x; t < nb; t += blockDim.x) ws[t] = W[ja * nb + t];
     __syncthreads();
     for (size_t ib = threadIdx.x; ib < nb; ib += blockDim.x) {
       const double wi = wbra[ib];
@@ -310,7 +314,7 @@ rdm_ab_kernel(const double* __restrict__ W, size_t nb, const uint64_t* __restric
       const uint64_t beta_bra = bstr[ib];
       const uint64_t m0 = b_off[ib], m1 = m0 + b_nsing[ib];
       for (uint64_t m = m0; m < m1; ++m) {
-        const double wj = ws[b_ket[m]];
+        const double wj = wket[b_ket[m]];
         if (wj == 0.0) continue;
         const uint32_t i2 = b_info[m];
         const int ib_h = (int)(i2 & 63u), ib_p = (int)((i2 >> 6) & 63u);
@@ -376,8 +380,8 @@ __device__ __forceinline__ void pair_parity_masks(int s1, int e1, int s2, int e2
 __global__ void __launch_bounds__(kAbDetThreads)
 rdm_ab_det_kernel(const double* __restrict__ W, size_t nb, const uint64_t* __restrict__ astr,
                   const uint64_t* __restrict__ bstr, const uint4* __restrict__ chunks,
-                  const uint32_t* __restrict__ arec, const uint32_t* __restrict__ bpat_off,
-                  const uint32_t* __restrict__ bpat_key, const uint32_t* __restrict__ brec, int npb,
+                  const uint64_t* __restrict__ arec, const uint32_t* __restrict__ bpat_off,
+                  const uint32_t* __restrict__ bpat_key, const uint64_t* __restrict__ brec, int npb,
                   double* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char smem[];
   double* wi = reinterpret_cast<double*>(smem);  // [nb] row ia
@@ -389,8 +393,8 @@ rdm_ab_det_kernel(const double* __restrict__ W, size_t nb, const uint64_t* __res
   constexpr int kWarps = kAbDetThreads / 32;
   for (int p = threadIdx.x; p < npb; p += kAbDetThreads) acc[p] = 0.0;
   for (uint32_t q = 0; q < ch.z; ++q) {
-    const uint32_t ar = arec[ch.y + q];
-    const size_t ia = ar & 0xffffu, ja = ar >> 16;
+    const uint64_t ar = arec[ch.y + q];
+    const size_t ia = (uint32_t)ar, ja = ar >> 32;
     __syncthreads();
     for (size_t t = threadIdx.x; t < nb; t += kAbDetThreads) {
       wi[t] = W[ia * nb + t];
@@ -409,8 +413,8 @@ rdm_ab_det_kernel(const double* __restrict__ W, size_t nb, const uint64_t* __res
       const uint32_t pa = (uint32_t)popc64(alpha_bra & ma) & 1u;
       double s = 0.0;
       for (uint32_t m = bpat_off[p] + lane; m < bpat_off[p + 1]; m += 32) {
-        const uint32_t br = brec[m];
-        const uint32_t ib = br & 0xffffu, jb = br >> 16;
+        const uint64_t br = brec[m];
+        const uint32_t ib = (uint32_t)br, jb = (uint32_t)(br >> 32);
         const double v = wi[ib] * wj[jb];
         const uint32_t par = (pa + (uint32_t)popc64(bstr[ib] & mb)) & 1u;
         s += par ? -v : v;
@@ -597,9 +601,9 @@ static int weights(Ctx* c, const double* dW, double* wa, double* wb, double* Pa,
 
 // The single excitations of one spin grouped by pattern key = hole << 6 |
 // particle (hole: the ket's orbital, particle: the bra's), each group in
-// ascending bra then ket order: keys, group offsets and records bra | ket << 16.
+// ascending bra then ket order: keys, group offsets and records bra | ket << 32.
 static int singles_by_pattern(Ctx* c, int spin, std::vector<uint32_t>& keys, std::vector<uint32_t>& goff,
-                              std::vector<uint32_t>& recs) {
+                              std::vector<uint64_t>& recs) {
   const Conn& cn = c->conn[spin];
   const size_t n = cn.n;
   std::vector<uint64_t> off(n + 1);
@@ -631,7 +635,7 @@ static int singles_by_pattern(Ctx* c, int spin, std::vector<uint32_t>& keys, std
   for (size_t r = 0; r < n; ++r)
     for (uint32_t e = 0; e < ns[r]; ++e) {
       const uint32_t k = info[off[r] + e] & 0xfffu;
-      recs[fill[k]++] = (uint32_t)r | (ket[off[r] + e] << 16);
+      recs[fill[k]++] = (uint64_t)r | ((uint64_t)ket[off[r] + e] << 32);
     }
   (void)where;
   return 0;
@@ -764,7 +768,8 @@ static int rdm_same_deterministic(Ctx* c, int spin, const double* Wm, double* on
 static int rdm_ab_deterministic(Ctx* c, const double* dW, double* two, bool& done) {
   done = false;
   const size_t nb = c->nb;
-  std::vector<uint32_t> akeys, agoff, arecs, bkeys, bgoff, brecs;
+  std::vector<uint32_t> akeys, agoff, bkeys, bgoff;
+  std::vector<uint64_t> arecs, brecs;
   int rc;
   if ((rc = singles_by_pattern(c, 0, akeys, agoff, arecs))) return rc;
   if ((rc = singles_by_pattern(c, 1, bkeys, bgoff, brecs))) return rc;
@@ -792,14 +797,15 @@ static int rdm_ab_deterministic(Ctx* c, const double* dW, double* two, bool& don
     return e;
   };
   uint4 *d_chunks = nullptr, *d_apat = nullptr;
-  uint32_t *d_arec = nullptr, *d_boff = nullptr, *d_bkey = nullptr, *d_brec = nullptr;
+  uint64_t *d_arec = nullptr, *d_brec = nullptr;
+  uint32_t *d_boff = nullptr, *d_bkey = nullptr;
   double* d_part = nullptr;
   SBDX_CUDA(c, up(chunks.data(), sizeof(uint4) * chunks.size(), (void**)&d_chunks));
   SBDX_CUDA(c, up(apat.data(), sizeof(uint4) * apat.size(), (void**)&d_apat));
-  SBDX_CUDA(c, up(arecs.data(), sizeof(uint32_t) * arecs.size(), (void**)&d_arec));
+  SBDX_CUDA(c, up(arecs.data(), sizeof(uint64_t) * arecs.size(), (void**)&d_arec));
   SBDX_CUDA(c, up(bgoff.data(), sizeof(uint32_t) * bgoff.size(), (void**)&d_boff));
   SBDX_CUDA(c, up(bkeys.data(), sizeof(uint32_t) * bkeys.size(), (void**)&d_bkey));
-  SBDX_CUDA(c, up(brecs.data(), sizeof(uint32_t) * brecs.size(), (void**)&d_brec));
+  SBDX_CUDA(c, up(brecs.data(), sizeof(uint64_t) * brecs.size(), (void**)&d_brec));
   SBDX_CUDA(c, up(nullptr, sizeof(double) * chunks.size() * (size_t)npb, (void**)&d_part));
   SBDX_CUDA(c, cudaFuncSetAttribute(rdm_ab_det_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAbSmemBudget));
   rdm_ab_det_kernel<<<(unsigned)chunks.size(), kAbDetThreads, smem, c->stream>>>(
@@ -851,13 +857,14 @@ int rdm_device(Ctx* c, const double* dW, double* d_one, double* d_two) {
   bool done = d_two == nullptr;  // the alpha-beta pairs only add to the 2-RDM
   if (!done && (rc = rdm_ab_deterministic(c, dW, two, done))) return rc;
   if (!done) {
-    const size_t smem = sizeof(double) * (L2 + nb);
-    if (smem > 220 * 1024) { c->err = "rdm: beta dimension too large for the shared-memory row"; return 1; }
+    const int staged = sizeof(double) * (L2 + nb) <= kAbSmemBudget;
+    const size_t smem = sizeof(double) * (L2 + (staged ? nb : 0));
+    if (smem > kAbSmemBudget) { c->err = "rdm: too many orbitals for the shared-memory accumulator"; return 1; }
     SBDX_CUDA(c, cudaFuncSetAttribute(rdm_ab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAbSmemBudget));
     const Conn& ca = c->conn[0];
     const Conn& cb = c->conn[1];
     rdm_ab_kernel<<<(unsigned)na, 512, smem, c->stream>>>(dW, nb, c->d_a, c->d_b, ca.off, ca.nsing, ca.ket, ca.info,
-                                                           cb.off, cb.nsing, cb.ket, cb.info, c->L, two);
+                                                           cb.off, cb.nsing, cb.ket, cb.info, c->L, two, staged);
     SBDX_LAUNCHED(c);
   }
   SBDX_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -37,8 +37,8 @@ constexpr uint32_t kInfoSingle = 1u << 30;
 // Balanced SELL-32 of the single-excitation records whose ket index lies in
 // [jb0, jb1). A bra string with more than `cap` such singles is split into
 // equal parts ("virtual rows") of at most `cap` records; the split parts come
-// first, then the unsplit rows longest first. vrow[v]: bits 0-15 bra string,
-// bits 16-31 = 1 + partial-sum slot of a split part (0 for an unsplit row).
+// first, then the unsplit rows longest first. vrow[v]: the bra string;
+// vslot[v] = 1 + partial-sum slot of a split part (0 for an unsplit row).
 // The parts of split string s occupy slots split_slot[s] .. split_slot[s+1]-1
 // and are summed in that order. Record m of lane l of slice s sits at
 // sell[soff[s] + 32m + l]; shorter lists are padded with records that have
@@ -46,7 +46,8 @@ constexpr uint32_t kInfoSingle = 1u << 30;
 struct SellPanel {
   uint64_t* sell = nullptr;        // [soff[nslice]]
   // the same records in 32 bits (bits 0-15 position of the ket in the staged
-  // rows, Conn::kpos; 16-27 pair index, 28 sign, 29 padding, 30 integral
+  // rows, Conn::kpos, relative to the panel's first ket; 16-27 pair index,
+  // 28 sign, 29 padding, 30 integral
   // copy), read by the packed alpha-beta kernel in blocks of 4 per lane (a
   // padding record repeats the addresses of a real record of its step):
   // record m of lane l of slice s at sell32[soff4[s] + 128*(m/4) + 4*l + m%4],
@@ -57,6 +58,7 @@ struct SellPanel {
   uint64_t* soff = nullptr;        // [nslice + 1]
   uint32_t* slen = nullptr;        // [nslice]
   uint32_t* vrow = nullptr;        // [nv]
+  uint32_t* vslot = nullptr;       // [nv]
   uint32_t* split_row = nullptr;   // [nsplit]
   uint32_t* split_slot = nullptr;  // [nsplit + 1]
   size_t nslice = 0, nv = 0;
@@ -77,8 +79,9 @@ struct Conn {
   uint64_t* omask = nullptr;  // [total] opposite-spin parity mask
   uint32_t* info = nullptr;   // [total]
   // compact record of single excitations (doubles slots unused), read by the
-  // alpha-beta kernels: bits 0-15 ket, 16-27 pair index pq(a,i), 28-33 lo,
-  // 34-39 hi (lo = min(i,a), hi = max(i,a)), bit 40 same-spin sign
+  // alpha-beta kernels: ket in bits 0-15 and 42-49 (rec_ket), 16-27 pair
+  // index pq(a,i), 28-33 lo, 34-39 hi (lo = min(i,a), hi = max(i,a)), bit 40
+  // same-spin sign (bit 41 marks a SELL padding record)
   uint64_t* srec = nullptr;   // [total]
   // opposite-spin sign as boundaries of prefix parities: four 7-bit fields
   // (bits 0-6, 7-13, 14-20, 21-27) hold positions x (0..64) with
@@ -301,6 +304,16 @@ bool set_cuda_err(Ctx* c, cudaError_t e, const char* what);
   } while (0)
 
 // ---- device helpers ------------------------------------------------------------
+// Ket index of a compact single record (Conn::srec and the SELL records):
+// bits 0-15 and 42-49, 24 bits in all (at most 16,777,215 strings per spin).
+__host__ __device__ __forceinline__ uint32_t rec_ket(uint64_t r) {
+  return (uint32_t)(r & 0xffffu) | ((uint32_t)(r >> 26) & 0xff0000u);
+}
+__host__ __device__ __forceinline__ uint64_t rec_ket_bits(uint32_t k) {
+  return (uint64_t)(k & 0xffffu) | ((uint64_t)(k >> 16) << 42);
+}
+constexpr size_t kMaxStrings = 16777215;  // strings per spin (24-bit record indices)
+
 __host__ __device__ __forceinline__ uint64_t range_mask(int lo, int hi) {
   // bits [lo, hi) for 0 <= lo <= hi <= 64
   uint64_t h = hi >= 64 ? ~0ull : ((1ull << hi) - 1ull);

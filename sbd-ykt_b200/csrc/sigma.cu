@@ -370,7 +370,7 @@ sigma_ab_v2_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
       for (uint64_t m = m0; m < m1; ++m) {
         const uint64_t rec = next;
         if (m + 1 < m1) next = __ldg(b_rec + m + 1);
-        const uint32_t jb = (uint32_t)(rec & 0xffffu);
+        const uint32_t jb = rec_ket(rec);
         const uint32_t pq = (uint32_t)((rec >> 16) & 0xfffu);
         const uint32_t lo = (uint32_t)((rec >> 28) & 63u), hi = (uint32_t)((rec >> 34) & 63u);
         const uint32_t sb = (uint32_t)(rec >> 40);
@@ -477,7 +477,7 @@ sigma_ab_v5_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
       for (uint32_t m = 0; m < len; ++m) {
         const uint64_t rec = next;
         if (m + 1 < len) next = __ldg(rp + 32ull * (m + 1));
-        const uint32_t jb = (uint32_t)(rec & 0xffffu);
+        const uint32_t jb = rec_ket(rec);
         const uint32_t pq = (uint32_t)((rec >> 16) & 0xfffu);
         const uint32_t lo = (uint32_t)((rec >> 28) & 63u), hi = (uint32_t)((rec >> 34) & 63u);
         const uint32_t sb = (uint32_t)(rec >> 40);
@@ -636,7 +636,7 @@ sigma_ab_v4_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
       for (uint64_t m = m0; m < m1; ++m) {
         const uint64_t rec = next;
         if (m + 1 < m1) next = __ldg(b_rec + m + 1);
-        const uint32_t jb = (uint32_t)(rec & 0xffffu);
+        const uint32_t jb = rec_ket(rec);
         const uint32_t pq = (uint32_t)((rec >> 16) & 0xfffu);
         const uint32_t lo = (uint32_t)((rec >> 28) & 63u), hi = (uint32_t)((rec >> 34) & 63u);
         const uint32_t sb = (uint32_t)(rec >> 40);
@@ -743,7 +743,7 @@ sigma_ab_v3_kernel(const T* __restrict__ X, size_t nb, const uint64_t* __restric
       for (uint64_t m = m0; m < m1; ++m) {
         const uint64_t rec = next;
         if (m + 1 < m1) next = __ldg(b_rec + m + 1);
-        const uint32_t jb = (uint32_t)(rec & 0xffffu);
+        const uint32_t jb = rec_ket(rec);
         const uint32_t pq = (uint32_t)((rec >> 16) & 0xfffu);
         const uint32_t lo = (uint32_t)((rec >> 28) & 63u), hi = (uint32_t)((rec >> 34) & 63u);
         const uint32_t sb = (uint32_t)(rec >> 40);
@@ -1298,8 +1298,8 @@ sigma_ab_v6_kernel(const T* __restrict__ Xp, size_t nb, size_t ldx, const uint64
                    const uint32_t* __restrict__ a_nsing, const uint32_t* __restrict__ a_ket,
                    const uint32_t* __restrict__ a_info, const uint64_t* __restrict__ sell,
                    const uint64_t* __restrict__ soff, const uint32_t* __restrict__ slen, size_t nslice,
-                   const uint32_t* __restrict__ vrow, size_t nv, const uint32_t* __restrict__ split_row,
-                   const uint32_t* __restrict__ split_slot, int nsplit,
+                   const uint32_t* __restrict__ vrow, const uint32_t* __restrict__ vslot, size_t nv,
+                   const uint32_t* __restrict__ split_row, const uint32_t* __restrict__ split_slot, int nsplit,
                    const typename Prec<T>::V* __restrict__ Vt, size_t vstride, size_t xstride,
                    double* __restrict__ Y) {
   using V = typename Prec<T>::V;
@@ -1350,7 +1350,7 @@ sigma_ab_v6_kernel(const T* __restrict__ Xp, size_t nb, size_t ldx, const uint64
       for (uint32_t m = 0; m < len; ++m) {
         const uint64_t rec = next;
         if (m + 1 < len) next = __ldg(rp + 32ull * (m + 1));
-        const uint32_t jb = (uint32_t)(rec & 0xffffu);
+        const uint32_t jb = rec_ket(rec);
         const uint32_t pq = (uint32_t)((rec >> 16) & 0xfffu);
         const uint32_t sb = (uint32_t)(rec >> 40) & 1u;
         const bool pad = (rec >> 41) & 1ull;
@@ -1370,9 +1370,8 @@ sigma_ab_v6_kernel(const T* __restrict__ Xp, size_t nb, size_t ldx, const uint64
     const size_t sl = slice_of(k);
     const size_t pos = sl * 32 + lane;
     if (sl < nslice && pos < nv) {
-      const uint32_t w = vrow[pos];
-      const uint32_t slot1 = w >> 16;
-      if (slot1 == 0) Y[ia * ldx + (w & 0xffffu)] += acc[k];
+      const uint32_t slot1 = vslot[pos];
+      if (slot1 == 0) Y[ia * ldx + vrow[pos]] += acc[k];
       else part[slot1 - 1] = acc[k];
     }
   }
@@ -1422,8 +1421,9 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
                    const uint32_t* __restrict__ a_ket,
                    const uint32_t* __restrict__ a_info, const uint32_t* __restrict__ sell,
                    const uint64_t* __restrict__ soff4, const uint32_t* __restrict__ slen4, size_t nslice,
-                   const uint32_t* __restrict__ vrow, size_t nv, const uint32_t* __restrict__ split_row,
-                   const uint32_t* __restrict__ split_slot, int nsplit, const T* __restrict__ Vt, size_t vstride,
+                   const uint32_t* __restrict__ vrow, const uint32_t* __restrict__ vslot, size_t nv,
+                   const uint32_t* __restrict__ split_row, const uint32_t* __restrict__ split_slot, int nsplit,
+                   const T* __restrict__ Vt, size_t vstride,
                    int npair, uint32_t epad, uint32_t jb0, size_t nbp, const uint32_t* __restrict__ kpos,
                    const uint4* __restrict__ items, double* __restrict__ ypart, double* __restrict__ Y) {
   using RP = RowPack<T>;
@@ -1497,7 +1497,7 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const uint32_t rec = recs[q];
-          const P x = xs[(rec & 0xffffu) - jb0];  // pad records repeat a real record's addresses
+          const P x = xs[rec & 0xffffu];  // panel-relative position; pad records repeat a real record's addresses
           const P ev = er[((rec >> 16) & 0xfffu) + ((rec >> 30) & 1u) * epad];
           double d = RP::dot(ev, x);
           d = ((rec >> 29) & 1u) ? 0.0 : d;
@@ -1513,9 +1513,8 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
     const size_t sl = slice_of(k);
     const size_t pos = sl * 32 + lane;
     if (sl < nslice && pos < nv) {
-      const uint32_t w = vrow[pos];
-      const uint32_t slot1 = w >> 16;
-      if (slot1 == 0) Yrow[w & 0xffffu] += acc[k];
+      const uint32_t slot1 = vslot[pos];
+      if (slot1 == 0) Yrow[vrow[pos]] += acc[k];
       else part[slot1 - 1] = acc[k];
     }
   }
@@ -1567,7 +1566,7 @@ int launch_ab_v7(Ctx* c, const T* Xp, const SellPanel& bp, const Conn& it) {
   dim3 grid((unsigned)it.n_item, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
   if (grid.y == 0) grid.y = 1;
   sigma_ab_v7_kernel<T, KS><<<grid, kAb6Threads, smem, c->stream>>>(
-      Xp, c->xsa, ca.off, ca.ket, ca.info, bp.sell32, bp.soff4, bp.slen4, bp.nslice, bp.vrow, bp.nv,
+      Xp, c->xsa, ca.off, ca.ket, ca.info, bp.sell32, bp.soff4, bp.slen4, bp.nslice, bp.vrow, bp.vslot, bp.nv,
       bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, (int)c->npair, (uint32_t)ab7_epad(c->npair), bp.jb0,
       (size_t)(bp.jb1 - bp.jb0), c->conn[1].kpos, it.ab_item, it.ypart, c->d_y);
   SBDX_LAUNCHED(c);
@@ -1686,7 +1685,8 @@ int launch_ab_v6(Ctx* c, const T* Xp, size_t smem, size_t xstride) {
   dim3 grid((unsigned)c->na, (unsigned)((bp.nslice + per_cta - 1) / per_cta));
   if (grid.y == 0) grid.y = 1;
   sigma_ab_v6_kernel<T, R, KS><<<grid, kAb6Threads, smem, c->stream>>>(
-      Xp, c->nb, c->xsa, ca.off, ca.nsing, ca.ket, ca.info, bp.sell, bp.soff, bp.slen, bp.nslice, bp.vrow, bp.nv,
+      Xp, c->nb, c->xsa, ca.off, ca.nsing, ca.ket, ca.info, bp.sell, bp.soff, bp.slen, bp.nslice, bp.vrow, bp.vslot,
+      bp.nv,
       bp.split_row, bp.split_slot, bp.nsplit, Vt, vs, xstride, c->d_y);
   SBDX_LAUNCHED(c);
   return 0;

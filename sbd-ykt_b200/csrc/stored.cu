@@ -11,7 +11,7 @@
 //     H' the alpha-first-basis matrix of the sigma kernels, so the product
 //     acts on vectors in determinant order with no phase pass;
 //   - the diagonal stays in the context's hii vector;
-//   - column indices are 32-bit (at most 65535 x 65535 determinants), values
+//   - column indices are 32-bit (at most 2^32 - 1 determinants), values
 //     FP64: 12 bytes per stored element.
 // Building it costs one count kernel, a device prefix sum and one fill kernel
 // (a warp per row, coalesced writes). The product is one warp per row, lanes
