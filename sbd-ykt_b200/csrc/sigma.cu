@@ -1463,12 +1463,23 @@ sigma_ab_v7_kernel(const T* __restrict__ Xp, size_t ldx, const uint64_t* __restr
     }
     __syncthreads();
     // ket jb goes to position kpos[jb] - jb0, a permutation within aligned
-    // groups of 8: the 8 lanes of a quarter-warp store to 8 different slots
-    for (size_t t = threadIdx.x; t < nbp; t += kAb6Threads) {
-      P p;
+    // groups of 8: the 8 lanes of a quarter-warp store to 8 different slots.
+    // Each thread loads kStage packs before it stores them, so as many loads
+    // of the ket rows are in flight.
+    constexpr int kStage = 4;
+    for (size_t t0 = threadIdx.x; t0 < nbp; t0 += (size_t)kStage * kAb6Threads) {
+      P p[kStage];
+      uint32_t at[kStage];
 #pragma unroll
-      for (int e = 0; e < VR; ++e) RP::set(p, e, e < nr ? __ldg(xrow[e] + t) : (T)0);
-      xs[__ldg(kpos + jb0 + t) - jb0] = p;
+      for (int u = 0; u < kStage; ++u) {
+        const size_t t = t0 + (size_t)u * kAb6Threads;
+        at[u] = t < nbp ? __ldg(kpos + jb0 + t) - jb0 : 0u;
+#pragma unroll
+        for (int e = 0; e < VR; ++e) RP::set(p[u], e, (e < nr && t < nbp) ? __ldg(xrow[e] + t) : (T)0);
+      }
+#pragma unroll
+      for (int u = 0; u < kStage; ++u)
+        if (t0 + (size_t)u * kAb6Threads < nbp) xs[at[u]] = p[u];
     }
     for (int t = threadIdx.x; t < npair; t += kAb6Threads) {
       P p;
