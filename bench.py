@@ -671,6 +671,14 @@ def run_sharded(args, rank, world, local):
     e1.record(stream)
     barrier()
     ms_e2e = max_over_ranks(max(e0.elapsed_time(e1) / n_e2e, 1e3 * (time.perf_counter() - t0) / n_e2e), dist)
+    # per-phase durations of this rank's row-range product (events between its
+    # kernels; every rank takes the same collective steps)
+    ctx.set_profiling(True)
+    for _ in range(max(2, min(args.steps, 5))):
+        op(C_loc, S_loc)
+    ncalls, phases = ctx.phase_times()
+    ctx.set_profiling(False)
+    phases = {k: v / max(ncalls, 1) for k, v in phases.items()}
     dav = None
     if not args.no_davidson:
         hii = torch.from_numpy(ctx.diag_terms()[a0 * nb:a1 * nb]).cuda()
@@ -683,6 +691,12 @@ def run_sharded(args, rank, world, local):
     hbm, peak_kind = peaks()
     B = roofline_bytes(prob, dp, 8)
     gbs = B / world / (ms * 1e-3) / 1e9
+    # the alpha-beta kernel of this rank's shard against the shared-memory
+    # pipe, as at N = 1: 16 conflict-free bytes per alpha-beta det-pair
+    ab_pairs = float(sa[a0:a1].sum()) * float(sb.sum())
+    ab_ms = phases.get("alpha_beta", 0.0)
+    smem_peak = smem_peak_gbs((clocks or {}).get("sm_mhz") or 1965.0)
+    ab_gbs = 16.0 * ab_pairs / (ab_ms * 1e-3) / 1e9 if ab_ms > 0 else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
@@ -692,9 +706,14 @@ def run_sharded(args, rank, world, local):
                    "parallelism": f"alpha-row shards x{world} (whole C gathered per step)",
                    "shards": bounds, "tuning": {"same_vec": tune[0], "ab_rows": tune[1]},
                    "l2": f"inputs larger than L2 (C = {8 * prob.D / 1e6:.0f} MB > 126 MB), no flush"},
-        "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
-                     "traffic": None, "kernel": "whole sigma of a row shard (SpMV byte model / N per GPU)",
-                     "peak_kind": peak_kind},
+        "roofline": {"bound": "smem", "achieved": ab_gbs, "peak": smem_peak, "unit": "GB/s",
+                     "frac": ab_gbs / smem_peak if ab_gbs else None, "traffic": None,
+                     "kernel": "sigma_ab_v7", "phase": "alpha_beta", "shard": [a0, a1],
+                     "ms_per_launch": ab_ms, "smem_bytes_per_launch": 16.0 * ab_pairs,
+                     "peak_kind": "128 B/clk/SM x SMs x sampled SM clock (rank 0's shard)",
+                     "phases": phases,
+                     "hbm": {"model": "whole sigma of a row shard (SpMV byte model / N per GPU)", "gbs": gbs,
+                             "model_frac": gbs / hbm, "peak_gbs": hbm, "peak_kind": peak_kind}},
         "e2e": {"value": dp["total"] / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 8 * prob.D,
                 "d2h_bytes_per_step": 8 * prob.D, "ms_per_step": ms_e2e},
         "gpu_launches": launches,

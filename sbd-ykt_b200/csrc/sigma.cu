@@ -1901,24 +1901,43 @@ int run_sigma_rows(Ctx* c, const Tune& tune, const T* X, T* S, size_t a0, size_t
   const V* Da = f64 ? (const V*)c->d_Da : (const V*)c->d_Da32;
   T* xp = reinterpret_cast<T*>(c->d_xp);
   T* xpt = reinterpret_cast<T*>(c->d_xt);
+  auto mark = [&](int k) {
+    if (c->profiling) cudaEventRecord(c->ev[k], c->stream);
+  };
   int rc = 0;
+  mark(0);
   {
     dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((na + 31) / 32));
     phase_split_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(X, na, nb, c->d_a, c->d_b, xp, xpt, c->xsa, c->xsb);
     SBDX_LAUNCHED(c);
   }
+  mark(1);
   if (nr == 0) return 0;
   if ((rc = run_same_v6<T>(c, tune.same_code, xp, na, nb, c->xsa, ra, valA, Db, c->db_stride, c->d_hii, c->d_y)))
     return rc;
+  mark(2);
   if ((rc = run_same_v6<T>(c, tune.same_code, xpt + a0, nb, nr, c->xsb, cb, valB, Da + a0, c->da_stride, nullptr,
                            c->d_yt + a0)))
     return rc;
+  mark(3);
   if ((rc = run_ab_v7<T>(c, xp, &rc_items))) return rc;
+  mark(4);
   {
     dim3 grid((unsigned)((nb + 31) / 32), (unsigned)((nr + 31) / 32));
     combine_phase_kernel<T><<<grid, dim3(32, 8), 0, c->stream>>>(c->d_y + a0 * c->xsa, c->d_yt + a0, nr, nb,
                                                                  c->d_a + a0, c->d_b, S, c->xsa, c->xsb);
     SBDX_LAUNCHED(c);
+  }
+  mark(5);
+  if (c->profiling) {  // the phase order of run_sigma_v6
+    const int from[kSigmaPhases] = {1, 0, 2, 3, 4};
+    SBDX_CUDA(c, cudaEventSynchronize(c->ev[5]));
+    for (int k = 0; k < kSigmaPhases; ++k) {
+      float ms = 0.f;
+      SBDX_CUDA(c, cudaEventElapsedTime(&ms, c->ev[from[k]], c->ev[from[k] + 1]));
+      c->phase_ms[k] += ms;
+    }
+    ++c->phase_calls;
   }
   return 0;
 }
