@@ -65,7 +65,9 @@ long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n);
  * both precisions; 0 selects the built-in default (alpha-first kernels).
  * Alpha-first kernels (the sigma evaluated in the alpha-before-beta
  * determinant ordering, conjugated by the +-1 basis phase):
- *   same_code: 21/22/24/28 = 1/2/4/8 columns per thread;
+ *   same_code: 21/22/24/28 = 1/2/4/8 columns per thread, one bra string per
+ *              CTA; 31/32/34/38 = the same widths for blocks of 4 bra strings
+ *              that walk the union of their double-excitation lists once;
  *   ab_code:   61-64 = 1-4 staged ket rows of the balanced alpha-beta kernel,
  *              71 = the same with the rows packed in 16-byte elements (2 FP64
  *              or 4 FP32 rows per group; falls back to 62/64 when nb is too

@@ -209,7 +209,8 @@ long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n) {
 int sbdx_set_tuning(sbdx_ctx* ctx, int same_code, int ab_code) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {
     const int v = same_code % 10;
-    const bool same_v6 = same_code > 20 && same_code < 30, ab_v6 = (ab_code > 60 && ab_code < 70) || ab_code == 71;
+    const bool same_v6 = (same_code > 20 && same_code < 30) || (same_code > 30 && same_code < 40),
+               ab_v6 = (ab_code > 60 && ab_code < 70) || ab_code == 71;
     const bool same_ok = same_code == 0 || ((same_code < 10 && (v == 1 || v == 2 || v == 4 || v == 8)) ||
                                             (same_code > 10 && same_code < 20 && (v == 1 || v == 2 || v == 4)) ||
                                             (same_v6 && (v == 1 || v == 2 || v == 4 || v == 8)));
@@ -220,7 +221,8 @@ int sbdx_set_tuning(sbdx_ctx* ctx, int same_code, int ab_code) {
     const bool mixed = (same_v6 && ab_code != 0 && !ab_v6) || (ab_v6 && same_code != 0 && !same_v6) ||
                        (same_code != 0 && !same_v6 && ab_code == 0) || (ab_code != 0 && !ab_v6 && same_code == 0);
     if (!same_ok || !ab_ok || mixed) {
-      c->err = "set_tuning: alpha-first codes same in {21,22,24,28} with ab in {61..64, 71}, or interleaved codes "
+      c->err = "set_tuning: alpha-first codes same in {21,22,24,28,31,32,34,38} with ab in {61..64, 71}, or "
+               "interleaved codes "
                "same in {1,2,4,8,11,12,14} with ab = 10*variant + rows (variant 0-4, rows 1-4); 0 = default";
       return SBDX_ERR_ARG;
     }

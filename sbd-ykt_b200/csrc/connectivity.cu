@@ -198,6 +198,7 @@ void free_conn(Conn& c) {
   for (auto& p : c.panels) free_panel(p);
   cudaFree(c.ab_item); cudaFree(c.ab_split); cudaFree(c.ypart);
   cudaFree(c.same_item); cudaFree(c.same_split); cudaFree(c.same_ypart);
+  free_blocks(c.blk);
   c = Conn{};
 }
 
@@ -269,6 +270,200 @@ int build_same_items(Ctx* c, Conn& cn, const std::vector<uint32_t>& hs, const st
   cn.n_same_split = (int)split.size();
   cn.n_same_part = nslot;
   return upload_items(c, items, split, nslot, ncol, &cn.same_item, &cn.same_split, &cn.same_ypart);
+}
+
+uint64_t bit_reverse64(uint64_t x) {
+  x = ((x >> 1) & 0x5555555555555555ull) | ((x & 0x5555555555555555ull) << 1);
+  x = ((x >> 2) & 0x3333333333333333ull) | ((x & 0x3333333333333333ull) << 2);
+  x = ((x >> 4) & 0x0f0f0f0f0f0f0f0full) | ((x & 0x0f0f0f0f0f0f0f0full) << 4);
+  x = ((x >> 8) & 0x00ff00ff00ff00ffull) | ((x & 0x00ff00ff00ff00ffull) << 8);
+  x = ((x >> 16) & 0x0000ffff0000ffffull) | ((x & 0x0000ffff0000ffffull) << 16);
+  return (x >> 32) | (x << 32);
+}
+
+// Blocks of the blocked same-spin kernel (see SameBlocks) over the bra
+// strings row0 .. row0 + n - 1 of connectivity cn; hs are their singles
+// counts, `strings` all strings of the spin, ncol the other spin's string
+// count (partial rows have stride pad8(ncol)). The unions are built on the
+// host from a copy of the rows' entries, blocks split over host threads.
+int build_same_blocks(Ctx* c, const Conn& cn, const std::vector<uint64_t>& strings, size_t row0, size_t n,
+                      const std::vector<uint32_t>& hs, size_t ncol, SameBlocks& B) {
+  free_blocks(B);
+  if (n == 0) return 0;
+  // the rows' entries (one contiguous range of the CSR)
+  std::vector<uint64_t> off(n + 1);
+  SBDX_CUDA(c, cudaMemcpyAsync(off.data(), cn.off + row0, sizeof(uint64_t) * (n + 1), cudaMemcpyDeviceToHost,
+                               c->stream));
+  SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  const uint64_t e0 = off[0], ne = off[n] - off[0];
+  std::vector<uint32_t> ket(ne ? ne : 1), info(ne ? ne : 1);
+  std::vector<double> val(ne ? ne : 1);
+  std::vector<float> val32(ne ? ne : 1);
+  if (ne) {
+    SBDX_CUDA(c, cudaMemcpyAsync(ket.data(), cn.ket + e0, sizeof(uint32_t) * ne, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaMemcpyAsync(info.data(), cn.info + e0, sizeof(uint32_t) * ne, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaMemcpyAsync(val.data(), cn.val + e0, sizeof(double) * ne, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaMemcpyAsync(val32.data(), cn.val32 + e0, sizeof(float) * ne, cudaMemcpyDeviceToHost, c->stream));
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  // rows in bit-reversed string order, cut into blocks
+  std::vector<uint32_t> order(n);
+  for (size_t i = 0; i < n; ++i) order[i] = (uint32_t)i;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+    return bit_reverse64(strings[row0 + x]) < bit_reverse64(strings[row0 + y]);
+  });
+  const size_t nblk = (n + kBlkRows - 1) / kBlkRows;
+  std::vector<uint4> rows(nblk);
+  for (size_t b = 0; b < nblk; ++b) {
+    uint32_t r[kBlkRows];
+    for (int k = 0; k < kBlkRows; ++k) {
+      const size_t i = b * kBlkRows + k;
+      r[k] = i < n ? (uint32_t)(row0 + order[i]) : kNoRow;
+    }
+    rows[b] = make_uint4(r[0], r[1], r[2], r[3]);
+  }
+  // per block: the doubles of its rows merged by ket (each row's doubles are
+  // ascending; a row that is not is sorted first), equal kets folded into one
+  // union entry with a value per row
+  struct Part {
+    std::vector<uint32_t> ket;
+    std::vector<double> val;
+    std::vector<float> val32;
+    std::vector<uint64_t> len;  // union entries per block of the part
+  };
+  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const size_t nth = std::max<size_t>(1, std::min<size_t>(hw, (nblk + 63) / 64));
+  std::vector<Part> parts(nth);
+  auto work = [&](size_t t) {
+    Part& P = parts[t];
+    const size_t b0 = nblk * t / nth, b1 = nblk * (t + 1) / nth;
+    std::vector<uint64_t> keys;
+    for (size_t b = b0; b < b1; ++b) {
+      keys.clear();
+      size_t bounds[kBlkRows + 1];
+      for (int k = 0; k < kBlkRows; ++k) {
+        bounds[k] = keys.size();
+        const size_t i = b * kBlkRows + k;
+        if (i >= n) continue;
+        const size_t r = order[i];
+        const uint64_t s0 = off[r] - e0 + hs[r], s1 = off[r + 1] - e0;
+        for (uint64_t e = s0; e < s1; ++e) keys.push_back(((uint64_t)ket[e] << 34) | ((uint64_t)k << 32) | (e - s0));
+        if (!std::is_sorted(keys.begin() + bounds[k], keys.end())) std::sort(keys.begin() + bounds[k], keys.end());
+      }
+      bounds[kBlkRows] = keys.size();
+      for (int w = 1; w < kBlkRows; w *= 2)
+        for (int k = 0; k + w < kBlkRows; k += 2 * w)
+          std::inplace_merge(keys.begin() + bounds[k], keys.begin() + bounds[k + w],
+                             keys.begin() + bounds[std::min(k + 2 * w, kBlkRows)]);
+      uint64_t cnt = 0;
+      for (size_t q = 0; q < keys.size();) {
+        const uint32_t kt = (uint32_t)(keys[q] >> 34);
+        double v[kBlkRows] = {};
+        float v32[kBlkRows] = {};
+        for (; q < keys.size() && (uint32_t)(keys[q] >> 34) == kt; ++q) {
+          const int k = (int)((keys[q] >> 32) & 3u);
+          const size_t r = order[b * kBlkRows + k];
+          const uint64_t e = off[r] - e0 + hs[r] + (keys[q] & 0xffffffffull);
+          const bool neg = (info[e] & kInfoNeg) != 0;
+          v[k] = neg ? -val[e] : val[e];
+          v32[k] = neg ? -val32[e] : val32[e];
+        }
+        P.ket.push_back(kt);
+        for (int k = 0; k < kBlkRows; ++k) {
+          P.val.push_back(v[k]);
+          P.val32.push_back(v32[k]);
+        }
+        ++cnt;
+      }
+      P.len.push_back(cnt);
+    }
+  };
+  {
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < nth; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+  }
+  std::vector<uint64_t> uoff(nblk + 1, 0);
+  {
+    size_t b = 0;
+    for (const Part& P : parts)
+      for (uint64_t l : P.len) { uoff[b + 1] = uoff[b] + l; ++b; }
+  }
+  const uint64_t nu = uoff[nblk];
+  // work items: union entries plus, for a block's first item, two loads per
+  // single; blocks above the cap are split (see build_same_items)
+  std::vector<uint64_t> sing(nblk, 0);
+  uint64_t total = 0;
+  for (size_t b = 0; b < nblk; ++b) {
+    for (int k = 0; k < kBlkRows; ++k) {
+      const size_t i = b * kBlkRows + k;
+      if (i < n) sing[b] += hs[order[i]];
+    }
+    total += (uoff[b + 1] - uoff[b]) + 2 * sing[b];
+  }
+  const uint64_t strips = std::max<uint64_t>(1, (ncol + 1023) / 1024);
+  const uint64_t slots = 8ull * sm_count(c);
+  const uint32_t cap = (uint32_t)std::max<uint64_t>(64, (total * strips + slots - 1) / slots);
+  std::vector<uint4> items, split;
+  std::vector<uint64_t> weight;
+  int nslot = 0;
+  for (size_t b = 0; b < nblk; ++b) {
+    const uint64_t len = uoff[b + 1] - uoff[b];
+    if (len <= cap) {
+      items.push_back(make_uint4((uint32_t)b, 0u, (uint32_t)len, 0u));
+      weight.push_back(len + 2 * sing[b]);
+      continue;
+    }
+    const uint32_t np = (uint32_t)((len + cap - 1) / cap);
+    split.push_back(make_uint4((uint32_t)b, (uint32_t)nslot, np, 0u));
+    for (uint32_t q = 0; q < np; ++q) {
+      const uint32_t u0 = q * cap, u1 = (uint32_t)std::min<uint64_t>(len, (uint64_t)(q + 1) * cap);
+      items.push_back(make_uint4((uint32_t)b, u0, u1, (uint32_t)(nslot + q + 1)));
+      weight.push_back((u1 - u0) + (q == 0 ? 2 * sing[b] : 0));
+    }
+    nslot += (int)np;
+  }
+  {
+    std::vector<size_t> perm(items.size());
+    for (size_t i = 0; i < perm.size(); ++i) perm[i] = i;
+    std::stable_sort(perm.begin(), perm.end(), [&](size_t x, size_t y) { return weight[x] > weight[y]; });
+    std::vector<uint4> sorted(items.size());
+    for (size_t i = 0; i < perm.size(); ++i) sorted[i] = items[perm[i]];
+    items.swap(sorted);
+  }
+  // upload
+  const size_t nu1 = nu ? nu : 1;
+  B.nblk = nblk;
+  B.nu = nu;
+  B.cap = (int)cap;
+  B.n_item = items.size();
+  B.n_split = (int)split.size();
+  B.n_part = nslot;
+  SBDX_CUDA(c, cudaMalloc(&B.rows, sizeof(uint4) * nblk));
+  SBDX_CUDA(c, cudaMalloc(&B.uoff, sizeof(uint64_t) * (nblk + 1)));
+  SBDX_CUDA(c, cudaMalloc(&B.uket, sizeof(uint32_t) * nu1));
+  SBDX_CUDA(c, cudaMalloc(&B.uval, sizeof(double) * kBlkRows * nu1));
+  SBDX_CUDA(c, cudaMalloc(&B.uval32, sizeof(float) * kBlkRows * nu1));
+  SBDX_CUDA(c, cudaMemcpyAsync(B.rows, rows.data(), sizeof(uint4) * nblk, cudaMemcpyHostToDevice, c->stream));
+  SBDX_CUDA(c, cudaMemcpyAsync(B.uoff, uoff.data(), sizeof(uint64_t) * (nblk + 1), cudaMemcpyHostToDevice, c->stream));
+  {
+    uint64_t at = 0;
+    for (const Part& P : parts) {
+      const size_t m = P.ket.size();
+      if (m) {
+        SBDX_CUDA(c, cudaMemcpyAsync(B.uket + at, P.ket.data(), sizeof(uint32_t) * m, cudaMemcpyHostToDevice,
+                                     c->stream));
+        SBDX_CUDA(c, cudaMemcpyAsync(B.uval + at * kBlkRows, P.val.data(), sizeof(double) * kBlkRows * m,
+                                     cudaMemcpyHostToDevice, c->stream));
+        SBDX_CUDA(c, cudaMemcpyAsync(B.uval32 + at * kBlkRows, P.val32.data(), sizeof(float) * kBlkRows * m,
+                                     cudaMemcpyHostToDevice, c->stream));
+      }
+      at += m;
+    }
+  }
+  // upload_items synchronises the stream before the host vectors die
+  return upload_items(c, items, split, nslot * kBlkRows, ncol, &B.item, &B.split, &B.ypart);
 }
 
 // Work items of the packed alpha-beta kernel (see Conn::ab_item; partial rows
@@ -693,6 +888,8 @@ int build_one(Ctx* c, int spin) {
   {
     int rc = build_same_items(c, cn, hs, hd, spin == 0 ? c->nb : c->na);
     if (rc) return rc;
+    if ((rc = build_same_blocks(c, cn, spin == 0 ? c->h_a : c->h_b, 0, n, hs, spin == 0 ? c->nb : c->na, cn.blk)))
+      return rc;
     if (spin == 0 && (rc = build_ab_items(c, cn, hs, c->nb))) return rc;
   }
   // SELL-32 copy of the single-excitation records in list-length order
@@ -755,7 +952,14 @@ int build_one(Ctx* c, int spin) {
 
 }  // namespace
 
+void free_blocks(SameBlocks& b) {
+  cudaFree(b.rows); cudaFree(b.uoff); cudaFree(b.uket); cudaFree(b.uval); cudaFree(b.uval32);
+  cudaFree(b.item); cudaFree(b.split); cudaFree(b.ypart);
+  b = SameBlocks{};
+}
+
 void free_range_items(Conn& r) {
+  free_blocks(r.blk);
   cudaFree(r.same_item); cudaFree(r.same_split); cudaFree(r.same_ypart);
   cudaFree(r.ab_item); cudaFree(r.ab_split); cudaFree(r.ypart);
   r.same_item = r.same_split = r.ab_item = r.ab_split = nullptr;
@@ -789,6 +993,7 @@ int build_range_items(Ctx* c, size_t a0, size_t a1, Conn& r) {
   hd.resize(n);
   int rc = build_same_items(c, r, hs, hd, c->nb, a0);
   if (rc) return rc;
+  if ((rc = build_same_blocks(c, ca, c->h_a, a0, n, hs, c->nb, r.blk))) return rc;
   return build_ab_items(c, r, hs, c->nb, a0);
 }
 

@@ -67,6 +67,38 @@ struct SellPanel {
   uint32_t jb0 = 0, jb1 = 0;
 };
 
+// Bra strings per block of the blocked same-spin kernel.
+constexpr int kBlkRows = 4;
+constexpr uint32_t kNoRow = 0xffffffffu;
+
+// Blocks of the blocked same-spin kernel over the bra strings [row0, row1)
+// of one spin. The strings are ordered by their bit-reversed words (strings
+// with the same low-orbital holes and different high-orbital particles side
+// by side: their double excitations reach largely the same ket strings; at
+// 8000 sampled strings per spin the union of four neighbours' double lists
+// holds 0.44 of their entries, against 0.74 in ascending order) and cut into
+// blocks of kBlkRows. Per block the union of its strings' double-excitation
+// kets, ascending, with one signed same-spin value per string of the block
+// (zero where that string does not connect). Singles stay in the CSR.
+// Work items {block, first union entry, one past the last, 1 + partial slot
+// or 0}, longest first; a block with more union entries than the cap is
+// split, its first item also does the diagonal and the singles, and the
+// parts' kBlkRows partial rows (ypart[(slot * kBlkRows + r) * ldx ..]) are
+// summed in slot order by a fix-up kernel.
+struct SameBlocks {
+  size_t nblk = 0, nu = 0;
+  uint4* rows = nullptr;     // [nblk] bra strings (kNoRow: none)
+  uint64_t* uoff = nullptr;  // [nblk + 1]
+  uint32_t* uket = nullptr;  // [nu]
+  double* uval = nullptr;    // [nu * kBlkRows]
+  float* uval32 = nullptr;   // [nu * kBlkRows]
+  uint4* item = nullptr;     // [n_item]
+  size_t n_item = 0;
+  uint4* split = nullptr;    // [n_split]: {block, first slot, parts, 0}
+  int n_split = 0, n_part = 0, cap = 0;
+  double* ypart = nullptr;   // [n_part * kBlkRows * pad8(ncol)]
+};
+
 struct Conn {
   size_t n = 0;          // number of bra strings
   size_t total = 0;      // number of entries
@@ -129,6 +161,8 @@ struct Conn {
   uint4* same_split = nullptr;
   int n_same_split = 0, n_same_part = 0, same_cap = 0;
   double* same_ypart = nullptr;
+  // blocks of the blocked same-spin kernel over the same rows as same_item
+  SameBlocks blk;
 };
 
 // Largest number of partial-sum slots of split rows (shared memory of the
@@ -380,6 +414,7 @@ void free_row_range(Ctx* c);
 // The work items of rows [a0, a1) into r, and their release.
 int build_range_items(Ctx* c, size_t a0, size_t a1, Conn& r);
 void free_range_items(Conn& r);
+void free_blocks(SameBlocks& b);
 // The host-buffer sigma's chunks (their work items, copy stream, events).
 void free_io_chunks(Ctx* c);
 // S = H C for host buffers (FP64), the copies overlapped with the kernels.

@@ -1279,6 +1279,192 @@ sigma_same_v6f_kernel(const float* __restrict__ X, size_t ncol, size_t ldx, cons
   }
 }
 
+// VEC consecutive elements in the storage type.
+template <typename T, int VEC> struct LoadT;
+template <int VEC> struct LoadT<double, VEC> {
+  static __device__ __forceinline__ void load(const double* p, double* o) { VecIO<double, VEC>::load(p, o); }
+};
+template <int VEC> struct LoadT<float, VEC> {
+  static __device__ __forceinline__ void load(const float* p, float* o) { VecF<VEC>::load(p, o); }
+};
+
+// Signed same-spin values of one union entry of the blocked kernel, one per
+// bra string of the block (kBlkRows = 4).
+template <typename V> struct Vals4;
+template <> struct Vals4<double> { using P = double4; };
+template <> struct Vals4<float> { using P = float4; };
+
+// Resident CTAs per SM the blocked kernel is compiled for, the union entries
+// summed in FP32 before the FP64 row accumulation (FP32 storage), and the
+// union entries whose ket loads the compiler may issue ahead.
+template <typename T> struct BlkShape { static constexpr int kMinBlocks = 1; };
+constexpr int kBlkRun = kRun;
+constexpr int kBlkUnroll = 4;
+
+// Blocked same-spin product (codes 31/32/34/38 = columns per thread): one CTA
+// per (work item of SameBlocks, strip of kSameThreads*VEC columns). The first
+// item of a block adds the diagonal and the singles of its kBlkRows bra
+// strings, one string at a time, as sigma_same_v6_kernel does; every item then
+// walks its range of the block's union of double-excitation kets: each ket
+// row strip is loaded once and applied to all strings of the block with their
+// signed values (zero where a string does not connect), so a ket shared by
+// several strings of the block costs one load instead of one per string.
+// FP32 storage (T = float): products summed in FP32 over runs of kBlkRun union
+// entries (or of kRun singles), each run's sum added to the FP64 row
+// accumulator.
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kSameThreads, BlkShape<T>::kMinBlocks)
+sigma_same_blk_kernel(const T* __restrict__ X, size_t ncol, size_t ldx, const uint64_t* __restrict__ off,
+                      const uint32_t* __restrict__ nsing, const uint32_t* __restrict__ ket,
+                      const T* __restrict__ val, const uint32_t* __restrict__ info, const T* __restrict__ Dt,
+                      size_t dstride, const double* __restrict__ hii, const uint4* __restrict__ brows,
+                      const uint64_t* __restrict__ uoff, const uint32_t* __restrict__ uket,
+                      const typename Vals4<T>::P* __restrict__ uval, const uint4* __restrict__ items,
+                      double* __restrict__ ypart, double* __restrict__ Y, int accumulate) {
+  using P4 = typename Vals4<T>::P;
+  constexpr bool kF32 = std::is_same<T, float>::value;
+  __shared__ uint32_t s_ket[kSameThreads], s_pq[kSameThreads];
+  __shared__ P4 s_val4[kSameThreads];
+  __shared__ T s_val[kSameThreads];
+  const uint4 item = items[blockIdx.x];  // block, union range, partial slot
+  const uint4 rw = brows[item.x];
+  const uint32_t rows[kBlkRows] = {rw.x, rw.y, rw.z, rw.w};
+  const size_t c0 = ((size_t)blockIdx.y * kSameThreads + threadIdx.x) * VEC;
+  const bool active = c0 < ncol;
+  const unsigned t = threadIdx.x;
+  double acc[kBlkRows][VEC];
+#pragma unroll
+  for (int k = 0; k < kBlkRows; ++k)
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[k][v] = 0.0;
+  if (item.y == 0) {  // the block's first item: diagonal and singles, string by string
+#pragma unroll
+    for (int k = 0; k < kBlkRows; ++k) {
+      const uint32_t r = rows[k];
+      if (r == kNoRow) continue;
+      if (hii != nullptr && active) {
+        T x[VEC];
+        LoadT<T, VEC>::load(X + (size_t)r * ldx + c0, x);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) acc[k][v] = c0 + v < ncol ? hii[(size_t)r * ncol + c0 + v] * (double)x[v] : 0.0;
+      }
+      const uint64_t beg = off[r], end = beg + nsing[r];
+      for (uint64_t base = beg; base < end; base += kSameThreads) {
+        const int cnt = (int)min((uint64_t)kSameThreads, end - base);
+        __syncthreads();
+        if ((int)t < cnt) {
+          const uint64_t e = base + t;
+          const uint32_t inf = info[e];
+          const T v = val[e];
+          s_ket[t] = ket[e];
+          s_val[t] = (inf >> 31) ? -v : v;
+          s_pq[t] = ((inf >> 12) & 0xfffu) | (inf & kInfoNeg);
+        }
+        __syncthreads();
+        if (!active) continue;
+        for (int e0 = 0; e0 < cnt; e0 += kRun) {
+          const int e1 = min(e0 + kRun, cnt);
+          T pf[VEC];
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) pf[v] = (T)0;
+          for (int e = e0; e < e1; ++e) {
+            const uint32_t pqs = s_pq[e];
+            const T hv = s_val[e];
+            T x[VEC], d[VEC];
+            LoadT<T, VEC>::load(X + (size_t)s_ket[e] * ldx + c0, x);
+            LoadT<T, VEC>::load(Dt + (size_t)(pqs & 0xfffu) * dstride + c0, d);
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) {
+              const T dv = (pqs >> 31) ? -d[v] : d[v];
+              if constexpr (kF32) pf[v] = fmaf(hv + dv, x[v], pf[v]);
+              else acc[k][v] = fma(hv + dv, x[v], acc[k][v]);
+            }
+          }
+          if constexpr (kF32) {
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) acc[k][v] += (double)pf[v];
+          }
+        }
+      }
+    }
+  }
+  // doubles: the block's union entries [u0, u1)
+  const uint64_t ub = uoff[item.x];
+  const uint64_t beg = ub + item.y, end = ub + item.z;
+  for (uint64_t base = beg; base < end; base += kSameThreads) {
+    const int cnt = (int)min((uint64_t)kSameThreads, end - base);
+    __syncthreads();
+    if ((int)t < cnt) {
+      s_ket[t] = uket[base + t];
+      s_val4[t] = uval[base + t];
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (int e0 = 0; e0 < cnt; e0 += kBlkRun) {
+      const int e1 = min(e0 + kBlkRun, cnt);
+      T pf[kBlkRows][VEC];
+#pragma unroll
+      for (int k = 0; k < kBlkRows; ++k)
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) pf[k][v] = (T)0;
+#pragma unroll kBlkUnroll
+      for (int e = e0; e < e1; ++e) {
+        T x[VEC];
+        LoadT<T, VEC>::load(X + (size_t)s_ket[e] * ldx + c0, x);
+        const P4 w = s_val4[e];
+        const T wv[kBlkRows] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int k = 0; k < kBlkRows; ++k)
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) {
+            if constexpr (kF32) pf[k][v] = fmaf(wv[k], x[v], pf[k][v]);
+            else acc[k][v] = fma(wv[k], x[v], acc[k][v]);
+          }
+      }
+      if constexpr (kF32) {
+#pragma unroll
+        for (int k = 0; k < kBlkRows; ++k)
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) acc[k][v] += (double)pf[k][v];
+      }
+    }
+  }
+  if (!active) return;
+#pragma unroll
+  for (int k = 0; k < kBlkRows; ++k) {
+    const uint32_t r = rows[k];
+    if (r == kNoRow) continue;
+    if (item.w) {  // a part of a split block: its partial row
+      double* y = ypart + ((size_t)(item.w - 1) * kBlkRows + k) * ldx + c0;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) y[v] = acc[k][v];
+    } else {
+      double* y = Y + (size_t)r * ldx + c0;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) y[v] = accumulate ? y[v] + acc[k][v] : acc[k][v];
+    }
+  }
+}
+
+// Assigns (or, with accumulate, adds) the sums of the partial rows of the
+// blocks split over several items of the blocked same-spin kernel, parts in
+// slot order; blockIdx.z = string of the block.
+__global__ void same_blk_fixup_kernel(const uint4* __restrict__ split, const uint4* __restrict__ brows,
+                                      const double* __restrict__ ypart, size_t ncol, size_t ldx,
+                                      double* __restrict__ Y, int accumulate) {
+  const uint4 sp = split[blockIdx.y];
+  const uint4 rw = brows[sp.x];
+  const int k = blockIdx.z;
+  const uint32_t r = k == 0 ? rw.x : k == 1 ? rw.y : k == 2 ? rw.z : rw.w;
+  if (r == kNoRow) return;
+  for (size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x; col < ncol; col += (size_t)gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (uint32_t q = 0; q < sp.z; ++q) t += ypart[((size_t)(sp.y + q) * kBlkRows + k) * ldx + col];
+    double* y = Y + (size_t)r * ldx + col;
+    *y = accumulate ? *y + t : t;
+  }
+}
+
 constexpr int kAb6Threads = 1024;
 
 // Alpha single x beta single in the alpha-first basis, balanced. One CTA per
@@ -1662,10 +1848,34 @@ int launch_same_v6(Ctx* c, const T* X, size_t nrow, size_t ncol, size_t ldx, con
   return 0;
 }
 
+template <typename T, int VEC>
+int launch_same_blk(Ctx* c, const T* X, size_t ncol, size_t ldx, const Conn& cn, const T* val, const T* Dt,
+                    size_t dstride, const double* hii, double* Y, int accumulate) {
+  const SameBlocks& B = cn.blk;
+  using P4 = typename Vals4<T>::P;
+  const P4* uval = reinterpret_cast<const P4*>(std::is_same<T, double>::value ? (const void*)B.uval
+                                                                              : (const void*)B.uval32);
+  if (B.n_item > 0) {
+    dim3 grid((unsigned)B.n_item, (unsigned)((ncol + (size_t)kSameThreads * VEC - 1) / ((size_t)kSameThreads * VEC)));
+    sigma_same_blk_kernel<T, VEC><<<grid, kSameThreads, 0, c->stream>>>(
+        X, ncol, ldx, cn.off, cn.nsing, cn.ket, val, cn.info, Dt, dstride, hii, B.rows, B.uoff, B.uket, uval, B.item,
+        B.ypart, Y, accumulate);
+    SBDX_LAUNCHED(c);
+  }
+  if (B.n_split > 0) {
+    const unsigned bx = (unsigned)std::min<size_t>((ncol + 255) / 256, 64);
+    same_blk_fixup_kernel<<<dim3(bx, (unsigned)B.n_split, kBlkRows), 256, 0, c->stream>>>(B.split, B.rows, B.ypart,
+                                                                                         ncol, ldx, Y, accumulate);
+    SBDX_LAUNCHED(c);
+  }
+  return 0;
+}
+
 // v6 same-spin codes: 21, 22, 24, 28 = 1, 2, 4, 8 columns per thread, narrowed
 // to the widest vector that divides the row stride and keeps 16-byte
 // alignment (the internal vectors have strides padded to 8 elements, so only
 // a misaligned base narrows).
+// Codes 31, 32, 34, 38: the blocked kernel with as many columns per thread.
 // accumulate: add to Y's rows instead of writing them (the pipelined
 // host-buffer sigma runs the alpha-beta kernel first).
 template <typename T>
@@ -1675,6 +1885,12 @@ int run_same_v6(Ctx* c, int code, const T* X, size_t nrow, size_t ncol, size_t l
   int vec = code % 10;
   const bool aligned = (reinterpret_cast<uintptr_t>(X) % 16) == 0;
   while (vec > 1 && (!aligned || ldx % vec != 0 || dstride % vec != 0)) vec >>= 1;
+  if (code / 10 == 3 && cn.blk.nblk > 0) {  // blocked kernel (31, 32, 34, 38)
+    if (vec >= 8) return launch_same_blk<T, 8>(c, X, ncol, ldx, cn, val, Dt, dstride, hii, Y, accumulate);
+    if (vec >= 4) return launch_same_blk<T, 4>(c, X, ncol, ldx, cn, val, Dt, dstride, hii, Y, accumulate);
+    if (vec == 2) return launch_same_blk<T, 2>(c, X, ncol, ldx, cn, val, Dt, dstride, hii, Y, accumulate);
+    return launch_same_blk<T, 1>(c, X, ncol, ldx, cn, val, Dt, dstride, hii, Y, accumulate);
+  }
   if (vec >= 8) return launch_same_v6<T, 8>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y, accumulate);
   if (vec >= 4) return launch_same_v6<T, 4>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y, accumulate);
   if (vec == 2) return launch_same_v6<T, 2>(c, X, nrow, ncol, ldx, cn, val, Dt, dstride, hii, Y, accumulate);
@@ -1742,8 +1958,10 @@ int run_ab_v6(Ctx* c, int code, const T* Xp) {
   return launch_ab_v6_ks<T, 1>(c, Xp, smem, xstride);
 }
 
+bool same_alpha_first(int code) { return (code > 20 && code < 30) || (code > 30 && code < 40); }
+
 bool is_v6(const Tune& t) {
-  return t.same_code > 20 && t.same_code < 30 && ((t.ab_code > 60 && t.ab_code < 70) || t.ab_code == 71);
+  return same_alpha_first(t.same_code) && ((t.ab_code > 60 && t.ab_code < 70) || t.ab_code == 71);
 }
 
 template <typename T>
@@ -1856,7 +2074,7 @@ constexpr Tune kDefaultTune[2] = {{24, 71}, {28, 71}};
 Tune effective_tune(const Ctx* c, bool f64) {
   Tune t = c->tune[f64 ? 0 : 1];
   const Tune& d = kDefaultTune[f64 ? 0 : 1];
-  const bool v6 = (t.same_code > 20 && t.same_code < 30) || (t.ab_code > 60 && t.ab_code < 70) ||
+  const bool v6 = same_alpha_first(t.same_code) || (t.ab_code > 60 && t.ab_code < 70) ||
                   t.ab_code == 71 || (t.same_code == 0 && t.ab_code == 0);
   if (v6) {
     if (t.same_code == 0) t.same_code = d.same_code;
@@ -1889,6 +2107,7 @@ int run_sigma_rows(Ctx* c, const Tune& tune, const T* X, T* S, size_t a0, size_t
   const Conn& cb = c->conn[1];
   const Conn& rc_items = c->range_conn;
   Conn ra = ca;  // the alpha lists with the range's same-spin work items
+  ra.blk = rc_items.blk;
   ra.same_item = rc_items.same_item;
   ra.n_same_item = rc_items.n_same_item;
   ra.same_split = rc_items.same_split;
@@ -2030,7 +2249,7 @@ int autotune(Ctx* c) {
   if (!c->ev[0])
     for (auto& e : c->ev) SBDX_CUDA(c, cudaEventCreate(&e));
   c->profiling = true;
-  const int same_cand[] = {24, 28, 22};
+  const int same_cand[] = {32, 34, 38, 24, 28, 22};
   const int ab_cand[] = {71, 62, 61, 63, 64};
   for (int prec = 0; prec < 2 && rc == 0; ++prec) {
     const Tune saved = c->tune[prec];
@@ -2320,6 +2539,7 @@ int sigma_host(Ctx* c, const double* hC, double* hS) {
     const size_t a0 = b[i], nr = b[i + 1] - b[i];
     const Conn& it = c->io_items[i];
     Conn ra = ca;
+    ra.blk = it.blk;
     ra.same_item = it.same_item;
     ra.n_same_item = it.n_same_item;
     ra.same_split = it.same_split;
