@@ -1294,12 +1294,16 @@ template <typename V> struct Vals4;
 template <> struct Vals4<double> { using P = double4; };
 template <> struct Vals4<float> { using P = float4; };
 
-// Resident CTAs per SM the blocked kernel is compiled for, the union entries
-// summed in FP32 before the FP64 row accumulation (FP32 storage), and the
-// union entries whose ket loads the compiler may issue ahead.
-template <typename T> struct BlkShape { static constexpr int kMinBlocks = 1; };
+// Resident CTAs per SM the blocked kernel is compiled for (0: no bound; FP32
+// storage: three, which caps its registers at 80 with the deeper unroll of
+// its union loop), and the union entries summed in FP32 before the FP64 row
+// accumulation. Measured at 8000 x 8000 strings: FP64 runs fastest with the
+// union loop unrolled 4 deep and no bound (52 registers, 4 CTAs per SM; an
+// explicit bound of 1 let it take 96 registers and ran 19% slower), FP32 with
+// 8 union entries' ket loads issued ahead.
+template <typename T> struct BlkShape { static constexpr int kMinBlocks = 0; };
+template <> struct BlkShape<float> { static constexpr int kMinBlocks = 3; };
 constexpr int kBlkRun = kRun;
-constexpr int kBlkUnroll = 4;
 
 // Blocked same-spin product (codes 31/32/34/38 = columns per thread): one CTA
 // per (work item of SameBlocks, strip of kSameThreads*VEC columns). The first
@@ -1407,25 +1411,34 @@ sigma_same_blk_kernel(const T* __restrict__ X, size_t ncol, size_t ldx, const ui
       for (int k = 0; k < kBlkRows; ++k)
 #pragma unroll
         for (int v = 0; v < VEC; ++v) pf[k][v] = (T)0;
-#pragma unroll kBlkUnroll
-      for (int e = e0; e < e1; ++e) {
-        T x[VEC];
-        LoadT<T, VEC>::load(X + (size_t)s_ket[e] * ldx + c0, x);
-        const P4 w = s_val4[e];
-        const T wv[kBlkRows] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-        for (int k = 0; k < kBlkRows; ++k)
-#pragma unroll
-          for (int v = 0; v < VEC; ++v) {
-            if constexpr (kF32) pf[k][v] = fmaf(wv[k], x[v], pf[k][v]);
-            else acc[k][v] = fma(wv[k], x[v], acc[k][v]);
-          }
-      }
       if constexpr (kF32) {
+#pragma unroll 8
+        for (int e = e0; e < e1; ++e) {
+          T x[VEC];
+          LoadT<T, VEC>::load(X + (size_t)s_ket[e] * ldx + c0, x);
+          const P4 w = s_val4[e];
+          const T wv[kBlkRows] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+          for (int k = 0; k < kBlkRows; ++k)
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) pf[k][v] = fmaf(wv[k], x[v], pf[k][v]);
+        }
 #pragma unroll
         for (int k = 0; k < kBlkRows; ++k)
 #pragma unroll
           for (int v = 0; v < VEC; ++v) acc[k][v] += (double)pf[k][v];
+      } else {
+#pragma unroll 4
+        for (int e = e0; e < e1; ++e) {
+          T x[VEC];
+          LoadT<T, VEC>::load(X + (size_t)s_ket[e] * ldx + c0, x);
+          const P4 w = s_val4[e];
+          const T wv[kBlkRows] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+          for (int k = 0; k < kBlkRows; ++k)
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) acc[k][v] = fma(wv[k], x[v], acc[k][v]);
+        }
       }
     }
   }
@@ -2068,8 +2081,8 @@ int run_sigma_v5(Ctx* c, const T* X, T* S) {
   return 0;
 }
 
-// Default launch codes: the alpha-first (v6) kernels.
-constexpr Tune kDefaultTune[2] = {{24, 71}, {28, 71}};
+// Default launch codes: the alpha-first kernels, blocked same-spin products.
+constexpr Tune kDefaultTune[2] = {{32, 71}, {34, 71}};
 
 Tune effective_tune(const Ctx* c, bool f64) {
   Tune t = c->tune[f64 ? 0 : 1];
