@@ -62,7 +62,9 @@ unsigned long long sbdx_launch_count(const sbdx_ctx* ctx);
 int sbdx_set_profiling(sbdx_ctx* ctx, int on);
 long long sbdx_phase_times(sbdx_ctx* ctx, double* ms, int n);
 /* Launch shapes of the sigma kernels (no reference counterpart), applied to
- * both precisions; 0 selects the built-in default (alpha-first kernels).
+ * both precisions; 0 selects the built-in default (alpha-first kernels; the
+ * blocked same-spin kernel from 2 M determinants in FP64 and 1 M with FP32
+ * storage, the one-string-per-CTA kernel below).
  * Alpha-first kernels (the sigma evaluated in the alpha-before-beta
  * determinant ordering, conjugated by the +-1 basis phase):
  *   same_code: 21/22/24/28 = 1/2/4/8 columns per thread, one bra string per
@@ -330,7 +332,8 @@ int sbdx_batch_dims(const sbdx_batch* batch, int index, size_t* na, size_t* nb);
 /* sbdx_set_graph_steps for every subspace of the batch (and those added later). */
 int sbdx_batch_set_graph_steps(sbdx_batch* batch, int on);
 /* Tunes the sigma launch shapes on the largest subspace (sbdx_autotune) and
- * applies them to all subspaces. */
+ * applies them to the subspaces with at least a quarter of its determinants;
+ * smaller ones keep the size-dependent defaults. */
 int sbdx_batch_tune(sbdx_batch* batch, int* same_code, int* ab_code);
 /* Lowest nroots (1-4) of every subspace, start vectors on the lowest diagonal
  * elements, nthreads host threads (0 = 8). energies, residuals: size*nroots

@@ -155,10 +155,15 @@ int sbdx_batch_tune(sbdx_batch* b, int* same_code, int* ab_code) {
   int s = 0, a = 0;
   int rc = sbdx_autotune(ref, &s, &a);
   if (rc) return fail(b, rc, std::string("batch_tune: ") + sbdx_last_error(ref));
+  // the tuned codes go to the subspaces of comparable size; much smaller ones
+  // keep the size-dependent defaults (a launch shape that fills the GPU on the
+  // largest subspace can leave it half idle on one a few times smaller)
+  const size_t dbig = ref->c.na * ref->c.nb;
   for (auto& sub : b->subs) {
     sbdx::Ctx* c = &sub.ctx->c;
-    c->tune[0] = ref->c.tune[0];
-    c->tune[1] = ref->c.tune[1];
+    const bool near = 4 * c->na * c->nb >= dbig;
+    c->tune[0] = near ? ref->c.tune[0] : sbdx::Tune{};
+    c->tune[1] = near ? ref->c.tune[1] : sbdx::Tune{};
     sbdx::clear_sigma_graphs(c);
   }
   if (same_code) *same_code = s;

@@ -285,7 +285,8 @@ uint64_t bit_reverse64(uint64_t x) {
 // strings row0 .. row0 + n - 1 of connectivity cn; hs are their singles
 // counts, `strings` all strings of the spin, ncol the other spin's string
 // count (partial rows have stride pad8(ncol)). The unions are built on the
-// host from a copy of the rows' entries, blocks split over host threads.
+// host from a copy of the rows' entries (a merge with one cursor per string
+// of a block), blocks split over host threads.
 int build_same_blocks(Ctx* c, const Conn& cn, const std::vector<uint64_t>& strings, size_t row0, size_t n,
                       const std::vector<uint32_t>& hs, size_t ncol, SameBlocks& B) {
   free_blocks(B);
@@ -307,11 +308,11 @@ int build_same_blocks(Ctx* c, const Conn& cn, const std::vector<uint64_t>& strin
     SBDX_CUDA(c, cudaStreamSynchronize(c->stream));
   }
   // rows in bit-reversed string order, cut into blocks
+  std::vector<std::pair<uint64_t, uint32_t>> rkey(n);
+  for (size_t i = 0; i < n; ++i) rkey[i] = {bit_reverse64(strings[row0 + i]), (uint32_t)i};
+  std::sort(rkey.begin(), rkey.end());
   std::vector<uint32_t> order(n);
-  for (size_t i = 0; i < n; ++i) order[i] = (uint32_t)i;
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
-    return bit_reverse64(strings[row0 + x]) < bit_reverse64(strings[row0 + y]);
-  });
+  for (size_t i = 0; i < n; ++i) order[i] = rkey[i].second;
   const size_t nblk = (n + kBlkRows - 1) / kBlkRows;
   std::vector<uint4> rows(nblk);
   for (size_t b = 0; b < nblk; ++b) {
@@ -322,9 +323,20 @@ int build_same_blocks(Ctx* c, const Conn& cn, const std::vector<uint64_t>& strin
     }
     rows[b] = make_uint4(r[0], r[1], r[2], r[3]);
   }
-  // per block: the doubles of its rows merged by ket (each row's doubles are
-  // ascending; a row that is not is sorted first), equal kets folded into one
-  // union entry with a value per row
+  // every row's doubles must be ascending by ket (the builder's scan order);
+  // a row that is not gets a sorted index of its doubles
+  std::vector<std::vector<uint32_t>> perm(n);
+  for (size_t r = 0; r < n; ++r) {
+    const uint32_t* k0 = ket.data() + (off[r] - e0 + hs[r]);
+    const uint32_t* k1 = ket.data() + (off[r + 1] - e0);
+    if (!std::is_sorted(k0, k1)) {
+      perm[r].resize(k1 - k0);
+      for (uint32_t q = 0; q < perm[r].size(); ++q) perm[r][q] = q;
+      std::sort(perm[r].begin(), perm[r].end(), [&](uint32_t x, uint32_t y) { return k0[x] < k0[y]; });
+    }
+  }
+  // per block: a merge of its rows' doubles by ket with one cursor per row;
+  // equal kets become one union entry with a value per row
   struct Part {
     std::vector<uint32_t> ket;
     std::vector<double> val;
@@ -337,41 +349,46 @@ int build_same_blocks(Ctx* c, const Conn& cn, const std::vector<uint64_t>& strin
   auto work = [&](size_t t) {
     Part& P = parts[t];
     const size_t b0 = nblk * t / nth, b1 = nblk * (t + 1) / nth;
-    std::vector<uint64_t> keys;
+    size_t est = 0;
+    for (size_t i = b0 * kBlkRows; i < std::min(n, b1 * kBlkRows); ++i) {
+      const size_t r = order[i];
+      est += off[r + 1] - off[r] - hs[r];
+    }
+    P.ket.reserve(est);
+    P.val.reserve(est * kBlkRows);
+    P.val32.reserve(est * kBlkRows);
+    P.len.reserve(b1 - b0);
     for (size_t b = b0; b < b1; ++b) {
-      keys.clear();
-      size_t bounds[kBlkRows + 1];
+      uint64_t base[kBlkRows] = {}, cur[kBlkRows] = {}, len[kBlkRows] = {};
+      const uint32_t* pm[kBlkRows] = {};
       for (int k = 0; k < kBlkRows; ++k) {
-        bounds[k] = keys.size();
         const size_t i = b * kBlkRows + k;
         if (i >= n) continue;
         const size_t r = order[i];
-        const uint64_t s0 = off[r] - e0 + hs[r], s1 = off[r + 1] - e0;
-        for (uint64_t e = s0; e < s1; ++e) keys.push_back(((uint64_t)ket[e] << 34) | ((uint64_t)k << 32) | (e - s0));
-        if (!std::is_sorted(keys.begin() + bounds[k], keys.end())) std::sort(keys.begin() + bounds[k], keys.end());
+        base[k] = off[r] - e0 + hs[r];
+        len[k] = off[r + 1] - off[r] - hs[r];
+        pm[k] = perm[r].empty() ? nullptr : perm[r].data();
       }
-      bounds[kBlkRows] = keys.size();
-      for (int w = 1; w < kBlkRows; w *= 2)
-        for (int k = 0; k + w < kBlkRows; k += 2 * w)
-          std::inplace_merge(keys.begin() + bounds[k], keys.begin() + bounds[k + w],
-                             keys.begin() + bounds[std::min(k + 2 * w, kBlkRows)]);
+      auto at = [&](int k) -> uint64_t { return base[k] + (pm[k] ? pm[k][cur[k]] : cur[k]); };
       uint64_t cnt = 0;
-      for (size_t q = 0; q < keys.size();) {
-        const uint32_t kt = (uint32_t)(keys[q] >> 34);
-        double v[kBlkRows] = {};
-        float v32[kBlkRows] = {};
-        for (; q < keys.size() && (uint32_t)(keys[q] >> 34) == kt; ++q) {
-          const int k = (int)((keys[q] >> 32) & 3u);
-          const size_t r = order[b * kBlkRows + k];
-          const uint64_t e = off[r] - e0 + hs[r] + (keys[q] & 0xffffffffull);
-          const bool neg = (info[e] & kInfoNeg) != 0;
-          v[k] = neg ? -val[e] : val[e];
-          v32[k] = neg ? -val32[e] : val32[e];
-        }
-        P.ket.push_back(kt);
+      while (true) {
+        uint32_t m = 0xffffffffu;
+        for (int k = 0; k < kBlkRows; ++k)
+          if (cur[k] < len[k]) m = std::min(m, ket[at(k)]);
+        if (m == 0xffffffffu) break;
+        P.ket.push_back(m);
         for (int k = 0; k < kBlkRows; ++k) {
-          P.val.push_back(v[k]);
-          P.val32.push_back(v32[k]);
+          double v = 0.0;
+          float v32 = 0.f;
+          if (cur[k] < len[k] && ket[at(k)] == m) {
+            const uint64_t e = at(k);
+            ++cur[k];
+            const bool neg = (info[e] & kInfoNeg) != 0;
+            v = neg ? -val[e] : val[e];
+            v32 = neg ? -val32[e] : val32[e];
+          }
+          P.val.push_back(v);
+          P.val32.push_back(v32);
         }
         ++cnt;
       }

@@ -67,8 +67,10 @@ struct SellPanel {
   uint32_t jb0 = 0, jb1 = 0;
 };
 
-// Bra strings per block of the blocked same-spin kernel.
+// Bra strings per block of the blocked same-spin kernel, and the determinant
+// counts from which the default launch codes use it (FP64, FP32 storage).
 constexpr int kBlkRows = 4;
+constexpr size_t kBlkMinDets64 = 2000000, kBlkMinDets32 = 1000000;
 constexpr uint32_t kNoRow = 0xffffffffu;
 
 // Blocks of the blocked same-spin kernel over the bra strings [row0, row1)

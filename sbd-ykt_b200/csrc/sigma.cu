@@ -2081,12 +2081,21 @@ int run_sigma_v5(Ctx* c, const T* X, T* S) {
   return 0;
 }
 
-// Default launch codes: the alpha-first kernels, blocked same-spin products.
-constexpr Tune kDefaultTune[2] = {{32, 71}, {34, 71}};
+// Default launch codes: the alpha-first kernels; the blocked same-spin kernel
+// above a size where its four-strings-per-CTA grid still fills the GPU, the
+// one-string-per-CTA kernel below it. Crossovers measured on B200 over the
+// 64 subspaces of the batched workload and the 400x400 to 8000x8000
+// workloads: FP64 about 2 M determinants (code 32 against 22), FP32 about
+// 1 M (code 34 against 24).
+Tune default_tune(const Ctx* c, bool f64) {
+  const size_t D = c->na * c->nb;
+  if (f64) return D >= kBlkMinDets64 ? Tune{32, 71} : Tune{22, 71};
+  return D >= kBlkMinDets32 ? Tune{34, 71} : Tune{24, 71};
+}
 
 Tune effective_tune(const Ctx* c, bool f64) {
   Tune t = c->tune[f64 ? 0 : 1];
-  const Tune& d = kDefaultTune[f64 ? 0 : 1];
+  const Tune d = default_tune(c, f64);
   const bool v6 = same_alpha_first(t.same_code) || (t.ab_code > 60 && t.ab_code < 70) ||
                   t.ab_code == 71 || (t.same_code == 0 && t.ab_code == 0);
   if (v6) {
@@ -2391,7 +2400,7 @@ int sigma_rows_device(Ctx* c, int precision, const void* X, void* S, size_t a0, 
   if (rc) return rc;
   const bool f64 = precision == 0;
   Tune t = effective_tune(c, f64);
-  if (!is_v6(t)) t = kDefaultTune[f64 ? 0 : 1];  // the row range runs the alpha-first kernels
+  if (!is_v6(t)) t = default_tune(c, f64);  // the row range runs the alpha-first kernels
   if (!ab7_fits(c)) {
     c->err = "sigma_rows: the packed alpha-beta kernel cannot stage this problem's rows";
     return SBDX_ERR_ARG;
