@@ -365,7 +365,7 @@ int sbdx_connectivity_size(sbdx_ctx* ctx, int spin, uint64_t* n_entries) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {
     if (spin != 0 && spin != 1) { c->err = "connectivity_size: spin must be 0 or 1"; return SBDX_ERR_ARG; }
     if (!n_entries) { c->err = "connectivity_size: null pointer"; return SBDX_ERR_ARG; }
-    if (!c->have_conn) { c->err = "connectivity_size: build the connectivity first"; return SBDX_ERR_STATE; }
+    if (!c->have_lists) { c->err = "connectivity_size: build the connectivity first"; return SBDX_ERR_STATE; }
     *n_entries = c->conn[spin].total;
     return SBDX_OK;
   });
@@ -374,7 +374,7 @@ int sbdx_connectivity_size(sbdx_ctx* ctx, int spin, uint64_t* n_entries) {
 int sbdx_get_connectivity(sbdx_ctx* ctx, int spin, uint64_t* slen, uint64_t* dlen, uint64_t* idx) {
   return sbdx::guarded(ctx, [&](Ctx* c) -> int {
     if (spin != 0 && spin != 1) { c->err = "get_connectivity: spin must be 0 or 1"; return SBDX_ERR_ARG; }
-    if (!c->have_conn) { c->err = "get_connectivity: build the connectivity first"; return SBDX_ERR_STATE; }
+    if (!c->have_lists) { c->err = "get_connectivity: build the connectivity first"; return SBDX_ERR_STATE; }
     const sbdx::Conn& cn = c->conn[spin];
     std::vector<uint32_t> ns(cn.n), nd(cn.n), ket(cn.total);
     SBDX_CUDA(c, cudaSetDevice(c->device));

@@ -864,7 +864,9 @@ int build_balanced_sell(Ctx* c, SellPanel& P, size_t n, const std::vector<uint32
   return 0;
 }
 
-int build_one(Ctx* c, int spin) {
+// full = false: the lists only (CSR, per-entry values, masks and records),
+// without the sigma's work items, SELL layouts, ket positions and blocks.
+int build_one(Ctx* c, int spin, bool full) {
   Conn& cn = c->conn[spin];
   free_conn(cn);
   const size_t n = spin == 0 ? c->na : c->nb;
@@ -896,6 +898,10 @@ int build_one(Ctx* c, int spin) {
                                                                  c->d_eri, cn.ket, cn.val, cn.val32,
                                                                  cn.omask, cn.info, cn.srec, cn.spos);
   SBDX_LAUNCHED(c);
+  if (!full) {
+    SBDX_CUDA(c, cudaStreamSynchronize(c->stream));  // the host copy of `off` dies at return
+    return 0;
+  }
   // bra strings ordered by their number of singles (longest first), so the
   // threads of one warp in the alpha-beta kernels walk lists of similar length
   std::vector<uint32_t> order(n);
@@ -1035,17 +1041,21 @@ void free_connectivity(Ctx* c) {
   c->d_Da = c->d_Db = nullptr;
   c->d_Da32 = c->d_Db32 = nullptr;
   c->have_conn = false;
+  c->have_lists = false;
 }
 
-int build_connectivity(Ctx* c) {
+int build_connectivity(Ctx* c, bool full) {
   if (!c->have_strings || !c->have_integrals) {
     c->err = "build_connectivity: set integrals and strings first";
     return 3;
   }
-  int rc = build_one(c, 0);
+  free_connectivity(c);
+  int rc = build_one(c, 0, full);
   if (rc) return rc;
-  rc = build_one(c, 1);
+  rc = build_one(c, 1, full);
   if (rc) return rc;
+  c->have_lists = true;
+  if (!full) return 0;
   rc = build_coulomb_tables(c);
   if (rc) return rc;
   c->have_conn = true;

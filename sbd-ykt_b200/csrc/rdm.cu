@@ -833,7 +833,7 @@ static int rdm_ab_deterministic(Ctx* c, const double* dW, double* two, bool& don
 }
 
 int rdm_device(Ctx* c, const double* dW, double* d_one, double* d_two) {
-  if (!c->have_conn) { int rc = build_connectivity(c); if (rc) return rc; }
+  if (!c->have_lists) { int rc = build_connectivity(c, false); if (rc) return rc; }
   int rc = ensure_sigma_scratch(c);
   if (rc) return rc;
   const size_t na = c->na, nb = c->nb, L = (size_t)c->L, L2 = L * L, L4 = L2 * L2;
@@ -900,9 +900,10 @@ int alpha_weights_device(Ctx* c, const double* dW, double* d_w) {
 }
 
 int backward_device(Ctx* c, const double* dW, double* dE_dh, double* dE_deri) {
-  // the connectivity is rebuilt from the strings; nothing of the forward solve is kept
-  free_connectivity(c);
-  int rc = build_connectivity(c);
+  // the excitation lists are rebuilt from the strings; nothing of the forward
+  // solve is kept (the sigma's layouts are not needed and not built: a later
+  // sigma rebuilds the full connectivity)
+  int rc = build_connectivity(c, false);
   if (rc) return rc;
   const size_t L = (size_t)c->L, L2 = L * L, L4 = L2 * L2;
   Scratch sc;

@@ -229,7 +229,8 @@ struct Ctx {
   bool have_strings = false;
   // connectivity (0 = alpha, 1 = beta)
   Conn conn[2];
-  bool have_conn = false;
+  bool have_conn = false;   // the full connectivity (everything the sigma reads)
+  bool have_lists = false;  // at least the excitation lists (Conn CSR and per-entry data)
   // a shard of the alpha strings: the work items (same-spin and alpha-beta
   // fields of a Conn, nothing else set) of the output rows [range_a0,
   // range_a1) of a row-range sigma (sigma_rows_device)
@@ -408,7 +409,9 @@ __host__ __device__ __forceinline__ uint64_t other_range(int spin, int x, int y)
 }
 
 // ---- internal entry points shared between translation units ------------------
-int build_connectivity(Ctx* c);
+// full = false builds the excitation lists only (what the RDM and adjoint
+// kernels read); the sigma entry points need (and rebuild) the full form.
+int build_connectivity(Ctx* c, bool full = true);
 void free_connectivity(Ctx* c);
 // Work items of the output rows [a0, a1) (Ctx::range_conn) and their release.
 int build_row_range(Ctx* c, size_t a0, size_t a1);
