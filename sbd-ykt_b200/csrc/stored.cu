@@ -104,30 +104,66 @@ stored_fill_kernel(size_t na, size_t nb, const uint64_t* __restrict__ astr, cons
   }
 }
 
-// S = hii o X + H_offdiag X, a warp per row.
+// S = hii o X + H_offdiag X, a warp per row. The matrix streams through in
+// chunks of 128 elements (four per lane); the columns and values of the next
+// chunk, or of the next row's first chunk, are loaded while the vector
+// gathers of the current one are in flight, so the stream always has a chunk
+// in flight. Partial sums in fixed lane and chunk order, then a fixed
+// shuffle tree (deterministic).
 __global__ void __launch_bounds__(kStoredThreads)
 stored_spmv_kernel(size_t D, const uint64_t* __restrict__ rowptr, const uint32_t* __restrict__ col,
                    const double* __restrict__ val, const double* __restrict__ hii, const double* __restrict__ X,
                    double* __restrict__ S) {
   const int lane = threadIdx.x & 31;
   const size_t warps = (size_t)gridDim.x * (blockDim.x >> 5);
-  for (size_t I = (size_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); I < D; I += warps) {
-    const uint64_t k0 = rowptr[I], k1 = rowptr[I + 1];
-    // four elements per lane in flight (column loads, then the gathers)
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    uint64_t k = k0 + lane;
-    for (; k + 96 < k1; k += 128) {
-      const uint32_t c0 = __ldg(col + k), c1 = __ldg(col + k + 32), c2 = __ldg(col + k + 64), c3 = __ldg(col + k + 96);
-      const double v0 = __ldg(val + k), v1 = __ldg(val + k + 32), v2 = __ldg(val + k + 64), v3 = __ldg(val + k + 96);
-      a0 = fma(v0, __ldg(X + c0), a0);
-      a1 = fma(v1, __ldg(X + c1), a1);
-      a2 = fma(v2, __ldg(X + c2), a2);
-      a3 = fma(v3, __ldg(X + c3), a3);
+  size_t I = (size_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (I >= D) return;
+  uint64_t k0 = rowptr[I], k1 = rowptr[I + 1];
+  // the chunk in hand: columns and values of elements k0 + lane + 32 u
+  uint32_t c[4];
+  double v[4];
+  auto fetch = [&](uint64_t base, uint64_t end, uint32_t* cc, double* vv) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint64_t k = base + lane + 32 * u;
+      const bool in = k < end;
+      cc[u] = in ? __ldg(col + k) : 0u;
+      vv[u] = in ? __ldg(val + k) : 0.0;
     }
-    for (; k < k1; k += 32) a0 = fma(__ldg(val + k), __ldg(X + __ldg(col + k)), a0);
-    double acc = (a0 + a1) + (a2 + a3);
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if (lane == 0) S[I] = fma(hii[I], X[I], acc);
+  };
+  fetch(k0, k1, c, v);
+  uint64_t k = k0;
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  for (;;) {
+    // the gathers of the chunk in hand first (they need only its columns)
+    double x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) x[u] = k + lane + 32 * u < k1 ? __ldg(X + c[u]) : 0.0;
+    // the next chunk: the rest of this row, or the next row of this warp
+    uint64_t kn = k + 128, e = k1;
+    size_t In = I;
+    if (kn >= k1) {
+      In = I + warps;
+      kn = In < D ? rowptr[In] : 0;
+      e = In < D ? rowptr[In + 1] : 0;
+    }
+    uint32_t cn[4];
+    double vn[4];
+    fetch(kn, e, cn, vn);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) a[u] = fma(v[u], x[u], a[u]);  // out-of-range lanes add 0 * 0
+    if (In != I) {  // row I complete
+      double acc = (a[0] + a[1]) + (a[2] + a[3]);
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+      if (lane == 0) S[I] = fma(hii[I], X[I], acc);
+      if (In >= D) return;
+      I = In;
+      k1 = e;
+      a[0] = a[1] = a[2] = a[3] = 0.0;
+    }
+    k = kn;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) { c[u] = cn[u]; v[u] = vn[u]; }
   }
 }
 
