@@ -71,3 +71,27 @@ def test_autograd_matches_central_differences():
             fd = (vals[0] - vals[1]) / (2 * step)
             an = gh[i] if kind == "h" else ge[i]
             assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (kind, i, fd, an)
+
+
+def test_products_after_backward_rebuild_full_connectivity():
+    """The backward pass rebuilds only the excitation lists; a later sigma,
+    RDM and solve on the same context must rebuild what they need and agree
+    with the oracle (FP64 sigma 1e-12 relative, energy 1e-9 Ha)."""
+    prob = synth.random_problem(14, 4, 4, 90, 110, seed=29, K=12)
+    port = Port()
+    C = np.random.default_rng(7).standard_normal(prob.D)
+    ref = port.sigma(prob, C)
+    with sbdx.Context(0) as ctx:
+        ctx.load(prob)
+        info, W = ctx.davidson(max_it=20, max_nb=12, eps=1e-10)
+        ctx.energy_backward(W)
+        sl, dl, idx = ctx.connectivity(0)  # the lists are there
+        rsl, rdl, ridx = port.connectivity(prob.alpha)
+        assert np.array_equal(sl, rsl) and np.array_equal(dl, rdl) and np.array_equal(idx, ridx)
+        S = ctx.sigma(C)
+        assert np.abs(S - ref).max() <= 1e-12 * np.abs(ref).max()
+        one, two = ctx.rdm(W)
+        r1, r2 = port.rdm(prob, W)
+        assert np.abs(one - r1).max() < 1e-8 and np.abs(two - r2).max() < 1e-8
+        info2, _ = ctx.davidson(max_it=20, max_nb=12, eps=1e-10)
+        assert abs(info2.energy - info.energy) < 1e-9
