@@ -171,7 +171,7 @@ int sbdx_diag_terms_noalloc(int norb, double I0, const double* d_h, const double
  * overlap; pageable ones give the same result, serialised). */
 int sbdx_sigma(sbdx_ctx* ctx, const double* C, double* S);
 /* Chunks of that pipeline: 0 = automatic (about 8 M determinants per chunk,
- * at most 8; none below 16 M determinants), 1 = no pipeline (one copy in, the
+ * at most 8; none below about 12.6 M determinants), 1 = no pipeline (one copy in, the
  * product, one copy out), K >= 2 = K chunks of equal alpha-row counts. The
  * pipeline runs with the default alpha-first launch codes and no stored
  * Hamiltonian; otherwise sbdx_sigma copies around one whole product. */
