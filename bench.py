@@ -908,6 +908,8 @@ def run_ours(args, rank, world, local):
     kern = PHASE_KERNELS[dominant]
     if dominant == "alpha_beta" and tune[1] // 10 != 7:
         kern = "sigma_ab_v6"  # codes 61-64: unpacked staged rows
+    if dominant in ("alpha_same_spin", "beta_same_spin") and tune[0] // 10 == 3:
+        kern = "sigma_same_blk"  # codes 31-38: blocks of 4 bra strings
     # The alpha-beta kernel gathers from rows staged in shared memory; DRAM
     # moves a few percent of the SpMV byte model (profiles/sigma_ab_v7_cfg2.md),
     # so its bound is the shared-memory pipe: frac = conflict-free shared bytes
