@@ -199,3 +199,70 @@ def test_alpha_first_basis_factorises_signs(spec):
         if n_checked > 6000:
             break
     assert n_checked > 500
+
+
+def bit_reverse64(x):
+    return int(format(int(x), "064b")[::-1], 2)
+
+
+@pytest.mark.parametrize("spec", [(12, 4, 4, 81, 60, 5), (16, 3, 5, 50, 70, 9)])
+def test_bit_reversed_blocks_reproduce_same_spin_doubles(spec):
+    """The blocked same-spin kernel's decomposition: bra strings ordered by
+    their bit-reversed words and cut into blocks of 4; per block the union of
+    the 4 strings' double-excitation kets (ascending) with a dense 4 x |union|
+    matrix of signed same-spin values (zero where a string does not connect).
+    Block-by-block products must reproduce the per-string products of the
+    reference lists (the oracle's connectivity, doubles ascending per row)."""
+    L, na_el, nb_el, Na, Nb, seed = spec
+    prob = synth.random_problem(L, na_el, nb_el, Na, Nb, seed=seed)
+    port = Port()
+    a = [int(x) for x in prob.alpha]
+    sl, dl, idx = port.connectivity(prob.alpha)
+    off = np.concatenate([[0], np.cumsum(sl.astype(np.int64) + dl.astype(np.int64))])
+    dbl = [idx[off[r] + int(sl[r]):off[r + 1]].astype(np.int64) for r in range(Na)]
+    for d in dbl:  # the builder merges rows whose doubles are ascending
+        assert np.all(np.diff(d) > 0)
+    val = {}
+    for r in range(Na):
+        for k in dbl[r]:
+            e = entry(prob, 0, a[r], a[int(k)])
+            val[(r, int(k))] = -e["val"] if e["neg"] else e["val"]
+    X = np.random.default_rng(seed).standard_normal((Na, Nb))
+    ref = np.zeros((Na, Nb))
+    for r in range(Na):
+        for k in dbl[r]:
+            ref[r] += val[(r, int(k))] * X[int(k)]
+    order = sorted(range(Na), key=lambda r: bit_reverse64(a[r]))
+    out = np.full((Na, Nb), np.nan)
+    for b0 in range(0, Na, 4):
+        rows = order[b0:b0 + 4]
+        union = sorted(set(int(k) for r in rows for k in dbl[r]))
+        V = np.zeros((len(rows), len(union)))
+        pos = {k: t for t, k in enumerate(union)}
+        for i, r in enumerate(rows):
+            for k in dbl[r]:
+                V[i, pos[int(k)]] = val[(r, int(k))]
+        out[rows] = V @ X[union] if union else 0.0
+    assert np.abs(out - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+
+
+def test_bit_reversed_order_shares_more_kets_than_ascending():
+    """Why the blocks use bit-reversed order: on the 400-string sample of the
+    24-orbital workload, four bit-reversed neighbours share more of their
+    double-excitation kets than four neighbours in ascending order."""
+    prob = synth.config("cfg1")
+    port = Port()
+    sl, dl, idx = port.connectivity(prob.alpha)
+    off = np.concatenate([[0], np.cumsum(sl.astype(np.int64) + dl.astype(np.int64))])
+    dbl = [idx[off[r] + int(sl[r]):off[r + 1]] for r in range(prob.na)]
+
+    def ratio(order):
+        tot = uni = 0
+        for b0 in range(0, len(order), 4):
+            seg = np.concatenate([dbl[r] for r in order[b0:b0 + 4]])
+            tot += len(seg)
+            uni += len(np.unique(seg))
+        return uni / tot
+
+    rev = sorted(range(prob.na), key=lambda r: bit_reverse64(prob.alpha[r]))
+    assert ratio(rev) < ratio(list(range(prob.na)))
